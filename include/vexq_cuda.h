@@ -1,0 +1,312 @@
+/*
+ * vexq_cuda.h — C ABI of libvexqcuda, the B200 (sm_100a) execution path for
+ * vexq's Filter → Project → HashAggregate / ParallelHashAggregate /
+ * ParallelHashJoinAggregate operators.
+ *
+ * The ABI is shaped for one cgo crossing per query phase (upload, plan, run,
+ * fetch), never one per 1024-row batch. Every entry point takes plain
+ * pointers and sizes, returns an int32 status (0 = ok, negative = error) and
+ * records a message retrievable with vexq_last_error() on the calling thread.
+ *
+ * Reference interfaces each group of entry points stands in for (paths are
+ * within the vexq repository):
+ *   tables    storage.Open / Reader.OpenColumn / ColumnReader.NextBlock +
+ *             Dictionary()            storage/reader.go:186,203; storage/rowgroup.go:101-193
+ *   zone maps planner.buildZonePredicate / zonePredEval / zoneRangePred
+ *                                     planner/physical.go:624-750
+ *   agg plan  exec.NewFilter / exec.NewHashAggregate /
+ *             exec.NewParallelHashAggregate
+ *                                     exec/filter.go:40; exec/aggregate.go:131;
+ *                                     exec/parallel.go:78
+ *   join plan exec.NewParallelHashJoinAggregate
+ *                                     exec/parallel_join.go:718
+ *   results   Operator.Next / Schema / Close
+ *                                     exec/operator.go:28-32
+ *   filter    Filter.Next + BoolToSelVecInto
+ *                                     exec/filter.go:49-78; exec/expr.go:1545-1564
+ */
+#ifndef VEXQ_CUDA_H
+#define VEXQ_CUDA_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VEXQ_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    VEXQ_OK         = 0,
+    VEXQ_EINVAL     = -22,   /* bad argument / unsupported plan shape        */
+    VEXQ_ENOMEM     = -12,   /* device or host allocation failed             */
+    VEXQ_EADMIT     = -11,   /* admission rejected: HBM footprint too large  */
+    VEXQ_ETIMEDOUT  = -110,  /* a bounded device wait ran out                */
+    VEXQ_EDEVICE    = -5,    /* CUDA runtime / driver error                  */
+    VEXQ_ECANCELED  = -125,  /* cancelled through vexq_cancel                */
+    VEXQ_ENOTSUP    = -95,   /* feature outside the supported subset         */
+    VEXQ_EJIT       = -201   /* kernel specialisation failed to compile      */
+};
+
+/* ---- column types: the numeric values of storage.DataType
+ *      (storage/format.go:30-36) ----------------------------------------- */
+enum {
+    VEXQ_TYPE_INT64   = 1,
+    VEXQ_TYPE_FLOAT64 = 2,
+    VEXQ_TYPE_BOOL    = 3,
+    VEXQ_TYPE_STRING  = 4,   /* dictionary coded, uint32 codes             */
+    VEXQ_TYPE_DATE    = 5    /* int32 days since 1970-01-01                */
+};
+
+/* BlockRows (storage/format.go:8): rows per batch handed out by Next. */
+#define VEXQ_BLOCK_ROWS 1024
+/* RowGroupRows (storage/format.go:10): default row-group size. */
+#define VEXQ_ROW_GROUP_ROWS 65536
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Binds the calling thread's CUDA device and creates the library state.
+ * Replaces nothing in the reference (the Go engine has no device). */
+int32_t vexq_init(int32_t device, uint32_t flags);
+/* Message of the last failing call on this thread ("" if none). */
+const char* vexq_last_error(void);
+/* ABI version compiled into the library. */
+int32_t vexq_abi_version(void);
+
+/* ---- tables --------------------------------------------------------------
+ * One host column as the reference's storage layer hands it to TableScan:
+ * fixed-width little-endian values plus an LSB-first validity bitmap
+ * (1 = valid, storage/codec.go:13-39). STRING columns carry per-row-group
+ * dictionaries whose codes are in first-occurrence order
+ * (storage/writer.go:374-420); the upload remaps them to one global
+ * dictionary per column, the remap accumulateIntKey performs per row group
+ * (exec/agg_intkey.go:118-134), done once. */
+typedef struct {
+    const char*     name;
+    int32_t         type;          /* VEXQ_TYPE_*                                  */
+    const void*     values;        /* nrows × {int64, double, uint8, uint32, int32} */
+    const uint8_t*  validity;      /* (nrows+7)/8 bytes, NULL = no NULLs           */
+    /* STRING only ---------------------------------------------------------- */
+    const uint32_t* dict_rg_first; /* n_rg+1 entry indices: RG r owns
+                                      [dict_rg_first[r], dict_rg_first[r+1]).
+                                      NULL: one table-wide dictionary of
+                                      dict_entries entries, codes are global    */
+    const uint32_t* dict_str_off;  /* total_entries+1 byte offsets into bytes     */
+    const char*     dict_bytes;
+    int64_t         dict_entries;  /* entries when dict_rg_first is NULL          */
+} vexq_column_desc;
+
+typedef struct vexq_table_s*  vexq_table_t;
+typedef struct vexq_plan_s*   vexq_plan_t;
+typedef struct vexq_result_s* vexq_result_t;
+
+/* Copies the columns to HBM (synchronous: the host buffers may be freed on
+ * return, as cgo requires) and computes per-row-group zone maps with the
+ * writer's rules (storage/writer.go:205-372). rg_rows = 0 selects 65,536. */
+int32_t vexq_table_upload(const vexq_column_desc* cols, int32_t ncols,
+                          int64_t nrows, int32_t rg_rows, vexq_table_t* out);
+int32_t vexq_table_destroy(vexq_table_t t);
+int32_t vexq_table_num_row_groups(vexq_table_t t, int32_t* out);
+/* Device bytes held by the table (columns, bitmaps, dictionaries). */
+int32_t vexq_table_device_bytes(vexq_table_t t, int64_t* out);
+/* Zone map of (column, row group): storage.ZoneMap (storage/schema.go:26-35). */
+typedef struct {
+    int64_t  null_count;
+    int64_t  sum;          /* raw bits, as the writer stores them */
+    uint64_t min, max;     /* raw bits                             */
+    int32_t  has_min_max;
+} vexq_zone_map;
+int32_t vexq_table_zone_map(vexq_table_t t, int32_t col, int32_t rg, vexq_zone_map* out);
+/* Global dictionary of a STRING column: number of entries and entry i. */
+int32_t vexq_table_dict_size(vexq_table_t t, int32_t col, int32_t* out);
+int32_t vexq_table_dict_entry(vexq_table_t t, int32_t col, int32_t code,
+                              const char** out, int32_t* len);
+
+/* ---- expressions -----------------------------------------------------------
+ * SQL-level expression nodes (sql/ast.go) over a table's columns. The library
+ * performs the planner's translation to executable form itself: literal
+ * coercion (planner/physical.go:773-818), StringEqExpr selection (:548-566),
+ * int→float casts (:575-588), BETWEEN→AND(GE,LE) (exec/expr.go:1328-1339),
+ * and derives the zone-map predicate from the same tree (:624-750).
+ * Children of node n are children[n.child0 .. n.child0+n.nchildren-1]:
+ *   BINARY  [left, right]             AND/OR [a, b, ...]     NOT/NEG [x]
+ *   IS_NULL / IS_NOT_NULL [x]         BETWEEN [x, lo, hi]    (op=1: NOT)
+ *   IN [x, lit...] (op=1: NOT IN)     LIKE [x, pattern] (op=1: NOT LIKE)
+ *   CASE [cond0, res0, cond1, res1, ..., else?]  (op=1: has ELSE)        */
+enum {
+    VEXQ_E_COLUMN = 1, VEXQ_E_LITERAL, VEXQ_E_BINARY, VEXQ_E_AND, VEXQ_E_OR,
+    VEXQ_E_NOT, VEXQ_E_NEG, VEXQ_E_IS_NULL, VEXQ_E_IS_NOT_NULL, VEXQ_E_BETWEEN,
+    VEXQ_E_IN, VEXQ_E_LIKE, VEXQ_E_CASE
+};
+enum {
+    VEXQ_OP_EQ = 1, VEXQ_OP_NE, VEXQ_OP_LT, VEXQ_OP_LE, VEXQ_OP_GT, VEXQ_OP_GE,
+    VEXQ_OP_ADD, VEXQ_OP_SUB, VEXQ_OP_MUL, VEXQ_OP_DIV
+};
+enum { VEXQ_LIT_INT = 1, VEXQ_LIT_FLOAT, VEXQ_LIT_STRING, VEXQ_LIT_BOOL };
+
+typedef struct {
+    int32_t     kind;       /* VEXQ_E_*                                        */
+    int32_t     op;         /* BINARY: VEXQ_OP_*; BETWEEN/IN/LIKE: 1 = negated;
+                               CASE: 1 = has ELSE                              */
+    int32_t     column;     /* COLUMN: column index in the node's scope        */
+    int32_t     lit_kind;   /* LITERAL: VEXQ_LIT_*                             */
+    int64_t     lit_int;    /* INT and BOOL literals                           */
+    double      lit_float;
+    const char* lit_str;    /* STRING literal, NUL terminated                  */
+    int32_t     child0;
+    int32_t     nchildren;
+} vexq_expr;
+
+/* AggKind values of exec/aggregate.go:15-21 (COUNT DISTINCT is not offered:
+ * the reference's planner runs it serially, planner/parallel.go:224-228). */
+enum { VEXQ_AGG_COUNT = 0, VEXQ_AGG_SUM = 1, VEXQ_AGG_AVG = 2,
+       VEXQ_AGG_MIN = 3, VEXQ_AGG_MAX = 4 };
+
+typedef struct {
+    int32_t     kind;       /* VEXQ_AGG_*                                      */
+    int32_t     input;      /* expression root; -1 = COUNT(*)                  */
+    const char* out_name;
+} vexq_agg_desc;
+
+/* ORDER BY <output column> [DESC] LIMIT n applied to the merged aggregate,
+ * as planner.Parallel wraps ExternalSort + Limit (planner/parallel.go:241-266).
+ * sort_col = -1: no sort; limit = -1: no limit. */
+typedef struct {
+    int32_t sort_col;
+    int32_t descending;
+    int64_t limit;
+} vexq_order_desc;
+
+/* Filter → (Project) → HashAggregate over one table. */
+typedef struct {
+    const vexq_expr*     nodes;     int32_t nnodes;
+    const int32_t*       children;  int32_t nchildren;
+    int32_t              predicate; /* root of WHERE, -1 = none            */
+    const int32_t*       group_by;  int32_t ngroup_by;  /* column indices   */
+    const vexq_agg_desc* aggs;      int32_t naggs;
+    vexq_order_desc      order;
+} vexq_agg_plan_desc;
+
+/* Filter(build) ⋈ Filter(probe) → (residual Filter) → HashAggregate.
+ * Node COLUMN indices are scoped: build_predicate over the build table,
+ * probe_predicate over the probe table, and residual / group_by / aggs over
+ * the joined schema (build columns, then probe columns), as HashJoin lays out
+ * its output (exec/join.go:59-61). */
+typedef struct {
+    const vexq_expr*     nodes;     int32_t nnodes;
+    const int32_t*       children;  int32_t nchildren;
+    int32_t              build_key;        /* build-table column (INT64/DATE) */
+    int32_t              probe_key;        /* probe-table column              */
+    int32_t              build_predicate;  /* -1 = none                       */
+    int32_t              probe_predicate;
+    int32_t              residual;         /* over the joined schema          */
+    const int32_t*       group_by;  int32_t ngroup_by;
+    const vexq_agg_desc* aggs;      int32_t naggs;
+    vexq_order_desc      order;
+    int32_t              radix_bits;       /* -1 = autotuned                  */
+} vexq_join_plan_desc;
+
+/* Compiles a plan against a table: resolves types, coerces literals, builds
+ * the zone predicate, chooses the aggregation strategy and generates the
+ * specialised sm_100a kernel (cached per plan signature). */
+int32_t vexq_agg_plan_create(vexq_table_t t, const vexq_agg_plan_desc* d, vexq_plan_t* out);
+int32_t vexq_join_plan_create(vexq_table_t build, vexq_table_t probe,
+                              const vexq_join_plan_desc* d, vexq_plan_t* out);
+int32_t vexq_plan_destroy(vexq_plan_t p);
+/* Short description of the chosen strategy (for logs and tests). */
+const char* vexq_plan_explain(vexq_plan_t p);
+
+/* Zone-map pruning on the host: out_mask[rg] = 1 where the row group may
+ * hold a matching row (TableScan's skip, exec/scan.go:212-215). */
+int32_t vexq_zone_prune(vexq_plan_t p, uint8_t* out_mask, int32_t n_rg);
+
+/* Runs the plan over row groups [rg_start, rg_end) (rg_end = -1: all) and
+ * returns the merged result on the host. Synchronous on the plan's stream. */
+int32_t vexq_plan_run(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_result_t* out);
+
+/* Same as vexq_plan_run, but the plan's table columns are first re-filled
+ * from the given HOST buffers (same layout as at upload) inside the call:
+ * the end-to-end form used when the caller owns the data in host memory. */
+int32_t vexq_plan_run_host(vexq_plan_t p, const vexq_column_desc* cols, int32_t ncols,
+                           vexq_result_t* out);
+
+/* ---- results: the Next/Schema contract --------------------------------- */
+typedef struct {
+    const char*     name;
+    int32_t         type;      /* VEXQ_TYPE_*                                */
+    const void*     values;    /* length × {int64, double, int32, uint32 code} */
+    const uint8_t*  validity;  /* LSB-first, 1 = valid                        */
+    /* STRING: codes index this batch's dictionary (exec.newStringVector) */
+    const uint32_t* dict_str_off;  /* dict_len+1 offsets */
+    const char*     dict_bytes;
+    int32_t         dict_len;
+} vexq_vector_view;
+
+typedef struct {
+    int32_t                 ncols;
+    int32_t                 length;   /* 0 at EOF                         */
+    const vexq_vector_view* cols;     /* valid until the next call        */
+} vexq_batch_view;
+
+int32_t vexq_result_num_rows(vexq_result_t r, int64_t* out);
+int32_t vexq_result_num_cols(vexq_result_t r, int32_t* out);
+/* Next(): ≤ VEXQ_BLOCK_ROWS rows in group-insertion order (first occurrence
+ * in row order, the serial HashAggregate's order, exec/aggregate.go:209-216);
+ * length 0 = EOF. A global aggregate over no rows yields one row
+ * (exec/aggregate.go:961-982). */
+int32_t vexq_result_next(vexq_result_t r, vexq_batch_view* out);
+int32_t vexq_result_free(vexq_result_t r);
+/* Device timing of the last run: kernel milliseconds and launches. */
+int32_t vexq_result_stats(vexq_result_t r, double* kernel_ms, int32_t* launches,
+                          int64_t* rows_scanned, int64_t* bytes_scanned);
+/* Duration of the run's scan kernel launches alone (CUDA events on the
+ * plan's stream), in milliseconds. */
+int32_t vexq_result_scan_ms(vexq_result_t r, double* out);
+
+/* Runs a plan on a caller-owned CUDA stream (a cudaStream_t, e.g. the stream
+ * the caller times with events); NULL restores the plan's own stream.
+ * No reference counterpart: the Go engine has no streams. */
+int32_t vexq_plan_set_stream(vexq_plan_t p, void* stream);
+
+/* ---- standalone filter: Filter.Next + BoolToSelVecInto ----------------- */
+/* Evaluates a predicate over rows [row_start, row_end) and writes a
+ * selection bitmap (bit i = row row_start+i passes; LSB-first) into out_bits
+ * (host, (n+7)/8 bytes) and the number of selected rows into *count. */
+int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
+                        const int32_t* children, int32_t nchildren, int32_t predicate,
+                        int64_t row_start, int64_t row_end,
+                        uint8_t* out_bits, int64_t* count);
+/* Selection vectors of one 1024-row block from a selection bitmap: the
+ * []uint16 SelVec of exec/batch.go:10 (physical indices within the block). */
+int32_t vexq_selvec_from_bits(const uint8_t* bits, int64_t nrows, int64_t block,
+                              uint16_t* out_sel, int32_t* out_len);
+
+/* ---- batching: many aggregates in one persistent launch ---------------- */
+/* Runs n independent plans (each over its own table) in one persistent
+ * kernel launch per plan shape, captured in a CUDA graph on first use. */
+int32_t vexq_batch_run(vexq_plan_t* plans, int32_t n, vexq_result_t* out_results);
+
+/* ---- serving loop ------------------------------------------------------ */
+typedef struct vexq_server_s* vexq_server_t;
+/* hbm_budget_bytes caps the summed hash-table footprint of in-flight
+ * queries (admission); max_inflight caps concurrent query slots. */
+int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, vexq_server_t* out);
+/* Queues plan p; returns a ticket. A plan may be submitted many times. */
+int32_t vexq_server_submit(vexq_server_t s, vexq_plan_t p, int64_t* ticket);
+/* Non-blocking poll: *done = 1 and *out set when the ticket has finished. */
+int32_t vexq_server_poll(vexq_server_t s, int64_t ticket, int32_t* done, vexq_result_t* out);
+/* Blocking wait with a timeout in milliseconds (VEXQ_ETIMEDOUT after it). */
+int32_t vexq_server_wait(vexq_server_t s, int64_t ticket, int64_t timeout_ms, vexq_result_t* out);
+/* Latency (submit → result ready) of a finished ticket, in milliseconds. */
+int32_t vexq_server_latency(vexq_server_t s, int64_t ticket, double* ms);
+int32_t vexq_server_stop(vexq_server_t s);
+
+/* Host-set cancellation flag polled between launches of a running plan. */
+int32_t vexq_cancel(vexq_plan_t p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VEXQ_CUDA_H */

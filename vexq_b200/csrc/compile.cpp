@@ -1,0 +1,1575 @@
+// compile.cpp — plan compilation: SQL-level expression nodes → typed IR
+// (the planner's translation, planner/physical.go:376-818), accumulator slot
+// layout (exec/aggregate.go:51-72, 255-279), group-key encoding, zone-map
+// predicate (planner/physical.go:624-750), and generation of the query-
+// specialised sm_100a scan kernels compiled at plan creation.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <set>
+#include <sstream>
+
+#include "plan.h"
+
+namespace vq {
+
+// ---- dates: time.ParseInLocation("2006-01-02", s, time.UTC) --------------------
+bool parse_date(const char* s, int64_t* days) {
+    if (!s || std::strlen(s) != 10 || s[4] != '-' || s[7] != '-') return false;
+    int digits[8] = {0, 1, 2, 3, 5, 6, 8, 9};
+    for (int i : digits) if (s[i] < '0' || s[i] > '9') return false;
+    int y = (s[0] - '0') * 1000 + (s[1] - '0') * 100 + (s[2] - '0') * 10 + (s[3] - '0');
+    int m = (s[5] - '0') * 10 + (s[6] - '0');
+    int d = (s[8] - '0') * 10 + (s[9] - '0');
+    static const int mdays[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+    if (m < 1 || m > 12 || d < 1) return false;
+    bool leap = (y % 4 == 0 && y % 100 != 0) || y % 400 == 0;
+    if (d > mdays[m - 1] + ((m == 2 && leap) ? 1 : 0)) return false;
+    // days since 1970-01-01 by counting whole years and months
+    int64_t n = 0;
+    auto isLeap = [](int yy) { return (yy % 4 == 0 && yy % 100 != 0) || yy % 400 == 0; };
+    if (y >= 1970) for (int yy = 1970; yy < y; yy++) n += isLeap(yy) ? 366 : 365;
+    else for (int yy = y; yy < 1970; yy++) n -= isLeap(yy) ? 366 : 365;
+    for (int mm = 1; mm < m; mm++) n += mdays[mm - 1] + ((mm == 2 && leap) ? 1 : 0);
+    *days = n + d - 1;
+    return true;
+}
+
+namespace {
+
+// likeMatch semantics of exec/expr.go:1277-1311 (% any run, _ one byte)
+bool like_match(const char* p, size_t pn, const char* s, size_t sn) {
+    while (pn > 0) {
+        if (*p == '%') {
+            p++; pn--;
+            if (pn == 0) return true;
+            for (size_t i = 0; i <= sn; i++)
+                if (like_match(p, pn, s + i, sn - i)) return true;
+            return false;
+        }
+        if (sn == 0) return false;
+        if (*p != '_' && *p != *s) return false;
+        p++; pn--; s++; sn--;
+    }
+    return sn == 0;
+}
+
+struct Translator {
+    Plan& p;
+    const vexq_expr* nodes;
+    int nnodes;
+    const int32_t* children;
+    int nchildren;
+    Table* t;        // column scope: the scan table
+    Table* bt;       // joined scope: build table (columns [0, nbuild))
+    int nbuild = 0;
+    bool joined = false;
+    std::vector<std::pair<int, int64_t>>* presence = nullptr;  // presence rows of the scanned table
+    std::vector<std::string> lit_strs;  // per IR node (string literals)
+
+    const vexq_expr& at(int i) const {
+        if (i < 0 || i >= nnodes) fail(VEXQ_EINVAL, "expression node index out of range");
+        return nodes[i];
+    }
+    int child(const vexq_expr& n, int k) const {
+        int idx = n.child0 + k;
+        if (k >= n.nchildren || idx < 0 || idx >= nchildren) fail(VEXQ_EINVAL, "expression child out of range");
+        return children[idx];
+    }
+    int add(INode n) {
+        p.ir.push_back(std::move(n));
+        lit_strs.resize(p.ir.size());
+        return (int)p.ir.size() - 1;
+    }
+    INode& N(int i) { return p.ir[i]; }
+
+    const Column& colref(int c, bool build) const {
+        const Table* tt = build ? bt : t;
+        return tt->cols[c];
+    }
+
+    int lit_node(int type) {
+        INode n;
+        n.k = NK::Lit;
+        n.type = type;
+        return add(n);
+    }
+
+    // coerceOneSide (planner/physical.go:782-818): coerce literal b to a's type.
+    int coerce(int a, int b) {
+        if (N(b).k != NK::Lit) return b;
+        int at_ = N(a).type, bt_ = N(b).type;
+        if (at_ == VEXQ_TYPE_DATE) {
+            if (bt_ == VEXQ_TYPE_STRING) {
+                int64_t days;
+                if (parse_date(lit_strs[b].c_str(), &days)) {
+                    int n = lit_node(VEXQ_TYPE_DATE);
+                    N(n).ld = (int32_t)days;
+                    return n;
+                }
+            } else if (bt_ == VEXQ_TYPE_INT64) {
+                int n = lit_node(VEXQ_TYPE_DATE);
+                N(n).ld = (int32_t)N(b).li;
+                return n;
+            }
+        } else if (at_ == VEXQ_TYPE_FLOAT64 && bt_ == VEXQ_TYPE_INT64) {
+            int n = lit_node(VEXQ_TYPE_FLOAT64);
+            N(n).lf = (double)N(b).li;
+            return n;
+        } else if (at_ == VEXQ_TYPE_INT64 && bt_ == VEXQ_TYPE_FLOAT64) {
+            double f = N(b).lf;
+            int n = lit_node(VEXQ_TYPE_INT64);
+            N(n).li = (std::isnan(f) || f >= 9.2233720368547758e18 || f < -9.2233720368547758e18)
+                          ? std::numeric_limits<int64_t>::min() : (int64_t)f;
+            return n;
+        }
+        return b;
+    }
+
+    int bool_node(NK k, std::vector<int> ch) {
+        INode n;
+        n.k = k;
+        n.type = VEXQ_TYPE_BOOL;
+        n.ch = std::move(ch);
+        return add(n);
+    }
+
+    int cmp_node(int op, int l, int r) {
+        int lt = N(l).type, rt = N(r).type;
+        if (lt != rt || lt == VEXQ_TYPE_STRING || lt == VEXQ_TYPE_BOOL)
+            fail(VEXQ_EINVAL, "comparison operands are not comparable (expr: cmp not supported)");
+        INode n;
+        n.k = NK::Cmp;
+        n.type = VEXQ_TYPE_BOOL;
+        n.op = op;
+        n.ch = {l, r};
+        return add(n);
+    }
+
+    int cast_float(int e) {
+        if (N(e).type != VEXQ_TYPE_INT64) return e;
+        INode n;
+        n.k = NK::Cast;
+        n.type = VEXQ_TYPE_FLOAT64;
+        n.ch = {e};
+        return add(n);
+    }
+
+    int string_col_of(int e) {
+        if (N(e).k != NK::Col || N(e).type != VEXQ_TYPE_STRING)
+            fail(VEXQ_ENOTSUP, "string predicate over a non-column operand");
+        return e;
+    }
+
+    // buildExecExpr (planner/physical.go:376-547) + buildBinExpr (:549-620)
+    int tr(int idx) {
+        const vexq_expr& n = at(idx);
+        switch (n.kind) {
+            case VEXQ_E_COLUMN: {
+                INode c;
+                c.k = NK::Col;
+                int ci = n.column;
+                if (joined) {
+                    if (ci < 0 || ci >= nbuild + (int)t->cols.size()) fail(VEXQ_EINVAL, "column index out of range");
+                    if (ci < nbuild) c.build = true;
+                    else ci -= nbuild;
+                } else if (ci < 0 || ci >= (int)t->cols.size()) {
+                    fail(VEXQ_EINVAL, "column index out of range");
+                }
+                c.col = ci;
+                const Column& col = colref(ci, c.build);
+                c.type = col.type;
+                c.nullable = col.nullable;
+                return add(c);
+            }
+            case VEXQ_E_LITERAL: {
+                INode c;
+                c.k = NK::Lit;
+                c.is_literal_raw = true;
+                c.lit_kind = n.lit_kind;
+                std::string s;
+                switch (n.lit_kind) {
+                    case VEXQ_LIT_INT: c.type = VEXQ_TYPE_INT64; c.li = n.lit_int; break;
+                    case VEXQ_LIT_FLOAT: c.type = VEXQ_TYPE_FLOAT64; c.lf = n.lit_float; break;
+                    case VEXQ_LIT_STRING: c.type = VEXQ_TYPE_STRING; s = n.lit_str ? n.lit_str : ""; break;
+                    case VEXQ_LIT_BOOL: c.type = VEXQ_TYPE_BOOL; c.lb = n.lit_int != 0; break;
+                    default: fail(VEXQ_EINVAL, "bad literal kind");
+                }
+                int id = add(c);
+                lit_strs[id] = s;
+                return id;
+            }
+            case VEXQ_E_AND:
+            case VEXQ_E_OR: {
+                std::vector<int> ch;
+                for (int k = 0; k < n.nchildren; k++) {
+                    int c = tr(child(n, k));
+                    if (N(c).type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "AND/OR operand is not boolean");
+                    ch.push_back(c);
+                }
+                if (ch.empty()) {  // empty AND → all true; empty OR → all false (valid)
+                    int l = lit_node(VEXQ_TYPE_BOOL);
+                    N(l).lb = n.kind == VEXQ_E_AND;
+                    return l;
+                }
+                return bool_node(n.kind == VEXQ_E_AND ? NK::And : NK::Or, ch);
+            }
+            case VEXQ_E_NOT: {
+                int c = tr(child(n, 0));
+                if (N(c).type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "NOT requires a boolean operand");
+                return bool_node(NK::Not, {c});
+            }
+            case VEXQ_E_NEG: {  // physical.go:414-436: child * -1
+                int c = tr(child(n, 0));
+                int t_ = N(c).type;
+                if (t_ != VEXQ_TYPE_FLOAT64 && t_ != VEXQ_TYPE_INT64) fail(VEXQ_EINVAL, "unary minus not supported for type");
+                int l = lit_node(t_);
+                N(l).lf = -1.0;
+                N(l).li = -1;
+                INode a;
+                a.k = NK::Arith;
+                a.op = VEXQ_OP_MUL;
+                a.type = t_;
+                a.ch = {c, l};
+                return add(a);
+            }
+            case VEXQ_E_IS_NULL:
+            case VEXQ_E_IS_NOT_NULL:
+                return bool_node(n.kind == VEXQ_E_IS_NULL ? NK::IsNull : NK::IsNotNull, {tr(child(n, 0))});
+            case VEXQ_E_BETWEEN: {  // BetweenExpr → AND(GE, LE) (exec/expr.go:1328-1339)
+                int c = tr(child(n, 0));
+                int lo = coerce(c, tr(child(n, 1)));
+                int hi = coerce(c, tr(child(n, 2)));
+                int a = bool_node(NK::And, {cmp_node(VEXQ_OP_GE, c, lo), cmp_node(VEXQ_OP_LE, c, hi)});
+                return n.op == 1 ? bool_node(NK::Not, {a}) : a;
+            }
+            case VEXQ_E_IN: {  // InExpr (exec/expr.go:1204-1243)
+                int c = tr(child(n, 0));
+                int kind = 0;
+                std::vector<int64_t> si;
+                std::vector<double> sf;
+                std::vector<std::string> ss;
+                for (int k = 1; k < n.nchildren; k++) {
+                    const vexq_expr& l = at(child(n, k));
+                    if (l.kind != VEXQ_E_LITERAL) continue;
+                    int lk = l.lit_kind == VEXQ_LIT_INT ? 1 : l.lit_kind == VEXQ_LIT_FLOAT ? 2 : l.lit_kind == VEXQ_LIT_STRING ? 3 : 0;
+                    if (!lk) continue;
+                    if (kind && kind != lk) fail(VEXQ_EINVAL, "IN list mixes literal types");
+                    kind = lk;
+                    if (lk == 1) si.push_back(l.lit_int);
+                    if (lk == 2) sf.push_back(l.lit_float);
+                    if (lk == 3) ss.push_back(l.lit_str ? l.lit_str : "");
+                }
+                int ct = N(c).type;
+                if (kind && ((ct == VEXQ_TYPE_INT64 && kind != 1) || (ct == VEXQ_TYPE_FLOAT64 && kind != 2) ||
+                             (ct == VEXQ_TYPE_STRING && kind != 3)))
+                    fail(VEXQ_EINVAL, "IN literal type does not match the operand");
+                INode x;
+                x.type = VEXQ_TYPE_BOOL;
+                x.ch = {c};
+                if (!kind || ct == VEXQ_TYPE_DATE || ct == VEXQ_TYPE_BOOL) {
+                    x.k = NK::InFalse;  // no literal matches these vector kinds
+                } else if (ct == VEXQ_TYPE_INT64) {
+                    x.k = NK::InInt;
+                    x.seti = si;
+                } else if (ct == VEXQ_TYPE_FLOAT64) {
+                    x.k = NK::InFloat;
+                    x.setf = sf;
+                } else {
+                    string_col_of(c);
+                    const Column& col = colref(N(c).col, N(c).build);
+                    x.k = NK::InCodes;
+                    x.col = N(c).col;
+                    x.build = N(c).build;
+                    x.codes.assign(col.dict.keys.size(), 0);
+                    for (auto& s : ss) {
+                        int64_t code = col.dict.find(s);
+                        if (code >= 0) x.codes[code] = 1;
+                    }
+                }
+                int id = add(x);
+                return n.op == 1 ? bool_node(NK::Not, {id}) : id;
+            }
+            case VEXQ_E_LIKE: {  // LikeExpr: evaluated once per dictionary entry
+                int c = tr(child(n, 0));
+                const vexq_expr& pt = at(child(n, 1));
+                if (pt.kind != VEXQ_E_LITERAL || pt.lit_kind != VEXQ_LIT_STRING)
+                    fail(VEXQ_EINVAL, "LIKE pattern must be a string literal");
+                if (N(c).type != VEXQ_TYPE_STRING) fail(VEXQ_EINVAL, "LIKE requires STRING column");
+                string_col_of(c);
+                std::string pat = pt.lit_str ? pt.lit_str : "";
+                const Column& col = colref(N(c).col, N(c).build);
+                INode x;
+                x.k = NK::InCodes;
+                x.type = VEXQ_TYPE_BOOL;
+                x.ch = {c};
+                x.col = N(c).col;
+                x.build = N(c).build;
+                x.codes.assign(col.dict.keys.size(), 0);
+                for (size_t i = 0; i < col.dict.keys.size(); i++)
+                    x.codes[i] = like_match(pat.data(), pat.size(), col.dict.keys[i].data(), col.dict.keys[i].size());
+                int id = add(x);
+                return n.op == 1 ? bool_node(NK::Not, {id}) : id;
+            }
+            case VEXQ_E_CASE: {  // CaseExpr (exec/expr.go:1405-1432), physical.go:508-546
+                bool has_else = n.op == 1;
+                int nw = (n.nchildren - (has_else ? 1 : 0)) / 2;
+                INode x;
+                x.k = NK::Case;
+                x.has_else = has_else;
+                for (int w = 0; w < nw; w++) {
+                    int cond = tr(child(n, 2 * w));
+                    int res = tr(child(n, 2 * w + 1));
+                    x.ch.push_back(cond);
+                    x.ch.push_back(res);
+                }
+                if (has_else) x.ch.push_back(tr(child(n, n.nchildren - 1)));
+                int t_ = nw > 0 ? N(x.ch[1]).type : VEXQ_TYPE_FLOAT64;
+                for (int w = 0; w < nw; w++) {
+                    if (N(x.ch[2 * w]).type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "CASE condition is not boolean");
+                    if (N(x.ch[2 * w + 1]).type != t_) fail(VEXQ_EINVAL, "CASE branches must have a common type");
+                }
+                if (has_else && N(x.ch.back()).type != t_) fail(VEXQ_EINVAL, "CASE ELSE type mismatch");
+                if (t_ != VEXQ_TYPE_INT64 && t_ != VEXQ_TYPE_FLOAT64)
+                    fail(VEXQ_ENOTSUP, "CASE with a non-numeric result type is not supported on the GPU path");
+                x.type = t_;
+                return add(x);
+            }
+            case VEXQ_E_BINARY: {
+                int l = tr(child(n, 0));
+                int r = tr(child(n, 1));
+                l = coerce(r, l);  // coercePair: both directions (physical.go:773-778)
+                r = coerce(l, r);
+                if ((n.op == VEXQ_OP_EQ || n.op == VEXQ_OP_NE) && N(l).type == VEXQ_TYPE_STRING &&
+                    N(r).type == VEXQ_TYPE_STRING) {
+                    int cidx = -1, lidx = -1;
+                    if (N(l).k == NK::Col && N(r).k == NK::Lit) { cidx = l; lidx = r; }
+                    else if (N(r).k == NK::Col && N(l).k == NK::Lit) { cidx = r; lidx = l; }
+                    if (cidx < 0) fail(VEXQ_EINVAL, "expr: cmp not supported for string operands");
+                    // StringEqExpr (exec/expr.go:1342-1388)
+                    INode x;
+                    x.k = NK::StrEq;
+                    x.type = VEXQ_TYPE_BOOL;
+                    x.col = N(cidx).col;
+                    x.build = N(cidx).build;
+                    x.negate = n.op == VEXQ_OP_NE;
+                    x.ch = {cidx};
+                    const Column& col = colref(x.col, x.build);
+                    x.streq_code = col.dict.find(lit_strs[lidx]);
+                    if (x.streq_code >= 0 && !x.build && col.per_rg_dicts) {
+                        bool all = true;
+                        for (auto& pr : col.rg_present) if (!pr[x.streq_code]) { all = false; break; }
+                        if (!all) {
+                            std::vector<std::pair<int, int64_t>>& pl = presence ? *presence : p.presence;
+                            x.present_idx = (int)pl.size();
+                            pl.push_back({x.col, x.streq_code});
+                        }
+                    }
+                    return add(x);
+                }
+                if (n.op < VEXQ_OP_EQ || n.op > VEXQ_OP_DIV) fail(VEXQ_EINVAL, "unknown binary op");
+                if (n.op <= VEXQ_OP_GE) return cmp_node(n.op, l, r);
+                int rt = N(l).type;
+                if (N(l).type == VEXQ_TYPE_FLOAT64 || N(r).type == VEXQ_TYPE_FLOAT64) rt = VEXQ_TYPE_FLOAT64;
+                if (rt == VEXQ_TYPE_FLOAT64) { l = cast_float(l); r = cast_float(r); }
+                if (N(l).type != N(r).type || (N(l).type != VEXQ_TYPE_INT64 && N(l).type != VEXQ_TYPE_FLOAT64))
+                    fail(VEXQ_EINVAL, "arithmetic operand types not supported (missing plan-time coercion?)");
+                INode a;
+                a.k = NK::Arith;
+                a.op = n.op;
+                a.type = rt;
+                a.ch = {l, r};
+                return add(a);
+            }
+        }
+        fail(VEXQ_EINVAL, "unsupported expression kind");
+    }
+};
+
+// Static NULL-ability and |value| bounds (interval arithmetic over the
+// table-wide min/max of each column) of every IR node.
+void analyze(Plan& p) {
+    for (size_t i = 0; i < p.ir.size(); i++) {
+        INode& n = p.ir[i];
+        auto C = [&](int k) -> INode& { return p.ir[n.ch[k]]; };
+        switch (n.k) {
+            case NK::Col: {
+                const Table* tt = n.build ? p.bt : p.t;
+                const Column& c = tt->cols[n.col];
+                n.nullable = c.nullable;
+                if (c.has_range) {
+                    n.bounded = true;
+                    if (c.type == VEXQ_TYPE_FLOAT64) { n.lo = c.fmin; n.hi = c.fmax; }
+                    else { n.lo = (double)c.imin; n.hi = (double)c.imax; }
+                    if (!std::isfinite(n.lo) || !std::isfinite(n.hi)) n.bounded = false;
+                } else if (c.type == VEXQ_TYPE_BOOL) {
+                    n.bounded = true; n.lo = 0; n.hi = 1;
+                }
+                break;
+            }
+            case NK::Lit:
+                n.nullable = false;
+                n.bounded = true;
+                n.lo = n.hi = n.type == VEXQ_TYPE_FLOAT64 ? n.lf : n.type == VEXQ_TYPE_DATE ? n.ld : (double)n.li;
+                if (!std::isfinite(n.lo)) n.bounded = false;
+                break;
+            case NK::Cast:
+                n.nullable = C(0).nullable;
+                n.bounded = C(0).bounded; n.lo = C(0).lo; n.hi = C(0).hi;
+                break;
+            case NK::Arith: {
+                n.nullable = C(0).nullable || C(1).nullable;
+                n.bounded = C(0).bounded && C(1).bounded;
+                if (!n.bounded) break;
+                double a = C(0).lo, b = C(0).hi, c = C(1).lo, d = C(1).hi;
+                switch (n.op) {
+                    case VEXQ_OP_ADD: n.lo = a + c; n.hi = b + d; break;
+                    case VEXQ_OP_SUB: n.lo = a - d; n.hi = b - c; break;
+                    case VEXQ_OP_MUL: {
+                        double v[4] = {a * c, a * d, b * c, b * d};
+                        n.lo = *std::min_element(v, v + 4);
+                        n.hi = *std::max_element(v, v + 4);
+                        break;
+                    }
+                    case VEXQ_OP_DIV: {
+                        if (n.type == VEXQ_TYPE_INT64) { n.lo = -std::max(std::fabs(a), std::fabs(b)); n.hi = -n.lo; break; }
+                        if (c <= 0 && d >= 0) { n.bounded = false; break; }
+                        double v[4] = {a / c, a / d, b / c, b / d};
+                        n.lo = *std::min_element(v, v + 4);
+                        n.hi = *std::max_element(v, v + 4);
+                        break;
+                    }
+                }
+                if (n.bounded && (!std::isfinite(n.lo) || !std::isfinite(n.hi))) n.bounded = false;
+                // widen by a relative ulp margin for rounding
+                if (n.bounded) { double m = std::max(std::fabs(n.lo), std::fabs(n.hi)) * 1e-12; n.lo -= m; n.hi += m; }
+                break;
+            }
+            case NK::Case: {
+                int nw = (int)(n.ch.size() - (n.has_else ? 1 : 0)) / 2;
+                n.nullable = !n.has_else;
+                n.bounded = true;
+                n.lo = INFINITY; n.hi = -INFINITY;
+                for (int w = 0; w <= nw; w++) {
+                    int ri = w < nw ? n.ch[2 * w + 1] : (n.has_else ? n.ch.back() : -1);
+                    if (ri < 0) continue;
+                    const INode& r = p.ir[ri];
+                    n.nullable = n.nullable || r.nullable;
+                    if (!r.bounded) { n.bounded = false; continue; }
+                    n.lo = std::min(n.lo, r.lo);
+                    n.hi = std::max(n.hi, r.hi);
+                }
+                if (!n.has_else) { n.lo = std::min(n.lo, 0.0); n.hi = std::max(n.hi, 0.0); }
+                break;
+            }
+            case NK::IsNull:
+            case NK::IsNotNull:
+                n.nullable = false;
+                break;
+            case NK::StrEq:
+                n.nullable = C(0).nullable || n.present_idx >= 0 || n.streq_code < 0;
+                break;
+            default: {
+                bool any = false;
+                for (int c : n.ch) any = any || p.ir[c].nullable;
+                n.nullable = any;
+                break;
+            }
+        }
+    }
+}
+
+std::string ctype(int t) {
+    switch (t) {
+        case VEXQ_TYPE_INT64: return "long long";
+        case VEXQ_TYPE_FLOAT64: return "double";
+        case VEXQ_TYPE_DATE: return "int";
+        case VEXQ_TYPE_STRING: return "unsigned";
+        case VEXQ_TYPE_BOOL: return "bool";
+    }
+    return "long long";
+}
+
+std::string dlit(double v) {  // exact double literal (bit cast keeps NaN payloads)
+    int64_t b;
+    std::memcpy(&b, &v, 8);
+    std::ostringstream o;
+    o << "__longlong_as_double(" << b << "LL)";
+    return o.str();
+}
+
+std::string ilit(int64_t v) {
+    if (v == std::numeric_limits<int64_t>::min()) return "(-9223372036854775807LL - 1LL)";
+    return std::to_string(v) + "LL";
+}
+
+const char* cmp_op(int op) {
+    switch (op) {
+        case VEXQ_OP_EQ: return "==";
+        case VEXQ_OP_NE: return "!=";
+        case VEXQ_OP_LT: return "<";
+        case VEXQ_OP_LE: return "<=";
+        case VEXQ_OP_GT: return ">";
+        case VEXQ_OP_GE: return ">=";
+    }
+    return "==";
+}
+
+// Emits straight-line code for IR nodes, memoised per scope.
+struct Gen {
+    Plan& p;
+    std::ostringstream& os;
+    std::vector<char> done;
+    std::string ind = "            ";
+    Gen(Plan& pp, std::ostringstream& o) : p(pp), os(o), done(pp.ir.size(), 0) {}
+
+    void emit(int i) {
+        if (done[i]) return;
+        INode& n = p.ir[i];
+        for (int c : n.ch) emit(c);
+        done[i] = 1;
+        std::string x = "x" + std::to_string(i), ok = "ok" + std::to_string(i);
+        auto X = [&](int k) { return "x" + std::to_string(n.ch[k]); };
+        auto OK = [&](int k) { return "ok" + std::to_string(n.ch[k]); };
+        switch (n.k) {
+            case NK::Col: {
+                std::string c = std::to_string(n.col);
+                if (n.build) {
+                    std::string ct = n.type == VEXQ_TYPE_BOOL ? "unsigned char" : ctype(n.type);
+                    os << ind << "const bool " << ok << " = " << (n.nullable ? "vq_bit(P.bvalid[" + c + "], brow)" : "true") << ";\n";
+                    std::string ld = "((const " + ct + "*)P.bcol[" + c + "])[brow]";
+                    if (n.type == VEXQ_TYPE_BOOL)  // a NULL bool reads false
+                        os << ind << "const bool " << x << " = " << ok << " && " << ld << " != 0;\n";
+                    else
+                        os << ind << "const " << ctype(n.type) << " " << x << " = " << ld << ";\n";
+                } else {
+                    os << ind << "const bool " << ok << " = " << (n.nullable ? "((cm" + c + " >> k) & 1u) != 0u" : "true") << ";\n";
+                    if (n.type == VEXQ_TYPE_BOOL)
+                        os << ind << "const bool " << x << " = " << ok << " && cv" << c << "[k] != 0u;\n";
+                    else
+                        os << ind << "const " << ctype(n.type) << " " << x << " = cv" << c << "[k];\n";
+                }
+                break;
+            }
+            case NK::Lit: {
+                os << ind << "const bool " << ok << " = true;\n";
+                switch (n.type) {
+                    case VEXQ_TYPE_INT64: os << ind << "const long long " << x << " = " << ilit(n.li) << ";\n"; break;
+                    case VEXQ_TYPE_FLOAT64: os << ind << "const double " << x << " = " << dlit(n.lf) << ";\n"; break;
+                    case VEXQ_TYPE_DATE: os << ind << "const int " << x << " = " << n.ld << ";\n"; break;
+                    case VEXQ_TYPE_BOOL: os << ind << "const bool " << x << " = " << (n.lb ? "true" : "false") << ";\n"; break;
+                    default: os << ind << "const unsigned " << x << " = 0u;\n"; break;
+                }
+                break;
+            }
+            case NK::Cmp:
+                os << ind << "const bool " << ok << " = " << OK(0) << " && " << OK(1) << ";\n";
+                os << ind << "const bool " << x << " = " << ok << " && (" << X(0) << " " << cmp_op(n.op) << " " << X(1) << ");\n";
+                break;
+            case NK::Arith: {
+                os << ind << "const bool " << ok << " = " << OK(0) << " && " << OK(1) << ";\n";
+                if (n.type == VEXQ_TYPE_FLOAT64) {
+                    std::string e;
+                    switch (n.op) {
+                        case VEXQ_OP_ADD: e = X(0) + " + " + X(1); break;
+                        case VEXQ_OP_SUB: e = X(0) + " - " + X(1); break;
+                        case VEXQ_OP_MUL: e = X(0) + " * " + X(1); break;
+                        case VEXQ_OP_DIV:  // applyArithFloat64: x/0 → math.NaN()
+                            e = "(" + X(1) + " == 0.0 ? __longlong_as_double(0x7FF8000000000001LL) : " + X(0) + " / " + X(1) + ")";
+                            break;
+                    }
+                    os << ind << "const double " << x << " = " << ok << " ? (" << e << ") : 0.0;\n";
+                } else {
+                    std::string a = "(unsigned long long)" + X(0), b = "(unsigned long long)" + X(1), e;
+                    switch (n.op) {
+                        case VEXQ_OP_ADD: e = "(long long)(" + a + " + " + b + ")"; break;
+                        case VEXQ_OP_SUB: e = "(long long)(" + a + " - " + b + ")"; break;
+                        case VEXQ_OP_MUL: e = "(long long)(" + a + " * " + b + ")"; break;
+                        case VEXQ_OP_DIV:
+                            e = "(" + X(1) + " == 0LL ? 0LL : (" + X(1) + " == -1LL ? (long long)(0ull - " + a + ") : " + X(0) +
+                                " / " + X(1) + "))";
+                            break;
+                    }
+                    os << ind << "const long long " << x << " = " << ok << " ? " << e << " : 0LL;\n";
+                }
+                break;
+            }
+            case NK::Cast:
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                os << ind << "const double " << x << " = (double)" << X(0) << ";\n";
+                break;
+            case NK::And:
+            case NK::Or: {
+                const char* o = n.k == NK::And ? " & " : " | ";
+                os << ind << "const bool " << x << " = ";
+                for (size_t k = 0; k < n.ch.size(); k++) os << (k ? o : "") << X((int)k);
+                os << ";\n" << ind << "const bool " << ok << " = ";
+                for (size_t k = 0; k < n.ch.size(); k++) os << (k ? o : "") << OK((int)k);
+                os << ";\n";
+                break;
+            }
+            case NK::Not:  // NotExpr: flip only valid bits (exec/expr.go:1134-1137)
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                os << ind << "const bool " << x << " = " << X(0) << " != " << OK(0) << ";\n";
+                break;
+            case NK::IsNull:
+            case NK::IsNotNull:
+                os << ind << "const bool " << ok << " = true;\n";
+                os << ind << "const bool " << x << " = " << (n.k == NK::IsNull ? "!" : "") << OK(0) << ";\n";
+                break;
+            case NK::InInt:
+            case NK::InFloat: {
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                os << ind << "const bool " << x << " = " << OK(0) << " && (false";
+                if (n.k == NK::InInt) for (auto v : n.seti) os << " || " << X(0) << " == " << ilit(v);
+                else for (auto v : n.setf) os << " || " << X(0) << " == " << dlit(v);
+                os << ");\n";
+                break;
+            }
+            case NK::InFalse:
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                os << ind << "const bool " << x << " = false;\n";
+                break;
+            case NK::InCodes: {
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                if (n.codes.size() <= 64) {
+                    uint64_t m = 0;
+                    for (size_t c = 0; c < n.codes.size(); c++) if (n.codes[c]) m |= 1ull << c;
+                    os << ind << "const bool " << x << " = " << OK(0) << " && " << X(0) << " < 64u && ((" << m << "ull >> "
+                       << X(0) << ") & 1ull);\n";
+                } else {
+                    os << ind << "const bool " << x << " = " << OK(0) << " && ((__ldg(P.sets[" << n.set_idx << "] + ("
+                       << X(0) << " >> 5)) >> (" << X(0) << " & 31u)) & 1u);\n";
+                }
+                break;
+            }
+            case NK::StrEq: {
+                std::string neg = n.negate ? "true" : "false";
+                if (n.streq_code < 0) {  // literal in no dictionary: no rows (= ) / all rows (<>)
+                    os << ind << "const bool " << ok << " = " << neg << ";\n";
+                    os << ind << "const bool " << x << " = " << neg << ";\n";
+                    break;
+                }
+                std::string m = "(" + OK(0) + " && ((" + X(0) + " == " + std::to_string(n.streq_code) + "u) != " + neg + "))";
+                if (n.present_idx < 0) {
+                    os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                    os << ind << "const bool " << x << " = " << m << ";\n";
+                } else {
+                    os << ind << "const bool pr" << i << " = __ldg(P.present + " << n.present_idx
+                       << " * P.n_rg + (int)(r / P.rg_rows)) != 0;\n";
+                    os << ind << "const bool " << ok << " = pr" << i << " ? " << OK(0) << " : " << neg << ";\n";
+                    os << ind << "const bool " << x << " = pr" << i << " ? " << m << " : " << neg << ";\n";
+                }
+                break;
+            }
+            case NK::Case: {
+                std::string t = ctype(n.type);
+                int nw = (int)(n.ch.size() - (n.has_else ? 1 : 0)) / 2;
+                os << ind << t << " " << x << " = " << (n.has_else ? X((int)n.ch.size() - 1) : std::string(n.type == VEXQ_TYPE_FLOAT64 ? "0.0" : "0LL")) << ";\n";
+                os << ind << "bool " << ok << " = " << (n.has_else ? OK((int)n.ch.size() - 1) : std::string("false")) << ";\n";
+                for (int w = nw - 1; w >= 0; w--)
+                    os << ind << "if (" << OK(2 * w) << " && " << X(2 * w) << ") { " << x << " = " << X(2 * w + 1) << "; " << ok
+                       << " = " << OK(2 * w + 1) << "; }\n";
+                break;
+            }
+        }
+    }
+};
+
+// Structural signature of an IR subtree (deduplicates accumulator slots).
+std::string sig(const Plan& p, int i) {
+    const INode& n = p.ir[i];
+    std::ostringstream o;
+    o << (int)n.k << ":" << n.type << ":" << n.op << ":" << n.col << ":" << n.build << ":" << n.li << ":";
+    int64_t fb;
+    std::memcpy(&fb, &n.lf, 8);
+    o << fb << ":" << n.ld << ":" << n.lb << ":" << n.streq_code << ":" << n.negate << ":" << n.has_else << "(";
+    for (int c : n.ch) o << sig(p, c) << ",";
+    for (auto v : n.seti) o << v << ";";
+    for (auto v : n.setf) o << v << ";";
+    for (auto v : n.codes) o << (int)v;
+    o << ")";
+    return o.str();
+}
+
+int add_slot(Plan& p, std::map<std::string, int>& seen, SlotKind k, int input) {
+    std::string key = std::to_string((int)k) + "|" + (input >= 0 ? sig(p, input) : std::string("*"));
+    auto it = seen.find(key);
+    if (it != seen.end()) return it->second;
+    p.slots.push_back(Slot{k, input});
+    seen[key] = (int)p.slots.size() - 1;
+    return (int)p.slots.size() - 1;
+}
+
+// AccumTypeFor + output typing (exec/aggregate.go:51-72, 161-175, 780-876).
+void plan_aggs(Plan& p, const std::vector<std::pair<int, int>>& aggs_ir, const vexq_agg_desc* aggs) {
+    std::map<std::string, int> seen;
+    add_slot(p, seen, S_CNT, -1);  // slot 0: group row count (COUNT(*))
+    for (size_t j = 0; j < aggs_ir.size(); j++) {
+        int kind = aggs_ir[j].first, in = aggs_ir[j].second;
+        AggOut o;
+        o.kind = kind;
+        o.name = aggs[j].out_name ? aggs[j].out_name : "";
+        if (kind < VEXQ_AGG_COUNT || kind > VEXQ_AGG_MAX) fail(VEXQ_EINVAL, "unknown aggregate kind");
+        if (in < 0) {
+            if (kind != VEXQ_AGG_COUNT) fail(VEXQ_EINVAL, "aggregate column not found in schema");
+            o.value_slot = 0;
+            o.nn_slot = 0;
+            o.out_type = VEXQ_TYPE_INT64;
+            p.outs.push_back(o);
+            continue;
+        }
+        const INode& x = p.ir[in];
+        int nn = x.nullable ? add_slot(p, seen, S_NN, in) : 0;
+        o.nn_slot = nn;
+        switch (kind) {
+            case VEXQ_AGG_COUNT:
+                o.value_slot = nn;
+                o.out_type = VEXQ_TYPE_INT64;
+                break;
+            case VEXQ_AGG_SUM:
+                if (x.type == VEXQ_TYPE_STRING) fail(VEXQ_ENOTSUP, "SUM over a STRING column is not supported on the GPU path");
+                if (x.type == VEXQ_TYPE_FLOAT64) { o.value_slot = add_slot(p, seen, S_FSUM, in); o.out_type = VEXQ_TYPE_FLOAT64; }
+                else { o.value_slot = add_slot(p, seen, S_ISUM, in); o.out_type = VEXQ_TYPE_INT64; }
+                break;
+            case VEXQ_AGG_AVG:
+                if (x.type == VEXQ_TYPE_STRING) fail(VEXQ_ENOTSUP, "AVG over a STRING column is not supported on the GPU path");
+                o.value_slot = add_slot(p, seen, S_FSUM, in);
+                o.out_type = VEXQ_TYPE_FLOAT64;
+                break;
+            case VEXQ_AGG_MIN:
+            case VEXQ_AGG_MAX:
+                if (x.type == VEXQ_TYPE_STRING)
+                    fail(VEXQ_ENOTSUP, "MIN/MAX over a STRING column is not supported on the GPU path");
+                if (x.type == VEXQ_TYPE_FLOAT64)
+                    o.value_slot = add_slot(p, seen, kind == VEXQ_AGG_MIN ? S_FMIN : S_FMAX, in);
+                else
+                    o.value_slot = add_slot(p, seen, kind == VEXQ_AGG_MIN ? S_IMIN : S_IMAX, in);
+                o.out_type = x.type;
+                break;
+        }
+        p.outs.push_back(o);
+    }
+}
+
+// Group-key encoding: dense codes when every key column has a small domain.
+void plan_keys(Plan& p) {
+    int64_t dom = 1;
+    bool dense = true;
+    for (auto& k : p.keys) {
+        const Table* tt = k.build ? p.bt : p.t;
+        const Column& c = tt->cols[k.col];
+        k.type = c.type;
+        k.nullable = c.nullable;
+        int64_t d = 0;
+        int64_t nul = c.nullable ? 1 : 0;  // NULL takes the last code of a nullable column
+        if (c.type == VEXQ_TYPE_STRING) d = std::max<int64_t>((int64_t)c.dict.keys.size(), 1) + nul;
+        else if (c.type == VEXQ_TYPE_BOOL) d = 2 + nul;
+        else if ((c.type == VEXQ_TYPE_DATE || c.type == VEXQ_TYPE_INT64) && c.has_range && c.imax - c.imin < (1 << 22)) {
+            k.vmin = c.imin;
+            d = c.imax - c.imin + 1 + nul;
+        } else if (!c.has_range && (c.type == VEXQ_TYPE_DATE || c.type == VEXQ_TYPE_INT64)) {
+            d = 1;  // all NULL
+            k.nullable = true;
+        }
+        if (d <= 0) { dense = false; k.domain = 0; continue; }
+        k.domain = d;
+        if (dom <= (int64_t(1) << 40)) dom *= d;
+    }
+    p.domain = dense ? dom : 0;
+    // packed-key layout for the hash path
+    int shift = 0;
+    for (auto& k : p.keys) {
+        if (k.domain > 0) {
+            int b = 0;
+            while ((int64_t(1) << b) < k.domain) b++;
+            k.bits = std::max(b, 1);
+        } else if (k.type == VEXQ_TYPE_DATE) {
+            k.bits = 33;
+        } else {
+            if (k.nullable) fail(VEXQ_ENOTSUP, "GROUP BY over a nullable 64-bit column is not supported on the GPU path");
+            k.bits = 64;
+        }
+        k.shift = shift;
+        shift += k.bits;
+    }
+    if (shift > 64 && !dense) fail(VEXQ_ENOTSUP, "GROUP BY key wider than 64 bits is not supported on the GPU path");
+}
+
+void choose_path(Plan& p) {
+    int regs_per_group = 1;  // first-occurrence key
+    for (auto& s : p.slots) regs_per_group += 1;
+    if (p.domain > 0 && p.domain <= 16 && p.domain * regs_per_group <= 64) p.path = AggPath::Regs;
+    else if (p.domain > 0 && p.domain <= (int64_t(1) << 22)) p.path = AggPath::Dense;
+    else p.path = AggPath::Hash;
+    // bank layout
+    p.slot_pos.assign(p.slots.size(), -1);
+    p.nf = p.ni = 0;
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        bool in_float = p.path == AggPath::Regs ? p.slots[s].is_float() : p.slots[s].kind == S_FSUM;
+        p.slot_pos[s] = in_float ? p.nf++ : p.ni++;
+    }
+    p.fx_lsb.assign(std::max(p.nf, 1), 0);
+    if (p.path != AggPath::Regs) {
+        if (p.nf > 16) fail(VEXQ_ENOTSUP, "more than 16 float sums in one aggregate");
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            if (p.slots[s].kind != S_FSUM) continue;
+            const INode& x = p.ir[p.slots[s].input];
+            double m = x.bounded ? std::max(std::fabs(x.lo), std::fabs(x.hi)) : 0;
+            if (!x.bounded) fail(VEXQ_ENOTSUP, "float sum over an unbounded expression (division by a range containing 0)");
+            int e = 0;
+            while (std::ldexp(1.0, e) <= m && e < 1100) e++;
+            // |x| < 2^e; 97 fractional bits below the top keep 2^-44 relative exactness
+            // for every value within 2^-44 of the bound and the window holds 2^31 rows.
+            p.fx_lsb[p.slot_pos[s]] = e - 97;
+        }
+    }
+}
+
+// ---- code generation --------------------------------------------------------------------------
+
+struct ColUse {
+    std::set<int> scan;  // scanned-table columns loaded per 4-row vector
+};
+
+void collect_cols(const Plan& p, int i, std::set<int>& scan) {
+    if (i < 0) return;
+    const INode& n = p.ir[i];
+    if (n.k == NK::Col && !n.build) scan.insert(n.col);
+    for (int c : n.ch) collect_cols(p, c, scan);
+}
+
+void emit_loads(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
+    for (int c : cols) {
+        const Column& col = t->cols[c];
+        std::string C = std::to_string(c);
+        switch (col.type) {
+            case VEXQ_TYPE_INT64: os << "        long long cv" << C << "[4]; vq_ld4_i64(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+            case VEXQ_TYPE_FLOAT64: os << "        double cv" << C << "[4]; vq_ld4_f64(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+            case VEXQ_TYPE_DATE: os << "        int cv" << C << "[4]; vq_ld4_i32(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+            case VEXQ_TYPE_STRING: os << "        unsigned cv" << C << "[4]; vq_ld4_u32(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+            case VEXQ_TYPE_BOOL: os << "        unsigned cv" << C << "[4]; vq_ld4_u8(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+        }
+        if (col.nullable) os << "        const unsigned cm" << C << " = vq_bits4(P.valid[" << C << "], r0);\n";
+    }
+    (void)p;
+}
+
+// Group-key expression: dense gid or packed key, plus "any key NULL".
+void emit_key(std::ostringstream& os, const Plan& p, const std::vector<int>& key_nodes, const std::string& ind) {
+    bool dense = p.path != AggPath::Hash;
+    os << ind << "unsigned long long key = 0ull;\n" << ind << "bool anynull = false;\n";
+    long long stride = 1;
+    for (size_t i = 0; i < p.keys.size(); i++) {
+        const KeyCol& k = p.keys[i];
+        std::string x = "x" + std::to_string(key_nodes[i]), ok = "ok" + std::to_string(key_nodes[i]);
+        std::string code;
+        os << ind << "anynull = anynull || !" << ok << ";\n";
+        if (k.domain > 0) {
+            std::string nullc = k.nullable ? std::to_string(k.domain - 1) + "ull" : std::string("0ull");
+            if (k.type == VEXQ_TYPE_STRING) code = "(" + ok + " ? (unsigned long long)" + x + " : " + nullc + ")";
+            else if (k.type == VEXQ_TYPE_BOOL) code = "(" + ok + " ? (" + x + " ? 1ull : 0ull) : " + nullc + ")";
+            else code = "(" + ok + " ? (unsigned long long)((long long)" + x + " - " + ilit(k.vmin) + ") : " + nullc + ")";
+        } else if (k.type == VEXQ_TYPE_DATE) {
+            code = "(" + ok + " ? (unsigned long long)(unsigned)" + x + " : 0x100000000ull)";
+        } else if (k.type == VEXQ_TYPE_FLOAT64) {
+            code = "(unsigned long long)__double_as_longlong(" + x + ")";
+        } else {
+            code = "(unsigned long long)" + x;
+        }
+        if (dense) {
+            os << ind << "key += " << code << " * " << stride << "ull;\n";
+            stride *= k.domain;
+        } else {
+            os << ind << "key |= " << code << (k.shift ? " << " + std::to_string(k.shift) : std::string()) << ";\n";
+        }
+    }
+}
+
+// Order key of a group's first row: reproduces HashAggregate's insertion order
+// (exec/aggregate.go:409-457; agg_intkey.go:249-255: NULL-keyed rows take the
+// string-key path and are appended before the int-key groups).
+std::string order_expr(const Plan& p, const std::string& pos) {
+    if (!p.intkey_order) return pos;
+    return "((anynull ? 0ll : (1ll << 56)) | " + pos + ")";
+}
+
+void emit_slot_values(std::ostringstream& os, const Plan& p, const std::string& ind) {
+    for (size_t s = 1; s < p.slots.size(); s++) {
+        const Slot& sl = p.slots[s];
+        const INode& x = p.ir[sl.input];
+        std::string X = "x" + std::to_string(sl.input), OK = "ok" + std::to_string(sl.input);
+        std::string S = std::to_string(s);
+        os << ind << "const bool sok" << S << " = " << OK << ";\n";
+        if (sl.is_float() || sl.kind == S_FSUM) {
+            os << ind << "const double sv" << S << " = (double)" << (x.type == VEXQ_TYPE_BOOL ? "(" + X + " ? 1 : 0)" : X) << ";\n";
+        } else if (sl.kind != S_NN) {
+            os << ind << "const long long sv" << S << " = (long long)" << (x.type == VEXQ_TYPE_BOOL ? "(" + X + " ? 1 : 0)" : X) << ";\n";
+        }
+    }
+}
+
+std::string acc_name(const Plan& p, int g, int s) {
+    return (p.slots[s].is_float() ? "af" : "ai") + std::to_string(g) + "_" + std::to_string(p.slot_pos[s]);
+}
+
+// Register path: accumulators live in registers, one set per dense group.
+void emit_regs_decl(std::ostringstream& os, const Plan& p) {
+    for (int64_t g = 0; g < p.domain; g++) {
+        os << "    long long fo" << g << " = 0x7FFFFFFFFFFFFFFFLL;\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            const Slot& sl = p.slots[s];
+            std::string init;
+            switch (sl.kind) {
+                case S_IMIN: init = "0x7FFFFFFFFFFFFFFFLL"; break;
+                case S_IMAX: init = "(-0x7FFFFFFFFFFFFFFFLL - 1LL)"; break;
+                case S_FMIN: init = "1.7976931348623157e308"; break;   // math.MaxFloat64 (aggregate.go:262)
+                case S_FMAX: init = "-1.7976931348623157e308"; break;
+                case S_FSUM: init = "0.0"; break;
+                default: init = "0LL"; break;
+            }
+            os << "    " << (sl.is_float() ? "double " : "long long ") << acc_name(p, (int)g, (int)s) << " = " << init << ";\n";
+        }
+    }
+}
+
+void emit_regs_update(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
+    os << ind << "switch ((int)key) {\n";
+    for (int64_t g = 0; g < p.domain; g++) {
+        os << ind << "case " << g << ": {\n";
+        std::string in = ind + "    ";
+        os << in << "fo" << g << " = min(fo" << g << ", " << order << ");\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string a = acc_name(p, (int)g, (int)s), S = std::to_string(s);
+            switch (p.slots[s].kind) {
+                case S_CNT: os << in << a << " += 1LL;\n"; break;
+                case S_NN: os << in << "if (sok" << S << ") " << a << " += 1LL;\n"; break;
+                case S_ISUM: os << in << "if (sok" << S << ") " << a << " = (long long)((unsigned long long)" << a
+                                << " + (unsigned long long)sv" << S << ");\n"; break;
+                case S_IMIN: os << in << "if (sok" << S << " && sv" << S << " < " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_IMAX: os << in << "if (sok" << S << " && sv" << S << " > " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_FSUM: os << in << "if (sok" << S << ") " << a << " += sv" << S << ";\n"; break;
+                case S_FMIN: os << in << "if (sok" << S << " && sv" << S << " < " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_FMAX: os << in << "if (sok" << S << " && sv" << S << " > " << a << ") " << a << " = sv" << S << ";\n"; break;
+            }
+        }
+        os << in << "break;\n" << ind << "}\n";
+    }
+    os << ind << "default: break;\n" << ind << "}\n";
+}
+
+// Block reduction of the register accumulators into per-block partials.
+void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
+    int warps = block / 32;
+    int G = (int)p.domain;
+    int nf = p.nf, ni = p.ni;
+    os << "    __shared__ double sh_f[" << warps << "][" << std::max(G * nf, 1) << "];\n";
+    os << "    __shared__ long long sh_i[" << warps << "][" << std::max(G * (ni + 1), 1) << "];\n";
+    os << "    const int warp = threadIdx.x >> 5;\n";
+    for (int g = 0; g < G; g++) {
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string a = acc_name(p, g, (int)s);
+            const char* op;
+            switch (p.slots[s].kind) {
+                case S_IMIN: op = "min"; break;
+                case S_IMAX: op = "max"; break;
+                case S_FMIN: op = "vq_fminr"; break;
+                case S_FMAX: op = "vq_fmaxr"; break;
+                default: op = nullptr; break;
+            }
+            os << "    for (int o = 16; o > 0; o >>= 1) { ";
+            if (p.slots[s].is_float()) os << "double t = __shfl_xor_sync(0xffffffffu, " << a << ", o); ";
+            else os << "long long t = __shfl_xor_sync(0xffffffffu, " << a << ", o); ";
+            if (op) os << a << " = " << op << "(" << a << ", t); }\n";
+            else if (p.slots[s].kind == S_ISUM) os << a << " = (long long)((unsigned long long)" << a << " + (unsigned long long)t); }\n";
+            else os << a << " += t; }\n";
+            int idx = p.slots[s].is_float() ? g * nf + p.slot_pos[s] : g * (ni + 1) + p.slot_pos[s];
+            os << "    if ((threadIdx.x & 31) == 0) sh_" << (p.slots[s].is_float() ? "f" : "i") << "[warp][" << idx << "] = " << a << ";\n";
+        }
+        os << "    for (int o = 16; o > 0; o >>= 1) fo" << g << " = min(fo" << g << ", __shfl_xor_sync(0xffffffffu, fo" << g << ", o));\n";
+        os << "    if ((threadIdx.x & 31) == 0) sh_i[warp][" << g * (ni + 1) + ni << "] = fo" << g << ";\n";
+    }
+    os << "    __syncthreads();\n";
+    // fixed-order combine over warps; kinds per bank entry
+    os << "    for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
+    os << "        const int s = t % " << std::max(nf, 1) << ";\n";
+    os << "        double v = sh_f[0][t];\n";
+    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_fcomb(P_fkind(s), v, sh_f[w][t]);\n";
+    os << "        P.part_f[(long long)blockIdx.x * " << G * nf << " + t] = v;\n    }\n";
+    os << "    for (int t = threadIdx.x; t < " << G * (ni + 1) << "; t += blockDim.x) {\n";
+    os << "        const int s = t % " << (ni + 1) << ";\n";
+    os << "        long long v = sh_i[0][t];\n";
+    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_icomb(P_ikind(s), v, sh_i[w][t]);\n";
+    os << "        P.part_i[(long long)blockIdx.x * " << G * (ni + 1) << " + t] = v;\n    }\n";
+}
+
+// Atomic path: group table in global memory.
+void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
+    if (p.path == AggPath::Dense) {
+        os << ind << "const unsigned long long slot = key;\n";
+    } else {
+        os << ind << "const unsigned long long slot = vq_insert(P.keys, P.cap_mask, P.cap, key, P.ngroups, P.error);\n";
+        os << ind << "if (slot == VQ_NOSLOT) continue;\n";
+    }
+    os << ind << "const long long stride = (long long)P.cap + 1;\n";
+    os << ind << "atomicMin(&P.first[slot], " << order << ");\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s);
+        const Slot& sl = p.slots[s];
+        int pos = p.slot_pos[s];
+        std::string ai = "P.acc_i[" + std::to_string(pos) + " * stride + slot]";
+        std::string aiu = "(unsigned long long*)&" + ai;
+        switch (sl.kind) {
+            case S_CNT: os << ind << "atomicAdd(" << aiu << ", 1ull);\n"; break;
+            case S_NN: os << ind << "if (sok" << S << ") atomicAdd(" << aiu << ", 1ull);\n"; break;
+            case S_ISUM: os << ind << "if (sok" << S << ") atomicAdd(" << aiu << ", (unsigned long long)sv" << S << ");\n"; break;
+            case S_IMIN: os << ind << "if (sok" << S << ") atomicMin(&" << ai << ", sv" << S << ");\n"; break;
+            case S_IMAX: os << ind << "if (sok" << S << ") atomicMax(&" << ai << ", sv" << S << ");\n"; break;
+            case S_FMIN: os << ind << "if (sok" << S << " && !isnan(sv" << S << ")) atomicMin(" << aiu << ", vq_fkey(sv" << S << "));\n"; break;
+            case S_FMAX: os << ind << "if (sok" << S << " && !isnan(sv" << S << ")) atomicMax(" << aiu << ", vq_fkey(sv" << S << "));\n"; break;
+            case S_FSUM:
+                os << ind << "if (sok" << S << ") vq_fx_add<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, sv" << S
+                   << ", " << p.fx_lsb[pos] << ", P.special + (long long)" << pos << " * stride + slot, P.error);\n";
+                break;
+        }
+    }
+}
+
+std::string kernel_head(const std::string& name, int block) {
+    std::ostringstream os;
+    os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") " << name
+       << "(const __grid_constant__ VQParams P) {\n";
+    return os.str();
+}
+
+// Chunk loop over the row segments: each warp takes 128-row chunks; lane l
+// handles rows r0..r0+3 with 128-bit loads.
+std::string chunk_loop_open() {
+    return
+        "    const int lane = threadIdx.x & 31;\n"
+        "    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;\n"
+        "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n"
+        "    for (long long c = gw; c < P.nchunks; c += nw) {\n"
+        "        int lo = 0, hi = P.nseg - 1;\n"
+        "        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= c) lo = mid; else hi = mid - 1; }\n"
+        "        const long long s0 = P.seg[3 * lo], s1 = P.seg[3 * lo + 1];\n"
+        "        const long long r0 = (s0 & ~127LL) + (c - P.seg[3 * lo + 2]) * 128 + lane * 4;\n";
+}
+
+}  // namespace
+
+// Generates the aggregate scan kernel (table → filter → project → aggregate).
+static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    for (int k : key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    os << kernel_head("vq_agg", block);
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    os << chunk_loop_open();
+    emit_loads(os, p, p.t, cols);
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(p, os);
+    if (p.pred >= 0) {
+        g.emit(p.pred);
+        os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
+    }
+    for (int k : key_nodes) g.emit(k);
+    for (auto& s : p.slots) if (s.input >= 0) g.emit(s.input);
+    emit_key(os, p, key_nodes, "            ");
+    emit_slot_values(os, p, "            ");
+    std::string order = order_expr(p, "r");
+    if (p.path == AggPath::Regs) emit_regs_update(os, p, "            ", order);
+    else emit_atomic_update(os, p, "            ", order);
+    os << "        }\n    }\n";
+    if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
+    os << "}\n";
+    return os.str();
+}
+
+// Join build kernel: filtered build rows with non-NULL keys are inserted into
+// the build table (mode 0: insert + count, mode 1: place row ids).
+static std::string gen_build_kernel(Plan& p, int key_node, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.bpred, cols);
+    collect_cols(p, key_node, cols);
+    os << kernel_head("vq_build", block);
+    os << chunk_loop_open();
+    emit_loads(os, p, p.bt, cols);
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(p, os);
+    if (p.bpred >= 0) {
+        g.emit(p.bpred);
+        os << "            if (!(x" << p.bpred << " && ok" << p.bpred << ")) continue;\n";
+    }
+    g.emit(key_node);
+    std::string K = std::to_string(key_node);
+    os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
+    os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
+    os << "            if (P.mode == 0) {\n";
+    os << "                const unsigned long long js = vq_insert(P.jkeys, P.jmask, P.jmask + 1, jk, P.jnkeys, P.error);\n";
+    os << "                if (js != VQ_NOSLOT) atomicAdd(P.jcount + js, 1);\n";
+    os << "            } else {\n";
+    os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
+    os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
+    os << "            }\n";
+    os << "        }\n    }\n}\n";
+    return os.str();
+}
+
+// Join probe kernel: probe rows pass the probe filter, look their key up, and
+// every (build row, probe row) match runs the residual filter and is folded
+// into the aggregate, in (probe row, chain position) order keys.
+static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    collect_cols(p, p.probe_key, cols);
+    collect_cols(p, p.resid, cols);
+    for (int k : key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    os << kernel_head("vq_agg", block);
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    os << chunk_loop_open();
+    emit_loads(os, p, p.t, cols);
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(p, os);
+    if (p.pred >= 0) {
+        g.emit(p.pred);
+        os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
+    }
+    g.emit(p.probe_key);
+    std::string K = std::to_string(p.probe_key);
+    os << "            if (!ok" << K << ") continue;\n";
+    os << "            const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, (unsigned long long)(long long)x" << K << ");\n";
+    os << "            if (js == VQ_NOSLOT) continue;\n";
+    os << "            const int jb = P.jstart[js], je = jb + P.jcount[js];\n";
+    os << "            for (int ji = jb; ji < je; ji++) {\n";
+    os << "                const long long brow = P.jrows[ji];\n";
+    // above-join expressions: a fresh memo scope per match for build-side reads
+    Gen g2(p, os);
+    g2.done = g.done;
+    g2.ind = "                ";
+    if (p.resid >= 0) {
+        g2.emit(p.resid);
+        os << "                if (!(x" << p.resid << " && ok" << p.resid << ")) continue;\n";
+    }
+    for (int k : key_nodes) g2.emit(k);
+    for (auto& s : p.slots) if (s.input >= 0) g2.emit(s.input);
+    emit_key(os, p, key_nodes, "                ");
+    emit_slot_values(os, p, "                ");
+    std::string order = order_expr(p, "((r << 16) | (long long)min(ji - jb, 65535))");
+    if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
+    else emit_atomic_update(os, p, "                ", order);
+    os << "            }\n        }\n    }\n";
+    if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
+    os << "}\n";
+    return os.str();
+}
+
+// Kind tables used by the register-path flush (per bank entry).
+static std::string gen_kind_tables(const Plan& p) {
+    std::ostringstream os;
+    std::vector<int> fk(std::max(p.nf, 1), 0), ik(p.ni + 1, 0);
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        int k = p.slots[s].kind;
+        int code = (k == S_IMIN || k == S_FMIN) ? 1 : (k == S_IMAX || k == S_FMAX) ? 2 : 0;
+        if (p.slots[s].is_float()) fk[p.slot_pos[s]] = code;
+        else ik[p.slot_pos[s]] = code;
+    }
+    ik[p.ni] = 1;  // first-occurrence key: min
+    os << "__device__ __forceinline__ int P_fkind(int s) { switch (s) {";
+    for (size_t i = 0; i < fk.size(); i++) os << " case " << i << ": return " << fk[i] << ";";
+    os << " } return 0; }\n";
+    os << "__device__ __forceinline__ int P_ikind(int s) { switch (s) {";
+    for (size_t i = 0; i < ik.size(); i++) os << " case " << i << ": return " << ik[i] << ";";
+    os << " } return 0; }\n";
+    return os.str();
+}
+
+static const int kBlock = 256;
+
+static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join, int build_key_node) {
+    analyze(p);
+    // large IN/LIKE code sets go to device bitsets
+    for (auto& n : p.ir) {
+        if (n.k == NK::InCodes && n.codes.size() > 64) {
+            if ((int)p.sets.size() >= VQ_MAXSETS) fail(VEXQ_ENOTSUP, "too many large IN/LIKE sets");
+            std::vector<uint32_t> bits((n.codes.size() + 31) / 32, 0);
+            for (size_t c = 0; c < n.codes.size(); c++) if (n.codes[c]) bits[c >> 5] |= 1u << (c & 31);
+            n.set_idx = (int)p.sets.size();
+            p.sets.push_back(std::move(bits));
+        }
+    }
+    choose_path(p);
+    std::ostringstream src;
+    src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
+    std::string body = join ? gen_probe_kernel(p, key_nodes, kBlock) : gen_agg_kernel(p, key_nodes, kBlock);
+    p.src_main = src.str() + body;
+    if (join) p.src_build = std::string(prelude_source()) + "\n" + gen_build_kernel(p, build_key_node, kBlock);
+    std::ostringstream ex;
+    ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
+       << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni;
+    p.explain = ex.str();
+    p.k_main = jit_get(p.src_main, "vq_agg", kBlock);
+    if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock);
+    // device-side tables of the plan
+    if (!p.sets.empty()) {
+        size_t tot = 0;
+        for (auto& s : p.sets) tot += s.size();
+        p.d_sets.alloc(tot * 4);
+        size_t off = 0;
+        for (auto& s : p.sets) {
+            VQ_CUDA(cudaMemcpy(p.d_sets.as<uint32_t>() + off, s.data(), s.size() * 4, cudaMemcpyHostToDevice));
+            off += s.size();
+        }
+    }
+    auto upload_presence = [](const Table* tt, const std::vector<std::pair<int, int64_t>>& pl, DevBuf& dst) {
+        if (pl.empty()) return;
+        std::vector<uint8_t> pres(pl.size() * (size_t)tt->n_rg, 0);
+        for (size_t i = 0; i < pl.size(); i++) {
+            const Column& c = tt->cols[pl[i].first];
+            for (int rg = 0; rg < tt->n_rg; rg++) pres[i * tt->n_rg + rg] = c.rg_present[rg][pl[i].second];
+        }
+        dst.alloc(pres.size());
+        VQ_CUDA(cudaMemcpy(dst.p, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+    };
+    upload_presence(p.t, p.presence, p.d_present);
+    if (p.bt) upload_presence(p.bt, p.bpresence, p.d_bpresent);
+}
+
+static void copy_zone_tree(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* ch, int nch) {
+    p.zn_nodes.assign(nodes, nodes + nnodes);
+    p.zn_children.assign(ch, ch + nch);
+    for (auto& n : p.zn_nodes) n.lit_str = nullptr;  // strings re-attached below
+}
+
+// Keeps string literals alive for the zone predicate (dates parse from them).
+struct ZoneStrings {
+    std::vector<std::string> s;
+};
+static std::map<const Plan*, ZoneStrings> g_zone_strings;
+static std::mutex g_zone_mu;
+
+static void keep_zone_strings(Plan& p, const vexq_expr* nodes, int nnodes) {
+    std::lock_guard<std::mutex> lk(g_zone_mu);
+    ZoneStrings& z = g_zone_strings[&p];
+    z.s.resize(nnodes);
+    for (int i = 0; i < nnodes; i++) {
+        if (nodes[i].lit_str) {
+            z.s[i] = nodes[i].lit_str;
+            p.zn_nodes[i].lit_str = z.s[i].c_str();
+        }
+    }
+}
+
+Plan::~Plan() {
+    std::lock_guard<std::mutex> lk(g_zone_mu);
+    g_zone_strings.erase(this);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+static void resolve_intkey(Plan& p) {
+    // canUseIntKey (exec/agg_intkey.go:104-116): every GROUP BY column a dictionary string, ≤ 8 columns
+    bool all_str = !p.keys.empty() && p.keys.size() <= 8;
+    for (auto& k : p.keys) if (k.type != VEXQ_TYPE_STRING) all_str = false;
+    p.intkey_order = all_str;
+    size_t n = p.keys.size();
+    p.intkey_width = n <= 2 ? 32 : n <= 4 ? 16 : 8;
+}
+
+Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d) {
+    if (!d || (d->naggs == 0 && d->ngroup_by == 0))
+        fail(VEXQ_EINVAL, "exec: hash aggregate: no group-by columns or aggregate expressions");
+    std::unique_ptr<Plan> p(new Plan);
+    p->t = t;
+    p->order = d->order;
+    Translator tr{*p, d->nodes, d->nnodes, d->children, d->nchildren, t, nullptr};
+    if (d->predicate >= 0) {
+        p->pred = tr.tr(d->predicate);
+        if (p->ir[p->pred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    }
+    std::vector<int> key_nodes;
+    for (int i = 0; i < d->ngroup_by; i++) {
+        int c = d->group_by[i];
+        if (c < 0 || c >= (int)t->cols.size()) fail(VEXQ_EINVAL, "GROUP BY column out of range");
+        KeyCol k;
+        k.col = c;
+        k.build = false;
+        p->keys.push_back(k);
+        INode n;
+        n.k = NK::Col;
+        n.col = c;
+        n.type = t->cols[c].type;
+        n.nullable = t->cols[c].nullable;
+        key_nodes.push_back(tr.add(n));
+        p->gb_types.push_back(n.type);
+    }
+    std::vector<std::pair<int, int>> aggs;
+    for (int j = 0; j < d->naggs; j++) aggs.push_back({d->aggs[j].kind, d->aggs[j].input >= 0 ? tr.tr(d->aggs[j].input) : -1});
+    analyze(*p);
+    plan_keys(*p);
+    resolve_intkey(*p);
+    plan_aggs(*p, aggs, d->aggs);
+    copy_zone_tree(*p, d->nodes, d->nnodes, d->children, d->nchildren);
+    keep_zone_strings(*p, d->nodes, d->nnodes);
+    p->zn_pred = d->predicate;
+    finish_compile(*p, key_nodes, false, -1);
+    return p.release();
+}
+
+Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
+    if (!d || (d->naggs == 0 && d->ngroup_by == 0))
+        fail(VEXQ_EINVAL, "exec: hash aggregate: no group-by columns or aggregate expressions");
+    std::unique_ptr<Plan> p(new Plan);
+    p->is_join = true;
+    p->t = pt;
+    p->bt = bt;
+    p->order = d->order;
+    int nb = (int)bt->cols.size();
+    if (d->build_key < 0 || d->build_key >= nb) fail(VEXQ_EINVAL, "exec: hash join: build key out of range");
+    if (d->probe_key < 0 || d->probe_key >= (int)pt->cols.size()) fail(VEXQ_EINVAL, "exec: hash join: probe key out of range");
+    int bkt = bt->cols[d->build_key].type, pkt = pt->cols[d->probe_key].type;
+    if ((bkt != VEXQ_TYPE_INT64 && bkt != VEXQ_TYPE_DATE) || (pkt != VEXQ_TYPE_INT64 && pkt != VEXQ_TYPE_DATE))
+        fail(VEXQ_ENOTSUP, "join keys must be INT64 or DATE columns on the GPU path");
+    // build side predicate + key: scoped to the build table
+    Translator tb{*p, d->nodes, d->nnodes, d->children, d->nchildren, bt, nullptr};
+    tb.presence = &p->bpresence;
+    if (d->build_predicate >= 0) {
+        p->bpred = tb.tr(d->build_predicate);
+        if (p->ir[p->bpred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    }
+    INode bk;
+    bk.k = NK::Col;
+    bk.col = d->build_key;
+    bk.type = bkt;
+    bk.nullable = bt->cols[d->build_key].nullable;
+    int bkey = tb.add(bk);
+    // probe side
+    Translator tp{*p, d->nodes, d->nnodes, d->children, d->nchildren, pt, nullptr};
+    tp.lit_strs = tb.lit_strs;
+    if (d->probe_predicate >= 0) {
+        p->pred = tp.tr(d->probe_predicate);
+        if (p->ir[p->pred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    }
+    INode pk;
+    pk.k = NK::Col;
+    pk.col = d->probe_key;
+    pk.type = pkt;
+    pk.nullable = pt->cols[d->probe_key].nullable;
+    p->probe_key = tp.add(pk);
+    // above the join: joined schema (build columns, then probe columns)
+    Translator ta{*p, d->nodes, d->nnodes, d->children, d->nchildren, pt, bt, nb, true};
+    ta.lit_strs = tp.lit_strs;
+    if (d->residual >= 0) {
+        p->resid = ta.tr(d->residual);
+        if (p->ir[p->resid].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    }
+    std::vector<int> key_nodes;
+    for (int i = 0; i < d->ngroup_by; i++) {
+        int c = d->group_by[i];
+        if (c < 0 || c >= nb + (int)pt->cols.size()) fail(VEXQ_EINVAL, "GROUP BY column out of range");
+        KeyCol k;
+        k.build = c < nb;
+        k.col = k.build ? c : c - nb;
+        p->keys.push_back(k);
+        INode n;
+        n.k = NK::Col;
+        n.col = k.col;
+        n.build = k.build;
+        const Column& col = (k.build ? bt : pt)->cols[k.col];
+        n.type = col.type;
+        n.nullable = col.nullable;
+        key_nodes.push_back(ta.add(n));
+        p->gb_types.push_back(n.type);
+    }
+    std::vector<std::pair<int, int>> aggs;
+    for (int j = 0; j < d->naggs; j++) aggs.push_back({d->aggs[j].kind, d->aggs[j].input >= 0 ? ta.tr(d->aggs[j].input) : -1});
+    analyze(*p);
+    plan_keys(*p);
+    resolve_intkey(*p);
+    plan_aggs(*p, aggs, d->aggs);
+    copy_zone_tree(*p, d->nodes, d->nnodes, d->children, d->nchildren);
+    keep_zone_strings(*p, d->nodes, d->nnodes);
+    p->zn_pred = d->probe_predicate;
+    p->zn_bpred = d->build_predicate;
+    p->radix_bits = d->radix_bits;
+    p->build_key = d->build_key;
+    finish_compile(*p, key_nodes, true, bkey);
+    return p.release();
+}
+
+// Standalone filter (Filter.Next + BoolToSelVecInto, exec/filter.go:49-78):
+// each lane evaluates four rows; warp ballots assemble a 128-row selection
+// bitmap (bit = row passes: predicate true AND valid) per chunk.
+Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred) {
+    std::unique_ptr<Plan> p(new Plan);
+    p->t = t;
+    Translator tr{*p, nodes, nnodes, children, nchildren, t, nullptr};
+    p->pred = tr.tr(pred);
+    if (p->ir[p->pred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    analyze(*p);
+    for (auto& n : p->ir) {
+        if (n.k == NK::InCodes && n.codes.size() > 64) {
+            if ((int)p->sets.size() >= VQ_MAXSETS) fail(VEXQ_ENOTSUP, "too many large IN/LIKE sets");
+            std::vector<uint32_t> bits((n.codes.size() + 31) / 32, 0);
+            for (size_t c = 0; c < n.codes.size(); c++) if (n.codes[c]) bits[c >> 5] |= 1u << (c & 31);
+            n.set_idx = (int)p->sets.size();
+            p->sets.push_back(std::move(bits));
+        }
+    }
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(*p, p->pred, cols);
+    os << prelude_source() << "\n" << kernel_head("vq_filter", kBlock) << chunk_loop_open();
+    emit_loads(os, *p, t, cols);
+    os << "        unsigned nib = 0u;\n";
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(*p, os);
+    g.emit(p->pred);
+    os << "            if (x" << p->pred << " && ok" << p->pred << ") nib |= 1u << k;\n";
+    os << "        }\n";
+    // lane l holds rows base+4l..base+4l+3; word w of the chunk = lanes 8w..8w+7
+    os << "        const unsigned long long spread = ((unsigned long long)nib) << (4 * (lane & 7));\n";
+    os << "        unsigned word = (unsigned)spread;\n";
+    os << "        for (int o = 1; o < 8; o <<= 1) word |= __shfl_xor_sync(0xffffffffu, word, o);\n";
+    os << "        if ((lane & 7) == 0 && word) {\n";
+    os << "            const long long wi = ((s0 & ~127LL) + (c - P.seg[3 * lo + 2]) * 128) / 32 + (lane >> 3);\n";
+    os << "            atomicOr(reinterpret_cast<unsigned*>(P.acc_i) + wi, word);\n";
+    os << "            atomicAdd(P.ngroups, (unsigned long long)__popc(word));\n";
+    os << "        }\n    }\n}\n";
+    p->src_main = os.str();
+    p->k_main = jit_get(p->src_main, "vq_filter", kBlock);
+    if (!p->sets.empty()) {
+        size_t tot = 0;
+        for (auto& st : p->sets) tot += st.size();
+        p->d_sets.alloc(tot * 4);
+        size_t off = 0;
+        for (auto& st : p->sets) {
+            VQ_CUDA(cudaMemcpy(p->d_sets.as<uint32_t>() + off, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+            off += st.size();
+        }
+    }
+    if (!p->presence.empty()) {
+        std::vector<uint8_t> pres(p->presence.size() * (size_t)t->n_rg, 0);
+        for (size_t i = 0; i < p->presence.size(); i++)
+            for (int rg = 0; rg < t->n_rg; rg++)
+                pres[i * t->n_rg + rg] = t->cols[p->presence[i].first].rg_present[rg][p->presence[i].second];
+        p->d_present.alloc(pres.size());
+        VQ_CUDA(cudaMemcpy(p->d_present.p, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+    }
+    p->explain = "filter";
+    return p.release();
+}
+
+// ---- zone maps (planner/physical.go:624-750) ----------------------------------------------------
+
+static bool literal_int64(const vexq_expr& e, int64_t* v, int* lk) {
+    if (e.kind != VEXQ_E_LITERAL) return false;
+    *lk = e.lit_kind;
+    if (e.lit_kind == VEXQ_LIT_INT) { *v = e.lit_int; return true; }
+    if (e.lit_kind == VEXQ_LIT_FLOAT) { std::memcpy(v, &e.lit_float, 8); return true; }
+    if (e.lit_kind == VEXQ_LIT_STRING) return parse_date(e.lit_str, v);
+    return false;
+}
+
+static bool zone_rec(const Plan& p, int idx, const Table& t, int rg) {
+    if (idx < 0 || idx >= (int)p.zn_nodes.size()) return true;
+    const vexq_expr& e = p.zn_nodes[idx];
+    auto ch = [&](int k) { return p.zn_children[e.child0 + k]; };
+    if (e.kind == VEXQ_E_AND) {
+        for (int k = 0; k < e.nchildren; k++) if (!zone_rec(p, ch(k), t, rg)) return false;
+        return true;
+    }
+    if (e.kind == VEXQ_E_OR) {
+        if (e.nchildren == 0) return true;
+        for (int k = 0; k < e.nchildren; k++) if (zone_rec(p, ch(k), t, rg)) return true;
+        return false;
+    }
+    if (e.kind == VEXQ_E_BETWEEN) {
+        const vexq_expr& c = p.zn_nodes[ch(0)];
+        if (c.kind != VEXQ_E_COLUMN || c.column < 0 || c.column >= (int)t.cols.size()) return true;
+        const vexq_zone_map& z = t.cols[c.column].zones[rg];
+        if (!z.has_min_max) return true;
+        int64_t lo, hi;
+        int lk;
+        if (!literal_int64(p.zn_nodes[ch(1)], &lo, &lk) || !literal_int64(p.zn_nodes[ch(2)], &hi, &lk)) return true;
+        if ((int64_t)z.max < lo || (int64_t)z.min > hi) return e.op == 1;
+        return true;
+    }
+    if (e.kind == VEXQ_E_BINARY && e.op >= VEXQ_OP_EQ && e.op <= VEXQ_OP_GE) {
+        const vexq_expr& L = p.zn_nodes[ch(0)];
+        const vexq_expr& R = p.zn_nodes[ch(1)];
+        const vexq_expr *cr, *lit;
+        bool rev = false;
+        if (L.kind == VEXQ_E_COLUMN) { cr = &L; lit = &R; }
+        else if (R.kind == VEXQ_E_COLUMN) { cr = &R; lit = &L; rev = true; }
+        else return true;
+        if (cr->column < 0 || cr->column >= (int)t.cols.size()) return true;
+        const vexq_zone_map& z = t.cols[cr->column].zones[rg];
+        if (!z.has_min_max) return true;
+        int64_t v;
+        int lk;
+        if (!literal_int64(*lit, &v, &lk)) return true;
+        if (t.cols[cr->column].type == VEXQ_TYPE_FLOAT64 && lk == VEXQ_LIT_INT) {
+            double f = (double)v;
+            std::memcpy(&v, &f, 8);
+        }
+        int64_t mn = (int64_t)z.min, mx = (int64_t)z.max;
+        int op = e.op;
+        if (rev) {
+            if (op == VEXQ_OP_LT) op = VEXQ_OP_GT;
+            else if (op == VEXQ_OP_LE) op = VEXQ_OP_GE;
+            else if (op == VEXQ_OP_GT) op = VEXQ_OP_LT;
+            else if (op == VEXQ_OP_GE) op = VEXQ_OP_LE;
+        }
+        switch (op) {
+            case VEXQ_OP_EQ: return mn <= v && v <= mx;
+            case VEXQ_OP_LT: return mn < v;
+            case VEXQ_OP_LE: return mn <= v;
+            case VEXQ_OP_GT: return mx > v;
+            case VEXQ_OP_GE: return mx >= v;
+            default: return true;
+        }
+    }
+    return true;
+}
+
+bool zone_eval(const Plan& p, int root, const Table& t, int rg) { return root < 0 ? true : zone_rec(p, root, t, rg); }
+
+ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_start, int rg_end) {
+    ScanSegs s;
+    long long chunks = 0;
+    int rg = rg_start;
+    while (rg < rg_end) {
+        if (!mask[rg]) { rg++; continue; }
+        int e = rg;
+        while (e < rg_end && mask[e]) e++;
+        long long a = t.rg_start(rg), b = t.rg_end(e - 1);
+        if (b > a) {
+            s.seg.push_back(a);
+            s.seg.push_back(b);
+            s.seg.push_back(chunks);
+            long long base = a & ~127LL;
+            chunks += (b - base + 127) / 128;
+            s.rows += b - a;
+        }
+        rg = e;
+    }
+    s.nchunks = chunks;
+    return s;
+}
+
+}  // namespace vq

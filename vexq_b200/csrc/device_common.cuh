@@ -1,0 +1,254 @@
+// device_common.cuh — device helpers shared by the runtime-specialised scan
+// kernels (prepended to every generated source) and the static kernels.
+#pragma once
+
+typedef long long vq_i64;
+typedef unsigned long long vq_u64;
+
+__device__ __host__ inline double __longlong_as_double_portable(vq_i64 b) {
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double(b);
+#else
+    double d;
+    __builtin_memcpy(&d, &b, 8);
+    return d;
+#endif
+}
+
+#define VQ_EMPTY_KEY 0xFFFFFFFFFFFFFFFFull
+#define VQ_MAX_PROBES 4096
+
+// Validity bit of row r in an LSB-first bitmap (1 = valid), storage/codec.go:13-39.
+__device__ __forceinline__ bool vq_bit(const unsigned char* bm, vq_i64 r) {
+    return (bm[r >> 3] >> (r & 7)) & 1;
+}
+// Four validity bits of rows r0..r0+3 (r0 % 4 == 0).
+__device__ __forceinline__ unsigned vq_bits4(const unsigned char* bm, vq_i64 r0) {
+    return (__ldg(bm + (r0 >> 3)) >> (r0 & 7)) & 0xFu;
+}
+
+// 128-bit vectorised loads of four consecutive rows (r0 % 4 == 0) through the
+// read-only path; columns are 256-byte aligned and padded past the last row.
+__device__ __forceinline__ void vq_ld4_i64(const void* p, vq_i64 r0, vq_i64* v) {
+    const longlong2* q = reinterpret_cast<const longlong2*>(static_cast<const vq_i64*>(p) + r0);
+    longlong2 a = __ldg(q), b = __ldg(q + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void vq_ld4_f64(const void* p, vq_i64 r0, double* v) {
+    const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + r0);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void vq_ld4_i32(const void* p, vq_i64 r0, int* v) {
+    int4 a = __ldg(reinterpret_cast<const int4*>(static_cast<const int*>(p) + r0));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void vq_ld4_u32(const void* p, vq_i64 r0, unsigned* v) {
+    uint4 a = __ldg(reinterpret_cast<const uint4*>(static_cast<const unsigned*>(p) + r0));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void vq_ld4_u8(const void* p, vq_i64 r0, unsigned* v) {
+    unsigned w = __ldg(reinterpret_cast<const unsigned*>(static_cast<const unsigned char*>(p) + r0));
+    v[0] = w & 0xFF; v[1] = (w >> 8) & 0xFF; v[2] = (w >> 16) & 0xFF; v[3] = w >> 24;
+}
+
+// radixHash (exec/parallel_join.go:91-99): the murmur3 64-bit finalizer.
+__device__ __forceinline__ vq_u64 vq_hash(vq_u64 x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+// Order-preserving map of doubles onto unsigned 64-bit keys (NaN excluded by callers).
+__device__ __forceinline__ vq_u64 vq_fkey(double d) {
+    vq_u64 b = (vq_u64)__double_as_longlong(d);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double vq_fkey_inv(vq_u64 k) {
+    vq_u64 b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    return __longlong_as_double((vq_i64)b);
+}
+
+// Exact float summation: x is added, as an integer multiple of 2^lsb, into
+// four signed 64-bit counters holding 32-bit digits (c[k] weighs 2^(32k+lsb)).
+// Integer addition is associative, so the sum is the same whatever order the
+// atomics land in. Bits of x below 2^lsb are truncated (the window is chosen
+// so that only values below 2^-64 of the largest possible |x| lose bits).
+// Non-finite values set flags instead. stride is the distance between digits.
+template <bool kAtomic>
+__device__ __forceinline__ void vq_fx_add(vq_i64* c, double x, int lsb, unsigned* special, int* err) {
+    vq_u64 b = (vq_u64)__double_as_longlong(x);
+    int e = (int)((b >> 52) & 0x7FF);
+    if (e == 0x7FF) {  // inf / nan
+        unsigned f = (b & 0xFFFFFFFFFFFFFull) ? 1u : ((b >> 63) ? 4u : 2u);
+        if (kAtomic) atomicOr(special, f); else *special |= f;
+        return;
+    }
+    vq_u64 m = b & 0xFFFFFFFFFFFFFull;
+    if (e == 0) { if (m == 0) return; e = 1; } else m |= 1ull << 52;
+    int sh = e - 1075 - lsb;  // position of m's bit 0 above the window's LSB
+    if (sh < 0) {
+        if (sh <= -53) return;
+        m >>= -sh;
+        sh = 0;
+        if (m == 0) return;
+    }
+    int d = sh >> 5, off = sh & 31;
+    vq_u64 lo = m << off;
+    unsigned hi = off ? (unsigned)(m >> (64 - off)) : 0u;
+    vq_i64 dg[3] = {(vq_i64)(lo & 0xFFFFFFFFull), (vq_i64)(lo >> 32), (vq_i64)hi};
+    bool neg = b >> 63;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (dg[k] == 0) continue;
+        int idx = d + k;
+        if (idx >= VQ_FX_DIGITS) { atomicOr(reinterpret_cast<unsigned*>(err), 2u); continue; }
+        vq_i64 v = neg ? -dg[k] : dg[k];
+        if (kAtomic) atomicAdd(reinterpret_cast<unsigned long long*>(c + idx), (unsigned long long)v);
+        else c[idx] += v;
+    }
+}
+
+__device__ __host__ inline int vq_clz64(vq_u64 x) {
+#ifdef __CUDA_ARCH__
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
+// mant · 2^e2 for a 53-bit mantissa (bit 52 set), built from the bits so no
+// math library is needed; results below the normal range flush through a
+// scaled multiply (sums that small do not occur in the workloads).
+__device__ __host__ inline double vq_make_double(vq_u64 mant, int e2) {
+    int eb = e2 + 52 + 1023;
+    if (eb >= 2047) return __longlong_as_double_portable(0x7FF0000000000000ll);
+    if (eb > 0) return __longlong_as_double_portable((vq_i64)(((vq_u64)eb << 52) | (mant & 0xFFFFFFFFFFFFFull)));
+    double m = (double)mant;
+    int e = e2;
+    while (e < -1000) { m *= 0x1p-1000; e += 1000; }
+    double scale = __longlong_as_double_portable((vq_i64)((vq_u64)(e + 1023) << 52));
+    return m * scale;
+}
+
+// Correctly rounded (nearest, ties to even) double of sum_k c[k]·2^(32k+lsb).
+__device__ __host__ inline double vq_fx_value(const vq_i64* c, int lsb) {
+    // exact 256-bit two's-complement accumulation of the four counters
+    vq_u64 w[4] = {0, 0, 0, 0};
+    for (int k = 0; k < VQ_FX_DIGITS; k++) {
+        // add c[k] << (32k) into w (sign-extended)
+        vq_i64 v = c[k];
+        int sh = 32 * k;
+        vq_u64 ext = v < 0 ? ~0ull : 0ull;
+        vq_u64 part[4];
+        int q = sh / 64, r = sh % 64;
+        for (int i = 0; i < 4; i++) part[i] = ext;
+        // (v as 256-bit sign-extended) << sh
+        vq_u64 src[4] = {(vq_u64)v, ext, ext, ext};
+        for (int i = 3; i >= 0; i--) {
+            int s = i - q;
+            vq_u64 x = 0;
+            if (s >= 0) {
+                x = src[s] << r;
+                if (r && s - 1 >= 0) x |= src[s - 1] >> (64 - r);
+            }
+            part[i] = x;
+        }
+        vq_u64 carry = 0;
+        for (int i = 0; i < 4; i++) {
+            vq_u64 t = w[i] + part[i];
+            vq_u64 c1 = t < w[i];
+            vq_u64 t2 = t + carry;
+            vq_u64 c2 = t2 < t;
+            w[i] = t2;
+            carry = c1 | c2;
+        }
+    }
+    bool neg = (w[3] >> 63) & 1;
+    if (neg) {  // magnitude = -w
+        vq_u64 carry = 1;
+        for (int i = 0; i < 4; i++) {
+            w[i] = ~w[i];
+            vq_u64 t = w[i] + carry;
+            carry = (t < w[i]) ? 1 : 0;
+            w[i] = t;
+        }
+    }
+    int top = -1;
+    for (int i = 3; i >= 0; i--)
+        if (w[i]) { top = i * 64 + 63 - vq_clz64(w[i]); break; }
+    if (top < 0) return 0.0;
+    // take 53 bits below and including `top`, then round with guard+sticky
+    int lo_bit = top - 52;
+    auto bitat = [&](int pos) -> vq_u64 { return (pos < 0) ? 0 : ((w[pos >> 6] >> (pos & 63)) & 1); };
+    vq_u64 mant = 0;
+    for (int i = 0; i < 53; i++) mant |= bitat(lo_bit + i) << i;
+    int exp2 = lo_bit + lsb;
+    if (lo_bit > 0) {
+        vq_u64 guard = bitat(lo_bit - 1);
+        bool sticky = false;
+        for (int pos = 0; pos < lo_bit - 1; pos++) if (bitat(pos)) { sticky = true; break; }
+        if (guard && (sticky || (mant & 1))) {
+            mant++;
+            if (mant >> 53) { mant >>= 1; exp2++; }
+        }
+    }
+    double r = vq_make_double(mant, exp2);
+    return neg ? -r : r;
+}
+
+#define VQ_NOSLOT 0xFFFFFFFFFFFFFFFFull
+
+// Open-addressing insert (linear probing, atomicCAS on the key). The key equal
+// to the empty sentinel lives in the extra slot `cap`, whose key word is a
+// used-flag. Returns VQ_NOSLOT and raises err bit 0 when the probe limit is
+// reached, so a full table ends the kernel's work instead of spinning.
+__device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key,
+                                            vq_u64* nkeys, int* err) {
+    if (key == VQ_EMPTY_KEY) {
+        if (atomicCAS(keys + cap, 0ull, 1ull) == 0ull) atomicAdd(nkeys, 1ull);
+        return cap;
+    }
+    vq_u64 i = vq_hash(key) & mask;
+    const vq_u64 limit = mask < (vq_u64)VQ_MAX_PROBES ? mask + 1 : (vq_u64)VQ_MAX_PROBES;
+    for (vq_u64 n = 0; n < limit; n++) {
+        vq_u64 k = *reinterpret_cast<volatile vq_u64*>(keys + i);
+        if (k == key) return i;
+        if (k == VQ_EMPTY_KEY) {
+            vq_u64 old = atomicCAS(keys + i, VQ_EMPTY_KEY, key);
+            if (old == VQ_EMPTY_KEY) { atomicAdd(nkeys, 1ull); return i; }
+            if (old == key) return i;
+        }
+        i = (i + 1) & mask;
+    }
+    atomicOr(err, 1);
+    return VQ_NOSLOT;
+}
+
+// Read-only lookup in a table no kernel is writing any more.
+__device__ __forceinline__ vq_u64 vq_find(const vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key) {
+    if (key == VQ_EMPTY_KEY) return __ldg(keys + cap) ? cap : VQ_NOSLOT;
+    vq_u64 i = vq_hash(key) & mask;
+    for (vq_u64 n = 0; n <= mask; n++) {
+        vq_u64 k = __ldg(keys + i);
+        if (k == key) return i;
+        if (k == VQ_EMPTY_KEY) return VQ_NOSLOT;
+        i = (i + 1) & mask;
+    }
+    return VQ_NOSLOT;
+}
+
+// Combiners of partial accumulators (kind 0 sum, 1 min, 2 max), following
+// mergePartialAgg (exec/parallel.go:262-297): a float MIN/MAX partial only
+// replaces the running value when strictly smaller/larger.
+__device__ __forceinline__ double vq_fminr(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double vq_fmaxr(double a, double b) { return b > a ? b : a; }
+__device__ __forceinline__ double vq_fcomb(int kind, double a, double b) {
+    return kind == 1 ? vq_fminr(a, b) : kind == 2 ? vq_fmaxr(a, b) : a + b;
+}
+__device__ __forceinline__ vq_i64 vq_icomb(int kind, vq_i64 a, vq_i64 b) {
+    return kind == 1 ? (b < a ? b : a) : kind == 2 ? (b > a ? b : a) : (vq_i64)((vq_u64)a + (vq_u64)b);
+}

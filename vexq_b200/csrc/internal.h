@@ -1,0 +1,124 @@
+// internal.h — shared declarations of libvexqcuda (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/vexq_cuda.h"
+#include "kparams.h"
+
+namespace vq {
+
+// ---- errors ---------------------------------------------------------------------
+struct Status : std::runtime_error {
+    int32_t code;
+    Status(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void fail(int32_t code, const std::string& msg);
+void set_error(const std::string& msg);
+#define VQ_CUDA(x)                                                                      \
+    do {                                                                                \
+        cudaError_t _e = (x);                                                           \
+        if (_e != cudaSuccess)                                                          \
+            ::vq::fail(_e == cudaErrorMemoryAllocation ? VEXQ_ENOMEM : VEXQ_EDEVICE,    \
+                       std::string(#x) + ": " + cudaGetErrorString(_e));                \
+    } while (0)
+
+// ---- device memory ------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t bytes) { alloc(bytes); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t bytes);
+    void ensure(size_t bytes) { if (bytes > n) { release(); alloc(bytes); } }
+    void release();
+    template <class T> T* as() const { return (T*)p; }
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf();
+    void ensure(size_t bytes);
+};
+
+// ---- tables ----------------------------------------------------------------------------
+struct GlobalDict {
+    std::vector<std::string> keys;
+    std::unordered_map<std::string, uint32_t> index;
+    uint32_t add(const std::string& s);
+    int64_t find(const std::string& s) const {
+        auto it = index.find(s);
+        return it == index.end() ? -1 : (int64_t)it->second;
+    }
+};
+
+struct Column {
+    std::string name;
+    int32_t type = 0;
+    bool nullable = false;
+    DevBuf values;      // padded to a multiple of kPadRows rows
+    DevBuf validity;    // LSB-first bitmap (nullable columns only)
+    // STRING
+    GlobalDict dict;
+    std::vector<std::vector<uint32_t>> rg_remap;   // per RG: local → global code
+    std::vector<std::vector<uint8_t>> rg_present;  // per RG: global code present in the RG's dictionary
+    bool per_rg_dicts = true;
+    std::vector<vexq_zone_map> zones;              // per RG
+    // table-wide min/max (numeric), for accumulator windows
+    bool has_range = false;
+    double fmin = 0, fmax = 0;      // FLOAT64
+    int64_t imin = 0, imax = 0;     // INT64 / DATE
+};
+
+struct Table {
+    std::vector<Column> cols;
+    int64_t nrows = 0;
+    int32_t rg_rows = 65536;
+    int32_t n_rg = 0;
+    int device = 0;
+    int64_t rg_start(int rg) const { return (int64_t)rg * rg_rows; }
+    int64_t rg_end(int rg) const { return std::min<int64_t>(nrows, (int64_t)(rg + 1) * rg_rows); }
+    int64_t device_bytes() const;
+};
+
+constexpr int64_t kPadRows = 4096;  // device columns are padded so 128-bit tail loads stay in bounds
+
+// ---- JIT ----------------------------------------------------------------------------------
+struct JitModule;  // opaque: driver module + functions
+struct JitKernel {
+    std::shared_ptr<JitModule> mod;
+    void* fn = nullptr;  // CUfunction
+    int block = 256;
+    int max_blocks_per_sm = 0;
+};
+JitKernel jit_get(const std::string& source, const std::string& entry, int block);
+void jit_launch(const JitKernel& k, int grid, const void* params, size_t params_size, cudaStream_t s);
+std::string jit_cache_dir();
+
+// ---- misc ----------------------------------------------------------------------------------
+int sm_count();
+const char* prelude_source();  // device helpers prepended to every generated kernel
+
+}  // namespace vq

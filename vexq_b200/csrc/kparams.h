@@ -1,0 +1,53 @@
+// kparams.h — the parameter block of every generated scan kernel. Shared
+// verbatim by the host (nvcc/g++) and by the runtime-compiled kernels
+// (NVRTC), so it uses only fixed-width scalar fields and raw pointers.
+#pragma once
+
+#define VQ_MAXCOLS 32
+#define VQ_MAXSETS 16
+#define VQ_FX_DIGITS 4  // 32-bit digits of the exact fixed-point float sums
+
+struct VQParams {
+    // ---- scanned table (aggregate: the table; join: probe or build side) ----
+    const void* col[VQ_MAXCOLS];
+    const unsigned char* valid[VQ_MAXCOLS];
+    // ---- build-side columns read through build row ids (join probe) ----
+    const void* bcol[VQ_MAXCOLS];
+    const unsigned char* bvalid[VQ_MAXCOLS];
+    // ---- code sets for IN / LIKE over large dictionaries ----
+    const unsigned* sets[VQ_MAXSETS];
+    // ---- row ranges: seg[3*i+0..2] = start row, end row, first chunk ----
+    const long long* seg;
+    // ---- StringEqExpr per-row-group dictionary presence, [npresent][n_rg] ----
+    const unsigned char* present;
+    // ---- register path: per-block partials ----
+    double* part_f;            // [grid][G][NF]
+    long long* part_i;         // [grid][G][NI]
+    long long* part_first;     // [grid][G]
+    // ---- atomic path: group table ----
+    unsigned long long* keys;  // [cap + 1]; slot cap holds the sentinel key
+    long long* first;          // [cap + 1] first-occurrence order key
+    long long* acc_i;          // [NI][cap + 1]
+    long long* acc_fx;         // [NF][cap + 1][4]
+    unsigned* special;         // [NF][cap + 1]: bit0 NaN, bit1 +inf, bit2 -inf
+    unsigned long long* ngroups;  // occupied slots
+    int* error;                // [0] overflow / probe-limit flag
+    // ---- join build table ----
+    unsigned long long* jkeys; // [jcap + 1]
+    int* jcount;               // [jcap + 1]
+    int* jstart;               // [jcap + 1]
+    int* jfill;                // [jcap + 1]
+    int* jrows;                // build row ids, grouped by slot in row order
+    unsigned long long* jnkeys;
+    // ---- 8-byte scalars ----
+    long long nchunks;
+    long long rg_rows;
+    unsigned long long cap_mask;   // atomic path: capacity - 1 (hash) or unused (dense)
+    unsigned long long cap;        // slots (hash: power of two; dense: domain)
+    unsigned long long jmask;      // join table capacity - 1
+    // ---- 4-byte scalars ----
+    int nseg;
+    int n_rg;
+    int mode;                  // join build: 0 = insert/count, 1 = fill
+    int fx_lsb[16];            // per float-sum slot: exponent of the window's LSB
+};

@@ -1,0 +1,153 @@
+// plan.h — compiled plans: typed expression IR, accumulator slots, and the
+// generated scan kernels.
+#pragma once
+
+#include "internal.h"
+
+namespace vq {
+
+enum class NK {
+    Col, Lit, Cmp, Arith, Cast, And, Or, Not, IsNull, IsNotNull,
+    InInt, InFloat, InCodes, InFalse, StrEq, Case
+};
+
+struct INode {
+    NK k = NK::Lit;
+    int type = 0;          // VEXQ_TYPE_*
+    int op = 0;
+    int col = -1;          // Col / StrEq / InCodes: column (in its side's table)
+    bool build = false;    // column read through the build row (join above-scope)
+    int64_t li = 0;
+    double lf = 0;
+    int32_t ld = 0;
+    bool lb = false;
+    std::vector<int> ch;
+    std::vector<int64_t> seti;
+    std::vector<double> setf;
+    std::vector<uint8_t> codes;   // InCodes: membership per global code
+    int set_idx = -1;             // InCodes with a large dictionary: device set index
+    int64_t streq_code = -1;      // StrEq: global code of the literal (-1 absent)
+    bool negate = false;
+    int present_idx = -1;         // StrEq: row of the presence table (-1: constant)
+    bool has_else = false;
+    bool nullable = false;
+    // |value| bound from zone maps by interval arithmetic (exact-sum windows)
+    bool bounded = false;
+    double lo = 0, hi = 0;
+    bool is_literal_raw = false;  // literal before coercion (SQL level)
+    int lit_kind = 0;
+};
+
+// Accumulator slot kinds.
+enum SlotKind { S_CNT = 0, S_NN, S_ISUM, S_IMIN, S_IMAX, S_FSUM, S_FMIN, S_FMAX };
+
+struct Slot {
+    SlotKind kind;
+    int input = -1;  // IR node (value), -1 for CNT
+    bool is_float() const { return kind == S_FSUM || kind == S_FMIN || kind == S_FMAX; }
+};
+
+struct AggOut {
+    int kind;         // VEXQ_AGG_*
+    int value_slot;   // slot index (-1 for COUNT(*))
+    int nn_slot;      // slot giving the non-null count (CNT when the input is never NULL)
+    int out_type;     // result vector type
+    std::string name;
+};
+
+struct KeyCol {
+    int col;          // column index in its side's table
+    bool build;       // join: build-side column
+    int type;
+    bool nullable;
+    // dense encoding: code in [0, domain): dict code / (value - vmin); NULL → domain-1
+    int64_t vmin = 0;
+    int64_t domain = 0;
+    int bits = 0;     // packed-key width
+    int shift = 0;
+};
+
+enum class AggPath { Regs, Dense, Hash };
+
+struct ScanSegs {
+    std::vector<long long> seg;  // start, end, chunk0 triples
+    long long nchunks = 0;
+    long long rows = 0;
+};
+
+struct Plan {
+    bool is_join = false;
+    Table* t = nullptr;        // aggregate table or probe table
+    Table* bt = nullptr;       // build table
+    std::vector<INode> ir;
+    int pred = -1;             // scan predicate (probe predicate for joins)
+    int bpred = -1;            // join build predicate
+    int resid = -1;            // join residual
+    int build_key = -1, probe_key = -1;
+    // SQL-level predicate trees kept for zone maps
+    std::vector<vexq_expr> zn_nodes;
+    std::vector<int32_t> zn_children;
+    int zn_pred = -1, zn_bpred = -1;
+    std::vector<KeyCol> keys;
+    bool intkey_order = false;     // reference int-key path ordering rules apply
+    int intkey_width = 32;
+    std::vector<Slot> slots;
+    std::vector<AggOut> outs;
+    std::vector<int> gb_types;
+    vexq_order_desc order{-1, 0, -1};
+    AggPath path = AggPath::Hash;
+    int64_t domain = 1;            // dense key domain
+    int nf = 0, ni = 0;            // float / int slots (path-specific layout)
+    std::vector<int> slot_pos;     // slot → index within its float/int bank
+    std::vector<int> fx_lsb;       // per float-sum slot
+    std::vector<std::vector<uint32_t>> sets;  // large InCodes sets (bitsets)
+    std::vector<std::pair<int, int64_t>> presence;   // (column, code) rows: scanned / probe table
+    std::vector<std::pair<int, int64_t>> bpresence;  // rows for the join build table
+    DevBuf d_sets, d_present, d_bpresent;
+    // generated kernels
+    std::string src_main, src_build;
+    JitKernel k_main, k_build;
+    std::string explain;
+    int radix_bits = 0;
+    std::atomic<bool> cancel{false};
+    cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
+    cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
+    // scratch reused across runs
+    DevBuf scratch_a, scratch_b, scratch_c, scratch_d, scratch_e, scratch_f, scratch_g;
+    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar;
+    ~Plan();
+};
+
+// Host result columns (group-insertion order, after ORDER BY / LIMIT).
+struct OutColumn {
+    std::string name;
+    int type;
+    std::vector<int64_t> v;      // raw bits (int64 / float64 / date / bool / string code)
+    std::vector<uint8_t> valid;
+    const GlobalDict* dict = nullptr;
+};
+
+Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d);
+Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d);
+Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred);
+bool zone_eval(const Plan& p, int root, const Table& t, int rg);
+ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end);
+bool parse_date(const char* s, int64_t* days);
+
+}  // namespace vq
+
+struct vexq_result_s {
+    std::vector<vq::OutColumn> cols;
+    int64_t nrows = 0;
+    int64_t pos = 0;
+    double kernel_ms = 0;
+    double scan_ms = 0;
+    int32_t launches = 0;
+    int64_t rows_scanned = 0, bytes_scanned = 0;
+    // current batch views and their storage
+    std::vector<vexq_vector_view> views;
+    std::vector<std::vector<char>> vbuf;
+    std::vector<std::vector<uint8_t>> bbuf;
+    std::vector<std::vector<uint32_t>> doff;
+    std::vector<std::string> dbytes;
+};

@@ -1,0 +1,987 @@
+// run.cu — plan execution: zone pruning → generated scan kernel → merge /
+// finalize → group ordering → ORDER BY / LIMIT → host result batches.
+//
+// Reference behaviour reproduced here: group output in insertion order
+// (exec/aggregate.go:209-216), SUM/MIN/MAX NULL when no non-NULL input, AVG =
+// sum / float64(non-null count), COUNT never NULL (aggregate.go:780-876), a
+// global aggregate over no rows emits one row (aggregate.go:961-982), and
+// ExternalSort's comparison on raw int64 bits with NULLs first
+// (exec/sort.go:130-163) followed by Limit (exec/limit.go:20-50).
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <functional>
+#include <numeric>
+#include <set>
+
+#include "plan.h"
+#include "device_common.cuh"
+
+namespace vq {
+
+void refill_table(Table& t, const vexq_column_desc* cols, int32_t ncols, cudaStream_t s);
+
+// ---- static kernels ----------------------------------------------------------------
+
+__global__ void k_fill_u64(unsigned long long* p, long long n, unsigned long long v) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+// Register path: merges per-block partials in block order. Float sums use a
+// compensated (TwoSum) accumulator so the merge adds no rounding of its own.
+__global__ void k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
+                             const int* fkind, const int* ikind, double* out_f, long long* out_i) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int totf = G * nf, toti = G * (ni + 1);
+    if (t < totf) {
+        int s = t % nf;
+        int kind = fkind[s];
+        double hi = part_f[t], lo = 0.0;
+        for (int b = 1; b < nblocks; b++) {
+            double x = part_f[(long long)b * totf + t];
+            if (kind == 0) {
+                double sum = hi + x;
+                double bb = sum - hi;
+                lo += (hi - (sum - bb)) + (x - bb);
+                hi = sum;
+            } else {
+                hi = vq_fcomb(kind, hi, x);
+            }
+        }
+        out_f[t] = kind == 0 ? hi + lo : hi;
+    } else if (t < totf + toti) {
+        int u = t - totf;
+        int s = u % (ni + 1);
+        int kind = ikind[s];
+        long long v = part_i[u];
+        for (int b = 1; b < nblocks; b++) v = vq_icomb(kind, v, part_i[(long long)b * toti + u]);
+        out_i[u] = v;
+    }
+}
+
+// Atomic path: per-slot initial values (counts 0, MIN/MAX identities).
+__global__ void k_init_table(unsigned long long* keys, long long* first, long long* acc_i, int ni, const long long* init_i,
+                             long long nslots, int hash) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
+        if (hash) keys[i] = (i == nslots - 1) ? 0ull : VQ_EMPTY_KEY;
+        first[i] = 0x7FFFFFFFFFFFFFFFLL;
+        for (int s = 0; s < ni; s++) acc_i[(long long)s * nslots + i] = init_i[s];
+    }
+}
+
+// Compacts occupied slots (count > 0) and turns exact fixed-point sums into
+// correctly rounded doubles (NaN / ±inf flags applied IEEE-style).
+__global__ void k_finalize(const unsigned long long* keys, const long long* first, const long long* acc_i,
+                           const long long* acc_fx, const unsigned* special, long long nslots, int ni, int nf,
+                           const int* fx_lsb, int hash, unsigned long long* n_out, unsigned long long* o_key,
+                           long long* o_first, long long* o_i, double* o_f, long long cap_out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
+        if (acc_i[i] == 0) continue;  // slot 0 of the int bank is the row count
+        unsigned long long pos = atomicAdd(n_out, 1ull);
+        if ((long long)pos >= cap_out) continue;
+        o_key[pos] = hash ? (i == nslots - 1 ? VQ_EMPTY_KEY : keys[i]) : (unsigned long long)i;
+        o_first[pos] = first[i];
+        for (int s = 0; s < ni; s++) o_i[(long long)s * cap_out + pos] = acc_i[(long long)s * nslots + i];
+        for (int f = 0; f < nf; f++) {
+            unsigned sp = special[(long long)f * nslots + i];
+            double v;
+            if ((sp & 1u) || (sp & 6u) == 6u) v = __longlong_as_double(0x7FF8000000000001LL);
+            else if (sp & 2u) v = __longlong_as_double(0x7FF0000000000000LL);
+            else if (sp & 4u) v = __longlong_as_double((long long)0xFFF0000000000000ULL);
+            else v = vq_fx_value(acc_fx + ((long long)f * nslots + i) * 4, fx_lsb[f]);
+            o_f[(long long)f * cap_out + pos] = v;
+        }
+    }
+}
+
+// ---- exclusive scan (join build: slot counts → chain starts) ------------------------
+__global__ void k_scan_blocks(const int* in, int* out, long long n, int* block_sums) {
+    __shared__ int s[1024];
+    long long base = (long long)blockIdx.x * 4096;
+    int t = threadIdx.x;
+    int v[4], sum = 0;
+    for (int k = 0; k < 4; k++) {
+        long long i = base + t * 4 + k;
+        v[k] = i < n ? in[i] : 0;
+        sum += v[k];
+    }
+    s[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int x = t >= o ? s[t - o] : 0;
+        __syncthreads();
+        s[t] += x;
+        __syncthreads();
+    }
+    int run = s[t] - sum;
+    for (int k = 0; k < 4; k++) {
+        long long i = base + t * 4 + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (t == 1023) block_sums[blockIdx.x] = s[1023];
+}
+__global__ void k_scan_sums(int* sums, int nb) {  // one block, sequential chunks
+    __shared__ int s[1024];
+    int carry = 0;
+    for (int base = 0; base < nb; base += 1024) {
+        int t = threadIdx.x;
+        int v = base + t < nb ? sums[base + t] : 0;
+        s[t] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int x = t >= o ? s[t - o] : 0;
+            __syncthreads();
+            s[t] += x;
+            __syncthreads();
+        }
+        if (base + t < nb) sums[base + t] = carry + s[t] - v;
+        int tot = s[1023];
+        __syncthreads();
+        carry += tot;
+    }
+}
+__global__ void k_scan_add(int* out, long long n, const int* sums) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += sums[i / 4096];
+}
+
+// Restores build-row order inside each key's chain (joinHashTable.insert keeps
+// insertion order, exec/join_table.go:496-517): one thread per slot.
+__global__ void k_sort_chains(const int* start, const int* count, int* rows, long long nslots, int* unsorted) {
+    for (long long sl = (long long)blockIdx.x * blockDim.x + threadIdx.x; sl < nslots; sl += (long long)gridDim.x * blockDim.x) {
+        int c = count[sl];
+        if (c < 2) continue;
+        if (c > 4096) { atomicOr(unsorted, 4); continue; }  // chain left in fill order
+        int* r = rows + start[sl];
+        for (int i = 1; i < c; i++) {
+            int x = r[i], j = i - 1;
+            while (j >= 0 && r[j] > x) { r[j + 1] = r[j]; j--; }
+            r[j + 1] = x;
+        }
+    }
+}
+
+// Top-k support: order-preserving "better is larger" transform of a sort key.
+__device__ __forceinline__ unsigned long long vq_rank(long long bits, bool isnull, int desc) {
+    if (isnull) return 0xFFFFFFFFFFFFFFFFull;  // NULLs sort first (exec/sort.go:141-146)
+    unsigned long long u = (unsigned long long)bits ^ 0x8000000000000000ull;  // signed order
+    u = desc ? u : ~u;
+    return u == 0xFFFFFFFFFFFFFFFFull ? u - 1 : u;
+}
+__global__ void k_hist(const long long* keyv, const unsigned char* keynull, long long n, int desc, unsigned* hist) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        atomicAdd(hist + (vq_rank(keyv[i], keynull[i], desc) >> 48), 1u);
+}
+__global__ void k_select(const long long* keyv, const unsigned char* keynull, long long n, int desc, unsigned thr_bin,
+                         unsigned long long* nsel, long long* sel, long long cap) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if ((vq_rank(keyv[i], keynull[i], desc) >> 48) >= thr_bin) {
+            unsigned long long p = atomicAdd(nsel, 1ull);
+            if ((long long)p < cap) sel[p] = i;
+        }
+    }
+}
+// Sort key of one aggregate output per compacted group (bits + NULL flag).
+__global__ void k_sortkey(const long long* o_i, const double* o_f, long long cap_out, long long n, int kind, int vbank,
+                          int vpos, int nnpos, long long* keyv, unsigned char* keynull, int fmin_key) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long nn = o_i[(long long)nnpos * cap_out + i];
+        bool isnull = kind != VEXQ_AGG_COUNT && nn == 0;
+        long long bits;
+        if (vbank == 1) {  // float sum bank
+            double v = o_f[(long long)vpos * cap_out + i];
+            if (kind == VEXQ_AGG_AVG) v = v / (double)nn;
+            bits = __double_as_longlong(v);
+        } else {
+            bits = o_i[(long long)vpos * cap_out + i];
+            if (fmin_key) bits = __double_as_longlong(vq_fkey_inv((unsigned long long)bits));
+        }
+        keyv[i] = bits;
+        keynull[i] = isnull;
+    }
+}
+
+// Gathers the selected compacted groups into a dense staging block.
+__global__ void k_gather(const long long* sel, long long n, const unsigned long long* key, const long long* first,
+                         const long long* ival, const double* fval, long long cap_out, int ni, int nf, long long* out) {
+    long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    long long i = sel[j];
+    long long w = 2 + ni + nf;
+    long long* o = out + j * w;
+    o[0] = (long long)key[i];
+    o[1] = first[i];
+    for (int s = 0; s < ni; s++) o[2 + s] = ival[(long long)s * cap_out + i];
+    for (int f = 0; f < nf; f++) o[2 + ni + f] = __double_as_longlong(fval[(long long)f * cap_out + i]);
+}
+
+}  // namespace vq
+
+namespace vq {
+
+double vq_fkey_inv_host(uint64_t k) {
+    uint64_t b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    double d;
+    std::memcpy(&d, &b, 8);
+    return d;
+}
+
+namespace {
+
+int grid_for(const JitKernel& k, long long nchunks) {
+    int per_sm = std::max(1, k.max_blocks_per_sm);
+    long long want = (nchunks + (k.block / 32) - 1) / (k.block / 32);
+    long long g = std::min<long long>((long long)sm_count() * per_sm, want);
+    return (int)std::max<long long>(g, 1);
+}
+
+void set_columns(VQParams& P, const Table& t, bool build_side) {
+    for (size_t c = 0; c < t.cols.size(); c++) {
+        const Column& col = t.cols[c];
+        if (build_side) {
+            P.bcol[c] = col.values.p;
+            P.bvalid[c] = col.nullable ? col.validity.as<unsigned char>() : nullptr;
+        } else {
+            P.col[c] = col.values.p;
+            P.valid[c] = col.nullable ? col.validity.as<unsigned char>() : nullptr;
+        }
+    }
+}
+
+struct Timer {
+    cudaEvent_t a, b;
+    cudaStream_t s;
+    explicit Timer(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    float stop() {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+    ~Timer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+// Host-side group rows collected from either path.
+struct Groups {
+    std::vector<uint64_t> key;
+    std::vector<int64_t> first;
+    std::vector<std::vector<int64_t>> ival;   // per int-bank slot
+    std::vector<std::vector<double>> fval;    // per float-bank slot
+    size_t n() const { return key.size(); }
+};
+
+int64_t slot_int(const Plan& p, const Groups& g, int slot, size_t i) { return g.ival[p.slot_pos[slot]][i]; }
+
+double slot_float(const Plan& p, const Groups& g, int slot, size_t i) {
+    if (p.path == AggPath::Regs || p.slots[slot].kind == S_FSUM) return g.fval[p.slot_pos[slot]][i];
+    return vq_fkey_inv_host((uint64_t)g.ival[p.slot_pos[slot]][i]);
+}
+
+std::vector<long long> init_values(const Plan& p) {
+    std::vector<long long> iv(std::max(p.ni, 1), 0);
+    auto fkey = [](double d) {
+        uint64_t b;
+        std::memcpy(&b, &d, 8);
+        return (long long)((b >> 63) ? ~b : (b | 0x8000000000000000ull));
+    };
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        if (p.slots[s].kind == S_FSUM) continue;
+        long long v = 0;
+        switch (p.slots[s].kind) {
+            case S_IMIN: v = 0x7FFFFFFFFFFFFFFFLL; break;
+            case S_IMAX: v = -0x7FFFFFFFFFFFFFFFLL - 1; break;
+            case S_FMIN: v = fkey(1.7976931348623157e308); break;
+            case S_FMAX: v = fkey(-1.7976931348623157e308); break;
+            default: break;
+        }
+        iv[p.slot_pos[s]] = v;
+    }
+    return iv;
+}
+
+struct RunCtx {
+    Plan& p;
+    cudaStream_t s;
+    float kernel_ms = 0;
+    float scan_ms = 0;
+    int launches = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
+};
+
+// Times one scan-kernel launch with events on the run's stream; the elapsed
+// time is read once the run has synchronised (collect_scan_ms).
+void launch_scan(RunCtx& rc, const JitKernel& k, int grid, VQParams& P) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, rc.s);
+    jit_launch(k, grid, &P, sizeof P, rc.s);
+    cudaEventRecord(b, rc.s);
+    rc.scan_events.push_back({a, b});
+}
+
+void collect_scan_ms(RunCtx& rc) {
+    for (auto& e : rc.scan_events) {
+        cudaEventSynchronize(e.second);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e.first, e.second);
+        rc.scan_ms += ms;
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    rc.scan_events.clear();
+}
+
+// Register path over prepared params: launch, merge, copy back.
+Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
+    Plan& p = rc.p;
+    Groups g;
+    int G = (int)p.domain, nf = p.nf, ni = p.ni;
+    int grid = grid_for(p.k_main, nchunks);
+    size_t pf = (size_t)grid * G * std::max(nf, 1), pi = (size_t)grid * G * (ni + 1);
+    p.scratch_a.ensure(pf * 8);
+    p.scratch_b.ensure(pi * 8);
+    P.part_f = p.scratch_a.as<double>();
+    P.part_i = p.scratch_b.as<long long>();
+    std::vector<int> fk(std::max(nf, 1), 0), ik(ni + 1, 0);
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        int k = p.slots[s].kind;
+        int code = (k == S_IMIN || k == S_FMIN) ? 1 : (k == S_IMAX || k == S_FMAX) ? 2 : 0;
+        if (p.slots[s].is_float()) fk[p.slot_pos[s]] = code;
+        else ik[p.slot_pos[s]] = code;
+    }
+    ik[ni] = 1;
+    size_t nout = (size_t)G * std::max(nf, 1) * 8 + (size_t)G * (ni + 1) * 8;
+    p.scratch_c.ensure(nout + (fk.size() + ik.size()) * 4);
+    double* out_f = p.scratch_c.as<double>();
+    long long* out_i = (long long*)((char*)p.scratch_c.p + (size_t)G * std::max(nf, 1) * 8);
+    int* d_kinds = (int*)((char*)p.scratch_c.p + nout);
+    VQ_CUDA(cudaMemcpyAsync(d_kinds, fk.data(), fk.size() * 4, cudaMemcpyHostToDevice, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(d_kinds + fk.size(), ik.data(), ik.size() * 4, cudaMemcpyHostToDevice, rc.s));
+    {
+        Timer tm(rc.s);
+        launch_scan(rc, p.k_main, grid, P);
+        int tot = G * nf + G * (ni + 1);
+        k_merge_regs<<<(tot + 127) / 128, 128, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + fk.size(),
+                                                         out_f, out_i);
+        VQ_CUDA(cudaGetLastError());
+        rc.kernel_ms += tm.stop();
+        rc.launches += 2;
+    }
+    std::vector<double> hf((size_t)G * std::max(nf, 1));
+    std::vector<long long> hi((size_t)G * (ni + 1));
+    if (nf) VQ_CUDA(cudaMemcpyAsync(hf.data(), out_f, (size_t)G * nf * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(hi.data(), out_i, hi.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    g.ival.assign(ni, {});
+    g.fval.assign(nf, {});
+    for (int gi = 0; gi < G; gi++) {
+        long long cnt = hi[(size_t)gi * (ni + 1) + p.slot_pos[0]];
+        if (cnt == 0) continue;
+        g.key.push_back((uint64_t)gi);
+        g.first.push_back(hi[(size_t)gi * (ni + 1) + ni]);
+        for (int s = 0; s < ni; s++) g.ival[s].push_back(hi[(size_t)gi * (ni + 1) + s]);
+        for (int s = 0; s < nf; s++) g.fval[s].push_back(hf[(size_t)gi * nf + s]);
+    }
+    return g;
+}
+
+// Atomic path: group table, main kernel (retried with a larger table when a
+// probe limit is hit), finalize + compaction on the device.
+struct Compacted {
+    long long n = 0;
+    long long cap_out = 0;
+    unsigned long long* key = nullptr;
+    long long* first = nullptr;
+    long long* ival = nullptr;
+    double* fval = nullptr;
+};
+
+Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate) {
+    Plan& p = rc.p;
+    bool hash = p.path == AggPath::Hash;
+    long long cap;
+    if (hash) {
+        cap = 16;
+        while (cap < 2 * std::max<long long>(estimate, 8)) cap <<= 1;
+    } else {
+        cap = p.domain;
+    }
+    std::vector<long long> iv = init_values(p);
+    for (int attempt = 0; attempt < 8; attempt++) {
+        long long nslots = cap + 1;
+        int ni = p.ni, nf = p.nf;
+        size_t b_keys = hash ? nslots * 8 : 0, b_first = nslots * 8, b_i = (size_t)ni * nslots * 8,
+               b_fx = (size_t)nf * nslots * 32, b_sp = (size_t)nf * nslots * 4;
+        size_t tot = b_keys + b_first + b_i + b_fx + b_sp + 64 + iv.size() * 8 + 64;
+        p.scratch_a.ensure(tot);
+        char* base = (char*)p.scratch_a.p;
+        P.keys = hash ? (unsigned long long*)base : nullptr;
+        P.first = (long long*)(base + b_keys);
+        P.acc_i = (long long*)(base + b_keys + b_first);
+        P.acc_fx = (long long*)(base + b_keys + b_first + b_i);
+        P.special = (unsigned*)(base + b_keys + b_first + b_i + b_fx);
+        char* tail = base + b_keys + b_first + b_i + b_fx + b_sp;
+        tail = (char*)(((uintptr_t)tail + 15) & ~(uintptr_t)15);
+        P.ngroups = (unsigned long long*)tail;
+        P.error = (int*)(tail + 8);
+        long long* d_init = (long long*)(tail + 16);
+        P.cap = (unsigned long long)cap;
+        P.cap_mask = hash ? (unsigned long long)(cap - 1) : 0;
+        for (int f = 0; f < nf && f < 16; f++) P.fx_lsb[f] = p.fx_lsb[f];
+        Timer tm(rc.s);
+        VQ_CUDA(cudaMemcpyAsync(d_init, iv.data(), iv.size() * 8, cudaMemcpyHostToDevice, rc.s));
+        VQ_CUDA(cudaMemsetAsync(P.ngroups, 0, 16, rc.s));
+        if (b_fx) VQ_CUDA(cudaMemsetAsync(P.acc_fx, 0, b_fx + b_sp, rc.s));
+        int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
+        k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
+        VQ_CUDA(cudaGetLastError());
+        int grid = grid_for(p.k_main, nchunks);
+        launch_scan(rc, p.k_main, grid, P);
+        int herr = 0;
+        VQ_CUDA(cudaMemcpyAsync(&herr, P.error, 4, cudaMemcpyDeviceToHost, rc.s));
+        rc.kernel_ms += tm.stop();
+        rc.launches += 2;
+        if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
+        if (herr & 1) {  // probe limit: grow the table and rerun
+            if (!hash) fail(VEXQ_EDEVICE, "dense group table reported a probe failure");
+            cap <<= 1;
+            continue;
+        }
+        // finalize + compact
+        unsigned long long ng = 0;
+        VQ_CUDA(cudaMemcpyAsync(&ng, P.ngroups, 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaStreamSynchronize(rc.s));
+        long long cap_out = hash ? (long long)ng + 1 : std::min<long long>(nslots, cap);
+        if (!hash) cap_out = nslots;
+        cap_out = std::max<long long>(cap_out, 1);
+        size_t o_bytes = 8 + cap_out * 8 + cap_out * 8 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8 + nf * 4 + 64;
+        p.scratch_b.ensure(o_bytes);
+        char* ob = (char*)p.scratch_b.p;
+        Compacted c;
+        c.cap_out = cap_out;
+        unsigned long long* n_out = (unsigned long long*)ob;
+        c.key = (unsigned long long*)(ob + 8);
+        c.first = (long long*)(ob + 8 + cap_out * 8);
+        c.ival = (long long*)(ob + 8 + cap_out * 16);
+        c.fval = (double*)(ob + 8 + cap_out * 16 + (size_t)ni * cap_out * 8);
+        int* d_lsb = (int*)(ob + 8 + cap_out * 16 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8);
+        Timer tm2(rc.s);
+        VQ_CUDA(cudaMemsetAsync(n_out, 0, 8, rc.s));
+        if (nf) VQ_CUDA(cudaMemcpyAsync(d_lsb, p.fx_lsb.data(), nf * 4, cudaMemcpyHostToDevice, rc.s));
+        int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
+        k_finalize<<<fg, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, P.acc_fx, P.special, nslots, ni, nf, d_lsb, hash, n_out,
+                                         c.key, c.first, c.ival, c.fval, cap_out);
+        VQ_CUDA(cudaGetLastError());
+        unsigned long long nn = 0;
+        VQ_CUDA(cudaMemcpyAsync(&nn, n_out, 8, cudaMemcpyDeviceToHost, rc.s));
+        rc.kernel_ms += tm2.stop();
+        rc.launches += 1;
+        c.n = (long long)std::min<unsigned long long>(nn, (unsigned long long)cap_out);
+        return c;
+    }
+    fail(VEXQ_ENOMEM, "group table could not be sized");
+}
+
+Groups fetch_groups(RunCtx& rc, const Compacted& c, const std::vector<long long>* subset) {
+    Plan& p = rc.p;
+    Groups g;
+    long long n = subset ? (long long)subset->size() : c.n;
+    g.key.resize(n);
+    g.first.resize(n);
+    g.ival.assign(p.ni, std::vector<int64_t>(n));
+    g.fval.assign(p.nf, std::vector<double>(n));
+    if (n == 0) return g;
+    if (!subset) {
+        VQ_CUDA(cudaMemcpyAsync(g.key.data(), c.key, n * 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaMemcpyAsync(g.first.data(), c.first, n * 8, cudaMemcpyDeviceToHost, rc.s));
+        for (int s = 0; s < p.ni; s++) VQ_CUDA(cudaMemcpyAsync(g.ival[s].data(), c.ival + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
+        for (int s = 0; s < p.nf; s++) VQ_CUDA(cudaMemcpyAsync(g.fval[s].data(), c.fval + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaStreamSynchronize(rc.s));
+        return g;
+    }
+    // gather the selected rows on the device, then one copy
+    long long w = 2 + p.ni + p.nf;
+    p.scratch_g.ensure((size_t)n * 8 + (size_t)n * w * 8);
+    long long* dsel = p.scratch_g.as<long long>();
+    long long* dout = dsel + n;
+    VQ_CUDA(cudaMemcpyAsync(dsel, subset->data(), n * 8, cudaMemcpyHostToDevice, rc.s));
+    k_gather<<<(int)((n + 127) / 128), 128, 0, rc.s>>>(dsel, n, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni, p.nf, dout);
+    VQ_CUDA(cudaGetLastError());
+    std::vector<long long> h((size_t)n * w);
+    VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    for (long long j = 0; j < n; j++) {
+        const long long* o = h.data() + j * w;
+        g.key[j] = (uint64_t)o[0];
+        g.first[j] = o[1];
+        for (int s = 0; s < p.ni; s++) g.ival[s][j] = o[2 + s];
+        for (int f = 0; f < p.nf; f++) std::memcpy(&g.fval[f][j], &o[2 + p.ni + f], 8);
+    }
+    return g;
+}
+
+// Device top-k candidates for ORDER BY <aggregate> LIMIT k: a 16-bit-radix
+// histogram picks a threshold bucket; every group at or above it is a
+// candidate (ties included) and the host finishes the stable sort.
+bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel) {
+    Plan& p = rc.p;
+    const vexq_order_desc& o = p.order;
+    int ngb = (int)p.keys.size();
+    if (o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 64) return false;
+    const AggOut& a = p.outs[o.sort_col - ngb];
+    int vslot = a.value_slot;
+    int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
+    int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
+    if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
+    size_t need = c.n * 9 + 65536 * 4 + 16 + 8 * 70000;
+    p.scratch_d.ensure(need);
+    char* b = (char*)p.scratch_d.p;
+    long long* keyv = (long long*)b;
+    unsigned char* keynull = (unsigned char*)(b + c.n * 8);
+    unsigned* hist = (unsigned*)(((uintptr_t)(b + c.n * 9) + 15) & ~(uintptr_t)15);
+    unsigned long long* nsel = (unsigned long long*)(hist + 65536);
+    long long* dsel = (long long*)(nsel + 2);
+    int g = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
+    Timer tm(rc.s);
+    k_sortkey<<<g, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot], keyv,
+                                   keynull, fmin_key);
+    VQ_CUDA(cudaMemsetAsync(hist, 0, 65536 * 4, rc.s));
+    k_hist<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, hist);
+    std::vector<unsigned> h(65536);
+    VQ_CUDA(cudaMemcpyAsync(h.data(), hist, 65536 * 4, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    long long acc = 0;
+    unsigned thr = 0;
+    for (int bin = 65535; bin >= 0; bin--) {
+        acc += h[bin];
+        if (acc >= o.limit) { thr = (unsigned)bin; break; }
+    }
+    if (acc > 65536) { rc.kernel_ms += tm.stop(); return false; }
+    VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
+    k_select<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, thr, nsel, dsel, 65536);
+    VQ_CUDA(cudaGetLastError());
+    unsigned long long ns = 0;
+    VQ_CUDA(cudaMemcpyAsync(&ns, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
+    rc.kernel_ms += tm.stop();
+    rc.launches += 3;
+    sel.resize(std::min<unsigned long long>(ns, 65536));
+    if (!sel.empty()) VQ_CUDA(cudaMemcpy(sel.data(), dsel, sel.size() * 8, cudaMemcpyDeviceToHost));
+    return true;
+}
+
+// Decodes group keys, computes aggregate outputs, orders groups, and applies
+// ORDER BY / LIMIT.
+vexq_result_s* build_result(Plan& p, Groups& g) {
+    auto* r = new vexq_result_s;
+    size_t n = g.n();
+    bool emptyGlobal = n == 0 && p.keys.empty();
+    // insertion order: first-occurrence order key
+    std::vector<size_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return g.first[a] < g.first[b]; });
+    size_t rows = emptyGlobal ? 1 : n;
+    r->nrows = (int64_t)rows;
+    // group-by columns
+    for (size_t ki = 0; ki < p.keys.size(); ki++) {
+        const KeyCol& k = p.keys[ki];
+        const Table* tt = k.build ? p.bt : p.t;
+        const Column& col = tt->cols[k.col];
+        OutColumn oc;
+        oc.name = col.name;
+        oc.type = k.type;
+        oc.v.assign(rows, 0);
+        oc.valid.assign(rows, 0);
+        if (k.type == VEXQ_TYPE_STRING) oc.dict = &col.dict;
+        int64_t stride = 1;
+        for (size_t kj = 0; kj < ki; kj++) stride *= p.keys[kj].domain > 0 ? p.keys[kj].domain : 1;
+        for (size_t j = 0; j < n; j++) {
+            uint64_t key = g.key[idx[j]];
+            int64_t code;
+            bool isnull = false;
+            if (p.path != AggPath::Hash) {
+                code = (int64_t)((key / (uint64_t)stride) % (uint64_t)k.domain);
+                isnull = k.nullable && code == k.domain - 1;
+            } else {
+                uint64_t m = k.bits >= 64 ? ~0ull : ((1ull << k.bits) - 1);
+                uint64_t raw = (key >> k.shift) & m;
+                if (k.domain > 0) { code = (int64_t)raw; isnull = k.nullable && code == k.domain - 1; }
+                else if (k.type == VEXQ_TYPE_DATE) { isnull = (raw >> 32) & 1; code = (int64_t)(int32_t)(uint32_t)raw; }
+                else code = (int64_t)raw;
+            }
+            if (isnull) continue;
+            oc.valid[j] = 1;
+            if (k.domain > 0 && (k.type == VEXQ_TYPE_DATE || k.type == VEXQ_TYPE_INT64)) oc.v[j] = code + k.vmin;
+            else oc.v[j] = code;
+        }
+        r->cols.push_back(std::move(oc));
+    }
+    // aggregates
+    for (auto& a : p.outs) {
+        OutColumn oc;
+        oc.name = a.name;
+        oc.type = a.out_type;
+        oc.v.assign(rows, 0);
+        oc.valid.assign(rows, 0);
+        if (emptyGlobal) {
+            if (a.kind == VEXQ_AGG_COUNT) oc.valid[0] = 1;
+            r->cols.push_back(std::move(oc));
+            continue;
+        }
+        for (size_t j = 0; j < n; j++) {
+            size_t i = idx[j];
+            int64_t nn = slot_int(p, g, a.nn_slot, i);
+            if (a.kind == VEXQ_AGG_COUNT) { oc.valid[j] = 1; oc.v[j] = slot_int(p, g, a.value_slot, i); continue; }
+            if (nn == 0) continue;
+            oc.valid[j] = 1;
+            const Slot& sl = p.slots[a.value_slot];
+            if (a.kind == VEXQ_AGG_AVG) {
+                double v = slot_float(p, g, a.value_slot, i) / (double)nn;
+                std::memcpy(&oc.v[j], &v, 8);
+            } else if (sl.is_float()) {
+                double v = slot_float(p, g, a.value_slot, i);
+                std::memcpy(&oc.v[j], &v, 8);
+            } else {
+                int64_t v = slot_int(p, g, a.value_slot, i);
+                if (a.out_type == VEXQ_TYPE_DATE) v = (int64_t)(int32_t)v;
+                if (a.out_type == VEXQ_TYPE_BOOL) v = v != 0;
+                oc.v[j] = v;
+            }
+        }
+        r->cols.push_back(std::move(oc));
+    }
+    // ORDER BY (stable, raw int64 bits, NULLs first) + LIMIT
+    const vexq_order_desc& o = p.order;
+    if (o.sort_col >= 0) {
+        if (o.sort_col >= (int)r->cols.size()) fail(VEXQ_EINVAL, "ORDER BY column out of range");
+        const OutColumn& k = r->cols[o.sort_col];
+        std::vector<size_t> ord(rows);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+            bool an = !k.valid[a], bn = !k.valid[b];
+            if (an && bn) return false;
+            if (an) return true;
+            if (bn) return false;
+            if (k.type == VEXQ_TYPE_STRING) {
+                const std::string &sa = k.dict->keys[k.v[a]], &sb = k.dict->keys[k.v[b]];
+                if (sa == sb) return false;
+                return o.descending ? sa > sb : sa < sb;
+            }
+            if (k.v[a] == k.v[b]) return false;
+            return o.descending ? k.v[a] > k.v[b] : k.v[a] < k.v[b];
+        });
+        for (auto& c : r->cols) {
+            std::vector<int64_t> v(rows);
+            std::vector<uint8_t> va(rows);
+            for (size_t j = 0; j < rows; j++) { v[j] = c.v[ord[j]]; va[j] = c.valid[ord[j]]; }
+            c.v.swap(v);
+            c.valid.swap(va);
+        }
+    }
+    if (o.limit >= 0 && (size_t)o.limit < rows) {
+        for (auto& c : r->cols) { c.v.resize(o.limit); c.valid.resize(o.limit); }
+        r->nrows = o.limit;
+    }
+    return r;
+}
+
+long long estimate_groups(const Plan& p, long long rows, long long join_keys) {
+    if (p.path != AggPath::Hash) return p.domain;
+    long long est = rows;
+    if (p.is_join) {
+        // a group key containing the join key has at most (distinct build keys) × (other domains) groups
+        long long other = 1;
+        bool has_join_key = false;
+        for (auto& k : p.keys) {
+            bool jk = (k.build && k.col == p.build_key) || (!k.build && k.col == p.ir[p.probe_key].col);
+            if (jk) has_join_key = true;
+            else other *= k.domain > 0 ? k.domain : (1LL << 30);
+            if (other > (1LL << 30)) other = 1LL << 30;
+        }
+        if (has_join_key) est = std::min<long long>(est, join_keys * other);
+    }
+    if (p.domain > 0) est = std::min<long long>(est, p.domain);
+    return std::max<long long>(est, 1);
+}
+
+}  // namespace
+
+std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge) {
+    std::vector<uint8_t> m(t.n_rg, 0);
+    for (int rg = rgs; rg < rge; rg++) m[rg] = zone_eval(p, root, t, rg);
+    return m;
+}
+
+// Runs the scan kernel over prepared params and returns host groups plus the
+// compacted device arrays (atomic path) for top-k.
+static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, long long estimate) {
+    Plan& p = rc.p;
+    Groups g;
+    if (p.path == AggPath::Regs) {
+        g = run_regs(rc, P, nchunks);
+    } else {
+        Compacted c = run_atomic(rc, P, nchunks, estimate);
+        std::vector<long long> sel;
+        if (topk_candidates(rc, c, sel)) g = fetch_groups(rc, c, &sel);
+        else g = fetch_groups(rc, c, nullptr);
+    }
+    vexq_result_s* r = build_result(p, g);
+    collect_scan_ms(rc);
+    r->kernel_ms = rc.kernel_ms;
+    r->scan_ms = rc.scan_ms;
+    r->launches = rc.launches;
+    return r;
+}
+
+static int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build) {
+    // algorithmic bytes: reference width of every referenced column × rows
+    std::set<int> cols;
+    std::function<void(int)> walk = [&](int i) {
+        if (i < 0) return;
+        const INode& n = p.ir[i];
+        if (n.k == NK::Col && n.build == build) cols.insert(n.col);
+        if ((n.k == NK::StrEq || n.k == NK::InCodes) && n.build == build) cols.insert(n.col);
+        for (int c : n.ch) walk(c);
+    };
+    if (build) {
+        walk(p.bpred);
+        cols.insert(p.build_key);
+    } else {
+        walk(p.pred);
+        if (p.is_join) walk(p.probe_key);
+        for (auto& k : p.keys) if (k.build == build) cols.insert(k.col);
+        for (auto& s : p.slots) walk(s.input);
+        if (p.is_join) walk(p.resid);
+    }
+    int64_t w = 0;
+    for (int c : cols) {
+        int ty = t.cols[c].type;
+        w += (ty == VEXQ_TYPE_INT64 || ty == VEXQ_TYPE_FLOAT64) ? 8 : (ty == VEXQ_TYPE_BOOL ? 1 : 4);
+    }
+    return w * rows;
+}
+
+cudaStream_t plan_stream(Plan& p) {
+    if (p.ext_stream) return p.ext_stream;
+    if (!p.stream) VQ_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+    return p.stream;
+}
+
+vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
+    if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
+    RunCtx rc{p, plan_stream(p)};
+    VQParams P;
+    std::memset(&P, 0, sizeof P);
+    Table& t = *p.t;
+    int rge = rg_end < 0 ? t.n_rg : std::min(rg_end, t.n_rg);
+    int rgs = std::max(0, rg_start);
+    long long join_keys = 0;
+    int64_t bytes = 0, rows_scanned = 0;
+    if (p.is_join) {
+        Table& bt = *p.bt;
+        // ---- build phase ----
+        std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
+        ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg);
+        long long jcap = 16;
+        while (jcap < 2 * std::max<long long>(bs.rows, 8)) jcap <<= 1;
+        VQParams B;
+        std::memset(&B, 0, sizeof B);
+        set_columns(B, bt, false);
+        DevBuf bseg(std::max<size_t>(bs.seg.size(), 3) * 8);
+        if (!bs.seg.empty()) VQ_CUDA(cudaMemcpyAsync(bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice, rc.s));
+        B.seg = bseg.as<long long>();
+        B.nseg = (int)bs.seg.size() / 3;
+        B.nchunks = bs.nchunks;
+        B.rg_rows = bt.rg_rows;
+        B.n_rg = bt.n_rg;
+        B.present = p.d_bpresent.as<unsigned char>();
+        B.sets[0] = nullptr;
+        for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
+        long long nslots = jcap + 1;
+        p.jt_keys.ensure(nslots * 8);
+        p.jt_count.ensure(nslots * 4);
+        p.jt_start.ensure(nslots * 4);
+        p.jt_fill.ensure(nslots * 4);
+        p.jt_rows.ensure(std::max<long long>(bs.rows, 1) * 4);
+        p.jt_scalar.ensure(64 + ((nslots + 4095) / 4096 + 1) * 4);
+        B.jkeys = p.jt_keys.as<unsigned long long>();
+        B.jcount = p.jt_count.as<int>();
+        B.jstart = p.jt_start.as<int>();
+        B.jfill = p.jt_fill.as<int>();
+        B.jrows = p.jt_rows.as<int>();
+        B.jnkeys = p.jt_scalar.as<unsigned long long>();
+        B.error = (int*)(p.jt_scalar.as<char>() + 8);
+        int* bsums = (int*)(p.jt_scalar.as<char>() + 64);
+        B.jmask = (unsigned long long)(jcap - 1);
+        {
+            Timer tm(rc.s);
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 16, rc.s));
+            VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
+            VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
+            int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
+            k_fill_u64<<<ig, 256, 0, rc.s>>>(B.jkeys, jcap, VQ_EMPTY_KEY);
+            VQ_CUDA(cudaMemsetAsync(B.jkeys + jcap, 0, 8, rc.s));
+            B.mode = 0;
+            int grid = grid_for(p.k_build, bs.nchunks);
+            if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
+            int nb = (int)((nslots + 4095) / 4096);
+            k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);
+            k_scan_sums<<<1, 1024, 0, rc.s>>>(bsums, nb);
+            k_scan_add<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, nslots, bsums);
+            B.mode = 1;
+            if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
+            k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error);
+            VQ_CUDA(cudaGetLastError());
+            int herr = 0;
+            unsigned long long nk = 0;
+            VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
+            rc.kernel_ms += tm.stop();
+            rc.launches += 7;
+            if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");
+            join_keys = (long long)nk;
+        }
+        bytes += scanned_bytes(p, bt, bs.rows, true);
+        rows_scanned += bs.rows;
+        // ---- probe phase parameters ----
+        set_columns(P, bt, true);
+        P.jkeys = B.jkeys;
+        P.jcount = B.jcount;
+        P.jstart = B.jstart;
+        P.jrows = B.jrows;
+        P.jmask = B.jmask;
+        if (join_keys == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
+            Groups g;
+            g.ival.assign(p.ni, {});
+            g.fval.assign(p.nf, {});
+            vexq_result_s* r = build_result(p, g);
+            r->kernel_ms = rc.kernel_ms;
+            r->launches = rc.launches;
+            r->rows_scanned = rows_scanned;
+            r->bytes_scanned = bytes;
+            return r;
+        }
+    }
+    std::vector<uint8_t> m = prune_mask(p, t, p.zn_pred, rgs, rge);
+    ScanSegs ss = make_segments(t, m, rgs, rge);
+    set_columns(P, t, false);
+    p.scratch_e.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
+    if (!ss.seg.empty()) VQ_CUDA(cudaMemcpyAsync(p.scratch_e.p, ss.seg.data(), ss.seg.size() * 8, cudaMemcpyHostToDevice, rc.s));
+    P.seg = p.scratch_e.as<long long>();
+    P.nseg = (int)ss.seg.size() / 3;
+    P.nchunks = ss.nchunks;
+    P.rg_rows = t.rg_rows;
+    P.n_rg = t.n_rg;
+    P.present = p.d_present.as<unsigned char>();
+    for (size_t i = 0, off = 0; i < p.sets.size(); i++) { P.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
+    p.scratch_f.ensure(64);
+    if (!P.error) {
+        P.error = p.scratch_f.as<int>();
+        VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
+    }
+    bytes += scanned_bytes(p, t, ss.rows, false);
+    rows_scanned += ss.rows;
+    vexq_result_s* r;
+    if (ss.nchunks == 0) {
+        Groups g;
+        g.ival.assign(p.ni, {});
+        g.fval.assign(p.nf, {});
+        r = build_result(p, g);
+        r->kernel_ms = rc.kernel_ms;
+        r->launches = rc.launches;
+    } else {
+        long long est = estimate_groups(p, ss.rows, join_keys);
+        r = finish_groups(rc, P, ss.nchunks, est);
+    }
+    r->rows_scanned = rows_scanned;
+    r->bytes_scanned = bytes;
+    return r;
+}
+
+vexq_result_s* run_plan_host(Plan& p, const vexq_column_desc* cols, int32_t ncols) {
+    refill_table(*p.t, cols, ncols, plan_stream(p));
+    return run_plan(p, 0, -1);
+}
+
+// ---- Next(): ≤ 1024-row batches (exec/aggregate.go:209-216) ----------------------------
+int32_t result_next(vexq_result_s* r, vexq_batch_view* out) {
+    int64_t n = std::min<int64_t>(VEXQ_BLOCK_ROWS, r->nrows - r->pos);
+    if (n < 0) n = 0;
+    size_t nc = r->cols.size();
+    r->views.assign(nc, vexq_vector_view{});
+    r->vbuf.assign(nc, {});
+    r->bbuf.assign(nc, {});
+    r->doff.assign(nc, {});
+    r->dbytes.assign(nc, {});
+    for (size_t c = 0; c < nc; c++) {
+        OutColumn& oc = r->cols[c];
+        vexq_vector_view& v = r->views[c];
+        v.name = oc.name.c_str();
+        v.type = oc.type;
+        std::vector<uint8_t>& bm = r->bbuf[c];
+        bm.assign((n + 7) / 8, 0);
+        for (int64_t i = 0; i < n; i++) if (oc.valid[r->pos + i]) bm[i >> 3] |= (uint8_t)(1u << (i & 7));
+        std::vector<char>& vb = r->vbuf[c];
+        switch (oc.type) {
+            case VEXQ_TYPE_INT64:
+            case VEXQ_TYPE_FLOAT64:
+                vb.resize(n * 8);
+                std::memcpy(vb.data(), oc.v.data() + r->pos, n * 8);
+                break;
+            case VEXQ_TYPE_DATE: {
+                vb.resize(n * 4);
+                for (int64_t i = 0; i < n; i++) { int32_t x = (int32_t)oc.v[r->pos + i]; std::memcpy(vb.data() + i * 4, &x, 4); }
+                break;
+            }
+            case VEXQ_TYPE_BOOL: {
+                vb.resize(n);
+                for (int64_t i = 0; i < n; i++) vb[i] = oc.v[r->pos + i] != 0;
+                break;
+            }
+            case VEXQ_TYPE_STRING: {  // a fresh per-batch dictionary (exec.newStringVector)
+                vb.resize(n * 4);
+                std::unordered_map<int64_t, uint32_t> local;
+                std::vector<uint32_t>& off = r->doff[c];
+                std::string& bytes = r->dbytes[c];
+                off.push_back(0);
+                for (int64_t i = 0; i < n; i++) {
+                    uint32_t code = 0;
+                    if (oc.valid[r->pos + i]) {
+                        auto it = local.find(oc.v[r->pos + i]);
+                        if (it == local.end()) {
+                            code = (uint32_t)local.size();
+                            local.emplace(oc.v[r->pos + i], code);
+                            bytes += oc.dict->keys[oc.v[r->pos + i]];
+                            off.push_back((uint32_t)bytes.size());
+                        } else {
+                            code = it->second;
+                        }
+                    }
+                    std::memcpy(vb.data() + i * 4, &code, 4);
+                }
+                v.dict_str_off = off.data();
+                v.dict_bytes = bytes.data();
+                v.dict_len = (int32_t)local.size();
+                break;
+            }
+        }
+        v.values = vb.data();
+        v.validity = bm.data();
+    }
+    out->ncols = (int32_t)nc;
+    out->length = (int32_t)n;
+    out->cols = r->views.data();
+    r->pos += n;
+    return VEXQ_OK;
+}
+
+}  // namespace vq

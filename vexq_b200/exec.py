@@ -1,0 +1,252 @@
+"""Python mirror of vexq's operator contract over libvexqcuda's C ABI.
+
+The Go engine would bind the same entry points through cgo;
+this module gives tests and the benchmark the reference's shapes:
+
+  GpuTable                     ≈ the uploaded columns a TableScan would read
+  GpuHashAggregate             ≈ exec.NewHashAggregate / NewParallelHashAggregate
+                                 (exec/aggregate.go:131, exec/parallel.go:78)
+  GpuParallelHashJoinAggregate ≈ exec.NewParallelHashJoinAggregate (exec/parallel_join.go:718)
+  GpuFilter                    ≈ exec.NewFilter + BoolToSelVecInto (exec/filter.go:40-78)
+
+Operators implement next() → Batch | None, schema() and close(), with ≤1024
+rows per batch and group-insertion order, like exec.Operator (exec/operator.go:28-32).
+Every call goes to the CUDA library; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import struct
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi
+from .plan import AggPlan, JoinPlan, predicate_arrays
+from .table import HostTable
+
+_initialised = False
+
+
+def init(device: int = 0) -> None:
+    global _initialised
+    if not _initialised:
+        abi.check(abi.load().vexq_init(device, 0))
+        _initialised = True
+
+
+@dataclass
+class Vector:
+    name: str
+    type: int
+    values: list          # Python values; None = NULL
+
+
+@dataclass
+class Batch:
+    vectors: List[Vector]
+    length: int
+
+
+class GpuTable:
+    """Columns uploaded once into HBM (dictionary codes remapped to global codes)."""
+
+    def __init__(self, t: HostTable):
+        init()
+        self.host = t
+        self.h = C.c_void_p()
+        abi.check(abi.load().vexq_table_upload(t.descs(), len(t.columns), t.nrows, t.rg_rows, C.byref(self.h)))
+
+    def zone_map(self, col: int, rg: int) -> abi.ZoneMap:
+        z = abi.ZoneMap()
+        abi.check(abi.load().vexq_table_zone_map(self.h, col, rg, C.byref(z)))
+        return z
+
+    def device_bytes(self) -> int:
+        v = C.c_int64()
+        abi.check(abi.load().vexq_table_device_bytes(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if self.h:
+            abi.load().vexq_table_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _decode(t: int, raw: bytes, n: int):
+    if t == abi.TYPE_INT64:
+        return list(struct.unpack(f"<{n}q", raw))
+    if t == abi.TYPE_FLOAT64:
+        return list(struct.unpack(f"<{n}d", raw))
+    if t == abi.TYPE_DATE:
+        return list(struct.unpack(f"<{n}i", raw))
+    if t == abi.TYPE_BOOL:
+        return [b != 0 for b in raw]
+    return list(struct.unpack(f"<{n}I", raw))
+
+
+class Result:
+    """A finished run: Next()-style batches plus device timing."""
+
+    def __init__(self, h: C.c_void_p):
+        self.h = h
+        L = abi.load()
+        n, nc = C.c_int64(), C.c_int32()
+        L.vexq_result_num_rows(h, C.byref(n))
+        L.vexq_result_num_cols(h, C.byref(nc))
+        self.nrows, self.ncols = n.value, nc.value
+        ms, la, rs, bs = C.c_double(), C.c_int32(), C.c_int64(), C.c_int64()
+        L.vexq_result_stats(h, C.byref(ms), C.byref(la), C.byref(rs), C.byref(bs))
+        self.kernel_ms, self.launches, self.rows_scanned, self.bytes_scanned = ms.value, la.value, rs.value, bs.value
+        sc = C.c_double()
+        L.vexq_result_scan_ms(h, C.byref(sc))
+        self.scan_ms = sc.value
+
+    def next(self) -> Optional[Batch]:
+        """Operator.Next: ≤1024 rows, None at EOF."""
+        bv = abi.BatchView()
+        abi.check(abi.load().vexq_result_next(self.h, C.byref(bv)))
+        if bv.length == 0:
+            return None
+        vecs = []
+        for c in range(bv.ncols):
+            v = bv.cols[c]
+            n = bv.length
+            width = {abi.TYPE_INT64: 8, abi.TYPE_FLOAT64: 8, abi.TYPE_DATE: 4, abi.TYPE_STRING: 4, abi.TYPE_BOOL: 1}[v.type]
+            raw = C.string_at(v.values, n * width)
+            bm = C.string_at(v.validity, (n + 7) // 8)
+            vals = _decode(v.type, raw, n)
+            if v.type == abi.TYPE_STRING:
+                off = np.frombuffer(C.string_at(v.dict_str_off, (v.dict_len + 1) * 4), dtype=np.uint32) if v.dict_len else []
+                data = C.string_at(v.dict_bytes, int(off[-1])) if v.dict_len else b""
+                strs = [data[off[i]:off[i + 1]].decode() for i in range(v.dict_len)]
+                vals = [strs[x] if x < len(strs) else "" for x in vals]
+            vals = [vals[i] if (bm[i >> 3] >> (i & 7)) & 1 else None for i in range(n)]
+            vecs.append(Vector(v.name.decode() if v.name else "", v.type, vals))
+        return Batch(vecs, bv.length)
+
+    def collect(self):
+        """All rows as columns (lists), draining next()."""
+        cols: List[list] = [[] for _ in range(self.ncols)]
+        names, types = [""] * self.ncols, [0] * self.ncols
+        while True:
+            b = self.next()
+            if b is None:
+                break
+            for i, v in enumerate(b.vectors):
+                cols[i] += v.values
+                names[i], types[i] = v.name, v.type
+        self.columns, self.names, self.types = cols, names, types
+        return cols
+
+    def rows(self):
+        if not hasattr(self, "columns"):
+            self.collect()
+        return [tuple(c[r] for c in self.columns) for r in range(self.nrows)]
+
+    def close(self):
+        if self.h:
+            abi.load().vexq_result_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _PlanOp:
+    h: C.c_void_p
+
+    def run(self, rg_start: int = 0, rg_end: int = -1) -> Result:
+        h = C.c_void_p()
+        abi.check(abi.load().vexq_plan_run(self.h, rg_start, rg_end, C.byref(h)))
+        return Result(h)
+
+    def run_host(self, table: HostTable) -> Result:
+        """End-to-end form: refills the columns from host buffers, then runs."""
+        h = C.c_void_p()
+        abi.check(abi.load().vexq_plan_run_host(self.h, table.descs(), len(table.columns), C.byref(h)))
+        return Result(h)
+
+    def explain(self) -> str:
+        return abi.load().vexq_plan_explain(self.h).decode()
+
+    def set_stream(self, stream_ptr: int) -> None:
+        """Runs on a caller-owned cudaStream_t (0 restores the plan's own)."""
+        abi.check(abi.load().vexq_plan_set_stream(self.h, C.c_void_p(stream_ptr or None)))
+
+    # exec.Operator contract -------------------------------------------------------
+    def next(self) -> Optional[Batch]:
+        if getattr(self, "_result", None) is None:
+            self._result = self.run()
+        return self._result.next()
+
+    def close(self):
+        if getattr(self, "_result", None) is not None:
+            self._result.close()
+            self._result = None
+        if self.h:
+            abi.load().vexq_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuHashAggregate(_PlanOp):
+    """Filter → (Project) → HashAggregate over one table; also stands in for
+    ParallelHashAggregate (numWorkers/morselSize have no GPU meaning)."""
+
+    def __init__(self, table: GpuTable, plan: AggPlan):
+        self.table, self.plan = table, plan
+        self.h = C.c_void_p()
+        abi.check(abi.load().vexq_agg_plan_create(table.h, C.byref(plan.desc), C.byref(self.h)))
+
+    def zone_prune(self) -> List[int]:
+        n = self.table.host.n_rg
+        m = (C.c_uint8 * max(n, 1))()
+        abi.check(abi.load().vexq_zone_prune(self.h, m, n))
+        return [int(m[i]) for i in range(n)]
+
+
+class GpuParallelHashJoinAggregate(_PlanOp):
+    def __init__(self, build: GpuTable, probe: GpuTable, plan: JoinPlan):
+        self.build, self.probe, self.plan = build, probe, plan
+        self.h = C.c_void_p()
+        abi.check(abi.load().vexq_join_plan_create(build.h, probe.h, C.byref(plan.desc), C.byref(self.h)))
+
+
+class GpuFilter:
+    """Filter over a table: a selection bitmap, handed out as per-block SelVecs."""
+
+    def __init__(self, table: GpuTable, predicate):
+        self.table, self.predicate = table, predicate
+        self._arena, self.nodes, self.nn, self.ch, self.nc, self.root = predicate_arrays(predicate)
+
+    def bitmap(self, row_start: int = 0, row_end: int = -1):
+        n = (self.table.host.nrows if row_end < 0 else row_end) - row_start
+        out = (C.c_uint8 * max((n + 7) // 8, 1))()
+        cnt = C.c_int64()
+        abi.check(abi.load().vexq_filter_run(self.table.h, self.nodes, self.nn, self.ch, self.nc, self.root,
+                                             row_start, row_end, out, C.byref(cnt)))
+        return bytes(out)[:(n + 7) // 8], cnt.value
+
+    @staticmethod
+    def selvec(bits: bytes, nrows: int, block: int) -> List[int]:
+        buf = (C.c_uint8 * len(bits)).from_buffer_copy(bits) if bits else (C.c_uint8 * 1)()
+        sel = (C.c_uint16 * abi.BLOCK_ROWS)()
+        n = C.c_int32()
+        abi.check(abi.load().vexq_selvec_from_bits(buf, nrows, block, sel, C.byref(n)))
+        return list(sel[:n.value])
