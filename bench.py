@@ -41,7 +41,22 @@ def parse():
     ap.add_argument("--impl", default="vexq", choices=["vexq", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling driver: three Q1 and three Q6 runs on the 6M-row table, no timing")
     return ap.parse_args()
+
+
+def profile_driver():
+    """Small fixed launch sequence for ncu: upload, 3 × Q1, 3 × Q6."""
+    from vexq_b200 import build, datagen as D, exec as X, workloads as W
+    build.build()
+    X.init(0)
+    gt = X.GpuTable(D.lineitem(NROWS, seed=43, rg_rows=RG_ROWS))
+    for mk in (W.q1_plan, W.q6_plan):
+        op = X.GpuHashAggregate(gt, mk())
+        for _ in range(3):
+            op.run().close()
+        print(op.explain(), flush=True)
 
 
 def measured_peaks():
@@ -161,6 +176,9 @@ def run_reference(args, world, rank):
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.profile:
+        profile_driver()
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         return

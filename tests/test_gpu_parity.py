@@ -9,7 +9,7 @@ import pytest
 
 from oracle import refcpu as R
 from tests.golden.fixtures import load_cases, make_plan, make_table, normalize
-from tests.helpers import assert_rows_match, close
+from tests.helpers import assert_float_vs_exact, assert_rows_match, close
 from vexq_b200 import abi, datagen as D, workloads as W
 from vexq_b200 import plan as P
 from vexq_b200.table import HostTable, date_column, float_column, int_column, string_column
@@ -72,22 +72,21 @@ def lineitem_6m():
 def test_q1_group_by_1m(gpu_lib, lineitem_1m):
     g, r = run_both(gpu_lib, lineitem_1m, W.q1_plan())
     assert g.nrows == 6
-    assert_rows_match(g.rows(), r.rows(), ordered=True)
-    assert check_exact(g, r) < 1e-12
+    eg, er = assert_float_vs_exact(g.rows(), r)
+    print(f"q1 1M: worst GPU error vs exact {eg:.3g}, reference {er:.3g}")
 
 
 def test_q1_group_by_6m(gpu_lib, lineitem_6m):
     g, r = run_both(gpu_lib, lineitem_6m, W.q1_plan())
-    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    eg, er = assert_float_vs_exact(g.rows(), r)
+    print(f"q1 6M: worst GPU error vs exact {eg:.3g}, reference {er:.3g}")
 
 
 def test_q6_range_sum_6m(gpu_lib, lineitem_6m):
     g, r = run_both(gpu_lib, lineitem_6m, W.q6_plan())
     assert g.nrows == 1
-    assert_rows_match(g.rows(), r.rows())
-    # selectivity ≈ 365/2526 × 3/11 × 23/50
-    sel = g.rows_scanned and r.rows()
-    assert sel
+    eg, er = assert_float_vs_exact(g.rows(), r)
+    print(f"q6 6M: GPU error vs exact {eg:.3g}, reference {er:.3g}")
 
 
 def test_q1_parallel_oracle_agrees(gpu_lib, lineitem_1m):

@@ -179,6 +179,7 @@ struct Translator {
                     fail(VEXQ_EINVAL, "column index out of range");
                 }
                 c.col = ci;
+                c.tab = c.build ? bt : t;
                 const Column& col = colref(ci, c.build);
                 c.type = col.type;
                 c.nullable = col.nullable;
@@ -396,7 +397,7 @@ void analyze(Plan& p) {
         auto C = [&](int k) -> INode& { return p.ir[n.ch[k]]; };
         switch (n.k) {
             case NK::Col: {
-                const Table* tt = n.build ? p.bt : p.t;
+                const Table* tt = n.tab ? n.tab : (n.build ? p.bt : p.t);
                 const Column& c = tt->cols[n.col];
                 n.nullable = c.nullable;
                 if (c.has_range) {
@@ -841,20 +842,53 @@ void collect_cols(const Plan& p, int i, std::set<int>& scan) {
     for (int c : n.ch) collect_cols(p, c, scan);
 }
 
-void emit_loads(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
+// 128-bit loads of four consecutive rows of every referenced column into
+// registers named <pfx><col>[4] (values) and <mpfx><col> (validity nibble).
+void emit_loads(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols,
+                const std::string& pfx = "cv", const std::string& mpfx = "cm", const std::string& r0 = "r0",
+                const std::string& ind = "        ", bool declare = true) {
     for (int c : cols) {
         const Column& col = t->cols[c];
-        std::string C = std::to_string(c);
+        std::string C = std::to_string(c), V = pfx + C;
+        const char* ty = "unsigned";
+        const char* fn = "vq_ld4_u32";
         switch (col.type) {
-            case VEXQ_TYPE_INT64: os << "        long long cv" << C << "[4]; vq_ld4_i64(P.col[" << C << "], r0, cv" << C << ");\n"; break;
-            case VEXQ_TYPE_FLOAT64: os << "        double cv" << C << "[4]; vq_ld4_f64(P.col[" << C << "], r0, cv" << C << ");\n"; break;
-            case VEXQ_TYPE_DATE: os << "        int cv" << C << "[4]; vq_ld4_i32(P.col[" << C << "], r0, cv" << C << ");\n"; break;
-            case VEXQ_TYPE_STRING: os << "        unsigned cv" << C << "[4]; vq_ld4_u32(P.col[" << C << "], r0, cv" << C << ");\n"; break;
-            case VEXQ_TYPE_BOOL: os << "        unsigned cv" << C << "[4]; vq_ld4_u8(P.col[" << C << "], r0, cv" << C << ");\n"; break;
+            case VEXQ_TYPE_INT64: ty = "long long"; fn = "vq_ld4_i64"; break;
+            case VEXQ_TYPE_FLOAT64: ty = "double"; fn = "vq_ld4_f64"; break;
+            case VEXQ_TYPE_DATE: ty = "int"; fn = "vq_ld4_i32"; break;
+            case VEXQ_TYPE_BOOL: ty = "unsigned"; fn = "vq_ld4_u8"; break;
         }
-        if (col.nullable) os << "        const unsigned cm" << C << " = vq_bits4(P.valid[" << C << "], r0);\n";
+        os << ind;
+        if (declare) os << ty << " " << V << "[4]; ";
+        os << fn << "(P.col[" << C << "], " << r0 << ", " << V << ");\n";
+        if (col.nullable) {
+            os << ind;
+            if (declare) os << "unsigned ";
+            os << mpfx << C << " = vq_bits4(P.valid[" << C << "], " << r0 << ");\n";
+        }
     }
     (void)p;
+}
+
+void emit_declare_regs(std::ostringstream& os, const Table* t, const std::set<int>& cols, const std::string& pfx,
+                       const std::string& mpfx, const std::string& ind) {
+    for (int c : cols) {
+        const Column& col = t->cols[c];
+        const char* ty = col.type == VEXQ_TYPE_INT64 ? "long long" : col.type == VEXQ_TYPE_FLOAT64 ? "double"
+                       : col.type == VEXQ_TYPE_DATE ? "int" : "unsigned";
+        os << ind << ty << " " << pfx << c << "[4];";
+        if (col.nullable) os << " unsigned " << mpfx << c << " = 0u;";
+        os << "\n";
+    }
+}
+
+void emit_copy_regs(std::ostringstream& os, const Table* t, const std::set<int>& cols, const std::string& ind) {
+    for (int c : cols) {
+        os << ind << "cv" << c << "[0] = nx" << c << "[0]; cv" << c << "[1] = nx" << c << "[1]; cv" << c << "[2] = nx" << c
+           << "[2]; cv" << c << "[3] = nx" << c << "[3];";
+        if (t->cols[c].nullable) os << " cm" << c << " = nm" << c << ";";
+        os << "\n";
+    }
 }
 
 // Group-key expression: dense gid or packed key, plus "any key NULL".
@@ -1045,17 +1079,51 @@ std::string kernel_head(const std::string& name, int block) {
 }
 
 // Chunk loop over the row segments: each warp takes 128-row chunks; lane l
-// handles rows r0..r0+3 with 128-bit loads.
-std::string chunk_loop_open() {
-    return
-        "    const int lane = threadIdx.x & 31;\n"
-        "    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;\n"
-        "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n"
-        "    for (long long c = gw; c < P.nchunks; c += nw) {\n"
-        "        int lo = 0, hi = P.nseg - 1;\n"
-        "        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= c) lo = mid; else hi = mid - 1; }\n"
-        "        const long long s0 = P.seg[3 * lo], s1 = P.seg[3 * lo + 1];\n"
-        "        const long long r0 = (s0 & ~127LL) + (c - P.seg[3 * lo + 2]) * 128 + lane * 4;\n";
+// handles rows r0..r0+3 with 128-bit loads. The loop is software-pipelined:
+// the loads of the warp's next chunk are issued before the current chunk is
+// processed, so a warp keeps two chunks of column data in flight.
+std::string seg_lookup(const std::string& c, const std::string& s0, const std::string& s1, const std::string& r0) {
+    return "{ int lo = 0, hi = P.nseg - 1;\n"
+           "          while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= " + c +
+           ") lo = mid; else hi = mid - 1; }\n"
+           "          " + s0 + " = P.seg[3 * lo]; " + s1 + " = P.seg[3 * lo + 1];\n"
+           "          " + r0 + " = (" + s0 + " & ~127LL) + (" + c + " - P.seg[3 * lo + 2]) * 128 + lane * 4; }\n";
+}
+
+void chunk_loop_open(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
+    if (!p.pipeline) {
+        os << "    const int lane = threadIdx.x & 31;\n"
+              "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n"
+              "    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < P.nchunks; c += nw) {\n"
+              "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+        emit_loads(os, p, t, cols, "cv", "cm", "r0", "        ", true);
+        return;
+    }
+    os << "    const int lane = threadIdx.x & 31;\n"
+          "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n"
+          "    long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;\n"
+          "    long long s0 = 0, s1 = 0, r0 = 0;\n";
+    emit_declare_regs(os, t, cols, "cv", "cm", "    ");
+    os << "    if (c < P.nchunks) {\n        " << seg_lookup("c", "s0", "s1", "r0");
+    emit_loads(os, p, t, cols, "cv", "cm", "r0", "        ", false);
+    os << "    }\n";
+    os << "    for (; c < P.nchunks; c += nw) {\n";
+    os << "        const long long cn = c + nw;\n";
+    os << "        long long ns0 = 0, ns1 = 0, nr0 = 0;\n";
+    emit_declare_regs(os, t, cols, "nx", "nm", "        ");
+    os << "        if (cn < P.nchunks) {\n        " << seg_lookup("cn", "ns0", "ns1", "nr0");
+    emit_loads(os, p, t, cols, "nx", "nm", "nr0", "            ", false);
+    os << "        }\n";
+}
+
+// Closes the pipelined loop: the prefetched chunk becomes the current one.
+void chunk_loop_close(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
+    if (!p.pipeline) {
+        os << "    }\n";
+        return;
+    }
+    emit_copy_regs(os, t, cols, "        ");
+    os << "        s0 = ns0; s1 = ns1; r0 = nr0;\n    }\n";
 }
 
 }  // namespace
@@ -1069,8 +1137,7 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    os << chunk_loop_open();
-    emit_loads(os, p, p.t, cols);
+    chunk_loop_open(os, p, p.t, cols);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -1086,7 +1153,8 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     std::string order = order_expr(p, "r");
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "            ", order);
     else emit_atomic_update(os, p, "            ", order);
-    os << "        }\n    }\n";
+    os << "        }\n";
+    chunk_loop_close(os, p, p.t, cols);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
     return os.str();
@@ -1100,8 +1168,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     collect_cols(p, p.bpred, cols);
     collect_cols(p, key_node, cols);
     os << kernel_head("vq_build", block);
-    os << chunk_loop_open();
-    emit_loads(os, p, p.bt, cols);
+    chunk_loop_open(os, p, p.bt, cols);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -1121,7 +1188,9 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
-    os << "        }\n    }\n}\n";
+    os << "        }\n";
+    chunk_loop_close(os, p, p.bt, cols);
+    os << "}\n";
     return os.str();
 }
 
@@ -1138,8 +1207,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    os << chunk_loop_open();
-    emit_loads(os, p, p.t, cols);
+    chunk_loop_open(os, p, p.t, cols);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -1171,7 +1239,8 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     std::string order = order_expr(p, "((r << 16) | (long long)min(ji - jb, 65535))");
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
     else emit_atomic_update(os, p, "                ", order);
-    os << "            }\n        }\n    }\n";
+    os << "            }\n        }\n";
+    chunk_loop_close(os, p, p.t, cols);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
     return os.str();
@@ -1199,6 +1268,25 @@ static std::string gen_kind_tables(const Plan& p) {
 
 static const int kBlock = 256;
 
+// Kernel tunables: the register path with many accumulators runs 128-thread
+// blocks (more blocks per SM at ~200 registers a thread); VEXQ_TUNE
+// ("block=128,pipeline=0") overrides for measurement sweeps.
+static void choose_tunables(Plan& p) {
+    int64_t acc = p.path == AggPath::Regs ? p.domain * (int64_t)(p.slots.size() + 1) : 0;
+    p.block = acc > 24 ? 128 : 256;
+    p.pipeline = true;
+    if (const char* e = std::getenv("VEXQ_TUNE")) {
+        std::string s(e);
+        auto get = [&](const char* k) -> int {
+            size_t at = s.find(k);
+            return at == std::string::npos ? -1 : std::atoi(s.c_str() + at + std::strlen(k));
+        };
+        int b = get("block="), pl = get("pipeline=");
+        if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
+        if (pl >= 0) p.pipeline = pl != 0;
+    }
+}
+
 static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join, int build_key_node) {
     analyze(p);
     // large IN/LIKE code sets go to device bitsets
@@ -1212,16 +1300,18 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         }
     }
     choose_path(p);
+    choose_tunables(p);
     std::ostringstream src;
     src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
-    std::string body = join ? gen_probe_kernel(p, key_nodes, kBlock) : gen_agg_kernel(p, key_nodes, kBlock);
+    std::string body = join ? gen_probe_kernel(p, key_nodes, p.block) : gen_agg_kernel(p, key_nodes, p.block);
     p.src_main = src.str() + body;
     if (join) p.src_build = std::string(prelude_source()) + "\n" + gen_build_kernel(p, build_key_node, kBlock);
     std::ostringstream ex;
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
-       << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni;
+       << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
+       << " block=" << p.block << " pipeline=" << p.pipeline;
     p.explain = ex.str();
-    p.k_main = jit_get(p.src_main, "vq_agg", kBlock);
+    p.k_main = jit_get(p.src_main, "vq_agg", p.block);
     if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock);
     // device-side tables of the plan
     if (!p.sets.empty()) {
@@ -1274,8 +1364,12 @@ static void keep_zone_strings(Plan& p, const vexq_expr* nodes, int nnodes) {
 }
 
 Plan::~Plan() {
-    std::lock_guard<std::mutex> lk(g_zone_mu);
-    g_zone_strings.erase(this);
+    {
+        std::lock_guard<std::mutex> lk(g_zone_mu);
+        g_zone_strings.erase(this);
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -1310,6 +1404,7 @@ Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d) {
         INode n;
         n.k = NK::Col;
         n.col = c;
+        n.tab = t;
         n.type = t->cols[c].type;
         n.nullable = t->cols[c].nullable;
         key_nodes.push_back(tr.add(n));
@@ -1352,6 +1447,7 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
     INode bk;
     bk.k = NK::Col;
     bk.col = d->build_key;
+    bk.tab = bt;
     bk.type = bkt;
     bk.nullable = bt->cols[d->build_key].nullable;
     int bkey = tb.add(bk);
@@ -1365,6 +1461,7 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
     INode pk;
     pk.k = NK::Col;
     pk.col = d->probe_key;
+    pk.tab = pt;
     pk.type = pkt;
     pk.nullable = pt->cols[d->probe_key].nullable;
     p->probe_key = tp.add(pk);
@@ -1387,6 +1484,7 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
         n.k = NK::Col;
         n.col = k.col;
         n.build = k.build;
+        n.tab = k.build ? bt : pt;
         const Column& col = (k.build ? bt : pt)->cols[k.col];
         n.type = col.type;
         n.nullable = col.nullable;
@@ -1431,8 +1529,8 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     std::ostringstream os;
     std::set<int> cols;
     collect_cols(*p, p->pred, cols);
-    os << prelude_source() << "\n" << kernel_head("vq_filter", kBlock) << chunk_loop_open();
-    emit_loads(os, *p, t, cols);
+    os << prelude_source() << "\n" << kernel_head("vq_filter", kBlock);
+    chunk_loop_open(os, *p, t, cols);
     os << "        unsigned nib = 0u;\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
@@ -1446,10 +1544,12 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     os << "        unsigned word = (unsigned)spread;\n";
     os << "        for (int o = 1; o < 8; o <<= 1) word |= __shfl_xor_sync(0xffffffffu, word, o);\n";
     os << "        if ((lane & 7) == 0 && word) {\n";
-    os << "            const long long wi = ((s0 & ~127LL) + (c - P.seg[3 * lo + 2]) * 128) / 32 + (lane >> 3);\n";
+    os << "            const long long wi = (r0 - lane * 4) / 32 + (lane >> 3);\n";
     os << "            atomicOr(reinterpret_cast<unsigned*>(P.acc_i) + wi, word);\n";
     os << "            atomicAdd(P.ngroups, (unsigned long long)__popc(word));\n";
-    os << "        }\n    }\n}\n";
+    os << "        }\n";
+    chunk_loop_close(os, *p, t, cols);
+    os << "}\n";
     p->src_main = os.str();
     p->k_main = jit_get(p->src_main, "vq_filter", kBlock);
     if (!p->sets.empty()) {

@@ -17,6 +17,7 @@ struct INode {
     int op = 0;
     int col = -1;          // Col / StrEq / InCodes: column (in its side's table)
     bool build = false;    // column read through the build row (join above-scope)
+    const Table* tab = nullptr;  // table the column belongs to
     int64_t li = 0;
     double lf = 0;
     int32_t ld = 0;
@@ -109,6 +110,15 @@ struct Plan {
     JitKernel k_main, k_build;
     std::string explain;
     int radix_bits = 0;
+    // tunables of the generated scan kernel (chosen at compile time)
+    int block = 256;
+    bool pipeline = true;
+    // per-run caches (host-side overhead of a run)
+    std::vector<long long> seg_cache;      // last uploaded segment list
+    DevBuf d_seg;
+    DevBuf d_kinds;                        // register-path combiner kinds
+    PinnedBuf h_stage;                     // pinned staging for small results
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set

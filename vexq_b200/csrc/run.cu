@@ -314,74 +314,64 @@ struct RunCtx {
     float kernel_ms = 0;
     float scan_ms = 0;
     int launches = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
 };
 
-// Times one scan-kernel launch with events on the run's stream; the elapsed
-// time is read once the run has synchronised (collect_scan_ms).
-void launch_scan(RunCtx& rc, const JitKernel& k, int grid, VQParams& P) {
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, rc.s);
-    jit_launch(k, grid, &P, sizeof P, rc.s);
-    cudaEventRecord(b, rc.s);
-    rc.scan_events.push_back({a, b});
+void ensure_events(Plan& p) {
+    for (auto& e : p.ev)
+        if (!e) VQ_CUDA(cudaEventCreate(&e));
 }
 
-void collect_scan_ms(RunCtx& rc) {
-    for (auto& e : rc.scan_events) {
-        cudaEventSynchronize(e.second);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e.first, e.second);
-        rc.scan_ms += ms;
-        cudaEventDestroy(e.first);
-        cudaEventDestroy(e.second);
-    }
-    rc.scan_events.clear();
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
 }
 
-// Register path over prepared params: launch, merge, copy back.
+// Register path over prepared params: launch, merge, one copy back, one sync.
 Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     Plan& p = rc.p;
     Groups g;
     int G = (int)p.domain, nf = p.nf, ni = p.ni;
+    int nfb = std::max(nf, 1);
     int grid = grid_for(p.k_main, nchunks);
-    size_t pf = (size_t)grid * G * std::max(nf, 1), pi = (size_t)grid * G * (ni + 1);
+    size_t pf = (size_t)grid * G * nfb, pi = (size_t)grid * G * (ni + 1);
     p.scratch_a.ensure(pf * 8);
     p.scratch_b.ensure(pi * 8);
     P.part_f = p.scratch_a.as<double>();
     P.part_i = p.scratch_b.as<long long>();
-    std::vector<int> fk(std::max(nf, 1), 0), ik(ni + 1, 0);
-    for (size_t s = 0; s < p.slots.size(); s++) {
-        int k = p.slots[s].kind;
-        int code = (k == S_IMIN || k == S_FMIN) ? 1 : (k == S_IMAX || k == S_FMAX) ? 2 : 0;
-        if (p.slots[s].is_float()) fk[p.slot_pos[s]] = code;
-        else ik[p.slot_pos[s]] = code;
+    if (!p.d_kinds.p) {  // combiner kind per bank entry (0 sum, 1 min, 2 max), uploaded once
+        std::vector<int> k(nfb + ni + 1, 0);
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            int kd = p.slots[s].kind;
+            int code = (kd == S_IMIN || kd == S_FMIN) ? 1 : (kd == S_IMAX || kd == S_FMAX) ? 2 : 0;
+            k[p.slots[s].is_float() ? p.slot_pos[s] : nfb + p.slot_pos[s]] = code;
+        }
+        k[nfb + ni] = 1;  // first-occurrence key: min
+        p.d_kinds.alloc(k.size() * 4);
+        VQ_CUDA(cudaMemcpy(p.d_kinds.p, k.data(), k.size() * 4, cudaMemcpyHostToDevice));
     }
-    ik[ni] = 1;
-    size_t nout = (size_t)G * std::max(nf, 1) * 8 + (size_t)G * (ni + 1) * 8;
-    p.scratch_c.ensure(nout + (fk.size() + ik.size()) * 4);
+    const int* d_kinds = p.d_kinds.as<int>();
+    size_t nout_f = (size_t)G * nfb * 8, nout_i = (size_t)G * (ni + 1) * 8;
+    p.scratch_c.ensure(nout_f + nout_i);
     double* out_f = p.scratch_c.as<double>();
-    long long* out_i = (long long*)((char*)p.scratch_c.p + (size_t)G * std::max(nf, 1) * 8);
-    int* d_kinds = (int*)((char*)p.scratch_c.p + nout);
-    VQ_CUDA(cudaMemcpyAsync(d_kinds, fk.data(), fk.size() * 4, cudaMemcpyHostToDevice, rc.s));
-    VQ_CUDA(cudaMemcpyAsync(d_kinds + fk.size(), ik.data(), ik.size() * 4, cudaMemcpyHostToDevice, rc.s));
-    {
-        Timer tm(rc.s);
-        launch_scan(rc, p.k_main, grid, P);
-        int tot = G * nf + G * (ni + 1);
-        k_merge_regs<<<(tot + 127) / 128, 128, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + fk.size(),
-                                                         out_f, out_i);
-        VQ_CUDA(cudaGetLastError());
-        rc.kernel_ms += tm.stop();
-        rc.launches += 2;
-    }
-    std::vector<double> hf((size_t)G * std::max(nf, 1));
-    std::vector<long long> hi((size_t)G * (ni + 1));
-    if (nf) VQ_CUDA(cudaMemcpyAsync(hf.data(), out_f, (size_t)G * nf * 8, cudaMemcpyDeviceToHost, rc.s));
-    VQ_CUDA(cudaMemcpyAsync(hi.data(), out_i, hi.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    long long* out_i = (long long*)((char*)p.scratch_c.p + nout_f);
+    p.h_stage.ensure(nout_f + nout_i);
+    ensure_events(p);
+    VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
+    jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+    VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
+    int tot = G * nf + G * (ni + 1);
+    k_merge_regs<<<(tot + 127) / 128, 128, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + nfb,
+                                                     out_f, out_i);
+    VQ_CUDA(cudaGetLastError());
+    VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
+    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
+    rc.scan_ms += elapsed(p.ev[0], p.ev[1]);
+    rc.kernel_ms += elapsed(p.ev[0], p.ev[2]);
+    rc.launches += 2;
+    const double* hf = (const double*)p.h_stage.p;
+    const long long* hi = (const long long*)((const char*)p.h_stage.p + nout_f);
     g.ival.assign(ni, {});
     g.fval.assign(nf, {});
     for (int gi = 0; gi < G; gi++) {
@@ -417,6 +407,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         cap = p.domain;
     }
     std::vector<long long> iv = init_values(p);
+    ensure_events(p);
     for (int attempt = 0; attempt < 8; attempt++) {
         long long nslots = cap + 1;
         int ni = p.ni, nf = p.nf;
@@ -438,54 +429,52 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         P.cap = (unsigned long long)cap;
         P.cap_mask = hash ? (unsigned long long)(cap - 1) : 0;
         for (int f = 0; f < nf && f < 16; f++) P.fx_lsb[f] = p.fx_lsb[f];
-        Timer tm(rc.s);
+        // compacted output (upper bound: every slot occupied)
+        long long cap_out = nslots;
+        size_t o_bytes = 16 + cap_out * 16 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8 + nf * 4 + 64;
+        p.scratch_b.ensure(o_bytes);
+        char* ob = (char*)p.scratch_b.p;
+        Compacted c;
+        c.cap_out = cap_out;
+        unsigned long long* n_out = (unsigned long long*)ob;
+        c.key = (unsigned long long*)(ob + 16);
+        c.first = (long long*)(ob + 16 + cap_out * 8);
+        c.ival = (long long*)(ob + 16 + cap_out * 16);
+        c.fval = (double*)(ob + 16 + cap_out * 16 + (size_t)ni * cap_out * 8);
+        int* d_lsb = (int*)(ob + 16 + cap_out * 16 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8);
+        VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
         VQ_CUDA(cudaMemcpyAsync(d_init, iv.data(), iv.size() * 8, cudaMemcpyHostToDevice, rc.s));
+        if (nf) VQ_CUDA(cudaMemcpyAsync(d_lsb, p.fx_lsb.data(), nf * 4, cudaMemcpyHostToDevice, rc.s));
         VQ_CUDA(cudaMemsetAsync(P.ngroups, 0, 16, rc.s));
+        VQ_CUDA(cudaMemsetAsync(n_out, 0, 8, rc.s));
         if (b_fx) VQ_CUDA(cudaMemsetAsync(P.acc_fx, 0, b_fx + b_sp, rc.s));
         int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
         k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
         VQ_CUDA(cudaGetLastError());
         int grid = grid_for(p.k_main, nchunks);
-        launch_scan(rc, p.k_main, grid, P);
-        int herr = 0;
-        VQ_CUDA(cudaMemcpyAsync(&herr, P.error, 4, cudaMemcpyDeviceToHost, rc.s));
-        rc.kernel_ms += tm.stop();
-        rc.launches += 2;
+        VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
+        jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+        VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
+        int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
+        k_finalize<<<fg, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, P.acc_fx, P.special, nslots, ni, nf, d_lsb, hash, n_out,
+                                         c.key, c.first, c.ival, c.fval, cap_out);
+        VQ_CUDA(cudaGetLastError());
+        VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
+        p.h_stage.ensure(32);
+        VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, n_out, 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaMemcpyAsync((char*)p.h_stage.p + 8, P.error, 4, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaStreamSynchronize(rc.s));
+        rc.scan_ms += elapsed(p.ev[1], p.ev[2]);
+        rc.kernel_ms += elapsed(p.ev[0], p.ev[3]);
+        rc.launches += 3;
+        unsigned long long nn = *(unsigned long long*)p.h_stage.p;
+        int herr = *(int*)((char*)p.h_stage.p + 8);
         if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
         if (herr & 1) {  // probe limit: grow the table and rerun
             if (!hash) fail(VEXQ_EDEVICE, "dense group table reported a probe failure");
             cap <<= 1;
             continue;
         }
-        // finalize + compact
-        unsigned long long ng = 0;
-        VQ_CUDA(cudaMemcpyAsync(&ng, P.ngroups, 8, cudaMemcpyDeviceToHost, rc.s));
-        VQ_CUDA(cudaStreamSynchronize(rc.s));
-        long long cap_out = hash ? (long long)ng + 1 : std::min<long long>(nslots, cap);
-        if (!hash) cap_out = nslots;
-        cap_out = std::max<long long>(cap_out, 1);
-        size_t o_bytes = 8 + cap_out * 8 + cap_out * 8 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8 + nf * 4 + 64;
-        p.scratch_b.ensure(o_bytes);
-        char* ob = (char*)p.scratch_b.p;
-        Compacted c;
-        c.cap_out = cap_out;
-        unsigned long long* n_out = (unsigned long long*)ob;
-        c.key = (unsigned long long*)(ob + 8);
-        c.first = (long long*)(ob + 8 + cap_out * 8);
-        c.ival = (long long*)(ob + 8 + cap_out * 16);
-        c.fval = (double*)(ob + 8 + cap_out * 16 + (size_t)ni * cap_out * 8);
-        int* d_lsb = (int*)(ob + 8 + cap_out * 16 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8);
-        Timer tm2(rc.s);
-        VQ_CUDA(cudaMemsetAsync(n_out, 0, 8, rc.s));
-        if (nf) VQ_CUDA(cudaMemcpyAsync(d_lsb, p.fx_lsb.data(), nf * 4, cudaMemcpyHostToDevice, rc.s));
-        int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
-        k_finalize<<<fg, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, P.acc_fx, P.special, nslots, ni, nf, d_lsb, hash, n_out,
-                                         c.key, c.first, c.ival, c.fval, cap_out);
-        VQ_CUDA(cudaGetLastError());
-        unsigned long long nn = 0;
-        VQ_CUDA(cudaMemcpyAsync(&nn, n_out, 8, cudaMemcpyDeviceToHost, rc.s));
-        rc.kernel_ms += tm2.stop();
-        rc.launches += 1;
         c.n = (long long)std::min<unsigned long long>(nn, (unsigned long long)cap_out);
         return c;
     }
@@ -735,7 +724,6 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
         else g = fetch_groups(rc, c, nullptr);
     }
     vexq_result_s* r = build_result(p, g);
-    collect_scan_ms(rc);
     r->kernel_ms = rc.kernel_ms;
     r->scan_ms = rc.scan_ms;
     r->launches = rc.launches;
@@ -743,13 +731,12 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
 }
 
 static int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build) {
-    // algorithmic bytes: reference width of every referenced column × rows
+    // algorithmic bytes: reference width of every column of `t` the scan reads × rows
     std::set<int> cols;
     std::function<void(int)> walk = [&](int i) {
         if (i < 0) return;
         const INode& n = p.ir[i];
-        if (n.k == NK::Col && n.build == build) cols.insert(n.col);
-        if ((n.k == NK::StrEq || n.k == NK::InCodes) && n.build == build) cols.insert(n.col);
+        if (n.k == NK::Col && n.tab == &t && !n.build) cols.insert(n.col);
         for (int c : n.ch) walk(c);
     };
     if (build) {
@@ -757,10 +744,9 @@ static int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool
         cols.insert(p.build_key);
     } else {
         walk(p.pred);
-        if (p.is_join) walk(p.probe_key);
-        for (auto& k : p.keys) if (k.build == build) cols.insert(k.col);
+        if (p.is_join) { walk(p.probe_key); walk(p.resid); }
+        for (auto& k : p.keys) if (!k.build) cols.insert(k.col);
         for (auto& s : p.slots) walk(s.input);
-        if (p.is_join) walk(p.resid);
     }
     int64_t w = 0;
     for (int c : cols) {
@@ -874,19 +860,24 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     std::vector<uint8_t> m = prune_mask(p, t, p.zn_pred, rgs, rge);
     ScanSegs ss = make_segments(t, m, rgs, rge);
     set_columns(P, t, false);
-    p.scratch_e.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
-    if (!ss.seg.empty()) VQ_CUDA(cudaMemcpyAsync(p.scratch_e.p, ss.seg.data(), ss.seg.size() * 8, cudaMemcpyHostToDevice, rc.s));
-    P.seg = p.scratch_e.as<long long>();
+    if (ss.seg != p.seg_cache || !p.d_seg.p) {  // segment list uploaded once per distinct pruning
+        p.d_seg.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
+        if (!ss.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_seg.p, ss.seg.data(), ss.seg.size() * 8, cudaMemcpyHostToDevice));
+        p.seg_cache = ss.seg;
+    }
+    P.seg = p.d_seg.as<long long>();
     P.nseg = (int)ss.seg.size() / 3;
     P.nchunks = ss.nchunks;
     P.rg_rows = t.rg_rows;
     P.n_rg = t.n_rg;
     P.present = p.d_present.as<unsigned char>();
     for (size_t i = 0, off = 0; i < p.sets.size(); i++) { P.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
-    p.scratch_f.ensure(64);
-    if (!P.error) {
-        P.error = p.scratch_f.as<int>();
-        VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
+    if (!P.error && p.path == AggPath::Regs) {
+        if (!p.scratch_f.p) {
+            p.scratch_f.alloc(64);
+            VQ_CUDA(cudaMemset(p.scratch_f.p, 0, 64));
+        }
+        P.error = p.scratch_f.as<int>();  // unused by the register path
     }
     bytes += scanned_bytes(p, t, ss.rows, false);
     rows_scanned += ss.rows;
