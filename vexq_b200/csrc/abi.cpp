@@ -249,12 +249,13 @@ int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes, 
         // one segment [row_start, row_end)
         std::vector<long long> seg;
         long long chunks = 0;
+        const long long U = p->tile;
         if (row_end > row_start) {
             seg = {row_start, row_end, 0};
-            chunks = (row_end - (row_start & ~127LL) + 127) / 128;
+            chunks = (row_end - (row_start & ~(U - 1)) + U - 1) / U;
         }
         size_t words = (size_t)(tb.nrows + kPadRows) / 32 + 8;
-        DevBuf bits(words * 4), dseg(24), scal(16);
+        DevBuf bits(words * 4), dseg(24), scal(32);
         VQParams P;
         std::memset(&P, 0, sizeof P);
         for (size_t c = 0; c < tb.cols.size(); c++) {
@@ -267,24 +268,27 @@ int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes, 
         P.n_rg = tb.n_rg;
         P.acc_i = bits.as<long long>();
         P.ngroups = scal.as<unsigned long long>();
+        P.error = (int*)(scal.as<char>() + 16);
         P.seg = dseg.as<long long>();
         P.nseg = seg.empty() ? 0 : 1;
         P.nchunks = chunks;
         cudaStream_t s = plan_stream(*p);
         VQ_CUDA(cudaMemsetAsync(bits.p, 0, bits.n, s));
-        VQ_CUDA(cudaMemsetAsync(scal.p, 0, 16, s));
+        VQ_CUDA(cudaMemsetAsync(scal.p, 0, 32, s));
         if (!seg.empty()) VQ_CUDA(cudaMemcpyAsync(dseg.p, seg.data(), 24, cudaMemcpyHostToDevice, s));
         if (chunks > 0) {
             int per_sm = std::max(1, p->k_main.max_blocks_per_sm);
-            long long want = (chunks + 7) / 8;
+            long long want = p->staged ? chunks : (chunks + 7) / 8;
             int grid = (int)std::max<long long>(1, std::min<long long>((long long)sm_count() * per_sm, want));
             jit_launch(p->k_main, grid, &P, sizeof P, s);
         }
         std::vector<uint32_t> h(words);
-        unsigned long long cnt = 0;
+        unsigned long long sc[4] = {0, 0, 0, 0};
         VQ_CUDA(cudaMemcpyAsync(h.data(), bits.p, words * 4, cudaMemcpyDeviceToHost, s));
-        VQ_CUDA(cudaMemcpyAsync(&cnt, scal.p, 8, cudaMemcpyDeviceToHost, s));
+        VQ_CUDA(cudaMemcpyAsync(sc, scal.p, 32, cudaMemcpyDeviceToHost, s));
         VQ_CUDA(cudaStreamSynchronize(s));
+        unsigned long long cnt = sc[0];
+        if ((int)(sc[2] & 0xFFFFFFFF) & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
         int64_t n = row_end - row_start;
         std::memset(out_bits, 0, (size_t)(n + 7) / 8);
         for (int64_t i = 0; i < n; i++) {

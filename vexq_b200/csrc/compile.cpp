@@ -1001,7 +1001,7 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
     int nf = p.nf, ni = p.ni;
     os << "    __shared__ double sh_f[" << warps << "][" << std::max(G * nf, 1) << "];\n";
     os << "    __shared__ long long sh_i[" << warps << "][" << std::max(G * (ni + 1), 1) << "];\n";
-    os << "    const int warp = threadIdx.x >> 5;\n";
+    os << "    const int fw = threadIdx.x >> 5;\n";
     for (int g = 0; g < G; g++) {
         for (size_t s = 0; s < p.slots.size(); s++) {
             std::string a = acc_name(p, g, (int)s);
@@ -1020,10 +1020,10 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
             else if (p.slots[s].kind == S_ISUM) os << a << " = (long long)((unsigned long long)" << a << " + (unsigned long long)t); }\n";
             else os << a << " += t; }\n";
             int idx = p.slots[s].is_float() ? g * nf + p.slot_pos[s] : g * (ni + 1) + p.slot_pos[s];
-            os << "    if ((threadIdx.x & 31) == 0) sh_" << (p.slots[s].is_float() ? "f" : "i") << "[warp][" << idx << "] = " << a << ";\n";
+            os << "    if ((threadIdx.x & 31) == 0) sh_" << (p.slots[s].is_float() ? "f" : "i") << "[fw][" << idx << "] = " << a << ";\n";
         }
         os << "    for (int o = 16; o > 0; o >>= 1) fo" << g << " = min(fo" << g << ", __shfl_xor_sync(0xffffffffu, fo" << g << ", o));\n";
-        os << "    if ((threadIdx.x & 31) == 0) sh_i[warp][" << g * (ni + 1) + ni << "] = fo" << g << ";\n";
+        os << "    if ((threadIdx.x & 31) == 0) sh_i[fw][" << g * (ni + 1) + ni << "] = fo" << g << ";\n";
     }
     os << "    __syncthreads();\n";
     // fixed-order combine over warps; kinds per bank entry
@@ -1071,6 +1071,87 @@ void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string
     }
 }
 
+// Atomic path with warp aggregation: lanes whose rows fall into the same
+// group are folded in lane order (shuffles among the __match_any_sync peers)
+// and only the lowest such lane updates the group table. Float sums of a peer
+// set are added in lane order before the exact fixed-point accumulation, so
+// the result is deterministic; its error is bounded by the ≤ 32-value folds.
+void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
+    const std::string in = ind + "    ";
+    os << ind << "unsigned long long slot = VQ_NOSLOT;\n";
+    if (p.path == AggPath::Dense) os << ind << "if (live) slot = key;\n";
+    else os << ind << "if (live) slot = vq_insert(P.keys, P.cap_mask, P.cap, key, P.ngroups, P.error);\n";
+    os << ind << "live = live && slot != VQ_NOSLOT;\n";
+    os << ind << "const unsigned act = __ballot_sync(0xffffffffu, live);\n";
+    os << ind << "if (live) {\n";
+    os << in << "const long long stride = (long long)P.cap + 1;\n";
+    os << in << "const unsigned peers = __match_any_sync(act, slot);\n";
+    os << in << "const bool lead = (__ffs(peers) - 1) == lane;\n";
+    os << in << "long long ag_first = " << order << ";\n";
+    // per-slot aggregate registers
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s);
+        switch (p.slots[s].kind) {
+            case S_CNT: os << in << "long long ag" << S << " = __popc(peers);\n"; break;
+            case S_NN: os << in << "long long ag" << S << " = __popc(__ballot_sync(peers, sok" << S << "));\n"; break;
+            case S_ISUM: os << in << "long long ag" << S << " = 0; bool ah" << S << " = false;\n"; break;
+            case S_IMIN: os << in << "long long ag" << S << " = 0x7FFFFFFFFFFFFFFFLL; bool ah" << S << " = false;\n"; break;
+            case S_IMAX: os << in << "long long ag" << S << " = (-0x7FFFFFFFFFFFFFFFLL - 1LL); bool ah" << S << " = false;\n"; break;
+            case S_FSUM: os << in << "double ag" << S << " = 0.0; bool ah" << S << " = false;\n"; break;
+            case S_FMIN: os << in << "unsigned long long ag" << S << " = 0xFFFFFFFFFFFFFFFFull; bool ah" << S << " = false;\n"; break;
+            case S_FMAX: os << in << "unsigned long long ag" << S << " = 0ull; bool ah" << S << " = false;\n"; break;
+        }
+    }
+    os << in << "for (unsigned m = peers; m; m &= m - 1u) {\n";
+    std::string in2 = in + "    ";
+    os << in2 << "const int src = __ffs(m) - 1;\n";
+    os << in2 << "ag_first = min(ag_first, (long long)__shfl_sync(peers, (long long)(" << order << "), src));\n";
+    for (size_t s = 1; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s);
+        SlotKind k = p.slots[s].kind;
+        if (k == S_NN) continue;
+        os << in2 << "{ const bool o = __shfl_sync(peers, (int)sok" << S << ", src) != 0; ";
+        if (k == S_FSUM || k == S_FMIN || k == S_FMAX)
+            os << "const double v = __shfl_sync(peers, sv" << S << ", src); ";
+        else
+            os << "const long long v = __shfl_sync(peers, sv" << S << ", src); ";
+        switch (k) {
+            case S_ISUM: os << "if (o) { ag" << S << " = (long long)((unsigned long long)ag" << S << " + (unsigned long long)v); ah" << S << " = true; }"; break;
+            case S_IMIN: os << "if (o) { ag" << S << " = min(ag" << S << ", v); ah" << S << " = true; }"; break;
+            case S_IMAX: os << "if (o) { ag" << S << " = max(ag" << S << ", v); ah" << S << " = true; }"; break;
+            case S_FSUM: os << "if (o) { ag" << S << " += v; ah" << S << " = true; }"; break;
+            case S_FMIN: os << "if (o && !isnan(v)) { ag" << S << " = min(ag" << S << ", vq_fkey(v)); ah" << S << " = true; }"; break;
+            case S_FMAX: os << "if (o && !isnan(v)) { ag" << S << " = max(ag" << S << ", vq_fkey(v)); ah" << S << " = true; }"; break;
+            default: break;
+        }
+        os << " }\n";
+    }
+    os << in << "}\n";
+    os << in << "if (lead) {\n";
+    std::string in3 = in + "    ";
+    os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s);
+        int pos = p.slot_pos[s];
+        std::string ai = "P.acc_i[" + std::to_string(pos) + " * stride + slot]";
+        std::string aiu = "(unsigned long long*)&" + ai;
+        switch (p.slots[s].kind) {
+            case S_CNT:
+            case S_NN: os << in3 << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_ISUM: os << in3 << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_IMIN: os << in3 << "if (ah" << S << ") atomicMin(&" << ai << ", ag" << S << ");\n"; break;
+            case S_IMAX: os << in3 << "if (ah" << S << ") atomicMax(&" << ai << ", ag" << S << ");\n"; break;
+            case S_FMIN: os << in3 << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FMAX: os << in3 << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FSUM:
+                os << in3 << "if (ah" << S << ") vq_fx_add<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, ag" << S
+                   << ", " << p.fx_lsb[pos] << ", P.special + (long long)" << pos << " * stride + slot, P.error);\n";
+                break;
+        }
+    }
+    os << in << "}\n" << ind << "}\n";
+}
+
 std::string kernel_head(const std::string& name, int block) {
     std::ostringstream os;
     os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") " << name
@@ -1116,6 +1197,118 @@ void chunk_loop_open(std::ostringstream& os, const Plan& p, const Table* t, cons
     os << "        }\n";
 }
 
+// ---- TMA-staged tile loop ---------------------------------------------------------------
+// Each block walks tiles of T = warps × 128 rows. Thread 0 streams the tiles'
+// column slices (and validity bitmaps) into a ring of S shared-memory stages
+// with cp.async.bulk, each stage completing on its mbarrier; all warps read
+// their 128-row slice from shared memory. A wait that does not complete within
+// its poll limit raises error bit 8 and the whole block leaves the loop.
+struct StageLayout {
+    int T = 1024, S = 3, stage_bytes = 0, tx = 0;
+    std::map<int, int> off, voff;
+};
+
+static int type_w(int t) {
+    return (t == VEXQ_TYPE_INT64 || t == VEXQ_TYPE_FLOAT64) ? 8 : t == VEXQ_TYPE_BOOL ? 1 : 4;
+}
+
+StageLayout stage_layout(const Table* t, const std::set<int>& cols, int block, int budget) {
+    StageLayout L;
+    L.T = (block / 32) * 128;
+    int o = 0;
+    for (int c : cols) {
+        L.off[c] = o;
+        o += (L.T * type_w(t->cols[c].type) + 127) & ~127;
+        L.tx += L.T * type_w(t->cols[c].type);
+    }
+    for (int c : cols) {
+        if (!t->cols[c].nullable) continue;
+        L.voff[c] = o;
+        o += (L.T / 8 + 127) & ~127;
+        L.tx += L.T / 8;
+    }
+    L.stage_bytes = std::max(o, 128);
+    L.S = std::max(2, std::min(6, budget / L.stage_bytes));
+    return L;
+}
+
+void emit_issue_fn(std::ostringstream& os, const Table* t, const std::set<int>& cols, const StageLayout& L,
+                   const std::string& name) {
+    os << "__device__ __forceinline__ void " << name
+       << "(const VQParams& P, unsigned char* smem, unsigned long long* full, int stage, long long tile) {\n";
+    os << "    int lo = 0, hi = P.nseg - 1;\n";
+    os << "    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= tile) lo = mid; else hi = mid - 1; }\n";
+    os << "    const long long base = (P.seg[3 * lo] & ~" << (L.T - 1) << "LL) + (tile - P.seg[3 * lo + 2]) * " << L.T << ";\n";
+    os << "    unsigned char* st = smem + stage * " << L.stage_bytes << ";\n";
+    os << "    vq_mbar_expect_tx(full + stage, " << L.tx << "u);\n";
+    for (int c : cols) {
+        int w = type_w(t->cols[c].type);
+        os << "    vq_bulk_g2s(st + " << L.off.at(c) << ", (const unsigned char*)P.col[" << c << "] + base * " << w << ", "
+           << L.T * w << "u, full + stage);\n";
+    }
+    for (auto& kv : L.voff)
+        os << "    vq_bulk_g2s(st + " << kv.second << ", P.valid[" << kv.first << "] + (base >> 3), " << L.T / 8
+           << "u, full + stage);\n";
+    os << "}\n";
+}
+
+void staged_loop_open(std::ostringstream& os, const Table* t, const std::set<int>& cols, const StageLayout& L,
+                      const std::string& issue) {
+    os << "    extern __shared__ __align__(128) unsigned char vq_smem[];\n";
+    os << "    __shared__ __align__(8) unsigned long long vq_full[" << L.S << "];\n";
+    os << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    os << "    if (threadIdx.x == 0) {\n";
+    os << "        for (int s = 0; s < " << L.S << "; s++) vq_mbar_init(&vq_full[s], 1u);\n";
+    os << "        vq_fence_mbar_init();\n    }\n    __syncthreads();\n";
+    os << "    if (threadIdx.x == 0)\n";
+    os << "        for (int s = 0; s < " << L.S << "; s++) {\n";
+    os << "            const long long tl = blockIdx.x + (long long)s * gridDim.x;\n";
+    os << "            if (tl < P.nchunks) " << issue << "(P, vq_smem, vq_full, s, tl);\n        }\n";
+    os << "    long long it = 0;\n    bool vq_timeout = false;\n";
+    os << "    for (;; it++) {\n";
+    os << "        const long long tile = blockIdx.x + it * gridDim.x;\n";
+    os << "        if (tile >= P.nchunks) break;\n";
+    os << "        const int stage = (int)(it % " << L.S << ");\n";
+    os << "        const bool got = vq_mbar_wait(&vq_full[stage], (unsigned)((it / " << L.S << ") & 1), 1 << 20);\n";
+    os << "        if (__syncthreads_or(!got)) { vq_timeout = true; break; }\n";
+    os << "        long long s0, s1, r0;\n";
+    os << "        { int lo = 0, hi = P.nseg - 1;\n";
+    os << "          while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= tile) lo = mid; else hi = mid - 1; }\n";
+    os << "          s0 = P.seg[3 * lo]; s1 = P.seg[3 * lo + 1];\n";
+    os << "          r0 = (s0 & ~" << (L.T - 1) << "LL) + (tile - P.seg[3 * lo + 2]) * " << L.T << " + warp * 128 + lane * 4; }\n";
+    os << "        const unsigned char* st = vq_smem + stage * " << L.stage_bytes << ";\n";
+    os << "        const int so = warp * 128 + lane * 4;\n";
+    for (int c : cols) {
+        const Column& col = t->cols[c];
+        std::string C = std::to_string(c);
+        const char* ty = "unsigned";
+        const char* fn = "vq_sld4_u32";
+        switch (col.type) {
+            case VEXQ_TYPE_INT64: ty = "long long"; fn = "vq_sld4_i64"; break;
+            case VEXQ_TYPE_FLOAT64: ty = "double"; fn = "vq_sld4_f64"; break;
+            case VEXQ_TYPE_DATE: ty = "int"; fn = "vq_sld4_i32"; break;
+            case VEXQ_TYPE_BOOL: ty = "unsigned"; fn = "vq_sld4_u8"; break;
+        }
+        os << "        " << ty << " cv" << C << "[4]; " << fn << "(st + " << L.off.at(c) << ", so, cv" << C << ");\n";
+        if (col.nullable) os << "        const unsigned cm" << C << " = vq_sbits4(st + " << L.voff.at(c) << ", so);\n";
+    }
+}
+
+void staged_loop_close(std::ostringstream& os, const StageLayout& L, const std::string& issue) {
+    os << "        __syncthreads();\n";
+    os << "        if (threadIdx.x == 0) {\n";
+    os << "            const long long nt = tile + (long long)" << L.S << " * gridDim.x;\n";
+    os << "            if (nt < P.nchunks) { vq_fence_proxy_async(); " << issue << "(P, vq_smem, vq_full, stage, nt); }\n";
+    os << "        }\n    }\n";
+    // on a timeout: flag it, then wait (bounded) for the copies still in flight
+    os << "    if (vq_timeout && threadIdx.x == 0) {\n";
+    os << "        atomicOr(P.error, 8);\n";
+    os << "        for (int k = 0; k < " << L.S << "; k++) {\n";
+    os << "            const long long j = it + k, tl = blockIdx.x + j * gridDim.x;\n";
+    os << "            if (tl < P.nchunks) vq_mbar_wait(&vq_full[j % " << L.S << "], (unsigned)((j / " << L.S << ") & 1), 1 << 20);\n";
+    os << "        }\n    }\n";
+}
+
 // Closes the pipelined loop: the prefetched chunk becomes the current one.
 void chunk_loop_close(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
     if (!p.pipeline) {
@@ -1126,6 +1319,37 @@ void chunk_loop_close(std::ostringstream& os, const Plan& p, const Table* t, con
     os << "        s0 = ns0; s1 = ns1; r0 = nr0;\n    }\n";
 }
 
+
+// Loop skeleton used by every scan kernel: TMA-staged tiles (default) or the
+// register-prefetch chunk loop.
+struct ScanLoop {
+    const Plan& p;
+    const Table* t;
+    std::set<int> cols;
+    StageLayout L;
+    std::string issue;
+    bool staged;
+    ScanLoop(const Plan& pp, const Table* tt, const std::set<int>& cc, int block, const std::string& name)
+        : p(pp), t(tt), cols(cc), staged(pp.staged) {
+        int budget = pp.stage_budget > 0 ? pp.stage_budget : (block >= 256 ? 160 * 1024 : 96 * 1024);
+        L = stage_layout(t, cols, block, budget);
+        issue = "vq_issue_" + name;
+    }
+    int tile_rows() const { return staged ? L.T : 128; }
+    int smem() const { return staged ? L.S * L.stage_bytes : 0; }
+    void prologue(std::ostringstream& os) const {
+        if (staged) emit_issue_fn(os, t, cols, L, issue);
+    }
+    void open(std::ostringstream& os) const {
+        if (staged) staged_loop_open(os, t, cols, L, issue);
+        else chunk_loop_open(os, p, t, cols);
+    }
+    void close(std::ostringstream& os) const {
+        if (staged) staged_loop_close(os, L, issue);
+        else chunk_loop_close(os, p, t, cols);
+    }
+};
+
 }  // namespace
 
 // Generates the aggregate scan kernel (table → filter → project → aggregate).
@@ -1135,16 +1359,23 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     collect_cols(p, p.pred, cols);
     for (int k : key_nodes) collect_cols(p, k, cols);
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    ScanLoop loop(p, p.t, cols, block, "agg");
+    p.tile = loop.tile_rows();
+    p.smem = loop.smem();
+    loop.prologue(os);
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    chunk_loop_open(os, p, p.t, cols);
+    loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
-    os << "            if (r < s0 || r >= s1) continue;\n";
+    bool warp_sync = p.path != AggPath::Regs;  // atomic paths aggregate across the warp
+    if (warp_sync) os << "            bool live = r >= s0 && r < s1;\n";
+    else os << "            if (r < s0 || r >= s1) continue;\n";
     Gen g(p, os);
     if (p.pred >= 0) {
         g.emit(p.pred);
-        os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
+        if (warp_sync) os << "            live = live && x" << p.pred << " && ok" << p.pred << ";\n";
+        else os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
     }
     for (int k : key_nodes) g.emit(k);
     for (auto& s : p.slots) if (s.input >= 0) g.emit(s.input);
@@ -1152,9 +1383,9 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     emit_slot_values(os, p, "            ");
     std::string order = order_expr(p, "r");
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "            ", order);
-    else emit_atomic_update(os, p, "            ", order);
+    else emit_atomic_update_warp(os, p, "            ", order);
     os << "        }\n";
-    chunk_loop_close(os, p, p.t, cols);
+    loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
     return os.str();
@@ -1167,8 +1398,12 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     std::set<int> cols;
     collect_cols(p, p.bpred, cols);
     collect_cols(p, key_node, cols);
+    ScanLoop loop(p, p.bt, cols, block, "build");
+    p.btile = loop.tile_rows();
+    p.bsmem = loop.smem();
+    loop.prologue(os);
     os << kernel_head("vq_build", block);
-    chunk_loop_open(os, p, p.bt, cols);
+    loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -1189,7 +1424,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
-    chunk_loop_close(os, p, p.bt, cols);
+    loop.close(os);
     os << "}\n";
     return os.str();
 }
@@ -1205,9 +1440,13 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     collect_cols(p, p.resid, cols);
     for (int k : key_nodes) collect_cols(p, k, cols);
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    ScanLoop loop(p, p.t, cols, block, "probe");
+    p.tile = loop.tile_rows();
+    p.smem = loop.smem();
+    loop.prologue(os);
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    chunk_loop_open(os, p, p.t, cols);
+    loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -1240,7 +1479,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
     else emit_atomic_update(os, p, "                ", order);
     os << "            }\n        }\n";
-    chunk_loop_close(os, p, p.t, cols);
+    loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
     return os.str();
@@ -1275,15 +1514,18 @@ static void choose_tunables(Plan& p) {
     int64_t acc = p.path == AggPath::Regs ? p.domain * (int64_t)(p.slots.size() + 1) : 0;
     p.block = acc > 24 ? 128 : 256;
     p.pipeline = true;
+    p.staged = true;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
         auto get = [&](const char* k) -> int {
             size_t at = s.find(k);
             return at == std::string::npos ? -1 : std::atoi(s.c_str() + at + std::strlen(k));
         };
-        int b = get("block="), pl = get("pipeline=");
+        int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb=");
         if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
         if (pl >= 0) p.pipeline = pl != 0;
+        if (st >= 0) p.staged = st != 0;
+        if (sb > 0) p.stage_budget = sb * 1024;
     }
 }
 
@@ -1309,10 +1551,11 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     std::ostringstream ex;
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
-       << " block=" << p.block << " pipeline=" << p.pipeline;
+       << " block=" << p.block << (p.staged ? " staged=tma" : p.pipeline ? " pipeline=1" : " pipeline=0")
+       << " tile=" << p.tile << " smem=" << p.smem;
     p.explain = ex.str();
-    p.k_main = jit_get(p.src_main, "vq_agg", p.block);
-    if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock);
+    p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
+    if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);
     // device-side tables of the plan
     if (!p.sets.empty()) {
         size_t tot = 0;
@@ -1529,8 +1772,13 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     std::ostringstream os;
     std::set<int> cols;
     collect_cols(*p, p->pred, cols);
-    os << prelude_source() << "\n" << kernel_head("vq_filter", kBlock);
-    chunk_loop_open(os, *p, t, cols);
+    ScanLoop loop(*p, t, cols, kBlock, "filter");
+    p->tile = loop.tile_rows();
+    p->smem = loop.smem();
+    os << prelude_source() << "\n";
+    loop.prologue(os);
+    os << kernel_head("vq_filter", kBlock);
+    loop.open(os);
     os << "        unsigned nib = 0u;\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
@@ -1548,10 +1796,10 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     os << "            atomicOr(reinterpret_cast<unsigned*>(P.acc_i) + wi, word);\n";
     os << "            atomicAdd(P.ngroups, (unsigned long long)__popc(word));\n";
     os << "        }\n";
-    chunk_loop_close(os, *p, t, cols);
+    loop.close(os);
     os << "}\n";
     p->src_main = os.str();
-    p->k_main = jit_get(p->src_main, "vq_filter", kBlock);
+    p->k_main = jit_get(p->src_main, "vq_filter", kBlock, p->smem);
     if (!p->sets.empty()) {
         size_t tot = 0;
         for (auto& st : p->sets) tot += st.size();
@@ -1649,8 +1897,9 @@ static bool zone_rec(const Plan& p, int idx, const Table& t, int rg) {
 
 bool zone_eval(const Plan& p, int root, const Table& t, int rg) { return root < 0 ? true : zone_rec(p, root, t, rg); }
 
-ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_start, int rg_end) {
+ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_start, int rg_end, int unit) {
     ScanSegs s;
+    const long long U = unit;
     long long chunks = 0;
     int rg = rg_start;
     while (rg < rg_end) {
@@ -1662,8 +1911,8 @@ ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_
             s.seg.push_back(a);
             s.seg.push_back(b);
             s.seg.push_back(chunks);
-            long long base = a & ~127LL;
-            chunks += (b - base + 127) / 128;
+            long long base = a & ~(U - 1);
+            chunks += (b - base + U - 1) / U;
             s.rows += b - a;
         }
         rg = e;

@@ -252,3 +252,71 @@ __device__ __forceinline__ double vq_fcomb(int kind, double a, double b) {
 __device__ __forceinline__ vq_i64 vq_icomb(int kind, vq_i64 a, vq_i64 b) {
     return kind == 1 ? (b < a ? b : a) : kind == 2 ? (b > a ? b : a) : (vq_i64)((vq_u64)a + (vq_u64)b);
 }
+
+// ---- bulk asynchronous copies (TMA, untiled) into a shared-memory ring ----
+// One thread issues cp.async.bulk copies of a tile's column slices into a
+// stage and arms the stage's mbarrier with the byte count; consumers wait on
+// the barrier's phase. Addresses and sizes are multiples of 16 bytes (tiles
+// start on 512-row boundaries of 256-byte aligned columns). No multicast.
+__device__ __forceinline__ unsigned vq_smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void vq_mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(vq_smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void vq_fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void vq_fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void vq_mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(vq_smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void vq_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(vq_smem_addr(dst)), "l"(src), "r"(bytes), "r"(vq_smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool vq_mbar_try_wait(unsigned long long* bar, unsigned phase) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(vq_smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls and reports false (the caller
+// raises the kernel's error flag and leaves the tile loop).
+__device__ __forceinline__ bool vq_mbar_wait(unsigned long long* bar, unsigned phase, int limit) {
+    for (int n = 0; n < limit; n++)
+        if (vq_mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+// Four consecutive rows from a staged shared-memory slice (row offset o % 4 == 0).
+__device__ __forceinline__ void vq_sld4_i64(const unsigned char* s, int o, vq_i64* v) {
+    const longlong2* q = reinterpret_cast<const longlong2*>(s) + (o >> 1);
+    longlong2 a = q[0], b = q[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void vq_sld4_f64(const unsigned char* s, int o, double* v) {
+    const double2* q = reinterpret_cast<const double2*>(s) + (o >> 1);
+    double2 a = q[0], b = q[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void vq_sld4_i32(const unsigned char* s, int o, int* v) {
+    int4 a = reinterpret_cast<const int4*>(s)[o >> 2];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void vq_sld4_u32(const unsigned char* s, int o, unsigned* v) {
+    uint4 a = reinterpret_cast<const uint4*>(s)[o >> 2];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void vq_sld4_u8(const unsigned char* s, int o, unsigned* v) {
+    unsigned w = reinterpret_cast<const unsigned*>(s)[o >> 2];
+    v[0] = w & 0xFF; v[1] = (w >> 8) & 0xFF; v[2] = (w >> 16) & 0xFF; v[3] = w >> 24;
+}
+__device__ __forceinline__ unsigned vq_sbits4(const unsigned char* s, int o) {
+    return (s[o >> 3] >> (o & 7)) & 0xFu;
+}

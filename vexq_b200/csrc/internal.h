@@ -111,9 +111,10 @@ struct JitKernel {
     std::shared_ptr<JitModule> mod;
     void* fn = nullptr;  // CUfunction
     int block = 256;
+    int smem = 0;        // dynamic shared memory bytes
     int max_blocks_per_sm = 0;
 };
-JitKernel jit_get(const std::string& source, const std::string& entry, int block);
+JitKernel jit_get(const std::string& source, const std::string& entry, int block, int smem = 0);
 void jit_launch(const JitKernel& k, int grid, const void* params, size_t params_size, cudaStream_t s);
 std::string jit_cache_dir();
 

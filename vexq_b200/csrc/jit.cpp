@@ -32,6 +32,7 @@ struct Driver {
     PFN_cuModuleGetFunction_v2000 get = nullptr;
     PFN_cuLaunchKernel_v7000_ptsz launch = nullptr;
     PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor_v6050 occ = nullptr;
+    PFN_cuFuncSetAttribute_v9000 setattr = nullptr;
     bool ok = false;
 };
 
@@ -45,7 +46,8 @@ Driver& drv() {
         };
         d.ok = get("cuModuleLoadData", (void**)&d.load) && get("cuModuleUnload", (void**)&d.unload) &&
                get("cuModuleGetFunction", (void**)&d.get) && get("cuLaunchKernel", (void**)&d.launch) &&
-               get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&d.occ);
+               get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&d.occ) &&
+               get("cuFuncSetAttribute", (void**)&d.setattr);
     });
     if (!d.ok) fail(VEXQ_EDEVICE, "CUDA driver entry points unavailable");
     return d;
@@ -140,7 +142,7 @@ std::string jit_cache_dir() {
 
 // Compiles (or fetches) the cubin for `source`; loading on the device
 // happens on first use in the calling thread's current device.
-JitKernel jit_get(const std::string& source, const std::string& entry, int block) {
+JitKernel jit_get(const std::string& source, const std::string& entry, int block, int smem) {
     uint64_t h = fnv1a(source) ^ (fnv1a(entry) * 31);
     for (const char* o : kOptions) h = h * 1099511628211ull ^ fnv1a(o);
     std::vector<char> cubin;
@@ -156,6 +158,7 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     }
     JitKernel k;
     k.block = block;
+    k.smem = smem;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return k;  // no device: compile-only
     int ndev = 0;
@@ -180,8 +183,12 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     if (r != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuModuleGetFunction failed for " + entry);
     k.mod = m;
     k.fn = (void*)f;
+    if (smem > 48 * 1024) {
+        CUresult ra = d.setattr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem);
+        if (ra != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuFuncSetAttribute(max dynamic smem) failed: " + std::to_string((int)ra));
+    }
     int nb = 0;
-    if (d.occ(&nb, f, block, 0) == CUDA_SUCCESS) k.max_blocks_per_sm = nb;
+    if (d.occ(&nb, f, block, (size_t)smem) == CUDA_SUCCESS) k.max_blocks_per_sm = nb;
     return k;
 }
 
@@ -190,7 +197,7 @@ void jit_launch(const JitKernel& k, int grid, const void* params, size_t params_
     if (!k.fn) fail(VEXQ_EDEVICE, "kernel not loaded (no CUDA device)");
     Driver& d = drv();
     void* args[] = {const_cast<void*>(params)};
-    CUresult r = d.launch((CUfunction)k.fn, grid, 1, 1, k.block, 1, 1, 0, (CUstream)s, args, nullptr);
+    CUresult r = d.launch((CUfunction)k.fn, grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)s, args, nullptr);
     if (r != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuLaunchKernel failed: " + std::to_string((int)r));
 }
 

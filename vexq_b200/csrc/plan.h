@@ -113,6 +113,10 @@ struct Plan {
     // tunables of the generated scan kernel (chosen at compile time)
     int block = 256;
     bool pipeline = true;
+    bool staged = true;        // TMA bulk-copy staging of row tiles into shared memory
+    int stage_budget = 0;      // bytes of the stage ring per block (0: default)
+    int tile = 128, smem = 0;  // main kernel: rows per loop unit, dynamic shared memory
+    int btile = 128, bsmem = 0;  // join build kernel
     // per-run caches (host-side overhead of a run)
     std::vector<long long> seg_cache;      // last uploaded segment list
     DevBuf d_seg;
@@ -141,7 +145,7 @@ Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d);
 Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d);
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred);
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
-ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end);
+ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end, int unit);
 bool parse_date(const char* s, int64_t* days);
 
 }  // namespace vq

@@ -27,35 +27,61 @@ __global__ void k_fill_u64(unsigned long long* p, long long n, unsigned long lon
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }
 
-// Register path: merges per-block partials in block order. Float sums use a
-// compensated (TwoSum) accumulator so the merge adds no rounding of its own.
-__global__ void k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
-                             const int* fkind, const int* ikind, double* out_f, long long* out_i) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int totf = G * nf, toti = G * (ni + 1);
-    if (t < totf) {
-        int s = t % nf;
-        int kind = fkind[s];
-        double hi = part_f[t], lo = 0.0;
-        for (int b = 1; b < nblocks; b++) {
-            double x = part_f[(long long)b * totf + t];
-            if (kind == 0) {
-                double sum = hi + x;
-                double bb = sum - hi;
-                lo += (hi - (sum - bb)) + (x - bb);
-                hi = sum;
-            } else {
-                hi = vq_fcomb(kind, hi, x);
-            }
+// Register path: merges the per-block partials. One block per output entry;
+// each thread folds a fixed stride of blocks, then a fixed-shape shared-memory
+// tree combines the threads, so the result does not depend on scheduling.
+// Float sums carry a (hi, lo) compensated pair through both stages.
+__device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
+    double s = hi + x;
+    double bb = s - hi;
+    lo += (hi - (s - bb)) + (x - bb);
+    hi = s;
+}
+
+__global__ void __launch_bounds__(256) k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G,
+                                                    int nf, int ni, const int* fkind, const int* ikind, double* out_f,
+                                                    long long* out_i) {
+    __shared__ double sh[256], sl[256];
+    __shared__ long long si[256];
+    const int e = blockIdx.x, t = threadIdx.x;
+    const int totf = G * nf, toti = G * (ni + 1);
+    if (e < totf) {
+        const int kind = fkind[e % nf];
+        double hi = kind == 1 ? 1.7976931348623157e308 : kind == 2 ? -1.7976931348623157e308 : 0.0, lo = 0.0;
+        for (int b = t; b < nblocks; b += blockDim.x) {
+            const double x = part_f[(long long)b * totf + e];
+            if (kind == 0) vq_two_sum(hi, lo, x);
+            else hi = vq_fcomb(kind, hi, x);
         }
-        out_f[t] = kind == 0 ? hi + lo : hi;
-    } else if (t < totf + toti) {
-        int u = t - totf;
-        int s = u % (ni + 1);
-        int kind = ikind[s];
-        long long v = part_i[u];
-        for (int b = 1; b < nblocks; b++) v = vq_icomb(kind, v, part_i[(long long)b * toti + u]);
-        out_i[u] = v;
+        sh[t] = hi;
+        sl[t] = lo;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (t < o) {
+                if (kind == 0) {
+                    double h = sh[t], l = sl[t] + sl[t + o];
+                    vq_two_sum(h, l, sh[t + o]);
+                    sh[t] = h;
+                    sl[t] = l;
+                } else {
+                    sh[t] = vq_fcomb(kind, sh[t], sh[t + o]);
+                }
+            }
+            __syncthreads();
+        }
+        if (t == 0) out_f[e] = kind == 0 ? sh[0] + sl[0] : sh[0];
+    } else if (e < totf + toti) {
+        const int u = e - totf;
+        const int kind = ikind[u % (ni + 1)];
+        long long v = kind == 1 ? 0x7FFFFFFFFFFFFFFFLL : kind == 2 ? (-0x7FFFFFFFFFFFFFFFLL - 1) : 0LL;
+        for (int b = t; b < nblocks; b += blockDim.x) v = vq_icomb(kind, v, part_i[(long long)b * toti + u]);
+        si[t] = v;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (t < o) si[t] = vq_icomb(kind, si[t], si[t + o]);
+            __syncthreads();
+        }
+        if (t == 0) out_i[u] = si[0];
     }
 }
 
@@ -229,9 +255,12 @@ double vq_fkey_inv_host(uint64_t k) {
 
 namespace {
 
-int grid_for(const JitKernel& k, long long nchunks) {
+// Grid of a scan kernel: every SM filled to its occupancy, never more blocks
+// than loop units (staged kernels: one tile per block per iteration; chunk
+// loops: one 128-row chunk per warp).
+int grid_for(const JitKernel& k, long long units, bool staged) {
     int per_sm = std::max(1, k.max_blocks_per_sm);
-    long long want = (nchunks + (k.block / 32) - 1) / (k.block / 32);
+    long long want = staged ? units : (units + (k.block / 32) - 1) / (k.block / 32);
     long long g = std::min<long long>((long long)sm_count() * per_sm, want);
     return (int)std::max<long long>(g, 1);
 }
@@ -333,7 +362,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     Groups g;
     int G = (int)p.domain, nf = p.nf, ni = p.ni;
     int nfb = std::max(nf, 1);
-    int grid = grid_for(p.k_main, nchunks);
+    int grid = grid_for(p.k_main, nchunks, p.staged);
     size_t pf = (size_t)grid * G * nfb, pi = (size_t)grid * G * (ni + 1);
     p.scratch_a.ensure(pf * 8);
     p.scratch_b.ensure(pi * 8);
@@ -352,21 +381,24 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     }
     const int* d_kinds = p.d_kinds.as<int>();
     size_t nout_f = (size_t)G * nfb * 8, nout_i = (size_t)G * (ni + 1) * 8;
-    p.scratch_c.ensure(nout_f + nout_i);
+    p.scratch_c.ensure(nout_f + nout_i + 16);
     double* out_f = p.scratch_c.as<double>();
     long long* out_i = (long long*)((char*)p.scratch_c.p + nout_f);
-    p.h_stage.ensure(nout_f + nout_i);
+    P.error = (int*)((char*)p.scratch_c.p + nout_f + nout_i);
+    p.h_stage.ensure(nout_f + nout_i + 16);
     ensure_events(p);
+    VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
     VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
     int tot = G * nf + G * (ni + 1);
-    k_merge_regs<<<(tot + 127) / 128, 128, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + nfb,
-                                                     out_f, out_i);
+    k_merge_regs<<<tot, 256, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + nfb, out_f, out_i);
     VQ_CUDA(cudaGetLastError());
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
-    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
+    if (*(const int*)((const char*)p.h_stage.p + nout_f + nout_i) & 8)
+        fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
     rc.scan_ms += elapsed(p.ev[0], p.ev[1]);
     rc.kernel_ms += elapsed(p.ev[0], p.ev[2]);
     rc.launches += 2;
@@ -451,7 +483,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
         k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
         VQ_CUDA(cudaGetLastError());
-        int grid = grid_for(p.k_main, nchunks);
+        int grid = grid_for(p.k_main, nchunks, p.staged);
         VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
         jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
         VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
@@ -469,6 +501,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         rc.launches += 3;
         unsigned long long nn = *(unsigned long long*)p.h_stage.p;
         int herr = *(int*)((char*)p.h_stage.p + 8);
+        if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
         if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
         if (herr & 1) {  // probe limit: grow the table and rerun
             if (!hash) fail(VEXQ_EDEVICE, "dense group table reported a probe failure");
@@ -776,7 +809,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         Table& bt = *p.bt;
         // ---- build phase ----
         std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
-        ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg);
+        ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
         long long jcap = 16;
         while (jcap < 2 * std::max<long long>(bs.rows, 8)) jcap <<= 1;
         VQParams B;
@@ -817,7 +850,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             k_fill_u64<<<ig, 256, 0, rc.s>>>(B.jkeys, jcap, VQ_EMPTY_KEY);
             VQ_CUDA(cudaMemsetAsync(B.jkeys + jcap, 0, 8, rc.s));
             B.mode = 0;
-            int grid = grid_for(p.k_build, bs.nchunks);
+            int grid = grid_for(p.k_build, bs.nchunks, p.staged);
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
             int nb = (int)((nslots + 4095) / 4096);
             k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);
@@ -833,6 +866,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
             rc.kernel_ms += tm.stop();
             rc.launches += 7;
+            if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");
             join_keys = (long long)nk;
         }
@@ -858,7 +892,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         }
     }
     std::vector<uint8_t> m = prune_mask(p, t, p.zn_pred, rgs, rge);
-    ScanSegs ss = make_segments(t, m, rgs, rge);
+    ScanSegs ss = make_segments(t, m, rgs, rge, p.tile);
     set_columns(P, t, false);
     if (ss.seg != p.seg_cache || !p.d_seg.p) {  // segment list uploaded once per distinct pruning
         p.d_seg.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
@@ -872,13 +906,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     P.n_rg = t.n_rg;
     P.present = p.d_present.as<unsigned char>();
     for (size_t i = 0, off = 0; i < p.sets.size(); i++) { P.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
-    if (!P.error && p.path == AggPath::Regs) {
-        if (!p.scratch_f.p) {
-            p.scratch_f.alloc(64);
-            VQ_CUDA(cudaMemset(p.scratch_f.p, 0, 64));
-        }
-        P.error = p.scratch_f.as<int>();  // unused by the register path
-    }
+
     bytes += scanned_bytes(p, t, ss.rows, false);
     rows_scanned += ss.rows;
     vexq_result_s* r;
