@@ -994,6 +994,34 @@ void emit_regs_update(std::ostringstream& os, const Plan& p, const std::string& 
     os << ind << "default: break;\n" << ind << "}\n";
 }
 
+// Branch-free register update: every group's accumulators are updated with a
+// select on (gid == g), so the four rows a lane holds form independent
+// dependency chains the scheduler can interleave (a switch serialises them).
+void emit_regs_update_pred(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
+    os << ind << "const long long ord = " << order << ";\n";
+    for (int64_t g = 0; g < p.domain; g++) {
+        std::string G = std::to_string(g);
+        os << ind << "{ const bool h = key == " << g << "ull;\n";
+        std::string in = ind + "  ";
+        os << in << "fo" << G << " = (h && ord < fo" << G << ") ? ord : fo" << G << ";\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string a = acc_name(p, (int)g, (int)s), S = std::to_string(s);
+            switch (p.slots[s].kind) {
+                case S_CNT: os << in << a << " += h ? 1LL : 0LL;\n"; break;
+                case S_NN: os << in << a << " += (h && sok" << S << ") ? 1LL : 0LL;\n"; break;
+                case S_ISUM: os << in << a << " = (long long)((unsigned long long)" << a << " + (unsigned long long)((h && sok" << S
+                                << ") ? sv" << S << " : 0LL));\n"; break;
+                case S_IMIN: os << in << "if (h && sok" << S << " && sv" << S << " < " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_IMAX: os << in << "if (h && sok" << S << " && sv" << S << " > " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_FSUM: os << in << a << " += (h && sok" << S << ") ? sv" << S << " : 0.0;\n"; break;
+                case S_FMIN: os << in << "if (h && sok" << S << " && sv" << S << " < " << a << ") " << a << " = sv" << S << ";\n"; break;
+                case S_FMAX: os << in << "if (h && sok" << S << " && sv" << S << " > " << a << ") " << a << " = sv" << S << ";\n"; break;
+            }
+        }
+        os << ind << "}\n";
+    }
+}
+
 // Block reduction of the register accumulators into per-block partials.
 void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
     int warps = block / 32;
@@ -1071,6 +1099,110 @@ void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string
     }
 }
 
+// Block-private shared-memory accumulators for the dense path: groups below
+// smem_groups are updated with shared-memory atomics and flushed to the global
+// table once per block; the layout is [first][int bank][fixed-point digits][flags].
+struct CacheLayout {
+    int C = 0;
+    std::string first, ints, fx, sp;
+};
+CacheLayout cache_layout(const Plan& p) {
+    CacheLayout L;
+    L.C = p.smem_groups;
+    std::string C = std::to_string(L.C);
+    L.first = "((long long*)vq_smem)";
+    L.ints = "(((long long*)vq_smem) + " + C + ")";
+    L.fx = "(((long long*)vq_smem) + " + std::to_string((long long)L.C * (1 + p.ni)) + ")";
+    L.sp = "((unsigned*)(((long long*)vq_smem) + " + std::to_string((long long)L.C * (1 + p.ni + 4 * p.nf)) + "))";
+    return L;
+}
+int cache_bytes(const Plan& p) { return p.smem_groups * (8 + 8 * p.ni + 36 * p.nf); }
+
+// Opens "if (slot < C) { shared-memory update } else {" — the caller emits the
+// global update and closes the brace.
+void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string& ind) {
+    CacheLayout L = cache_layout(p);
+    std::string C = std::to_string(L.C);
+    os << ind << "if (slot < " << C << "ull) {\n";
+    std::string in = ind + "    ";
+    os << in << "atomicMin(" << L.first << " + slot, ag_first);\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s), pos = std::to_string(p.slot_pos[s]);
+        std::string ai = L.ints + " + " + pos + " * " + C + " + slot";
+        std::string aiu = "(unsigned long long*)(" + ai + ")";
+        switch (p.slots[s].kind) {
+            case S_CNT:
+            case S_NN: os << in << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_ISUM: os << in << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_IMIN: os << in << "if (ah" << S << ") atomicMin(" << ai << ", ag" << S << ");\n"; break;
+            case S_IMAX: os << in << "if (ah" << S << ") atomicMax(" << ai << ", ag" << S << ");\n"; break;
+            case S_FMIN: os << in << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FMAX: os << in << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FSUM:
+                os << in << "if (ah" << S << ") vq_fx_add<true>(" << L.fx << " + (" << pos << " * " << C << " + (long long)slot) * 4, ag"
+                   << S << ", " << p.fx_lsb[p.slot_pos[s]] << ", " << L.sp << " + " << pos << " * " << C << " + slot, P.error);\n";
+                break;
+        }
+    }
+    os << ind << "} else {\n";
+}
+
+void emit_cache_init(std::ostringstream& os, const Plan& p) {
+    CacheLayout L = cache_layout(p);
+    std::string C = std::to_string(L.C);
+    os << "    extern __shared__ __align__(16) unsigned char vq_smem[];\n";
+    os << "    for (int i = threadIdx.x; i < " << C << "; i += blockDim.x) {\n";
+    os << "        " << L.first << "[i] = 0x7FFFFFFFFFFFFFFFLL;\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        const Slot& sl = p.slots[s];
+        if (sl.kind == S_FSUM) {
+            std::string pos = std::to_string(p.slot_pos[s]);
+            os << "        for (int d = 0; d < 4; d++) " << L.fx << "[(" << pos << " * " << C << " + i) * 4 + d] = 0;\n";
+            os << "        " << L.sp << "[" << pos << " * " << C << " + i] = 0u;\n";
+            continue;
+        }
+        std::string init = "0LL";
+        if (sl.kind == S_IMIN) init = "0x7FFFFFFFFFFFFFFFLL";
+        if (sl.kind == S_IMAX) init = "(-0x7FFFFFFFFFFFFFFFLL - 1LL)";
+        if (sl.kind == S_FMIN) init = "(long long)vq_fkey(1.7976931348623157e308)";
+        if (sl.kind == S_FMAX) init = "(long long)vq_fkey(-1.7976931348623157e308)";
+        os << "        " << L.ints << "[" << p.slot_pos[s] << " * " << C << " + i] = " << init << ";\n";
+    }
+    os << "    }\n    __syncthreads();\n";
+}
+
+void emit_cache_flush(std::ostringstream& os, const Plan& p) {
+    CacheLayout L = cache_layout(p);
+    std::string C = std::to_string(L.C);
+    os << "    __syncthreads();\n";
+    os << "    for (int i = threadIdx.x; i < " << C << "; i += blockDim.x) {\n";
+    os << "        if (" << L.ints << "[" << p.slot_pos[0] << " * " << C << " + i] == 0) continue;\n";
+    os << "        const long long stride = (long long)P.cap + 1;\n";
+    os << "        atomicMin(&P.first[i], " << L.first << "[i]);\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        int pos = p.slot_pos[s];
+        std::string P_ = std::to_string(pos);
+        std::string v = L.ints + "[" + P_ + " * " + C + " + i]";
+        std::string g = "P.acc_i[" + P_ + " * stride + i]";
+        switch (p.slots[s].kind) {
+            case S_CNT:
+            case S_NN:
+            case S_ISUM: os << "        if (" << v << ") atomicAdd((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
+            case S_IMIN: os << "        atomicMin(&" << g << ", " << v << ");\n"; break;
+            case S_IMAX: os << "        atomicMax(&" << g << ", " << v << ");\n"; break;
+            case S_FMIN: os << "        atomicMin((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
+            case S_FMAX: os << "        atomicMax((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
+            case S_FSUM:
+                os << "        for (int d = 0; d < 4; d++) { const long long x = " << L.fx << "[(" << P_ << " * " << C
+                   << " + i) * 4 + d]; if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_ << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
+                os << "        if (" << L.sp << "[" << P_ << " * " << C << " + i]) atomicOr(&P.special[" << P_ << " * stride + i], "
+                   << L.sp << "[" << P_ << " * " << C << " + i]);\n";
+                break;
+        }
+    }
+    os << "    }\n";
+}
+
 // Atomic path with warp aggregation: lanes whose rows fall into the same
 // group are folded in lane order (shuffles among the __match_any_sync peers)
 // and only the lowest such lane updates the group table. Float sums of a peer
@@ -1129,6 +1261,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     os << in << "}\n";
     os << in << "if (lead) {\n";
     std::string in3 = in + "    ";
+    if (p.smem_groups > 0) emit_cache_update(os, p, in3);
     os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s);
@@ -1149,6 +1282,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
                 break;
         }
     }
+    if (p.smem_groups > 0) os << in3 << "}\n";  // closes the global branch opened by emit_cache_update
     os << in << "}\n" << ind << "}\n";
 }
 
@@ -1361,10 +1495,11 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
     ScanLoop loop(p, p.t, cols, block, "agg");
     p.tile = loop.tile_rows();
-    p.smem = loop.smem();
+    p.smem = p.smem_groups > 0 ? cache_bytes(p) : loop.smem();
     loop.prologue(os);
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    if (p.smem_groups > 0) emit_cache_init(os, p);
     loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
@@ -1382,11 +1517,16 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     emit_key(os, p, key_nodes, "            ");
     emit_slot_values(os, p, "            ");
     std::string order = order_expr(p, "r");
-    if (p.path == AggPath::Regs) emit_regs_update(os, p, "            ", order);
-    else emit_atomic_update_warp(os, p, "            ", order);
+    if (p.path == AggPath::Regs) {
+        if (p.regs_pred) emit_regs_update_pred(os, p, "            ", order);
+        else emit_regs_update(os, p, "            ", order);
+    } else {
+        emit_atomic_update_warp(os, p, "            ", order);
+    }
     os << "        }\n";
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
+    if (p.smem_groups > 0) emit_cache_flush(os, p);
     os << "}\n";
     return os.str();
 }
@@ -1514,18 +1654,29 @@ static void choose_tunables(Plan& p) {
     int64_t acc = p.path == AggPath::Regs ? p.domain * (int64_t)(p.slots.size() + 1) : 0;
     p.block = acc > 24 ? 128 : 256;
     p.pipeline = true;
-    p.staged = true;
+    p.staged = false;  // measured: TMA staging is not faster for these scans yet
+    p.regs_pred = true;
+    int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
         auto get = [&](const char* k) -> int {
             size_t at = s.find(k);
             return at == std::string::npos ? -1 : std::atoi(s.c_str() + at + std::strlen(k));
         };
-        int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb=");
+        int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
+        if (rp >= 0) p.regs_pred = rp != 0;
+        int ck = get("cache_kb=");
+        if (ck >= 0) cache_kb = ck;
         if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
         if (pl >= 0) p.pipeline = pl != 0;
         if (st >= 0) p.staged = st != 0;
         if (sb > 0) p.stage_budget = sb * 1024;
+    }
+    p.smem_groups = 0;
+    if (p.path == AggPath::Dense && !p.is_join && cache_kb > 0) {
+        int per = 8 + 8 * p.ni + 36 * p.nf;
+        p.smem_groups = (int)std::min<int64_t>(p.domain, (int64_t)cache_kb * 1024 / per);
+        p.staged = false;  // the cache owns the dynamic shared memory
     }
 }
 
@@ -1552,7 +1703,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
        << " block=" << p.block << (p.staged ? " staged=tma" : p.pipeline ? " pipeline=1" : " pipeline=0")
-       << " tile=" << p.tile << " smem=" << p.smem;
+       << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups;
     p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
     if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);

@@ -183,7 +183,7 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     if (r != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuModuleGetFunction failed for " + entry);
     k.mod = m;
     k.fn = (void*)f;
-    if (smem > 48 * 1024) {
+    if (smem > 0) {  // static shared memory counts against the default 48 KB limit too
         CUresult ra = d.setattr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem);
         if (ra != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuFuncSetAttribute(max dynamic smem) failed: " + std::to_string((int)ra));
     }
