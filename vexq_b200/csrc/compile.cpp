@@ -802,7 +802,14 @@ void plan_keys(Plan& p) {
 void choose_path(Plan& p) {
     int regs_per_group = 1;  // first-occurrence key
     for (auto& s : p.slots) regs_per_group += 1;
-    if (p.domain > 0 && p.domain <= 16 && p.domain * regs_per_group <= 64) p.path = AggPath::Regs;
+    int max_groups = 16, max_acc = 64;
+    if (const char* e = std::getenv("VEXQ_TUNE")) {
+        const char* a = std::strstr(e, "regs_groups=");
+        if (a) max_groups = std::atoi(a + 12);
+        const char* b = std::strstr(e, "regs_acc=");
+        if (b) max_acc = std::atoi(b + 9);
+    }
+    if (p.domain > 0 && p.domain <= max_groups && p.domain * regs_per_group <= max_acc) p.path = AggPath::Regs;
     else if (p.domain > 0 && p.domain <= (int64_t(1) << 22)) p.path = AggPath::Dense;
     else p.path = AggPath::Hash;
     // bank layout
@@ -1217,8 +1224,13 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     os << ind << "const unsigned act = __ballot_sync(0xffffffffu, live);\n";
     os << ind << "if (live) {\n";
     os << in << "const long long stride = (long long)P.cap + 1;\n";
-    os << in << "const unsigned peers = __match_any_sync(act, slot);\n";
-    os << in << "const bool lead = (__ffs(peers) - 1) == lane;\n";
+    if (p.warp_agg) {
+        os << in << "const unsigned peers = __match_any_sync(act, slot);\n";
+        os << in << "const bool lead = (__ffs(peers) - 1) == lane;\n";
+    } else {
+        os << in << "const unsigned peers = 1u << lane; (void)act;\n";
+        os << in << "const bool lead = true;\n";
+    }
     os << in << "long long ag_first = " << order << ";\n";
     // per-slot aggregate registers
     for (size_t s = 0; s < p.slots.size(); s++) {
@@ -1234,7 +1246,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
             case S_FMAX: os << in << "unsigned long long ag" << S << " = 0ull; bool ah" << S << " = false;\n"; break;
         }
     }
-    os << in << "for (unsigned m = peers; m; m &= m - 1u) {\n";
+    os << in << "for (unsigned m = peers; m; m &= m - 1u) {  // peers fold in lane order\n";
     std::string in2 = in + "    ";
     os << in2 << "const int src = __ffs(m) - 1;\n";
     os << in2 << "ag_first = min(ag_first, (long long)__shfl_sync(peers, (long long)(" << order << "), src));\n";
@@ -1656,6 +1668,7 @@ static void choose_tunables(Plan& p) {
     p.pipeline = true;
     p.staged = false;  // measured: TMA staging is not faster for these scans yet
     p.regs_pred = true;
+    p.warp_agg = true;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -1665,8 +1678,9 @@ static void choose_tunables(Plan& p) {
         };
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
-        int ck = get("cache_kb=");
+        int ck = get("cache_kb="), wa = get("warp_agg=");
         if (ck >= 0) cache_kb = ck;
+        if (wa >= 0) p.warp_agg = wa != 0;
         if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
         if (pl >= 0) p.pipeline = pl != 0;
         if (st >= 0) p.staged = st != 0;
@@ -1703,7 +1717,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
        << " block=" << p.block << (p.staged ? " staged=tma" : p.pipeline ? " pipeline=1" : " pipeline=0")
-       << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups;
+       << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
     p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
     if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);

@@ -115,6 +115,7 @@ struct Plan {
     bool pipeline = true;
     bool staged = true;        // TMA bulk-copy staging of row tiles into shared memory
     bool regs_pred = true;     // register path: branch-free predicated updates
+    bool warp_agg = true;      // atomic path: fold lanes of one group before updating
     int smem_groups = 0;       // dense path: groups cached in block-private shared memory
     int stage_budget = 0;      // bytes of the stage ring per block (0: default)
     int tile = 128, smem = 0;  // main kernel: rows per loop unit, dynamic shared memory
