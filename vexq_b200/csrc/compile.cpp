@@ -828,9 +828,9 @@ void choose_path(Plan& p) {
             double m = x.bounded ? std::max(std::fabs(x.lo), std::fabs(x.hi)) : 0;
             if (!x.bounded) fail(VEXQ_ENOTSUP, "float sum over an unbounded expression (division by a range containing 0)");
             int e = 0;
-            while (std::ldexp(1.0, e) <= m && e < 1100) e++;
-            // |x| < 2^e; 97 fractional bits below the top keep 2^-44 relative exactness
-            // for every value within 2^-44 of the bound and the window holds 2^31 rows.
+            if (m > 0) std::frexp(m, &e);  // |x| <= m < 2^e
+            // values of magnitude ≥ 2^(e-45) keep every mantissa bit; the top 31
+            // bits of the 128-bit window hold sums of 2^31 rows
             p.fx_lsb[p.slot_pos[s]] = e - 97;
         }
     }
@@ -1132,7 +1132,10 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
     std::string C = std::to_string(L.C);
     os << ind << "if (slot < " << C << "ull) {\n";
     std::string in = ind + "    ";
-    os << in << "atomicMin(" << L.first << " + slot, ag_first);\n";
+    // MIN/MAX and first-row keys only ever move one way, so a plain read that
+    // shows no improvement (possibly stale, never past the true value) skips
+    // the atomic; most rows after the first few of a group skip it
+    os << in << "if (ag_first < " << L.first << "[slot]) atomicMin(" << L.first << " + slot, ag_first);\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s), pos = std::to_string(p.slot_pos[s]);
         std::string ai = L.ints + " + " + pos + " * " + C + " + slot";
@@ -1141,13 +1144,14 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
             case S_CNT:
             case S_NN: os << in << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
             case S_ISUM: os << in << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
-            case S_IMIN: os << in << "if (ah" << S << ") atomicMin(" << ai << ", ag" << S << ");\n"; break;
-            case S_IMAX: os << in << "if (ah" << S << ") atomicMax(" << ai << ", ag" << S << ");\n"; break;
-            case S_FMIN: os << in << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
-            case S_FMAX: os << in << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
+            case S_IMIN: os << in << "if (ah" << S << " && ag" << S << " < *(" << ai << ")) atomicMin(" << ai << ", ag" << S << ");\n"; break;
+            case S_IMAX: os << in << "if (ah" << S << " && ag" << S << " > *(" << ai << ")) atomicMax(" << ai << ", ag" << S << ");\n"; break;
+            case S_FMIN: os << in << "if (ah" << S << " && ag" << S << " < *" << aiu << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FMAX: os << in << "if (ah" << S << " && ag" << S << " > *" << aiu << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
             case S_FSUM:
-                os << in << "if (ah" << S << ") vq_fx_add<true>(" << L.fx << " + (" << pos << " * " << C << " + (long long)slot) * 4, ag"
-                   << S << ", " << p.fx_lsb[p.slot_pos[s]] << ", " << L.sp << " + " << pos << " * " << C << " + slot, P.error);\n";
+                os << in << "if (ah" << S << ") { vq_fx_add_digits<true>(" << L.fx << " + (" << pos << " * " << C
+                   << " + (long long)slot) * 4, fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
+                   << ") atomicOr(" << L.sp << " + " << pos << " * " << C << " + slot, fsp" << S << "); }\n";
                 break;
         }
     }
@@ -1211,10 +1215,12 @@ void emit_cache_flush(std::ostringstream& os, const Plan& p) {
 }
 
 // Atomic path with warp aggregation: lanes whose rows fall into the same
-// group are folded in lane order (shuffles among the __match_any_sync peers)
-// and only the lowest such lane updates the group table. Float sums of a peer
-// set are added in lane order before the exact fixed-point accumulation, so
-// the result is deterministic; its error is bounded by the ≤ 32-value folds.
+// group (__match_any_sync peers) are reduced with redux.sync and only the
+// lowest such lane updates the group table. Every reduction is exact and
+// order-free: counts and integer sums wrap in 64 bits, MIN/MAX compare order
+// keys, and float sums fold 128-bit fixed-point images of the values (the
+// same integers the single-row update would add). When no two lanes of the
+// warp share a group every lane updates its own row without reducing.
 void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
     const std::string in = ind + "    ";
     os << ind << "unsigned long long slot = VQ_NOSLOT;\n";
@@ -1225,50 +1231,93 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     os << ind << "if (live) {\n";
     os << in << "const long long stride = (long long)P.cap + 1;\n";
     if (p.warp_agg) {
-        os << in << "const unsigned peers = __match_any_sync(act, slot);\n";
+        os << in << "const unsigned peers = __match_any_sync(act, (unsigned)slot);\n";
         os << in << "const bool lead = (__ffs(peers) - 1) == lane;\n";
+        os << in << "const bool solo = __all_sync(act, peers == (1u << lane));\n";
     } else {
         os << in << "const unsigned peers = 1u << lane; (void)act;\n";
-        os << in << "const bool lead = true;\n";
+        os << in << "const bool lead = true, solo = true;\n";
     }
-    os << in << "long long ag_first = " << order << ";\n";
-    // per-slot aggregate registers
+    // per-lane fixed-point images of the float-sum inputs
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        if (p.slots[s].kind != S_FSUM) continue;
+        std::string S = std::to_string(s);
+        os << in << "unsigned fw" << S << "[4], fs" << S << " = 0u; fw" << S << "[0] = fw" << S << "[1] = fw" << S << "[2] = fw" << S
+           << "[3] = 0u;\n";
+        os << in << "if (sok" << S << ") vq_fx_words(sv" << S << ", " << p.fx_lsb[p.slot_pos[s]] << ", fw" << S << ", fs" << S
+           << ", P.error);\n";
+    }
+    os << in << "long long ag_first;\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s);
         switch (p.slots[s].kind) {
-            case S_CNT: os << in << "long long ag" << S << " = __popc(peers);\n"; break;
-            case S_NN: os << in << "long long ag" << S << " = __popc(__ballot_sync(peers, sok" << S << "));\n"; break;
-            case S_ISUM: os << in << "long long ag" << S << " = 0; bool ah" << S << " = false;\n"; break;
-            case S_IMIN: os << in << "long long ag" << S << " = 0x7FFFFFFFFFFFFFFFLL; bool ah" << S << " = false;\n"; break;
-            case S_IMAX: os << in << "long long ag" << S << " = (-0x7FFFFFFFFFFFFFFFLL - 1LL); bool ah" << S << " = false;\n"; break;
-            case S_FSUM: os << in << "double ag" << S << " = 0.0; bool ah" << S << " = false;\n"; break;
-            case S_FMIN: os << in << "unsigned long long ag" << S << " = 0xFFFFFFFFFFFFFFFFull; bool ah" << S << " = false;\n"; break;
-            case S_FMAX: os << in << "unsigned long long ag" << S << " = 0ull; bool ah" << S << " = false;\n"; break;
+            case S_CNT: case S_NN: os << in << "long long ag" << S << ";\n"; break;
+            case S_ISUM: case S_IMIN: case S_IMAX: os << in << "long long ag" << S << "; bool ah" << S << ";\n"; break;
+            case S_FMIN: case S_FMAX: os << in << "unsigned long long ag" << S << "; bool ah" << S << ";\n"; break;
+            case S_FSUM:
+                os << in << "long long fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3; unsigned fsp" << S << "; bool ah" << S
+                   << ";\n";
+                break;
         }
     }
-    os << in << "for (unsigned m = peers; m; m &= m - 1u) {  // peers fold in lane order\n";
-    std::string in2 = in + "    ";
-    os << in2 << "const int src = __ffs(m) - 1;\n";
-    os << in2 << "ag_first = min(ag_first, (long long)__shfl_sync(peers, (long long)(" << order << "), src));\n";
-    for (size_t s = 1; s < p.slots.size(); s++) {
+    // single-row values
+    os << in << "if (solo) {\n";
+    std::string i2 = in + "    ";
+    os << i2 << "ag_first = " << order << ";\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s);
-        SlotKind k = p.slots[s].kind;
-        if (k == S_NN) continue;
-        os << in2 << "{ const bool o = __shfl_sync(peers, (int)sok" << S << ", src) != 0; ";
-        if (k == S_FSUM || k == S_FMIN || k == S_FMAX)
-            os << "const double v = __shfl_sync(peers, sv" << S << ", src); ";
-        else
-            os << "const long long v = __shfl_sync(peers, sv" << S << ", src); ";
-        switch (k) {
-            case S_ISUM: os << "if (o) { ag" << S << " = (long long)((unsigned long long)ag" << S << " + (unsigned long long)v); ah" << S << " = true; }"; break;
-            case S_IMIN: os << "if (o) { ag" << S << " = min(ag" << S << ", v); ah" << S << " = true; }"; break;
-            case S_IMAX: os << "if (o) { ag" << S << " = max(ag" << S << ", v); ah" << S << " = true; }"; break;
-            case S_FSUM: os << "if (o) { ag" << S << " += v; ah" << S << " = true; }"; break;
-            case S_FMIN: os << "if (o && !isnan(v)) { ag" << S << " = min(ag" << S << ", vq_fkey(v)); ah" << S << " = true; }"; break;
-            case S_FMAX: os << "if (o && !isnan(v)) { ag" << S << " = max(ag" << S << ", vq_fkey(v)); ah" << S << " = true; }"; break;
-            default: break;
+        switch (p.slots[s].kind) {
+            case S_CNT: os << i2 << "ag" << S << " = 1;\n"; break;
+            case S_NN: os << i2 << "ag" << S << " = sok" << S << " ? 1 : 0;\n"; break;
+            case S_ISUM: case S_IMIN: case S_IMAX: os << i2 << "ag" << S << " = sv" << S << "; ah" << S << " = sok" << S << ";\n"; break;
+            case S_FMIN: case S_FMAX:
+                os << i2 << "ah" << S << " = sok" << S << " && !isnan(sv" << S << "); ag" << S << " = vq_fkey(sv" << S << ");\n";
+                break;
+            case S_FSUM:
+                os << i2 << "fd" << S << "_0 = fw" << S << "[0]; fd" << S << "_1 = fw" << S << "[1]; fd" << S << "_2 = fw" << S << "[2]; fd"
+                   << S << "_3 = (long long)(int)fw" << S << "[3]; fsp" << S << " = fs" << S << "; ah" << S << " = sok" << S << ";\n";
+                break;
         }
-        os << " }\n";
+    }
+    if (p.warp_agg) {
+        // peer reductions
+        os << in << "} else {\n";
+        os << i2 << "ag_first = (long long)vq_wmin64(peers, (unsigned long long)(" << order << "));\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string S = std::to_string(s);
+            std::string any = "__ballot_sync(peers, sok" + S + ") != 0u";
+            switch (p.slots[s].kind) {
+                case S_CNT: os << i2 << "ag" << S << " = __popc(peers);\n"; break;
+                case S_NN: os << i2 << "ag" << S << " = __popc(__ballot_sync(peers, sok" << S << "));\n"; break;
+                case S_ISUM:
+                    os << i2 << "ag" << S << " = (long long)vq_wsum64(peers, sok" << S << " ? (unsigned long long)sv" << S << " : 0ull); ah"
+                       << S << " = " << any << ";\n";
+                    break;
+                case S_IMIN:
+                    os << i2 << "ag" << S << " = (long long)(vq_wmin64(peers, (sok" << S << " ? (unsigned long long)sv" << S
+                       << " : 0x7FFFFFFFFFFFFFFFull) ^ 0x8000000000000000ull) ^ 0x8000000000000000ull); ah" << S << " = " << any << ";\n";
+                    break;
+                case S_IMAX:
+                    os << i2 << "ag" << S << " = (long long)(vq_wmax64(peers, (sok" << S << " ? (unsigned long long)sv" << S
+                       << " : 0x8000000000000000ull) ^ 0x8000000000000000ull) ^ 0x8000000000000000ull); ah" << S << " = " << any << ";\n";
+                    break;
+                case S_FMIN:
+                    os << i2 << "{ const bool o = sok" << S << " && !isnan(sv" << S << "); ag" << S << " = vq_wmin64(peers, o ? vq_fkey(sv" << S
+                       << ") : 0xFFFFFFFFFFFFFFFFull); ah" << S << " = __ballot_sync(peers, o) != 0u; }\n";
+                    break;
+                case S_FMAX:
+                    os << i2 << "{ const bool o = sok" << S << " && !isnan(sv" << S << "); ag" << S << " = vq_wmax64(peers, o ? vq_fkey(sv" << S
+                       << ") : 0ull); ah" << S << " = __ballot_sync(peers, o) != 0u; }\n";
+                    break;
+                case S_FSUM:
+                    os << i2 << "fd" << S << "_0 = vq_wsum32(peers, fw" << S << "[0]); fd" << S << "_1 = vq_wsum32(peers, fw" << S << "[1]); fd" << S
+                       << "_2 = vq_wsum32(peers, fw" << S << "[2]);\n";
+                    os << i2 << "fd" << S << "_3 = vq_wsum32(peers, fw" << S << "[3]) - ((long long)__popc(__ballot_sync(peers, (fw" << S
+                       << "[3] >> 31) != 0u)) << 32);\n";
+                    os << i2 << "fsp" << S << " = vq_redux_or(peers, fs" << S << "); ah" << S << " = " << any << ";\n";
+                    break;
+            }
+        }
     }
     os << in << "}\n";
     os << in << "if (lead) {\n";
@@ -1289,8 +1338,9 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
             case S_FMIN: os << in3 << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
             case S_FMAX: os << in3 << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
             case S_FSUM:
-                os << in3 << "if (ah" << S << ") vq_fx_add<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, ag" << S
-                   << ", " << p.fx_lsb[pos] << ", P.special + (long long)" << pos << " * stride + slot, P.error);\n";
+                os << in3 << "if (ah" << S << ") { vq_fx_add_digits<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, fd"
+                   << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S << ") atomicOr(P.special + (long long)" << pos
+                   << " * stride + slot, fsp" << S << "); }\n";
                 break;
         }
     }
@@ -1612,7 +1662,8 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     os << "            if (!ok" << K << ") continue;\n";
     os << "            const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, (unsigned long long)(long long)x" << K << ");\n";
     os << "            if (js == VQ_NOSLOT) continue;\n";
-    os << "            const int jb = P.jstart[js], je = jb + P.jcount[js];\n";
+    os << "            const int2 jm = P.jmeta[js];\n";
+    os << "            const int jb = jm.x, je = jb + jm.y;\n";
     os << "            for (int ji = jb; ji < je; ji++) {\n";
     os << "                const long long brow = P.jrows[ji];\n";
     // above-join expressions: a fresh memo scope per match for build-side reads
@@ -1665,10 +1716,14 @@ static const int kBlock = 256;
 static void choose_tunables(Plan& p) {
     int64_t acc = p.path == AggPath::Regs ? p.domain * (int64_t)(p.slots.size() + 1) : 0;
     p.block = acc > 24 ? 128 : 256;
-    p.pipeline = true;
+    // measured: software prefetch costs registers the register-accumulator path
+    // needs (6M-row Q1: 74.9 µs without, 87.0 µs with); neutral for Q6
+    p.pipeline = p.path != AggPath::Regs;
     p.staged = false;  // measured: TMA staging is not faster for these scans yet
     p.regs_pred = true;
-    p.warp_agg = true;
+    // measured on Zipf(1.1) keys: per-lane shared-memory atomics beat folding
+    // the peers of a warp first (the fold serialises over distinct groups)
+    p.warp_agg = false;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -1808,6 +1863,7 @@ Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d) {
         KeyCol k;
         k.col = c;
         k.build = false;
+        k.name = t->cols[c].name;
         p->keys.push_back(k);
         INode n;
         n.k = NK::Col;
@@ -1887,6 +1943,17 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
         KeyCol k;
         k.build = c < nb;
         k.col = k.build ? c : c - nb;
+        k.name = (k.build ? bt : pt)->cols[k.col].name;
+        if (k.build && k.col == d->build_key && bkt == pkt && !bt->cols[k.col].nullable) {
+            // equal to the probe key on every joined row: read it from the probe side
+            // instead of gathering the build row
+            k.build = false;
+            k.col = d->probe_key;
+            p->keys.push_back(k);
+            key_nodes.push_back(p->probe_key);
+            p->gb_types.push_back(bkt);
+            continue;
+        }
         p->keys.push_back(k);
         INode n;
         n.k = NK::Col;

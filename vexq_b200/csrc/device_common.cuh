@@ -76,7 +76,7 @@ __device__ __forceinline__ double vq_fkey_inv(vq_u64 k) {
 // four signed 64-bit counters holding 32-bit digits (c[k] weighs 2^(32k+lsb)).
 // Integer addition is associative, so the sum is the same whatever order the
 // atomics land in. Bits of x below 2^lsb are truncated (the window is chosen
-// so that only values below 2^-64 of the largest possible |x| lose bits).
+// so that only values below 2^-45 of the largest possible |x| lose bits).
 // Non-finite values set flags instead. stride is the distance between digits.
 template <bool kAtomic>
 __device__ __forceinline__ void vq_fx_add(vq_i64* c, double x, int lsb, unsigned* special, int* err) {
@@ -112,6 +112,101 @@ __device__ __forceinline__ void vq_fx_add(vq_i64* c, double x, int lsb, unsigned
     }
 }
 
+// The same fixed-point image as a 128-bit two's-complement integer in four
+// 32-bit words (w[0] least significant), for folding the values of several
+// lanes before one accumulator update. Magnitudes above 2^121 (impossible
+// inside the window's bounds) raise err bit 1 so a 32-value fold cannot wrap.
+__device__ __forceinline__ void vq_fx_words(double x, int lsb, unsigned* w, unsigned& special, int* err) {
+    w[0] = w[1] = w[2] = w[3] = 0u;
+    special = 0u;
+    vq_u64 b = (vq_u64)__double_as_longlong(x);
+    int e = (int)((b >> 52) & 0x7FF);
+    if (e == 0x7FF) {
+        special = (b & 0xFFFFFFFFFFFFFull) ? 1u : ((b >> 63) ? 4u : 2u);
+        return;
+    }
+    vq_u64 m = b & 0xFFFFFFFFFFFFFull;
+    if (e == 0) { if (m == 0) return; e = 1; } else m |= 1ull << 52;
+    int sh = e - 1075 - lsb;
+    if (sh < 0) {
+        if (sh <= -53) return;
+        m >>= -sh;
+        sh = 0;
+    }
+    if (sh > 69) { atomicOr(reinterpret_cast<unsigned*>(err), 2u); return; }
+    vq_u64 lo = sh < 64 ? m << sh : 0ull;
+    vq_u64 hi = sh == 0 ? 0ull : (sh < 64 ? m >> (64 - sh) : m << (sh - 64));
+    if (b >> 63) { lo = ~lo + 1ull; hi = ~hi + (lo == 0ull ? 1ull : 0ull); }
+    w[0] = (unsigned)lo; w[1] = (unsigned)(lo >> 32); w[2] = (unsigned)hi; w[3] = (unsigned)(hi >> 32);
+}
+
+// Adds carry-save digits (d[k] weighs 2^(32k+lsb)) to the four counters.
+template <bool kAtomic>
+__device__ __forceinline__ void vq_fx_add_digits(vq_i64* c, vq_i64 d0, vq_i64 d1, vq_i64 d2, vq_i64 d3) {
+    if (kAtomic) {
+        if (d0) atomicAdd(reinterpret_cast<unsigned long long*>(c + 0), (unsigned long long)d0);
+        if (d1) atomicAdd(reinterpret_cast<unsigned long long*>(c + 1), (unsigned long long)d1);
+        if (d2) atomicAdd(reinterpret_cast<unsigned long long*>(c + 2), (unsigned long long)d2);
+        if (d3) atomicAdd(reinterpret_cast<unsigned long long*>(c + 3), (unsigned long long)d3);
+    } else {
+        c[0] += d0; c[1] += d1; c[2] += d2; c[3] += d3;
+    }
+}
+
+// ---- warp reductions over a peer mask (redux.sync; every lane named in the
+// mask executes the same call with the same mask) ----
+__device__ __forceinline__ unsigned vq_redux_add(unsigned mask, unsigned v) {
+    unsigned r;
+    asm volatile("redux.sync.add.u32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(mask));
+    return r;
+}
+__device__ __forceinline__ unsigned vq_redux_min(unsigned mask, unsigned v) {
+    unsigned r;
+    asm volatile("redux.sync.min.u32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(mask));
+    return r;
+}
+__device__ __forceinline__ unsigned vq_redux_max(unsigned mask, unsigned v) {
+    unsigned r;
+    asm volatile("redux.sync.max.u32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(mask));
+    return r;
+}
+__device__ __forceinline__ unsigned vq_redux_or(unsigned mask, unsigned v) {
+    unsigned r;
+    asm volatile("redux.sync.or.b32 %0, %1, %2;" : "=r"(r) : "r"(v), "r"(mask));
+    return r;
+}
+// Sum of one 32-bit word over the peers, exact in 64 bits (two 16-bit halves).
+__device__ __forceinline__ vq_i64 vq_wsum32(unsigned mask, unsigned v) {
+    return (vq_i64)vq_redux_add(mask, v & 0xFFFFu) + ((vq_i64)vq_redux_add(mask, v >> 16) << 16);
+}
+// Wrapping 64-bit sum over the peers (four 16-bit quarters).
+__device__ __forceinline__ vq_u64 vq_wsum64(unsigned mask, vq_u64 v) {
+    vq_u64 r = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) r += (vq_u64)vq_redux_add(mask, (unsigned)(v >> (16 * q)) & 0xFFFFu) << (16 * q);
+    return r;
+}
+// Unsigned 64-bit min / max over the peers: the high words first, then the
+// low words among the lanes holding the extreme high word.
+__device__ __forceinline__ vq_u64 vq_wmin64(unsigned mask, vq_u64 v) {
+    const unsigned h = (unsigned)(v >> 32);
+    const unsigned mh = vq_redux_min(mask, h);
+    const unsigned m2 = __ballot_sync(mask, h == mh);
+    unsigned ml = 0u;
+    if (h == mh) ml = vq_redux_min(m2, (unsigned)v);
+    ml = __shfl_sync(mask, ml, __ffs(m2) - 1);
+    return ((vq_u64)mh << 32) | ml;
+}
+__device__ __forceinline__ vq_u64 vq_wmax64(unsigned mask, vq_u64 v) {
+    const unsigned h = (unsigned)(v >> 32);
+    const unsigned mh = vq_redux_max(mask, h);
+    const unsigned m2 = __ballot_sync(mask, h == mh);
+    unsigned ml = 0u;
+    if (h == mh) ml = vq_redux_max(m2, (unsigned)v);
+    ml = __shfl_sync(mask, ml, __ffs(m2) - 1);
+    return ((vq_u64)mh << 32) | ml;
+}
+
 __device__ __host__ inline int vq_clz64(vq_u64 x) {
 #ifdef __CUDA_ARCH__
     return __clzll((long long)x);
@@ -136,44 +231,37 @@ __device__ __host__ inline double vq_make_double(vq_u64 mant, int e2) {
 
 // Correctly rounded (nearest, ties to even) double of sum_k c[k]·2^(32k+lsb).
 __device__ __host__ inline double vq_fx_value(const vq_i64* c, int lsb) {
-    // exact 256-bit two's-complement accumulation of the four counters
+    // exact 256-bit two's-complement sum of the four counters (c[k] << 32k)
     vq_u64 w[4] = {0, 0, 0, 0};
     for (int k = 0; k < VQ_FX_DIGITS; k++) {
-        // add c[k] << (32k) into w (sign-extended)
-        vq_i64 v = c[k];
-        int sh = 32 * k;
-        vq_u64 ext = v < 0 ? ~0ull : 0ull;
+        const vq_i64 v = c[k];
+        const vq_u64 ext = v < 0 ? ~0ull : 0ull;
+        const int q = (32 * k) >> 6, r = (32 * k) & 63;
         vq_u64 part[4];
-        int q = sh / 64, r = sh % 64;
-        for (int i = 0; i < 4; i++) part[i] = ext;
-        // (v as 256-bit sign-extended) << sh
-        vq_u64 src[4] = {(vq_u64)v, ext, ext, ext};
-        for (int i = 3; i >= 0; i--) {
-            int s = i - q;
-            vq_u64 x = 0;
-            if (s >= 0) {
-                x = src[s] << r;
-                if (r && s - 1 >= 0) x |= src[s - 1] >> (64 - r);
-            }
-            part[i] = x;
+        // part = v sign-extended to 256 bits, shifted left by 32k
+        for (int i = 0; i < 4; i++) {
+            const int s = i - q;
+            const vq_u64 lo_word = s == 0 ? (vq_u64)v : (s >= 1 ? ext : 0);
+            const vq_u64 below = s == 1 ? (vq_u64)v : (s >= 2 ? ext : 0);
+            part[i] = s < 0 ? 0 : (r ? ((lo_word << r) | (below >> (64 - r))) : lo_word);
         }
         vq_u64 carry = 0;
         for (int i = 0; i < 4; i++) {
-            vq_u64 t = w[i] + part[i];
-            vq_u64 c1 = t < w[i];
-            vq_u64 t2 = t + carry;
-            vq_u64 c2 = t2 < t;
+            const vq_u64 t = w[i] + part[i];
+            const vq_u64 c1 = t < w[i];
+            const vq_u64 t2 = t + carry;
+            const vq_u64 c2 = t2 < t;
             w[i] = t2;
             carry = c1 | c2;
         }
     }
-    bool neg = (w[3] >> 63) & 1;
+    const bool neg = (w[3] >> 63) & 1;
     if (neg) {  // magnitude = -w
         vq_u64 carry = 1;
         for (int i = 0; i < 4; i++) {
             w[i] = ~w[i];
-            vq_u64 t = w[i] + carry;
-            carry = (t < w[i]) ? 1 : 0;
+            const vq_u64 t = w[i] + carry;
+            carry = t < w[i] ? 1 : 0;
             w[i] = t;
         }
     }
@@ -181,22 +269,34 @@ __device__ __host__ inline double vq_fx_value(const vq_i64* c, int lsb) {
     for (int i = 3; i >= 0; i--)
         if (w[i]) { top = i * 64 + 63 - vq_clz64(w[i]); break; }
     if (top < 0) return 0.0;
-    // take 53 bits below and including `top`, then round with guard+sticky
-    int lo_bit = top - 52;
-    auto bitat = [&](int pos) -> vq_u64 { return (pos < 0) ? 0 : ((w[pos >> 6] >> (pos & 63)) & 1); };
-    vq_u64 mant = 0;
-    for (int i = 0; i < 53; i++) mant |= bitat(lo_bit + i) << i;
-    int exp2 = lo_bit + lsb;
-    if (lo_bit > 0) {
-        vq_u64 guard = bitat(lo_bit - 1);
-        bool sticky = false;
-        for (int pos = 0; pos < lo_bit - 1; pos++) if (bitat(pos)) { sticky = true; break; }
-        if (guard && (sticky || (mant & 1))) {
-            mant++;
-            if (mant >> 53) { mant >>= 1; exp2++; }
+    // 64-bit window ending at `top`: bits [top-63, top]
+    const int lo_bit = top - 63;
+    auto word_at = [&](int pos) -> vq_u64 {  // 64 bits starting at bit pos (pos may be < 0)
+        if (pos <= -64) return 0;
+        if (pos < 0) return w[0] << (-pos);
+        const int q = pos >> 6, r = pos & 63;
+        const vq_u64 a = q < 4 ? w[q] : 0, b = q + 1 < 4 ? w[q + 1] : 0;
+        return r ? (a >> r) | (b << (64 - r)) : a;
+    };
+    const vq_u64 top64 = word_at(lo_bit);  // bit 63 is the leading one
+    vq_u64 mant = top64 >> 11;             // 53 bits
+    const vq_u64 rest = top64 & 0x7FFull;  // 11 bits below the mantissa
+    bool sticky = (rest & 0x3FFull) != 0;
+    if (!sticky && lo_bit > 0) {           // any set bit below the 64-bit window
+        for (int i = 0; i < 4 && !sticky; i++) {
+            const int base = i * 64;
+            if (base >= lo_bit) break;
+            const vq_u64 m = (lo_bit - base >= 64) ? ~0ull : ((1ull << (lo_bit - base)) - 1);
+            if (w[i] & m) sticky = true;
         }
     }
-    double r = vq_make_double(mant, exp2);
+    const bool guard = (rest >> 10) & 1;
+    int exp2 = lo_bit + 11 + lsb;
+    if (guard && (sticky || (mant & 1))) {
+        mant++;
+        if (mant >> 53) { mant >>= 1; exp2++; }
+    }
+    const double r = vq_make_double(mant, exp2);
     return neg ? -r : r;
 }
 
@@ -215,13 +315,10 @@ __device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 ca
     vq_u64 i = vq_hash(key) & mask;
     const vq_u64 limit = mask < (vq_u64)VQ_MAX_PROBES ? mask + 1 : (vq_u64)VQ_MAX_PROBES;
     for (vq_u64 n = 0; n < limit; n++) {
-        vq_u64 k = *reinterpret_cast<volatile vq_u64*>(keys + i);
-        if (k == key) return i;
-        if (k == VQ_EMPTY_KEY) {
-            vq_u64 old = atomicCAS(keys + i, VQ_EMPTY_KEY, key);
-            if (old == VQ_EMPTY_KEY) { atomicAdd(nkeys, 1ull); return i; }
-            if (old == key) return i;
-        }
+        // one round trip: claim the slot or learn its key
+        vq_u64 old = atomicCAS(keys + i, VQ_EMPTY_KEY, key);
+        if (old == VQ_EMPTY_KEY) { atomicAdd(nkeys, 1ull); return i; }
+        if (old == key) return i;
         i = (i + 1) & mask;
     }
     atomicOr(err, 1);

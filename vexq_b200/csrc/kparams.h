@@ -38,6 +38,7 @@ struct VQParams {
     int* jstart;               // [jcap + 1]
     int* jfill;                // [jcap + 1]
     int* jrows;                // build row ids, grouped by slot in row order
+    int2* jmeta;               // [jcap + 1] {first row position, row count} per slot
     unsigned long long* jnkeys;
     // ---- 8-byte scalars ----
     long long nchunks;

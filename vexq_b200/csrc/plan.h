@@ -57,6 +57,7 @@ struct AggOut {
 };
 
 struct KeyCol {
+    std::string name; // output column name
     int col;          // column index in its side's table
     bool build;       // join: build-side column
     int type;
@@ -131,7 +132,7 @@ struct Plan {
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
     // scratch reused across runs
     DevBuf scratch_a, scratch_b, scratch_c, scratch_d, scratch_e, scratch_f, scratch_g;
-    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar;
+    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta;
     ~Plan();
 };
 

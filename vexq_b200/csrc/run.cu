@@ -171,6 +171,11 @@ __global__ void k_scan_add(int* out, long long n, const int* sums) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += sums[i / 4096];
 }
+// Packs each slot's chain start and length into one 8-byte probe read.
+__global__ void k_pack_meta(const int* start, const int* count, int2* meta, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) meta[i] = make_int2(start[i], count[i]);
+}
 
 // Restores build-row order inside each key's chain (joinHashTable.insert keeps
 // insertion order, exec/join_table.go:496-517): one thread per slot.
@@ -195,14 +200,19 @@ __device__ __forceinline__ unsigned long long vq_rank(long long bits, bool isnul
     u = desc ? u : ~u;
     return u == 0xFFFFFFFFFFFFFFFFull ? u - 1 : u;
 }
-__global__ void k_hist(const long long* keyv, const unsigned char* keynull, long long n, int desc, unsigned* hist) {
+__global__ void k_rank(const long long* keyv, const unsigned char* keynull, long long n, int desc,
+                       unsigned long long* rank) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        atomicAdd(hist + (vq_rank(keyv[i], keynull[i], desc) >> 48), 1u);
+        rank[i] = vq_rank(keyv[i], keynull[i], desc);
 }
-__global__ void k_select(const long long* keyv, const unsigned char* keynull, long long n, int desc, unsigned thr_bin,
-                         unsigned long long* nsel, long long* sel, long long cap) {
+__global__ void k_sample(const unsigned long long* rank, long long n, int S, unsigned long long* out) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < S) out[j] = rank[(long long)j * n / S];
+}
+__global__ void k_select(const unsigned long long* rank, long long n, unsigned long long thr, unsigned long long* nsel,
+                         long long* sel, long long cap) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        if ((vq_rank(keyv[i], keynull[i], desc) >> 48) >= thr_bin) {
+        if (rank[i] >= thr) {
             unsigned long long p = atomicAdd(nsel, 1ull);
             if ((long long)p < cap) sel[p] = i;
         }
@@ -552,53 +562,66 @@ Groups fetch_groups(RunCtx& rc, const Compacted& c, const std::vector<long long>
     return g;
 }
 
-// Device top-k candidates for ORDER BY <aggregate> LIMIT k: a 16-bit-radix
-// histogram picks a threshold bucket; every group at or above it is a
-// candidate (ties included) and the host finishes the stable sort.
+// Device top-k candidates for ORDER BY <aggregate> LIMIT k: every group's sort
+// rank (raw int64 bits in the ExternalSort order, NULLs first) is computed on
+// the device; a 4096-point sample gives a threshold that keeps a few hundred
+// groups per LIMIT row; groups at or above it (ties included) are the
+// candidates, and the host finishes the stable sort on them.
 bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel) {
     Plan& p = rc.p;
     const vexq_order_desc& o = p.order;
     int ngb = (int)p.keys.size();
-    if (o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 64) return false;
+    const long long kCap = 65536;
+    if (o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096) return false;
     const AggOut& a = p.outs[o.sort_col - ngb];
     int vslot = a.value_slot;
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
     int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
     if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
-    size_t need = c.n * 9 + 65536 * 4 + 16 + 8 * 70000;
+    const int S = 4096;
+    size_t need = c.n * 17 + 64 + S * 8 + kCap * 8 + 64;
     p.scratch_d.ensure(need);
     char* b = (char*)p.scratch_d.p;
     long long* keyv = (long long*)b;
-    unsigned char* keynull = (unsigned char*)(b + c.n * 8);
-    unsigned* hist = (unsigned*)(((uintptr_t)(b + c.n * 9) + 15) & ~(uintptr_t)15);
-    unsigned long long* nsel = (unsigned long long*)(hist + 65536);
+    unsigned long long* rank = (unsigned long long*)(b + c.n * 8);
+    unsigned char* keynull = (unsigned char*)(b + c.n * 16);
+    unsigned long long* samp = (unsigned long long*)(((uintptr_t)(b + c.n * 17) + 63) & ~(uintptr_t)63);
+    unsigned long long* nsel = samp + S;
     long long* dsel = (long long*)(nsel + 2);
     int g = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
-    Timer tm(rc.s);
     k_sortkey<<<g, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot], keyv,
                                    keynull, fmin_key);
-    VQ_CUDA(cudaMemsetAsync(hist, 0, 65536 * 4, rc.s));
-    k_hist<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, hist);
-    std::vector<unsigned> h(65536);
-    VQ_CUDA(cudaMemcpyAsync(h.data(), hist, 65536 * 4, cudaMemcpyDeviceToHost, rc.s));
+    k_rank<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, rank);
+    k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n, S, samp);
+    std::vector<unsigned long long> hs(S);
+    VQ_CUDA(cudaMemcpyAsync(hs.data(), samp, S * 8, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
-    long long acc = 0;
-    unsigned thr = 0;
-    for (int bin = 65535; bin >= 0; bin--) {
-        acc += h[bin];
-        if (acc >= o.limit) { thr = (unsigned)bin; break; }
+    // threshold: expected (q+1)·n/S groups at or above the q-th largest sample
+    long long q = (long long)std::ceil((4.0 * o.limit + 64.0) * S / (double)c.n) - 1;
+    unsigned long long thr = 0;
+    if (q < S) {
+        std::nth_element(hs.begin(), hs.begin() + q, hs.end(), std::greater<unsigned long long>());
+        thr = hs[q];
     }
-    if (acc > 65536) { rc.kernel_ms += tm.stop(); return false; }
-    VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
-    k_select<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, thr, nsel, dsel, 65536);
-    VQ_CUDA(cudaGetLastError());
-    unsigned long long ns = 0;
-    VQ_CUDA(cudaMemcpyAsync(&ns, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
-    rc.kernel_ms += tm.stop();
-    rc.launches += 3;
-    sel.resize(std::min<unsigned long long>(ns, 65536));
-    if (!sel.empty()) VQ_CUDA(cudaMemcpy(sel.data(), dsel, sel.size() * 8, cudaMemcpyDeviceToHost));
-    return true;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
+        k_select<<<g, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
+        VQ_CUDA(cudaGetLastError());
+        unsigned long long ns = 0;
+        VQ_CUDA(cudaMemcpyAsync(&ns, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaStreamSynchronize(rc.s));
+        rc.launches += 1;
+        if ((long long)ns >= o.limit && (long long)ns <= kCap) {
+            sel.resize(ns);
+            VQ_CUDA(cudaMemcpy(sel.data(), dsel, ns * 8, cudaMemcpyDeviceToHost));
+            rc.launches += 3;
+            return true;
+        }
+        if ((long long)ns > kCap) return false;  // too many ties at the threshold: fetch everything
+        thr = 0;                                  // unlucky sample: every group qualifies
+        if (c.n > kCap) return false;
+    }
+    return false;
 }
 
 // Decodes group keys, computes aggregate outputs, orders groups, and applies
@@ -619,7 +642,7 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
         const Table* tt = k.build ? p.bt : p.t;
         const Column& col = tt->cols[k.col];
         OutColumn oc;
-        oc.name = col.name;
+        oc.name = k.name.empty() ? col.name : k.name;
         oc.type = k.type;
         oc.v.assign(rows, 0);
         oc.valid.assign(rows, 0);
@@ -831,6 +854,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         p.jt_start.ensure(nslots * 4);
         p.jt_fill.ensure(nslots * 4);
         p.jt_rows.ensure(std::max<long long>(bs.rows, 1) * 4);
+        p.jt_meta.ensure(nslots * 8);
         p.jt_scalar.ensure(64 + ((nslots + 4095) / 4096 + 1) * 4);
         B.jkeys = p.jt_keys.as<unsigned long long>();
         B.jcount = p.jt_count.as<int>();
@@ -859,13 +883,14 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             B.mode = 1;
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
             k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error);
+            k_pack_meta<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, B.jcount, p.jt_meta.as<int2>(), nslots);
             VQ_CUDA(cudaGetLastError());
             int herr = 0;
             unsigned long long nk = 0;
             VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
             VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
             rc.kernel_ms += tm.stop();
-            rc.launches += 7;
+            rc.launches += 8;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");
             join_keys = (long long)nk;
@@ -878,6 +903,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         P.jcount = B.jcount;
         P.jstart = B.jstart;
         P.jrows = B.jrows;
+        P.jmeta = p.jt_meta.as<int2>();
         P.jmask = B.jmask;
         if (join_keys == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
             Groups g;
