@@ -306,6 +306,33 @@ int32_t vexq_server_stop(vexq_server_t s);
 /* Host-set cancellation flag polled between launches of a running plan. */
 int32_t vexq_cancel(vexq_plan_t p);
 
+/* ---- global aggregate without allocation --------------------------------
+ * No counterpart in the reference: its operators work on the Go heap.
+ * Runs an aggregate plan without GROUP BY (one result row) through the same
+ * kernels as vexq_plan_run but allocates no device, pinned or managed
+ * memory: the per-block partials, row ranges, merge outputs and error flag
+ * live in one static device array of VEXQ_NOALLOC_SCRATCH_BYTES per device,
+ * and the row is written to caller memory. Meant for callers that must not
+ * allocate: a serving loop with other queries in flight (cudaMalloc and
+ * cudaFree synchronise the whole device) or a caller held to a fixed HBM
+ * budget.
+ *   stream      cudaStream_t to run on (NULL: the legacy default stream); the
+ *               call synchronises it before returning.
+ *   out_values  n_out 8-byte cells, one per output column in plan order:
+ *               int64 values, float64 bit patterns, dates sign-extended,
+ *               bools 0/1.
+ *   out_valid   n_out bytes, 0 where the cell is NULL.
+ * The first call on a device does set-up (looks up the scratch address and
+ * loads the merge kernel's module); make it before any stream capture.
+ * Calls that overlap in time race on the shared scratch: issue them one at a
+ * time per device. Errors: VEXQ_ENOTSUP for joins and plans with GROUP BY;
+ * VEXQ_EINVAL when n_out differs from the plan's output columns, when more
+ * than 512 row ranges remain after zone-map pruning, or when the partials do
+ * not fit in the scratch even at one block per SM. */
+#define VEXQ_NOALLOC_SCRATCH_BYTES (1 << 20)
+int32_t vexq_plan_run_global_noalloc(vexq_plan_t plan, int32_t rg_start, int32_t rg_end, void* stream,
+                                     int64_t* out_values, uint8_t* out_valid, int32_t n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,6 +130,7 @@ EXPORTS = [
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
     "vexq_cancel",
+    "vexq_plan_run_global_noalloc",
 ]
 
 _lib = None
@@ -188,6 +189,7 @@ def load() -> C.CDLL:
         "vexq_server_latency": (i32, [vp, i64, C.POINTER(C.c_double)]),
         "vexq_server_stop": (i32, [vp]),
         "vexq_cancel": (i32, [vp]),
+        "vexq_plan_run_global_noalloc": (i32, [vp, i32, i32, vp, C.POINTER(i64), C.POINTER(C.c_uint8), i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

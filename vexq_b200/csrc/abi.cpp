@@ -8,15 +8,6 @@
 
 #include "plan.h"
 
-struct vexq_table_s {
-    vq::Table* t;
-};
-struct vexq_plan_s {
-    vq::Plan* p;
-    vexq_table_s* table;
-    int64_t footprint;  // bytes of group/join tables a run allocates (admission)
-};
-
 namespace vq {
 Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows);
 void destroy_table(Table* t);

@@ -169,3 +169,13 @@ struct vexq_result_s {
     std::vector<std::vector<uint32_t>> doff;
     std::vector<std::string> dbytes;
 };
+
+// Opaque handles of the C ABI.
+struct vexq_table_s {
+    vq::Table* t;
+};
+struct vexq_plan_s {
+    vq::Plan* p;
+    vexq_table_s* table;
+    int64_t footprint;  // bytes of group/join tables a run allocates (admission)
+};

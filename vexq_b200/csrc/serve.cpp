@@ -6,15 +6,6 @@
 
 #include "plan.h"
 
-struct vexq_table_s {
-    vq::Table* t;
-};
-struct vexq_plan_s {
-    vq::Plan* p;
-    vexq_table_s* table;
-    int64_t footprint;
-};
-
 namespace vq {
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end);
 }  // namespace vq
