@@ -556,6 +556,13 @@ struct Gen {
             }
             case NK::Lit: {
                 os << ind << "const bool " << ok << " = true;\n";
+                if (n.lit_slot >= 0) {  // value passed at launch
+                    std::string L = "P.lit[" + std::to_string(n.lit_slot) + "]";
+                    if (n.type == VEXQ_TYPE_INT64) os << ind << "const long long " << x << " = " << L << ";\n";
+                    else if (n.type == VEXQ_TYPE_FLOAT64) os << ind << "const double " << x << " = __longlong_as_double(" << L << ");\n";
+                    else os << ind << "const int " << x << " = (int)" << L << ";\n";
+                    break;
+                }
                 switch (n.type) {
                     case VEXQ_TYPE_INT64: os << ind << "const long long " << x << " = " << ilit(n.li) << ";\n"; break;
                     case VEXQ_TYPE_FLOAT64: os << ind << "const double " << x << " = " << dlit(n.lf) << ";\n"; break;
@@ -1100,7 +1107,7 @@ void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string
             case S_FMAX: os << ind << "if (sok" << S << " && !isnan(sv" << S << ")) atomicMax(" << aiu << ", vq_fkey(sv" << S << "));\n"; break;
             case S_FSUM:
                 os << ind << "if (sok" << S << ") vq_fx_add<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, sv" << S
-                   << ", " << p.fx_lsb[pos] << ", P.special + (long long)" << pos << " * stride + slot, P.error);\n";
+                   << ", P.fx_lsb[" << pos << "], P.special + (long long)" << pos << " * stride + slot, P.error);\n";
                 break;
         }
     }
@@ -1113,14 +1120,15 @@ struct CacheLayout {
     int C = 0;
     std::string first, ints, fx, sp;
 };
+// The cached group count is the launch-time value P.cache_n (vq_C in the
+// generated code), so plans that differ only in domain share a kernel.
 CacheLayout cache_layout(const Plan& p) {
     CacheLayout L;
     L.C = p.smem_groups;
-    std::string C = std::to_string(L.C);
     L.first = "((long long*)vq_smem)";
-    L.ints = "(((long long*)vq_smem) + " + C + ")";
-    L.fx = "(((long long*)vq_smem) + " + std::to_string((long long)L.C * (1 + p.ni)) + ")";
-    L.sp = "((unsigned*)(((long long*)vq_smem) + " + std::to_string((long long)L.C * (1 + p.ni + 4 * p.nf)) + "))";
+    L.ints = "(((long long*)vq_smem) + vq_C)";
+    L.fx = "(((long long*)vq_smem) + (long long)vq_C * " + std::to_string(1 + p.ni) + ")";
+    L.sp = "((unsigned*)(((long long*)vq_smem) + (long long)vq_C * " + std::to_string(1 + p.ni + 4 * p.nf) + "))";
     return L;
 }
 int cache_bytes(const Plan& p) { return p.smem_groups * (8 + 8 * p.ni + 36 * p.nf); }
@@ -1129,8 +1137,8 @@ int cache_bytes(const Plan& p) { return p.smem_groups * (8 + 8 * p.ni + 36 * p.n
 // global update and closes the brace.
 void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string& ind) {
     CacheLayout L = cache_layout(p);
-    std::string C = std::to_string(L.C);
-    os << ind << "if (slot < " << C << "ull) {\n";
+    const std::string C = "vq_C";
+    os << ind << "if (slot < (unsigned long long)vq_C) {\n";
     std::string in = ind + "    ";
     // MIN/MAX and first-row keys only ever move one way, so a plain read that
     // shows no improvement (possibly stale, never past the true value) skips
@@ -1160,8 +1168,9 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
 
 void emit_cache_init(std::ostringstream& os, const Plan& p) {
     CacheLayout L = cache_layout(p);
-    std::string C = std::to_string(L.C);
+    const std::string C = "vq_C";
     os << "    extern __shared__ __align__(16) unsigned char vq_smem[];\n";
+    os << "    const int vq_C = P.cache_n;\n";
     os << "    for (int i = threadIdx.x; i < " << C << "; i += blockDim.x) {\n";
     os << "        " << L.first << "[i] = 0x7FFFFFFFFFFFFFFFLL;\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
@@ -1184,7 +1193,7 @@ void emit_cache_init(std::ostringstream& os, const Plan& p) {
 
 void emit_cache_flush(std::ostringstream& os, const Plan& p) {
     CacheLayout L = cache_layout(p);
-    std::string C = std::to_string(L.C);
+    const std::string C = "vq_C";
     os << "    __syncthreads();\n";
     os << "    for (int i = threadIdx.x; i < " << C << "; i += blockDim.x) {\n";
     os << "        if (" << L.ints << "[" << p.slot_pos[0] << " * " << C << " + i] == 0) continue;\n";
@@ -1244,7 +1253,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
         std::string S = std::to_string(s);
         os << in << "unsigned fw" << S << "[4], fs" << S << " = 0u; fw" << S << "[0] = fw" << S << "[1] = fw" << S << "[2] = fw" << S
            << "[3] = 0u;\n";
-        os << in << "if (sok" << S << ") vq_fx_words(sv" << S << ", " << p.fx_lsb[p.slot_pos[s]] << ", fw" << S << ", fs" << S
+        os << in << "if (sok" << S << ") vq_fx_words(sv" << S << ", P.fx_lsb[" << p.slot_pos[s] << "], fw" << S << ", fs" << S
            << ", P.error);\n";
     }
     os << in << "long long ag_first;\n";
@@ -1763,6 +1772,19 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     }
     choose_path(p);
     choose_tunables(p);
+    // numeric literals become launch-time values (first VQ_MAXLITS of them)
+    p.lits.clear();
+    for (auto& n : p.ir) {
+        n.lit_slot = -1;
+        if (n.k != NK::Lit || (int)p.lits.size() >= VQ_MAXLITS) continue;
+        long long v;
+        if (n.type == VEXQ_TYPE_INT64) v = n.li;
+        else if (n.type == VEXQ_TYPE_DATE) v = n.ld;
+        else if (n.type == VEXQ_TYPE_FLOAT64) std::memcpy(&v, &n.lf, 8);
+        else continue;
+        n.lit_slot = (int)p.lits.size();
+        p.lits.push_back(v);
+    }
     std::ostringstream src;
     src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
     std::string body = join ? gen_probe_kernel(p, key_nodes, p.block) : gen_agg_kernel(p, key_nodes, p.block);
@@ -2128,6 +2150,12 @@ static bool zone_rec(const Plan& p, int idx, const Table& t, int rg) {
 }
 
 bool zone_eval(const Plan& p, int root, const Table& t, int rg) { return root < 0 ? true : zone_rec(p, root, t, rg); }
+
+void set_plan_constants(const Plan& p, VQParams& P) {
+    for (size_t i = 0; i < p.lits.size() && i < VQ_MAXLITS; i++) P.lit[i] = p.lits[i];
+    for (size_t f = 0; f < p.fx_lsb.size() && f < 16; f++) P.fx_lsb[f] = p.fx_lsb[f];
+    P.cache_n = p.smem_groups;
+}
 
 ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_start, int rg_end, int unit) {
     ScanSegs s;

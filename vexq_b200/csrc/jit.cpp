@@ -21,6 +21,8 @@ namespace vq {
 
 struct JitModule {
     CUmodule mod = nullptr;
+    std::mutex mu;
+    std::map<std::string, int> smem_limit;  // per entry: dynamic shared memory opted in so far
     ~JitModule();
 };
 
@@ -184,8 +186,14 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     k.mod = m;
     k.fn = (void*)f;
     if (smem > 0) {  // static shared memory counts against the default 48 KB limit too
-        CUresult ra = d.setattr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem);
-        if (ra != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuFuncSetAttribute(max dynamic smem) failed: " + std::to_string((int)ra));
+        // plans sharing a kernel may need different sizes: the limit only grows
+        std::lock_guard<std::mutex> lk(m->mu);
+        int& cur = m->smem_limit[entry];
+        if (smem > cur) {
+            CUresult ra = d.setattr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem);
+            if (ra != CUDA_SUCCESS) fail(VEXQ_EDEVICE, "cuFuncSetAttribute(max dynamic smem) failed: " + std::to_string((int)ra));
+            cur = smem;
+        }
     }
     int nb = 0;
     if (d.occ(&nb, f, block, (size_t)smem) == CUDA_SUCCESS) k.max_blocks_per_sm = nb;

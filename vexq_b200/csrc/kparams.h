@@ -6,6 +6,7 @@
 #define VQ_MAXCOLS 32
 #define VQ_MAXSETS 16
 #define VQ_FX_DIGITS 4  // 32-bit digits of the exact fixed-point float sums
+#define VQ_MAXLITS 32   // numeric literals passed at launch (raw 8-byte images)
 
 struct VQParams {
     // ---- scanned table (aggregate: the table; join: probe or build side) ----
@@ -40,6 +41,9 @@ struct VQParams {
     int* jrows;                // build row ids, grouped by slot in row order
     int2* jmeta;               // [jcap + 1] {first row position, row count} per slot
     unsigned long long* jnkeys;
+    // ---- numeric literals of the plan's expressions (int64, date, float64 bits):
+    //      plans that differ only in constants share one compiled kernel ----
+    long long lit[VQ_MAXLITS];
     // ---- 8-byte scalars ----
     long long nchunks;
     long long rg_rows;
@@ -50,5 +54,6 @@ struct VQParams {
     int nseg;
     int n_rg;
     int mode;                  // join build: 0 = insert/count, 1 = fill
+    int cache_n;               // dense path: groups held in the block's shared-memory cache
     int fx_lsb[16];            // per float-sum slot: exponent of the window's LSB
 };

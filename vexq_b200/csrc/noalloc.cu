@@ -156,6 +156,7 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
 
         VQParams P;
         std::memset(&P, 0, sizeof P);
+        set_plan_constants(p, P);
         for (size_t c = 0; c < t.cols.size(); c++) {
             P.col[c] = t.cols[c].values.p;
             P.valid[c] = t.cols[c].nullable ? t.cols[c].validity.as<unsigned char>() : nullptr;

@@ -37,6 +37,7 @@ struct INode {
     double lo = 0, hi = 0;
     bool is_literal_raw = false;  // literal before coercion (SQL level)
     int lit_kind = 0;
+    int lit_slot = -1;            // numeric literal passed at launch: index into VQParams::lit
 };
 
 // Accumulator slot kinds.
@@ -102,6 +103,7 @@ struct Plan {
     int nf = 0, ni = 0;            // float / int slots (path-specific layout)
     std::vector<int> slot_pos;     // slot → index within its float/int bank
     std::vector<int> fx_lsb;       // per float-sum slot
+    std::vector<long long> lits;   // launch-time literal table (VQParams::lit)
     std::vector<std::vector<uint32_t>> sets;  // large InCodes sets (bitsets)
     std::vector<std::pair<int, int64_t>> presence;   // (column, code) rows: scanned / probe table
     std::vector<std::pair<int, int64_t>> bpresence;  // rows for the join build table
@@ -124,9 +126,11 @@ struct Plan {
     // per-run caches (host-side overhead of a run)
     std::vector<long long> seg_cache;      // last uploaded segment list
     DevBuf d_seg;
+    std::vector<long long> bseg_cache;     // join build side: last uploaded segment list
+    DevBuf d_bseg;
     DevBuf d_kinds;                        // register-path combiner kinds
     PinnedBuf h_stage;                     // pinned staging for small results
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
@@ -149,6 +153,8 @@ Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d);
 Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d);
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred);
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
+// Copies the plan's launch-time constants (literals, float-sum windows, cache size) into P.
+void set_plan_constants(const Plan& p, VQParams& P);
 ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end, int unit);
 bool parse_date(const char* s, int64_t* days);
 

@@ -288,27 +288,6 @@ void set_columns(VQParams& P, const Table& t, bool build_side) {
     }
 }
 
-struct Timer {
-    cudaEvent_t a, b;
-    cudaStream_t s;
-    explicit Timer(cudaStream_t st) : s(st) {
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-        cudaEventRecord(a, s);
-    }
-    float stop() {
-        cudaEventRecord(b, s);
-        cudaEventSynchronize(b);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
-        return ms;
-    }
-    ~Timer() {
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-    }
-};
-
 // Host-side group rows collected from either path.
 struct Groups {
     std::vector<uint64_t> key;
@@ -823,6 +802,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     RunCtx rc{p, plan_stream(p)};
     VQParams P;
     std::memset(&P, 0, sizeof P);
+    set_plan_constants(p, P);
     Table& t = *p.t;
     int rge = rg_end < 0 ? t.n_rg : std::min(rg_end, t.n_rg);
     int rgs = std::max(0, rg_start);
@@ -837,10 +817,14 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         while (jcap < 2 * std::max<long long>(bs.rows, 8)) jcap <<= 1;
         VQParams B;
         std::memset(&B, 0, sizeof B);
+        set_plan_constants(p, B);
         set_columns(B, bt, false);
-        DevBuf bseg(std::max<size_t>(bs.seg.size(), 3) * 8);
-        if (!bs.seg.empty()) VQ_CUDA(cudaMemcpyAsync(bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice, rc.s));
-        B.seg = bseg.as<long long>();
+        if (bs.seg != p.bseg_cache || !p.d_bseg.p) {  // uploaded once per distinct pruning
+            p.d_bseg.ensure(std::max<size_t>(bs.seg.size(), 3) * 8);
+            if (!bs.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice));
+            p.bseg_cache = bs.seg;
+        }
+        B.seg = p.d_bseg.as<long long>();
         B.nseg = (int)bs.seg.size() / 3;
         B.nchunks = bs.nchunks;
         B.rg_rows = bt.rg_rows;
@@ -866,7 +850,8 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         int* bsums = (int*)(p.jt_scalar.as<char>() + 64);
         B.jmask = (unsigned long long)(jcap - 1);
         {
-            Timer tm(rc.s);
+            ensure_events(p);
+            VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
             VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 16, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
@@ -889,7 +874,9 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             unsigned long long nk = 0;
             VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
             VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
-            rc.kernel_ms += tm.stop();
+            VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+            VQ_CUDA(cudaEventSynchronize(p.ev[5]));
+            rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
             rc.launches += 8;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");

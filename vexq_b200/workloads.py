@@ -17,11 +17,11 @@ Q1_CUTOFF = "1998-09-02"          # date '1998-12-01' - interval '90' day
 Q6_LO, Q6_HI = "1994-01-01", "1995-01-01"
 
 
-def q1_plan() -> AggPlan:
+def q1_plan(cutoff: str = Q1_CUTOFF) -> AggPlan:
     price, disc, tax = col(D.L_PRICE), col(D.L_DISC), col(D.L_TAX)
     disc_price = price * (1 - disc)
     return AggPlan(
-        predicate=col(D.L_SHIPDATE) <= lit(Q1_CUTOFF),
+        predicate=col(D.L_SHIPDATE) <= lit(cutoff),
         group_by=[D.L_FLAG, D.L_STATUS],
         aggs=[sum_(col(D.L_QTY), "sum_qty"), sum_(price, "sum_base_price"),
               sum_(disc_price, "sum_disc_price"), sum_(disc_price * (1 + tax), "sum_charge"),
@@ -29,9 +29,9 @@ def q1_plan() -> AggPlan:
               count_star("count_order")])
 
 
-def q6_plan() -> AggPlan:
+def q6_plan(lo: str = Q6_LO, hi: str = Q6_HI) -> AggPlan:
     return AggPlan(
-        predicate=and_(col(D.L_SHIPDATE) >= lit(Q6_LO), col(D.L_SHIPDATE) < lit(Q6_HI),
+        predicate=and_(col(D.L_SHIPDATE) >= lit(lo), col(D.L_SHIPDATE) < lit(hi),
                        between(col(D.L_DISC), 0.05, 0.07), col(D.L_QTY) < 24),
         group_by=[],
         aggs=[sum_(col(D.L_PRICE) * col(D.L_DISC), "revenue")])
