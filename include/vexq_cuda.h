@@ -283,9 +283,35 @@ int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
 int32_t vexq_selvec_from_bits(const uint8_t* bits, int64_t nrows, int64_t block,
                               uint16_t* out_sel, int32_t* out_len);
 
-/* ---- batching: many aggregates in one persistent launch ---------------- */
-/* Runs n independent plans (each over its own table) in one persistent
- * kernel launch per plan shape, captured in a CUDA graph on first use. */
+/* ---- batching: many aggregates in one persistent launch ----------------
+ * No reference counterpart: the Go engine runs one operator tree per query.
+ * A batch holds n prepared plans (each over its own table). Aggregate plans
+ * are split by path (register accumulators / group tables); each class runs
+ * as ONE persistent launch of a generated kernel with a body per distinct
+ * plan shape, whose blocks take (plan, row-chunk range) units from an atomic
+ * ticket, largest first. Table init, both launches (on forked streams), the
+ * partial merge, the table finalize and one copy of all outputs to pinned
+ * host memory are captured in a CUDA graph at creation and replayed by every
+ * vexq_batch_exec. Join plans are not batched; they run after the graph, one
+ * after another. Results match vexq_plan_run's: keys, counts, integer
+ * aggregates and group-table float sums bit for bit; register-path float sums
+ * may differ in the last bits (a different row partition), both within their
+ * stated tolerance. Repeated execs give identical bits.
+ * flags: VEXQ_BATCH_AUTOTUNE times graph replays over the shared-memory
+ * group-cache size (the shared-versus-global table cutover) and the unit
+ * size, and keeps the fastest. */
+#define VEXQ_BATCH_AUTOTUNE 1u
+typedef struct vexq_batch_s* vexq_batch_t;
+int32_t vexq_batch_create(vexq_plan_t* plans, int32_t n, uint32_t flags, vexq_batch_t* out);
+/* One result per plan, in plan order (each freed with vexq_result_free). */
+int32_t vexq_batch_exec(vexq_batch_t b, vexq_result_t* out_results);
+/* Last exec: device time of the whole graph replay and of its kernels alone
+ * (before the copy back), CUDA events; algorithmic bytes and rows scanned. */
+int32_t vexq_batch_stats(vexq_batch_t b, double* device_ms, double* kernel_ms, int64_t* bytes_scanned,
+                         int64_t* rows_scanned);
+const char* vexq_batch_explain(vexq_batch_t b);
+int32_t vexq_batch_destroy(vexq_batch_t b);
+/* create + exec + destroy in one call. */
 int32_t vexq_batch_run(vexq_plan_t* plans, int32_t n, vexq_result_t* out_results);
 
 /* ---- serving loop ------------------------------------------------------ */

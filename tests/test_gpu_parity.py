@@ -276,7 +276,8 @@ def test_batch_and_server_equal_single_runs(gpu_lib, lineitem_1m):
     plans = (C.c_void_p * 2)(ops[0].h, ops[1].h)
     outs = (C.c_void_p * 2)()
     abi.check(L.vexq_batch_run(plans, 2, outs))
-    assert [X.Result(C.c_void_p(outs[k])).rows() for k in range(2)] == single
+    for k in range(2):  # register-path FP64 sums: another row partition, last-bit differences
+        assert_rows_match(X.Result(C.c_void_p(outs[k])).rows(), single[k], ordered=True, rtol=1e-13)
     srv = C.c_void_p()
     abi.check(L.vexq_server_start(1 << 34, 3, C.byref(srv)))
     tickets = []

@@ -116,6 +116,8 @@ class BatchView(C.Structure):
 
 
 # Every symbol include/vexq_cuda.h declares (checked by the CPU test suite).
+BATCH_AUTOTUNE = 1  # VEXQ_BATCH_AUTOTUNE
+
 EXPORTS = [
     "vexq_init", "vexq_last_error", "vexq_abi_version",
     "vexq_table_upload", "vexq_table_destroy", "vexq_table_num_row_groups",
@@ -131,6 +133,11 @@ EXPORTS = [
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
     "vexq_cancel",
     "vexq_plan_run_global_noalloc",
+    "vexq_batch_create",
+    "vexq_batch_exec",
+    "vexq_batch_stats",
+    "vexq_batch_explain",
+    "vexq_batch_destroy",
 ]
 
 _lib = None
@@ -190,6 +197,11 @@ def load() -> C.CDLL:
         "vexq_server_stop": (i32, [vp]),
         "vexq_cancel": (i32, [vp]),
         "vexq_plan_run_global_noalloc": (i32, [vp, i32, i32, vp, C.POINTER(i64), C.POINTER(C.c_uint8), i32]),
+        "vexq_batch_create": (i32, [C.POINTER(vp), i32, C.c_uint32, C.POINTER(vp)]),
+        "vexq_batch_exec": (i32, [vp, C.POINTER(vp)]),
+        "vexq_batch_stats": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64)]),
+        "vexq_batch_explain": (C.c_char_p, [vp]),
+        "vexq_batch_destroy": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1037,12 +1037,33 @@ void emit_regs_update_pred(std::ostringstream& os, const Plan& p, const std::str
 }
 
 // Block reduction of the register accumulators into per-block partials.
-void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
+// Where a register-path flush writes: the partial row index (the block in a
+// plain launch, the unit's slot in a batch), the kind-table prefix and whether
+// the staging arrays are carved from dynamic shared memory (batch bodies).
+struct FlushCtx {
+    std::string part_index = "blockIdx.x";
+    std::string kinds = "P_";
+    bool dyn_smem = false;
+};
+
+int regs_flush_smem(const Plan& p, int block) {
+    int G = (int)p.domain;
+    return (block / 32) * 8 * (std::max(G * p.nf, 1) + std::max(G * (p.ni + 1), 1));
+}
+
+void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const FlushCtx& fc = FlushCtx()) {
     int warps = block / 32;
     int G = (int)p.domain;
     int nf = p.nf, ni = p.ni;
-    os << "    __shared__ double sh_f[" << warps << "][" << std::max(G * nf, 1) << "];\n";
-    os << "    __shared__ long long sh_i[" << warps << "][" << std::max(G * (ni + 1), 1) << "];\n";
+    const int WF = std::max(G * nf, 1), WI = std::max(G * (ni + 1), 1);
+    if (fc.dyn_smem) {
+        os << "    __syncthreads();\n";
+        os << "    double (*sh_f)[" << WF << "] = (double (*)[" << WF << "])vq_smem;\n";
+        os << "    long long (*sh_i)[" << WI << "] = (long long (*)[" << WI << "])(vq_smem + " << warps * WF * 8 << ");\n";
+    } else {
+        os << "    __shared__ double sh_f[" << warps << "][" << WF << "];\n";
+        os << "    __shared__ long long sh_i[" << warps << "][" << WI << "];\n";
+    }
     os << "    const int fw = threadIdx.x >> 5;\n";
     for (int g = 0; g < G; g++) {
         for (size_t s = 0; s < p.slots.size(); s++) {
@@ -1072,13 +1093,13 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block) {
     os << "    for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
     os << "        const int s = t % " << std::max(nf, 1) << ";\n";
     os << "        double v = sh_f[0][t];\n";
-    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_fcomb(P_fkind(s), v, sh_f[w][t]);\n";
-    os << "        P.part_f[(long long)blockIdx.x * " << G * nf << " + t] = v;\n    }\n";
+    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_fcomb(" << fc.kinds << "fkind(s), v, sh_f[w][t]);\n";
+    os << "        P.part_f[(long long)(" << fc.part_index << ") * " << G * nf << " + t] = v;\n    }\n";
     os << "    for (int t = threadIdx.x; t < " << G * (ni + 1) << "; t += blockDim.x) {\n";
     os << "        const int s = t % " << (ni + 1) << ";\n";
     os << "        long long v = sh_i[0][t];\n";
-    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_icomb(P_ikind(s), v, sh_i[w][t]);\n";
-    os << "        P.part_i[(long long)blockIdx.x * " << G * (ni + 1) << " + t] = v;\n    }\n";
+    os << "        for (int w = 1; w < " << warps << "; w++) v = vq_icomb(" << fc.kinds << "ikind(s), v, sh_i[w][t]);\n";
+    os << "        P.part_i[(long long)(" << fc.part_index << ") * " << G * (ni + 1) << " + t] = v;\n    }\n";
 }
 
 // Atomic path: group table in global memory.
@@ -1166,10 +1187,10 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
     os << ind << "} else {\n";
 }
 
-void emit_cache_init(std::ostringstream& os, const Plan& p) {
+void emit_cache_init(std::ostringstream& os, const Plan& p, bool declare_smem = true) {
     CacheLayout L = cache_layout(p);
     const std::string C = "vq_C";
-    os << "    extern __shared__ __align__(16) unsigned char vq_smem[];\n";
+    if (declare_smem) os << "    extern __shared__ __align__(16) unsigned char vq_smem[];\n";
     os << "    const int vq_C = P.cache_n;\n";
     os << "    for (int i = threadIdx.x; i < " << C << "; i += blockDim.x) {\n";
     os << "        " << L.first << "[i] = 0x7FFFFFFFFFFFFFFFLL;\n";
@@ -1557,21 +1578,10 @@ struct ScanLoop {
 
 }  // namespace
 
-// Generates the aggregate scan kernel (table → filter → project → aggregate).
-static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
-    std::ostringstream os;
-    std::set<int> cols;
-    collect_cols(p, p.pred, cols);
-    for (int k : key_nodes) collect_cols(p, k, cols);
-    for (auto& s : p.slots) collect_cols(p, s.input, cols);
-    ScanLoop loop(p, p.t, cols, block, "agg");
-    p.tile = loop.tile_rows();
-    p.smem = p.smem_groups > 0 ? cache_bytes(p) : loop.smem();
-    loop.prologue(os);
-    os << kernel_head("vq_agg", block);
-    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    if (p.smem_groups > 0) emit_cache_init(os, p);
-    loop.open(os);
+static std::string gen_kind_tables(const Plan& p, const std::string& prefix = "P_");
+
+// The four rows a lane holds in the current chunk: filter, project, aggregate.
+static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes) {
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     bool warp_sync = p.path != AggPath::Regs;  // atomic paths aggregate across the warp
@@ -1595,11 +1605,118 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
         emit_atomic_update_warp(os, p, "            ", order);
     }
     os << "        }\n";
+}
+
+// Generates the aggregate scan kernel (table → filter → project → aggregate).
+static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    for (int k : key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    ScanLoop loop(p, p.t, cols, block, "agg");
+    p.tile = loop.tile_rows();
+    p.smem = p.smem_groups > 0 ? cache_bytes(p) : loop.smem();
+    loop.prologue(os);
+    os << kernel_head("vq_agg", block);
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    if (p.smem_groups > 0) emit_cache_init(os, p);
+    loop.open(os);
+    emit_agg_rows(os, p, key_nodes);
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     if (p.smem_groups > 0) emit_cache_flush(os, p);
     os << "}\n";
     return os.str();
+}
+
+// Batch body: one plan's aggregate scan over chunks [cbeg, cend), run by all
+// warps of one block (warp w takes chunks cbeg+w, cbeg+w+warps, ...). The
+// register path writes its partial row at pslot; the dense path always carries
+// the shared-memory cache, sized at launch by P.cache_n (0 = none).
+static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    for (int k : p.key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    const int saved_groups = p.smem_groups;
+    if (p.path == AggPath::Dense) p.smem_groups = std::max(p.smem_groups, 1);
+    if (p.path == AggPath::Regs) os << gen_kind_tables(p, name + "_");
+    os << "__device__ __noinline__ void " << name
+       << "(const VQParams& P, const long long cbeg, const long long cend, const long long pslot, unsigned char* vq_smem) {\n";
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    if (p.smem_groups > 0) emit_cache_init(os, p, false);
+    os << "    const int lane = threadIdx.x & 31;\n";
+    os << "    for (long long c = cbeg + (threadIdx.x >> 5); c < cend; c += " << block / 32 << ") {\n";
+    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    emit_loads(os, p, p.t, cols, "cv", "cm", "r0", "        ", true);
+    emit_agg_rows(os, p, p.key_nodes);
+    os << "    }\n";
+    if (p.path == AggPath::Regs) {
+        FlushCtx fc;
+        fc.part_index = "pslot";
+        fc.kinds = name + "_";
+        fc.dyn_smem = true;
+        emit_regs_flush(os, p, block, fc);
+    }
+    if (p.smem_groups > 0) emit_cache_flush(os, p);
+    os << "}\n";
+    p.smem_groups = saved_groups;
+    return os.str();
+}
+
+std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::vector<int>& body_of, int& smem,
+                             int& nbodies) {
+    std::vector<std::string> bodies;
+    std::map<std::string, int> index;
+    body_of.clear();
+    smem = 0;
+    const std::string ph = "VQ_BODY_PLACEHOLDER";
+    for (Plan* p : plans) {
+        if (p->is_join) fail(VEXQ_ENOTSUP, "batched launches take aggregate plans");
+        std::string text = gen_agg_body(*p, ph, block);
+        auto it = index.find(text);
+        int b;
+        if (it == index.end()) {
+            b = (int)bodies.size();
+            index[text] = b;
+            bodies.push_back(text);
+        } else {
+            b = it->second;
+        }
+        body_of.push_back(b);
+        if (p->path == AggPath::Regs) smem = std::max(smem, regs_flush_smem(*p, block));
+    }
+    std::ostringstream os;
+    os << prelude_source() << "\n";
+    for (size_t b = 0; b < bodies.size(); b++) {
+        std::string t = bodies[b], nm = "vq_body_" + std::to_string(b);
+        for (size_t at = t.find(ph); at != std::string::npos; at = t.find(ph, at + nm.size())) t.replace(at, ph.size(), nm);
+        os << t << "\n";
+    }
+    os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") vq_batch(const __grid_constant__ VQBatchArgs A) {\n";
+    os << "    extern __shared__ __align__(16) unsigned char vq_smem[];\n";
+    os << "    __shared__ unsigned vq_unit;\n";
+    os << "    for (;;) {\n";
+    os << "        if (threadIdx.x == 0) vq_unit = atomicAdd(A.ticket, 1u);\n";
+    os << "        __syncthreads();\n";
+    os << "        const unsigned u = vq_unit;\n";
+    os << "        __syncthreads();\n";
+    os << "        if (u >= (unsigned)A.nunits) break;\n";
+    os << "        const VQUnit U = A.units[u];\n";
+    os << "        switch (U.body) {\n";
+    for (size_t b = 0; b < bodies.size(); b++)
+        os << "            case " << b << ": vq_body_" << b << "(A.params[U.plan], U.cbeg, U.cend, U.pslot, vq_smem); break;\n";
+    os << "        }\n    }\n}\n";
+    nbodies = (int)bodies.size();
+    return os.str();
+}
+
+int dense_cache_groups(const Plan& p, int cache_kb) {
+    if (p.path != AggPath::Dense || p.is_join || cache_kb <= 0) return 0;
+    int per = 8 + 8 * p.ni + 36 * p.nf;
+    return (int)std::min<int64_t>(p.domain, (int64_t)cache_kb * 1024 / per);
 }
 
 // Join build kernel: filtered build rows with non-NULL keys are inserted into
@@ -1698,7 +1815,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
 }
 
 // Kind tables used by the register-path flush (per bank entry).
-static std::string gen_kind_tables(const Plan& p) {
+static std::string gen_kind_tables(const Plan& p, const std::string& prefix) {
     std::ostringstream os;
     std::vector<int> fk(std::max(p.nf, 1), 0), ik(p.ni + 1, 0);
     for (size_t s = 0; s < p.slots.size(); s++) {
@@ -1708,10 +1825,10 @@ static std::string gen_kind_tables(const Plan& p) {
         else ik[p.slot_pos[s]] = code;
     }
     ik[p.ni] = 1;  // first-occurrence key: min
-    os << "__device__ __forceinline__ int P_fkind(int s) { switch (s) {";
+    os << "__device__ __forceinline__ int " << prefix << "fkind(int s) { switch (s) {";
     for (size_t i = 0; i < fk.size(); i++) os << " case " << i << ": return " << fk[i] << ";";
     os << " } return 0; }\n";
-    os << "__device__ __forceinline__ int P_ikind(int s) { switch (s) {";
+    os << "__device__ __forceinline__ int " << prefix << "ikind(int s) { switch (s) {";
     for (size_t i = 0; i < ik.size(); i++) os << " case " << i << ": return " << ik[i] << ";";
     os << " } return 0; }\n";
     return os.str();
@@ -1759,6 +1876,7 @@ static void choose_tunables(Plan& p) {
 }
 
 static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join, int build_key_node) {
+    p.key_nodes = key_nodes;
     analyze(p);
     // large IN/LIKE code sets go to device bitsets
     for (auto& n : p.ir) {

@@ -57,3 +57,20 @@ struct VQParams {
     int cache_n;               // dense path: groups held in the block's shared-memory cache
     int fx_lsb[16];            // per float-sum slot: exponent of the window's LSB
 };
+
+// One unit of a batched launch: chunks [cbeg, cend) of one plan, run by one
+// block; pslot is the unit's partial row within its plan (register path).
+struct VQUnit {
+    int plan;
+    int body;
+    long long cbeg, cend;
+    long long pslot;
+};
+
+// Parameters of a batched launch: blocks take units from *ticket in order.
+struct VQBatchArgs {
+    const VQParams* params;
+    const VQUnit* units;
+    unsigned* ticket;
+    int nunits;
+};

@@ -104,6 +104,7 @@ struct Plan {
     std::vector<int> slot_pos;     // slot → index within its float/int bank
     std::vector<int> fx_lsb;       // per float-sum slot
     std::vector<long long> lits;   // launch-time literal table (VQParams::lit)
+    std::vector<int> key_nodes;    // IR roots of the GROUP BY keys
     std::vector<std::vector<uint32_t>> sets;  // large InCodes sets (bitsets)
     std::vector<std::pair<int, int64_t>> presence;   // (column, code) rows: scanned / probe table
     std::vector<std::pair<int, int64_t>> bpresence;  // rows for the join build table
@@ -155,6 +156,68 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
 // Copies the plan's launch-time constants (literals, float-sum windows, cache size) into P.
 void set_plan_constants(const Plan& p, VQParams& P);
+// Source of one batched launch over aggregate plans of one class: a body per
+// distinct plan shape (body_of[i] for plans[i]) and the vq_batch dispatcher;
+// smem = dynamic shared memory the bodies need beyond the dense caches.
+std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::vector<int>& body_of, int& smem,
+                             int& nbodies);
+// Groups a dense plan caches in shared memory within cache_kb KB (0: not dense).
+int dense_cache_groups(const Plan& p, int cache_kb);
+
+// ---- runtime pieces shared by the plain and batched paths (run.cu) ----
+// Host-side group rows collected from either path.
+struct Groups {
+    std::vector<uint64_t> key;
+    std::vector<int64_t> first;
+    std::vector<std::vector<int64_t>> ival;   // per int-bank slot
+    std::vector<std::vector<double>> fval;    // per float-bank slot
+    size_t n() const { return key.size(); }
+};
+std::vector<long long> init_values(const Plan& p);
+vexq_result_s* build_result(Plan& p, Groups& g);
+int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build);
+long long estimate_groups(const Plan& p, long long rows, long long join_keys);
+void set_columns(VQParams& P, const Table& t, bool build_side);
+vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end);
+std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge);
+
+// Batched execution of many plans (batch.cu).
+struct Batch;
+Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags);
+void exec_batch(Batch& b, vexq_result_s** out);
+void destroy_batch(Batch* b);
+
+// Descriptors of batched launches (device arrays).
+struct VQTableDesc {           // one group table
+    unsigned long long* keys;
+    long long* first;
+    long long* acc_i;
+    long long* acc_fx;
+    unsigned* special;
+    const long long* init_i;
+    const int* fx_lsb;
+    long long nslots;
+    int ni, nf, hash;
+    unsigned long long* n_out;
+    unsigned long long* ngroups;
+    int* error;
+    unsigned long long* o_key;
+    long long* o_first;
+    long long* o_i;
+    double* o_f;
+    long long cap_out;
+    long long slot0;           // first global slot of this table
+};
+struct VQMergeDesc {           // one register-path plan's partials
+    const double* part_f;
+    const long long* part_i;
+    int nblocks, G, nf, ni;
+    const int* fkind;
+    const int* ikind;
+    double* out_f;
+    long long* out_i;
+    int e0;                    // first global merge entry of this plan
+};
 ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end, int unit);
 bool parse_date(const char* s, int64_t* days);
 

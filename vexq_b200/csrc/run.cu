@@ -38,12 +38,13 @@ __device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
     hi = s;
 }
 
-__global__ void __launch_bounds__(256) k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G,
-                                                    int nf, int ni, const int* fkind, const int* ikind, double* out_f,
-                                                    long long* out_i) {
+// One merged output entry of the register path: a fixed-order TwoSum tree
+// over the per-block partials (floats) or a min/max/sum fold (ints).
+__device__ void merge_entry(int e, const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
+                            const int* fkind, const int* ikind, double* out_f, long long* out_i) {
     __shared__ double sh[256], sl[256];
     __shared__ long long si[256];
-    const int e = blockIdx.x, t = threadIdx.x;
+    const int t = threadIdx.x;
     const int totf = G * nf, toti = G * (ni + 1);
     if (e < totf) {
         const int kind = fkind[e % nf];
@@ -85,6 +86,23 @@ __global__ void __launch_bounds__(256) k_merge_regs(const double* part_f, const 
     }
 }
 
+__global__ void __launch_bounds__(256) k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G,
+                                                    int nf, int ni, const int* fkind, const int* ikind, double* out_f,
+                                                    long long* out_i) {
+    merge_entry(blockIdx.x, part_f, part_i, nblocks, G, nf, ni, fkind, ikind, out_f, out_i);
+}
+
+// Batched merge: block b serves entry b - e0 of the plan whose range holds b.
+__global__ void __launch_bounds__(256) k_merge_batch(const VQMergeDesc* d, int n) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d[mid].e0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    const VQMergeDesc m = d[lo];
+    merge_entry((int)blockIdx.x - m.e0, m.part_f, m.part_i, m.nblocks, m.G, m.nf, m.ni, m.fkind, m.ikind, m.out_f, m.out_i);
+}
+
 // Atomic path: per-slot initial values (counts 0, MIN/MAX identities).
 __global__ void k_init_table(unsigned long long* keys, long long* first, long long* acc_i, int ni, const long long* init_i,
                              long long nslots, int hash) {
@@ -97,26 +115,72 @@ __global__ void k_init_table(unsigned long long* keys, long long* first, long lo
 
 // Compacts occupied slots (count > 0) and turns exact fixed-point sums into
 // correctly rounded doubles (NaN / ±inf flags applied IEEE-style).
+__device__ __forceinline__ void finalize_slot(long long i, const unsigned long long* keys, const long long* first,
+                                              const long long* acc_i, const long long* acc_fx, const unsigned* special,
+                                              long long nslots, int ni, int nf, const int* fx_lsb, int hash,
+                                              unsigned long long* n_out, unsigned long long* o_key, long long* o_first,
+                                              long long* o_i, double* o_f, long long cap_out) {
+    if (acc_i[i] == 0) return;  // slot 0 of the int bank is the row count
+    unsigned long long pos = atomicAdd(n_out, 1ull);
+    if ((long long)pos >= cap_out) return;
+    o_key[pos] = hash ? (i == nslots - 1 ? VQ_EMPTY_KEY : keys[i]) : (unsigned long long)i;
+    o_first[pos] = first[i];
+    for (int s = 0; s < ni; s++) o_i[(long long)s * cap_out + pos] = acc_i[(long long)s * nslots + i];
+    for (int f = 0; f < nf; f++) {
+        unsigned sp = special[(long long)f * nslots + i];
+        double v;
+        if ((sp & 1u) || (sp & 6u) == 6u) v = __longlong_as_double(0x7FF8000000000001LL);
+        else if (sp & 2u) v = __longlong_as_double(0x7FF0000000000000LL);
+        else if (sp & 4u) v = __longlong_as_double((long long)0xFFF0000000000000ULL);
+        else v = vq_fx_value(acc_fx + ((long long)f * nslots + i) * 4, fx_lsb[f]);
+        o_f[(long long)f * cap_out + pos] = v;
+    }
+}
+
 __global__ void k_finalize(const unsigned long long* keys, const long long* first, const long long* acc_i,
                            const long long* acc_fx, const unsigned* special, long long nslots, int ni, int nf,
                            const int* fx_lsb, int hash, unsigned long long* n_out, unsigned long long* o_key,
                            long long* o_first, long long* o_i, double* o_f, long long cap_out) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
-        if (acc_i[i] == 0) continue;  // slot 0 of the int bank is the row count
-        unsigned long long pos = atomicAdd(n_out, 1ull);
-        if ((long long)pos >= cap_out) continue;
-        o_key[pos] = hash ? (i == nslots - 1 ? VQ_EMPTY_KEY : keys[i]) : (unsigned long long)i;
-        o_first[pos] = first[i];
-        for (int s = 0; s < ni; s++) o_i[(long long)s * cap_out + pos] = acc_i[(long long)s * nslots + i];
-        for (int f = 0; f < nf; f++) {
-            unsigned sp = special[(long long)f * nslots + i];
-            double v;
-            if ((sp & 1u) || (sp & 6u) == 6u) v = __longlong_as_double(0x7FF8000000000001LL);
-            else if (sp & 2u) v = __longlong_as_double(0x7FF0000000000000LL);
-            else if (sp & 4u) v = __longlong_as_double((long long)0xFFF0000000000000ULL);
-            else v = vq_fx_value(acc_fx + ((long long)f * nslots + i) * 4, fx_lsb[f]);
-            o_f[(long long)f * cap_out + pos] = v;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x)
+        finalize_slot(i, keys, first, acc_i, acc_fx, special, nslots, ni, nf, fx_lsb, hash, n_out, o_key, o_first, o_i,
+                      o_f, cap_out);
+}
+
+// Batched group tables: global slot g belongs to the table whose slot0 is the
+// largest not above g.
+__device__ __forceinline__ int table_of(const VQTableDesc* d, int n, long long g) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d[mid].slot0 <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_init_batch(const VQTableDesc* d, int n, long long total) {
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        const VQTableDesc& t = d[table_of(d, n, g)];
+        const long long i = g - t.slot0;
+        if (t.hash) t.keys[i] = (i == t.nslots - 1) ? 0ull : VQ_EMPTY_KEY;
+        t.first[i] = 0x7FFFFFFFFFFFFFFFLL;
+        for (int s = 0; s < t.ni; s++) t.acc_i[(long long)s * t.nslots + i] = t.init_i[s];
+        for (int f = 0; f < t.nf; f++) {
+            for (int k = 0; k < 4; k++) t.acc_fx[((long long)f * t.nslots + i) * 4 + k] = 0;
+            t.special[(long long)f * t.nslots + i] = 0u;
         }
+        if (i == 0) {
+            *t.n_out = 0ull;
+            *t.ngroups = 0ull;
+            *t.error = 0;
+        }
+    }
+}
+
+__global__ void k_finalize_batch(const VQTableDesc* d, int n, long long total) {
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        const VQTableDesc& t = d[table_of(d, n, g)];
+        finalize_slot(g - t.slot0, t.keys, t.first, t.acc_i, t.acc_fx, t.special, t.nslots, t.ni, t.nf, t.fx_lsb, t.hash,
+                      t.n_out, t.o_key, t.o_first, t.o_i, t.o_f, t.cap_out);
     }
 }
 
@@ -263,8 +327,6 @@ double vq_fkey_inv_host(uint64_t k) {
     return d;
 }
 
-namespace {
-
 // Grid of a scan kernel: every SM filled to its occupancy, never more blocks
 // than loop units (staged kernels: one tile per block per iteration; chunk
 // loops: one 128-row chunk per warp).
@@ -287,15 +349,6 @@ void set_columns(VQParams& P, const Table& t, bool build_side) {
         }
     }
 }
-
-// Host-side group rows collected from either path.
-struct Groups {
-    std::vector<uint64_t> key;
-    std::vector<int64_t> first;
-    std::vector<std::vector<int64_t>> ival;   // per int-bank slot
-    std::vector<std::vector<double>> fval;    // per float-bank slot
-    size_t n() const { return key.size(); }
-};
 
 int64_t slot_int(const Plan& p, const Groups& g, int slot, size_t i) { return g.ival[p.slot_pos[slot]][i]; }
 
@@ -737,8 +790,6 @@ long long estimate_groups(const Plan& p, long long rows, long long join_keys) {
     return std::max<long long>(est, 1);
 }
 
-}  // namespace
-
 std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge) {
     std::vector<uint8_t> m(t.n_rg, 0);
     for (int rg = rgs; rg < rge; rg++) m[rg] = zone_eval(p, root, t, rg);
@@ -765,7 +816,7 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
     return r;
 }
 
-static int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build) {
+int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build) {
     // algorithmic bytes: reference width of every column of `t` the scan reads × rows
     std::set<int> cols;
     std::function<void(int)> walk = [&](int i) {

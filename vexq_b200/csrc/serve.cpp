@@ -69,10 +69,9 @@ int32_t vexq_batch_run(vexq_plan_t* plans, int32_t n, vexq_result_t* out_results
     return guard2([&]() -> int32_t {
         if (n < 0 || (n > 0 && (!plans || !out_results))) fail(VEXQ_EINVAL, "null argument");
         for (int i = 0; i < n; i++) out_results[i] = nullptr;
-        for (int i = 0; i < n; i++) {
-            std::lock_guard<std::mutex> lk(plan_mutex(plans[i]->p));
-            out_results[i] = run_plan(*plans[i]->p, 0, -1);
-        }
+        if (n == 0) return VEXQ_OK;
+        std::unique_ptr<Batch, void (*)(Batch*)> b(create_batch(plans, n, 0), destroy_batch);
+        exec_batch(*b, out_results);
         return VEXQ_OK;
     });
 }

@@ -8,6 +8,8 @@ this module gives tests and the benchmark the reference's shapes:
                                  (exec/aggregate.go:131, exec/parallel.go:78)
   GpuParallelHashJoinAggregate ≈ exec.NewParallelHashJoinAggregate (exec/parallel_join.go:718)
   GpuFilter                    ≈ exec.NewFilter + BoolToSelVecInto (exec/filter.go:40-78)
+  GpuBatch                     many prepared plans in one persistent launch per path class
+                               under a captured CUDA graph (no reference counterpart)
 
 Operators implement next() → Batch | None, schema() and close(), with ≤1024
 rows per batch and group-insertion order, like exec.Operator (exec/operator.go:28-32).
@@ -250,3 +252,41 @@ class GpuFilter:
         n = C.c_int32()
         abi.check(abi.load().vexq_selvec_from_bits(buf, nrows, block, sel, C.byref(n)))
         return list(sel[:n.value])
+
+
+class GpuBatch:
+    """Many prepared plans executed together: one persistent launch per path
+    class, replayed from a captured CUDA graph on every exec()."""
+
+    def __init__(self, ops, autotune: bool = False):
+        self.ops = list(ops)  # keeps the plans (and their tables) alive
+        n = len(self.ops)
+        arr = (C.c_void_p * max(n, 1))(*[op.h for op in self.ops])
+        self.h = C.c_void_p()
+        abi.check(abi.load().vexq_batch_create(arr, n, abi.BATCH_AUTOTUNE if autotune else 0, C.byref(self.h)))
+
+    def exec(self) -> List[Result]:
+        n = len(self.ops)
+        outs = (C.c_void_p * max(n, 1))()
+        abi.check(abi.load().vexq_batch_exec(self.h, outs))
+        return [Result(C.c_void_p(outs[i])) for i in range(n)]
+
+    def stats(self):
+        """(device ms of the replay, ms of its kernels alone, bytes scanned, rows scanned)"""
+        ms, km, b, r = C.c_double(), C.c_double(), C.c_int64(), C.c_int64()
+        abi.check(abi.load().vexq_batch_stats(self.h, C.byref(ms), C.byref(km), C.byref(b), C.byref(r)))
+        return ms.value, km.value, b.value, r.value
+
+    def explain(self) -> str:
+        return abi.load().vexq_batch_explain(self.h).decode()
+
+    def close(self):
+        if self.h:
+            abi.load().vexq_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
