@@ -290,9 +290,9 @@ int32_t vexq_selvec_from_bits(const uint8_t* bits, int64_t nrows, int64_t block,
  * as ONE persistent launch of a generated kernel with a body per distinct
  * plan shape, whose blocks take (plan, row-chunk range) units from an atomic
  * ticket, largest first. Table init, both launches (on forked streams), the
- * partial merge, the table finalize and one copy of all outputs to pinned
- * host memory are captured in a CUDA graph at creation and replayed by every
- * vexq_batch_exec. Join plans are not batched; they run after the graph, one
+ * partial merge and the table finalize are captured in a CUDA graph on the
+ * first vexq_batch_exec and replayed by every later one, each followed by one
+ * copy of all outputs to pinned host memory. Join plans are not batched; they run after the graph, one
  * after another. Results match vexq_plan_run's: keys, counts, integer
  * aggregates and group-table float sums bit for bit; register-path float sums
  * may differ in the last bits (a different row partition), both within their
@@ -314,11 +314,27 @@ int32_t vexq_batch_destroy(vexq_batch_t b);
 /* create + exec + destroy in one call. */
 int32_t vexq_batch_run(vexq_plan_t* plans, int32_t n, vexq_result_t* out_results);
 
-/* ---- serving loop ------------------------------------------------------ */
+/* ---- serving loop ------------------------------------------------------
+ * No reference counterpart (the Go engine serves no request loop).
+ * Tables and plans stay resident; queries are submitted as prepared plans.
+ * Admission: the head of the FIFO queue starts when a query slot is free
+ * (max_inflight) and its group/join-table footprint fits hbm_budget_bytes
+ * beside the queries in flight. Continuous batching: a free worker takes
+ * the queued aggregate queries that fit at that moment (up to
+ * max_inflight / nworkers) into ONE batched execution, or one join, so queries
+ * arriving while others are on the GPU join the next launch, and the
+ * launches of different workers (nworkers, each on its own streams) overlap
+ * on the device. flags: VEXQ_SERVE_NO_BATCH runs one query per launch
+ * through the plain per-query path. Results match vexq_plan_run's, as the
+ * batched execution's do. */
 typedef struct vexq_server_s* vexq_server_t;
-/* hbm_budget_bytes caps the summed hash-table footprint of in-flight
- * queries (admission); max_inflight caps concurrent query slots. */
-int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, vexq_server_t* out);
+#define VEXQ_SERVE_NO_BATCH 1u
+int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t nworkers, uint32_t flags,
+                          vexq_server_t* out);
+/* Launches so far, queries they carried, the largest launch and the most
+ * launches that were running at once. */
+int32_t vexq_server_stats(vexq_server_t s, int64_t* launches, int64_t* queries, int32_t* max_batch,
+                          int32_t* max_concurrent);
 /* Queues plan p; returns a ticket. A plan may be submitted many times. */
 int32_t vexq_server_submit(vexq_server_t s, vexq_plan_t p, int64_t* ticket);
 /* Non-blocking poll: *done = 1 and *out set when the ticket has finished. */

@@ -279,7 +279,7 @@ def test_batch_and_server_equal_single_runs(gpu_lib, lineitem_1m):
     for k in range(2):  # register-path FP64 sums: another row partition, last-bit differences
         assert_rows_match(X.Result(C.c_void_p(outs[k])).rows(), single[k], ordered=True, rtol=1e-13)
     srv = C.c_void_p()
-    abi.check(L.vexq_server_start(1 << 34, 3, C.byref(srv)))
+    abi.check(L.vexq_server_start(1 << 34, 3, 2, 0, C.byref(srv)))
     tickets = []
     for k in range(8):
         tk = C.c_int64()
@@ -288,5 +288,5 @@ def test_batch_and_server_equal_single_runs(gpu_lib, lineitem_1m):
     for k, tk in enumerate(tickets):
         h = C.c_void_p()
         abi.check(L.vexq_server_wait(srv, tk, 60000, C.byref(h)))
-        assert X.Result(h).rows() == single[k % 2]
+        assert_rows_match(X.Result(h).rows(), single[k % 2], ordered=True, rtol=1e-13)
     abi.check(L.vexq_server_stop(srv))

@@ -117,6 +117,7 @@ class BatchView(C.Structure):
 
 # Every symbol include/vexq_cuda.h declares (checked by the CPU test suite).
 BATCH_AUTOTUNE = 1  # VEXQ_BATCH_AUTOTUNE
+SERVE_NO_BATCH = 1  # VEXQ_SERVE_NO_BATCH
 
 EXPORTS = [
     "vexq_init", "vexq_last_error", "vexq_abi_version",
@@ -138,6 +139,7 @@ EXPORTS = [
     "vexq_batch_stats",
     "vexq_batch_explain",
     "vexq_batch_destroy",
+    "vexq_server_stats",
 ]
 
 _lib = None
@@ -189,7 +191,8 @@ def load() -> C.CDLL:
                                   C.POINTER(C.c_uint8), C.POINTER(i64)]),
         "vexq_selvec_from_bits": (i32, [C.POINTER(C.c_uint8), i64, i64, C.POINTER(C.c_uint16), C.POINTER(i32)]),
         "vexq_batch_run": (i32, [C.POINTER(vp), i32, C.POINTER(vp)]),
-        "vexq_server_start": (i32, [i64, i32, C.POINTER(vp)]),
+        "vexq_server_start": (i32, [i64, i32, i32, C.c_uint32, C.POINTER(vp)]),
+        "vexq_server_stats": (i32, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]),
         "vexq_server_submit": (i32, [vp, vp, C.POINTER(i64)]),
         "vexq_server_poll": (i32, [vp, i64, C.POINTER(i32), C.POINTER(vp)]),
         "vexq_server_wait": (i32, [vp, i64, i64, C.POINTER(vp)]),

@@ -6,9 +6,9 @@
 // holds a body per distinct plan shape: blocks take (plan, chunk range) units
 // from an atomic ticket, largest units first, so uneven plans share the GPU
 // without one launch each. Table init, the class launches (on two forked
-// streams), the partial merge, the table finalize and one copy of every
-// output back to pinned host memory are captured once in a CUDA graph and
-// replayed by each execution. The autotuner picks the shared-memory group
+// streams), the partial merge and the table finalize are captured once in a
+// CUDA graph and replayed by each execution, followed by one copy of every
+// output back to pinned host memory. The autotuner picks the shared-memory group
 // cache size (the shared-versus-global table cutover) and the unit size by
 // timing graph replays. Join plans are not batched: they run after the graph,
 // one after another, as vexq_plan_run would run them.
@@ -80,6 +80,8 @@ struct Batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     double device_ms = 0, kernel_ms = 0;
+    bool capturing = false;
+    void chk(cudaStream_t st, const char* what) const { if (!capturing) launch_check(st, what); }
     int64_t bytes = 0, rows = 0;
     std::string explain;
 
@@ -303,16 +305,17 @@ struct Batch {
         return m;
     }
 
-    void capture() {
-        drop_graph();
+    // Issues one execution on s (group tables, copy back) and s2 (register
+    // path), forked and joined with events; captured once or launched directly.
+    void enqueue() {
         char* D = (char*)dev.p;
-        VQ_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         VQ_CUDA(cudaMemsetAsync(D + a_ticket, 0, 16, s));
         VQ_CUDA(cudaMemsetAsync((char*)out.p + o_aerr, 0, 8, s));
         if (table_slots > 0) {
             int g = (int)std::min<long long>((table_slots + 255) / 256, (long long)sm_count() * 16);
             k_init_batch<<<g, 256, 0, s>>>((const VQTableDesc*)(D + a_tdesc), n_tdesc, table_slots);
             VQ_CUDA(cudaGetLastError());
+            chk(s, "k_init_batch");
         }
         VQ_CUDA(cudaEventRecord(ev[2], s));
         VQ_CUDA(cudaStreamWaitEvent(s2, ev[2], 0));
@@ -321,41 +324,74 @@ struct Batch {
                 VQBatchArgs A{(const VQParams*)(D + a_params), (const VQUnit*)(D + ck[0].a_units), (unsigned*)(D + a_ticket),
                               (int)ck[0].nunits};
                 jit_launch(ck[0].k, ck[0].grid, &A, sizeof A, s2);
+                chk(s2, "vq_batch (register path)");
             }
             if (merge_entries > 0) {
                 k_merge_batch<<<merge_entries, 256, 0, s2>>>((const VQMergeDesc*)(D + a_mdesc), n_mdesc);
                 VQ_CUDA(cudaGetLastError());
+                chk(s2, "k_merge_batch");
             }
         }
         if (ck[1].nunits > 0) {
             VQBatchArgs A{(const VQParams*)(D + a_params), (const VQUnit*)(D + ck[1].a_units), (unsigned*)(D + a_ticket) + 1,
                           (int)ck[1].nunits};
             jit_launch(ck[1].k, ck[1].grid, &A, sizeof A, s);
+            chk(s, "vq_batch (group tables)");
         }
         if (table_slots > 0) {
             int g = (int)std::min<long long>((table_slots + 255) / 256, (long long)sm_count() * 16);
             k_finalize_batch<<<g, 256, 0, s>>>((const VQTableDesc*)(D + a_tdesc), n_tdesc, table_slots);
             VQ_CUDA(cudaGetLastError());
+            chk(s, "k_finalize_batch");
         }
         VQ_CUDA(cudaEventRecord(ev[3], s2));
         VQ_CUDA(cudaStreamWaitEvent(s, ev[3], 0));
-        VQ_CUDA(cudaEventRecord(ev[4], s));
-        VQ_CUDA(cudaMemcpyAsync(h_out.p, out.p, out_bytes, cudaMemcpyDeviceToHost, s));
+    }
+
+    void capture() {
+        drop_graph();
+        VQ_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        try {
+            enqueue();
+        } catch (...) {
+            capturing = false;
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        capturing = false;
         VQ_CUDA(cudaStreamEndCapture(s, &graph));
         VQ_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
     }
 
-    float replay() {
-        if (!gexec) capture();
-        VQ_CUDA(cudaEventRecord(ev[0], s));
-        VQ_CUDA(cudaGraphLaunch(gexec, s));
+    // kernels done → copy every output back → done (events outside any graph)
+    float finish_timing() {
+        VQ_CUDA(cudaEventRecord(ev[4], s));
+        VQ_CUDA(cudaMemcpyAsync(h_out.p, out.p, out_bytes, cudaMemcpyDeviceToHost, s));
         VQ_CUDA(cudaEventRecord(ev[1], s));
         VQ_CUDA(cudaStreamSynchronize(s));
         float ms = 0, km = 0;
         VQ_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
         VQ_CUDA(cudaEventElapsedTime(&km, ev[0], ev[4]));
         kernel_ms = km;
+        device_ms = ms;
         return ms;
+    }
+
+    float replay() {
+        if (!gexec) capture();
+        VQ_CUDA(cudaEventRecord(ev[0], s));
+        VQ_CUDA(cudaGraphLaunch(gexec, s));
+        return finish_timing();
+    }
+
+    // One execution launched directly, for plan sets that run once.
+    float run_direct() {
+        VQ_CUDA(cudaEventRecord(ev[0], s));
+        enqueue();
+        return finish_timing();
     }
 
     // grid of each class at the current shared-memory size
@@ -396,9 +432,21 @@ struct Batch {
     }
 };
 
-Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags) {
-    std::unique_ptr<Batch> b(new Batch);
+// (Re)builds a batch over a plan set: ranges, classes, generated source,
+// grids and layout. Device buffers only grow, so a reused batch allocates
+// nothing once it has seen its largest plan set.
+void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
+    b->drop_graph();
     b->handles.assign(handles, handles + n);
+    b->items.clear();
+    b->bytes = b->rows = 0;
+    for (int c = 0; c < 2; c++) {
+        b->ck[c].items.clear();
+        b->ck[c].k_src.clear();
+        b->ck[c].nunits = 0;
+        b->ck[c].nbodies = 0;
+        b->ck[c].smem_extra = 0;
+    }
     for (int i = 0; i < n; i++) {
         Item it;
         Plan* p = handles[i]->p;
@@ -454,20 +502,30 @@ Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags) {
         b->ck[c].nbodies = nb;
         for (size_t j = 0; j < ps.size(); j++) b->items[b->ck[c].items[j]].body = body_of[j];
     }
+    b->size_grids();
+    b->layout();
+}
+
+Batch* new_batch() {
+    std::unique_ptr<Batch> b(new Batch);
     VQ_CUDA(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
     VQ_CUDA(cudaStreamCreateWithFlags(&b->s2, cudaStreamNonBlocking));
     for (auto& e : b->ev) VQ_CUDA(cudaEventCreate(&e));
-    b->size_grids();
-    b->layout();
+    return b.release();
+}
+
+Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags) {
+    std::unique_ptr<Batch> b(new_batch());
+    build_batch(b.get(), handles, n);
     if (flags & VEXQ_BATCH_AUTOTUNE) b->autotune();
     return b.release();
 }
 
-// One result per plan, in plan order.
-void exec_batch(Batch& b, vexq_result_s** out) {
+// Results of the last execution, one per plan in plan order; plans that did
+// not run in the batch (joins, hash-table overflow) run on their own here.
+static void collect(Batch& b, vexq_result_s** out) {
     const size_t n = b.items.size();
     for (size_t i = 0; i < n; i++) out[i] = nullptr;
-    b.device_ms = b.replay();
     const char* H = (const char*)b.h_out.p;
     std::vector<char> plain(n, 0);
     std::vector<std::string> errs(n);
@@ -524,7 +582,11 @@ void exec_batch(Batch& b, vexq_result_s** out) {
             }
         }
     };
-    const int nt = (int)std::max<size_t>(1, std::min<size_t>({n, (size_t)16, (size_t)std::max(1u, std::thread::hardware_concurrency())}));
+    // host threads only pay off when there are many groups to order
+    size_t groups = 0;
+    for (const Item& it : b.items) groups += it.cls == 1 ? (size_t)it.cap_out : (size_t)it.G;
+    const int nt = groups < 200000 ? 1
+                   : (int)std::max<size_t>(1, std::min<size_t>({n, (size_t)16, (size_t)std::max(1u, std::thread::hardware_concurrency())}));
     std::vector<std::thread> th;
     for (int t = 1; t < nt; t++) th.emplace_back(work);
     work();
@@ -539,12 +601,28 @@ void exec_batch(Batch& b, vexq_result_s** out) {
         if (codes[i]) { release(); fail(codes[i], errs[i]); }
     try {
         for (size_t i = 0; i < n; i++)
-            if (plain[i]) out[i] = run_plan(*b.items[i].p, 0, -1);
+            if (plain[i]) {
+                std::lock_guard<std::mutex> lk(plan_mutex(b.items[i].p));
+                out[i] = run_plan(*b.items[i].p, 0, -1);
+            }
     } catch (...) {
         release();
         throw;
     }
 }
+
+void exec_batch(Batch& b, vexq_result_s** out) {
+    b.replay();
+    collect(b, out);
+}
+
+void run_batch_direct(Batch& b, vexq_plan_s* const* handles, int n, vexq_result_s** out) {
+    build_batch(&b, handles, n);
+    b.run_direct();
+    collect(b, out);
+}
+
+double batch_kernel_ms(const Batch& b) { return b.kernel_ms; }
 
 void destroy_batch(Batch* b) { delete b; }
 

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <numeric>
 #include <set>
 #include <sstream>
 
@@ -1251,7 +1252,8 @@ void emit_cache_flush(std::ostringstream& os, const Plan& p) {
 // keys, and float sums fold 128-bit fixed-point images of the values (the
 // same integers the single-row update would add). When no two lanes of the
 // warp share a group every lane updates its own row without reducing.
-void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
+void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order,
+                             bool cache) {
     const std::string in = ind + "    ";
     os << ind << "unsigned long long slot = VQ_NOSLOT;\n";
     if (p.path == AggPath::Dense) os << ind << "if (live) slot = key;\n";
@@ -1352,7 +1354,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     os << in << "}\n";
     os << in << "if (lead) {\n";
     std::string in3 = in + "    ";
-    if (p.smem_groups > 0) emit_cache_update(os, p, in3);
+    if (cache) emit_cache_update(os, p, in3);
     os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s);
@@ -1374,7 +1376,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
                 break;
         }
     }
-    if (p.smem_groups > 0) os << in3 << "}\n";  // closes the global branch opened by emit_cache_update
+    if (cache) os << in3 << "}\n";  // closes the global branch opened by emit_cache_update
     os << in << "}\n" << ind << "}\n";
 }
 
@@ -1581,7 +1583,7 @@ struct ScanLoop {
 static std::string gen_kind_tables(const Plan& p, const std::string& prefix = "P_");
 
 // The four rows a lane holds in the current chunk: filter, project, aggregate.
-static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes) {
+static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool cache) {
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     bool warp_sync = p.path != AggPath::Regs;  // atomic paths aggregate across the warp
@@ -1602,7 +1604,7 @@ static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int
         if (p.regs_pred) emit_regs_update_pred(os, p, "            ", order);
         else emit_regs_update(os, p, "            ", order);
     } else {
-        emit_atomic_update_warp(os, p, "            ", order);
+        emit_atomic_update_warp(os, p, "            ", order, cache);
     }
     os << "        }\n";
 }
@@ -1622,7 +1624,7 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     if (p.smem_groups > 0) emit_cache_init(os, p);
     loop.open(os);
-    emit_agg_rows(os, p, key_nodes);
+    emit_agg_rows(os, p, key_nodes, p.smem_groups > 0);
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     if (p.smem_groups > 0) emit_cache_flush(os, p);
@@ -1640,18 +1642,17 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
     collect_cols(p, p.pred, cols);
     for (int k : p.key_nodes) collect_cols(p, k, cols);
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
-    const int saved_groups = p.smem_groups;
-    if (p.path == AggPath::Dense) p.smem_groups = std::max(p.smem_groups, 1);
+    const bool cache = p.path == AggPath::Dense;  // sized at launch by P.cache_n (0 = none)
     if (p.path == AggPath::Regs) os << gen_kind_tables(p, name + "_");
     os << "__device__ __noinline__ void " << name
        << "(const VQParams& P, const long long cbeg, const long long cend, const long long pslot, unsigned char* vq_smem) {\n";
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    if (p.smem_groups > 0) emit_cache_init(os, p, false);
+    if (cache) emit_cache_init(os, p, false);
     os << "    const int lane = threadIdx.x & 31;\n";
     os << "    for (long long c = cbeg + (threadIdx.x >> 5); c < cend; c += " << block / 32 << ") {\n";
     os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
     emit_loads(os, p, p.t, cols, "cv", "cm", "r0", "        ", true);
-    emit_agg_rows(os, p, p.key_nodes);
+    emit_agg_rows(os, p, p.key_nodes, cache);
     os << "    }\n";
     if (p.path == AggPath::Regs) {
         FlushCtx fc;
@@ -1660,9 +1661,8 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
         fc.dyn_smem = true;
         emit_regs_flush(os, p, block, fc);
     }
-    if (p.smem_groups > 0) emit_cache_flush(os, p);
+    if (cache) emit_cache_flush(os, p);
     os << "}\n";
-    p.smem_groups = saved_groups;
     return os.str();
 }
 
@@ -1675,7 +1675,13 @@ std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::ve
     const std::string ph = "VQ_BODY_PLACEHOLDER";
     for (Plan* p : plans) {
         if (p->is_join) fail(VEXQ_ENOTSUP, "batched launches take aggregate plans");
-        std::string text = gen_agg_body(*p, ph, block);
+        std::string text;
+        {
+            std::lock_guard<std::mutex> lk(p->body_mu);
+            auto it = p->batch_body.find(block);
+            if (it == p->batch_body.end()) it = p->batch_body.emplace(block, gen_agg_body(*p, ph, block)).first;
+            text = it->second;
+        }
         auto it = index.find(text);
         int b;
         if (it == index.end()) {
@@ -1688,6 +1694,16 @@ std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::ve
         body_of.push_back(b);
         if (p->path == AggPath::Regs) smem = std::max(smem, regs_flush_smem(*p, block));
     }
+    // number the bodies in text order, so the same set of plan shapes gives the
+    // same source (and one compiled module) whatever order the plans come in
+    std::vector<int> order(bodies.size()), rank(bodies.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int c) { return bodies[a] < bodies[c]; });
+    for (size_t r = 0; r < order.size(); r++) rank[order[r]] = (int)r;
+    for (int& b : body_of) b = rank[b];
+    std::vector<std::string> sorted(bodies.size());
+    for (size_t b = 0; b < bodies.size(); b++) sorted[rank[b]] = bodies[b];
+    bodies.swap(sorted);
     std::ostringstream os;
     os << prelude_source() << "\n";
     for (size_t b = 0; b < bodies.size(); b++) {

@@ -10,6 +10,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -62,6 +63,7 @@ uint64_t fnv1a(const std::string& s) {
 }
 
 std::mutex g_mu;
+std::map<uint64_t, std::shared_ptr<std::mutex>> g_compiling;  // per source: compile and load once
 std::map<uint64_t, std::vector<char>> g_cubins;
 std::map<std::pair<uint64_t, int>, std::shared_ptr<JitModule>> g_modules;  // (hash, device)
 
@@ -99,7 +101,9 @@ std::vector<char> compile_cubin(const std::string& src, uint64_t h) {
     std::vector<char> cubin(n);
     nvrtcGetCUBIN(prog, cubin.data());
     nvrtcDestroyProgram(&prog);
-    std::string tmp = path + ".tmp" + std::to_string(getpid());
+    // unique per writer: threads of one process compile the same source too
+    static std::atomic<unsigned long long> seq{0};
+    std::string tmp = path + ".tmp" + std::to_string(getpid()) + "." + std::to_string(seq++);
     {
         std::ofstream f(tmp, std::ios::binary);
         f.write(cubin.data(), (std::streamsize)cubin.size());
@@ -147,6 +151,16 @@ std::string jit_cache_dir() {
 JitKernel jit_get(const std::string& source, const std::string& entry, int block, int smem) {
     uint64_t h = fnv1a(source) ^ (fnv1a(entry) * 31);
     for (const char* o : kOptions) h = h * 1099511628211ull ^ fnv1a(o);
+    // one compile and one module load per source: a thread that finds another
+    // working on the same source waits for it
+    std::shared_ptr<std::mutex> cm;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto& slot = g_compiling[h];
+        if (!slot) slot = std::make_shared<std::mutex>();
+        cm = slot;
+    }
+    std::lock_guard<std::mutex> same_source(*cm);
     std::vector<char> cubin;
     {
         std::lock_guard<std::mutex> lk(g_mu);

@@ -105,6 +105,8 @@ struct Plan {
     std::vector<int> fx_lsb;       // per float-sum slot
     std::vector<long long> lits;   // launch-time literal table (VQParams::lit)
     std::vector<int> key_nodes;    // IR roots of the GROUP BY keys
+    std::mutex body_mu;            // batch body text per block size, generated once
+    std::map<int, std::string> batch_body;
     std::vector<std::vector<uint32_t>> sets;  // large InCodes sets (bitsets)
     std::vector<std::pair<int, int64_t>> presence;   // (column, code) rows: scanned / probe table
     std::vector<std::pair<int, int64_t>> bpresence;  // rows for the join build table
@@ -179,6 +181,11 @@ int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build)
 long long estimate_groups(const Plan& p, long long rows, long long join_keys);
 void set_columns(VQParams& P, const Table& t, bool build_side);
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end);
+// One plain run of a plan at a time: its group/join tables are per plan.
+std::mutex& plan_mutex(Plan* p);
+// VEXQ_SYNC_CHECK=1: synchronise after every launch and name the kernel on
+// an error (diagnostics; off by default).
+void launch_check(cudaStream_t s, const char* what);
 std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge);
 
 // Batched execution of many plans (batch.cu).
@@ -186,6 +193,11 @@ struct Batch;
 Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags);
 void exec_batch(Batch& b, vexq_result_s** out);
 void destroy_batch(Batch* b);
+// A reusable batch workspace (streams, events, grow-only buffers) and one
+// direct, uncaptured execution of a plan set on it (the serving loop's launch).
+Batch* new_batch();
+void run_batch_direct(Batch& b, vexq_plan_s* const* handles, int n, vexq_result_s** out);
+double batch_kernel_ms(const Batch& b);
 
 // Descriptors of batched launches (device arrays).
 struct VQTableDesc {           // one group table

@@ -432,9 +432,11 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+    launch_check(rc.s, "p.k_main");
     VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
     int tot = G * nf + G * (ni + 1);
     k_merge_regs<<<tot, 256, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + nfb, out_f, out_i);
+    launch_check(rc.s, "k_merge_regs");
     VQ_CUDA(cudaGetLastError());
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
     VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
@@ -524,14 +526,17 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         if (b_fx) VQ_CUDA(cudaMemsetAsync(P.acc_fx, 0, b_fx + b_sp, rc.s));
         int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
         k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
+        launch_check(rc.s, "k_init_table");
         VQ_CUDA(cudaGetLastError());
         int grid = grid_for(p.k_main, nchunks, p.staged);
         VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
         jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+        launch_check(rc.s, "p.k_main");
         VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
         int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
         k_finalize<<<fg, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, P.acc_fx, P.special, nslots, ni, nf, d_lsb, hash, n_out,
                                          c.key, c.first, c.ival, c.fval, cap_out);
+        launch_check(rc.s, "k_finalize");
         VQ_CUDA(cudaGetLastError());
         VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
         p.h_stage.ensure(32);
@@ -580,6 +585,7 @@ Groups fetch_groups(RunCtx& rc, const Compacted& c, const std::vector<long long>
     long long* dout = dsel + n;
     VQ_CUDA(cudaMemcpyAsync(dsel, subset->data(), n * 8, cudaMemcpyHostToDevice, rc.s));
     k_gather<<<(int)((n + 127) / 128), 128, 0, rc.s>>>(dsel, n, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni, p.nf, dout);
+    launch_check(rc.s, "k_gather");
     VQ_CUDA(cudaGetLastError());
     std::vector<long long> h((size_t)n * w);
     VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
@@ -623,8 +629,11 @@ bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel
     int g = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
     k_sortkey<<<g, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot], keyv,
                                    keynull, fmin_key);
+    launch_check(rc.s, "k_sortkey");
     k_rank<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, rank);
+    launch_check(rc.s, "k_rank");
     k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n, S, samp);
+    launch_check(rc.s, "k_sample");
     std::vector<unsigned long long> hs(S);
     VQ_CUDA(cudaMemcpyAsync(hs.data(), samp, S * 8, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
@@ -638,6 +647,7 @@ bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel
     for (int attempt = 0; attempt < 2; attempt++) {
         VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
         k_select<<<g, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
+        launch_check(rc.s, "k_select");
         VQ_CUDA(cudaGetLastError());
         unsigned long long ns = 0;
         VQ_CUDA(cudaMemcpyAsync(&ns, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
@@ -842,6 +852,26 @@ int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build)
     return w * rows;
 }
 
+std::mutex& plan_mutex(Plan* p) {
+    static std::mutex m;
+    static std::map<Plan*, std::unique_ptr<std::mutex>> mus;
+    std::lock_guard<std::mutex> lk(m);
+    auto& u = mus[p];
+    if (!u) u.reset(new std::mutex);
+    return *u;
+}
+
+void launch_check(cudaStream_t s, const char* what) {
+    static const bool on = [] {
+        const char* e = std::getenv("VEXQ_SYNC_CHECK");
+        return e && *e && *e != '0';
+    }();
+    if (!on) return;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) fail(VEXQ_EDEVICE, std::string("after ") + what + ": " + cudaGetErrorString(e));
+}
+
 cudaStream_t plan_stream(Plan& p) {
     if (p.ext_stream) return p.ext_stream;
     if (!p.stream) VQ_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
@@ -908,18 +938,26 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
             int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
             k_fill_u64<<<ig, 256, 0, rc.s>>>(B.jkeys, jcap, VQ_EMPTY_KEY);
+            launch_check(rc.s, "k_fill_u64");
             VQ_CUDA(cudaMemsetAsync(B.jkeys + jcap, 0, 8, rc.s));
             B.mode = 0;
             int grid = grid_for(p.k_build, bs.nchunks, p.staged);
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
+            if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
             int nb = (int)((nslots + 4095) / 4096);
             k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);
+            launch_check(rc.s, "k_scan_blocks");
             k_scan_sums<<<1, 1024, 0, rc.s>>>(bsums, nb);
+            launch_check(rc.s, "k_scan_sums");
             k_scan_add<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, nslots, bsums);
+            launch_check(rc.s, "k_scan_add");
             B.mode = 1;
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
+            if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
             k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error);
+            launch_check(rc.s, "k_sort_chains");
             k_pack_meta<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, B.jcount, p.jt_meta.as<int2>(), nslots);
+            launch_check(rc.s, "k_pack_meta");
             VQ_CUDA(cudaGetLastError());
             int herr = 0;
             unsigned long long nk = 0;

@@ -28,20 +28,13 @@ int32_t guard2(F&& f) {
     }
 }
 
-std::mutex& plan_mutex(Plan* p) {
-    static std::mutex m;
-    static std::map<Plan*, std::unique_ptr<std::mutex>> mus;
-    std::lock_guard<std::mutex> lk(m);
-    auto& u = mus[p];
-    if (!u) u.reset(new std::mutex);
-    return *u;
-}
-
 }  // namespace
 
 struct vexq_server_s {
     int64_t budget;
     int max_inflight;
+    int nworkers = 1;
+    bool batching = true;
     std::mutex mu;
     std::condition_variable cv, done_cv;
     struct Ticket {
@@ -61,7 +54,59 @@ struct vexq_server_s {
     bool stop = false;
     std::vector<std::thread> workers;
     int device = 0;
+    // launch statistics
+    int64_t launches = 0, launched_queries = 0;
+    int max_batch = 0, running = 0, max_running = 0;
 };
+
+namespace {
+
+// Runs one admitted set: aggregate plans together in one direct batched
+// execution on the worker's workspace, joins on their own (their plan owns the
+// join-table buffers, so one run at a time per plan). A failing batch is rerun
+// plan by plan so each ticket gets its own status.
+void run_admitted(Batch* ws, const std::vector<vexq_plan_s*>& pls, std::vector<vexq_result_s*>& res,
+                  std::vector<int32_t>& st, std::vector<std::string>& err, bool batching) {
+    const size_t n = pls.size();
+    res.assign(n, nullptr);
+    st.assign(n, VEXQ_OK);
+    err.assign(n, std::string());
+    auto one = [&](size_t i) {
+        try {
+            std::lock_guard<std::mutex> plk(plan_mutex(pls[i]->p));
+            res[i] = run_plan(*pls[i]->p, 0, -1);
+        } catch (const Status& e) {
+            st[i] = e.code;
+            err[i] = e.what();
+        } catch (const std::exception& e) {
+            st[i] = VEXQ_EINVAL;
+            err[i] = e.what();
+        }
+    };
+    std::vector<size_t> aggs;
+    for (size_t i = 0; i < n; i++) {
+        if (batching && !pls[i]->p->is_join) aggs.push_back(i);
+        else one(i);
+    }
+    if (aggs.empty()) return;
+    std::vector<vexq_plan_s*> ap;
+    for (size_t i : aggs) ap.push_back(pls[i]);
+    std::vector<vexq_result_s*> out(ap.size(), nullptr);
+    std::string first_err;
+    try {
+        run_batch_direct(*ws, ap.data(), (int)ap.size(), out.data());
+        for (size_t k = 0; k < aggs.size(); k++) res[aggs[k]] = out[k];
+        return;
+    } catch (const std::exception& e) {
+        first_err = e.what();
+    }
+    for (size_t i : aggs) {
+        one(i);
+        if (st[i] != VEXQ_OK) err[i] += " (the batched run failed first: " + first_err + ")";
+    }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -76,60 +121,81 @@ int32_t vexq_batch_run(vexq_plan_t* plans, int32_t n, vexq_result_t* out_results
     });
 }
 
-int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, vexq_server_t* out) {
+int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t nworkers, uint32_t flags,
+                          vexq_server_t* out) {
     return guard2([&]() -> int32_t {
-        if (!out || max_inflight < 1 || hbm_budget_bytes <= 0) fail(VEXQ_EINVAL, "bad server parameters");
+        if (!out || max_inflight < 1 || hbm_budget_bytes <= 0 || nworkers < 1) fail(VEXQ_EINVAL, "bad server parameters");
         auto* s = new vexq_server_s;
         s->budget = hbm_budget_bytes;
         s->max_inflight = max_inflight;
+        s->nworkers = nworkers;
+        s->batching = !(flags & VEXQ_SERVE_NO_BATCH);
         cudaGetDevice(&s->device);
-        for (int w = 0; w < max_inflight; w++) {
+        for (int w = 0; w < nworkers; w++) {
             s->workers.emplace_back([s]() {
                 cudaSetDevice(s->device);
+                std::unique_ptr<Batch, void (*)(Batch*)> ws(nullptr, destroy_batch);
+                try {
+                    ws.reset(new_batch());
+                } catch (...) {
+                    return;
+                }
                 for (;;) {
-                    int64_t id;
-                    vexq_plan_s* pl;
-                    int64_t fp;
+                    std::vector<int64_t> ids;
+                    std::vector<vexq_plan_s*> pls;
+                    int64_t fp = 0;
                     {
                         std::unique_lock<std::mutex> lk(s->mu);
-                        // admission: the head of the queue starts when its footprint fits
+                        // admission: the head of the queue starts when a slot is free
+                        // and its footprint fits the budget beside what is in flight
                         s->cv.wait(lk, [&] {
                             if (s->stop) return true;
-                            if (s->queue.empty()) return false;
+                            if (s->queue.empty() || s->inflight >= s->max_inflight) return false;
                             auto& t = s->tickets[s->queue.front()];
                             return s->inflight == 0 || s->inflight_bytes + t.plan->footprint <= s->budget;
                         });
                         if (s->stop) return;
-                        id = s->queue.front();
-                        s->queue.pop_front();
-                        pl = s->tickets[id].plan;
-                        fp = pl->footprint;
-                        s->inflight_bytes += fp;
-                        s->inflight++;
+                        // continuous batching: queued aggregates that fit join this
+                        // launch, up to an equal share of the slots so the other
+                        // workers can launch beside it; a join is a launch of its own
+                        const int cap = std::max(1, s->max_inflight / s->nworkers);
+                        while (!s->queue.empty() && s->inflight < s->max_inflight && (int)ids.size() < cap) {
+                            auto& t = s->tickets[s->queue.front()];
+                            if (s->inflight > 0 && s->inflight_bytes + t.plan->footprint > s->budget) break;
+                            const bool join = t.plan->p->is_join;
+                            if (join && !ids.empty()) break;
+                            ids.push_back(s->queue.front());
+                            pls.push_back(t.plan);
+                            fp += t.plan->footprint;
+                            s->inflight_bytes += t.plan->footprint;
+                            s->inflight++;
+                            s->queue.pop_front();
+                            if (!s->batching || join) break;
+                        }
+                        s->launches++;
+                        s->launched_queries += (int64_t)ids.size();
+                        s->max_batch = std::max(s->max_batch, (int)ids.size());
+                        s->running++;
+                        s->max_running = std::max(s->max_running, s->running);
                     }
-                    vexq_result_s* r = nullptr;
-                    int32_t st = VEXQ_OK;
-                    std::string err;
-                    try {
-                        std::lock_guard<std::mutex> plk(plan_mutex(pl->p));
-                        r = run_plan(*pl->p, 0, -1);
-                    } catch (const Status& e) {
-                        st = e.code;
-                        err = e.what();
-                    } catch (const std::exception& e) {
-                        st = VEXQ_EINVAL;
-                        err = e.what();
-                    }
+                    std::vector<vexq_result_s*> res;
+                    std::vector<int32_t> st;
+                    std::vector<std::string> err;
+                    run_admitted(ws.get(), pls, res, st, err, s->batching);
                     {
                         std::lock_guard<std::mutex> lk(s->mu);
-                        auto& t = s->tickets[id];
-                        t.result = r;
-                        t.status = st;
-                        t.err = err;
-                        t.done = true;
-                        t.finished = std::chrono::steady_clock::now();
+                        auto now = std::chrono::steady_clock::now();
+                        for (size_t k = 0; k < ids.size(); k++) {
+                            auto& t = s->tickets[ids[k]];
+                            t.result = res[k];
+                            t.status = st[k];
+                            t.err = err[k];
+                            t.done = true;
+                            t.finished = now;
+                        }
                         s->inflight_bytes -= fp;
-                        s->inflight--;
+                        s->inflight -= (int)ids.size();
+                        s->running--;
                     }
                     s->cv.notify_all();
                     s->done_cv.notify_all();
@@ -137,6 +203,19 @@ int32_t vexq_server_start(int64_t hbm_budget_bytes, int32_t max_inflight, vexq_s
             });
         }
         *out = s;
+        return VEXQ_OK;
+    });
+}
+
+int32_t vexq_server_stats(vexq_server_t s, int64_t* launches, int64_t* queries, int32_t* max_batch,
+                          int32_t* max_concurrent) {
+    return guard2([&]() -> int32_t {
+        if (!s) fail(VEXQ_EINVAL, "null argument");
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (launches) *launches = s->launches;
+        if (queries) *queries = s->launched_queries;
+        if (max_batch) *max_batch = s->max_batch;
+        if (max_concurrent) *max_concurrent = s->max_running;
         return VEXQ_OK;
     });
 }
