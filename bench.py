@@ -210,34 +210,36 @@ def main():
         r6.close()
         return out
 
-    for _ in range(max(args.warmup, 3)):
-        step()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+    from vexq_b200.replicas import job_rate_gbs, max_over_ranks, run_timed
+
     clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    stats = [step() for _ in range(args.steps)]
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def start():
+        clocks.start()
+        time.sleep(0.3)
+        ev0.record(stream)
+
+    def stop():
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    ms, stats = run_timed(step, args.steps, args.warmup, start, stop, barrier)
     clk = clocks.stop()
     step_bytes = stats[0][0] + stats[0][1]
     q1_bytes = stats[0][0]
     q1_scan = statistics.mean(s[2] for s in stats)
     q6_scan = statistics.mean(s[3] for s in stats)
     launches = sum(s[4] for s in stats)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = t.item()
+    max_ms = max_over_ranks(ms, dist if world > 1 else None, device="cuda")
     ms_step = max_ms / args.steps
-    value = step_bytes * world / (ms_step / 1e3) / 1e9
+    value = job_rate_gbs(step_bytes, world, ms_step)
 
     # ---- end to end: host buffers, H2D inside the timed region ----
     e2e = None
@@ -270,10 +272,7 @@ def main():
             r6.close()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / args.steps
-        te = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        dt = te.item()
+        dt = max_over_ranks(dt, dist if world > 1 else None, device="cuda")
         for a in regs:
             cudart.cudaHostUnregister(a.ctypes.data)
         e2e = {"value": round(step_bytes * world / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d,
