@@ -72,11 +72,11 @@ def aggs(spec):
     return out
 
 
-def make_plan(c):
+def make_plan(c, radix_bits: int = -1):
     p = c["plan"]
     if c["kind"] == "join":
         return P.JoinPlan(p["build_key"], p["probe_key"], expr(p["build_predicate"]), expr(p["probe_predicate"]),
-                          expr(p["residual"]), p["group_by"], aggs(p["aggs"]))
+                          expr(p["residual"]), p["group_by"], aggs(p["aggs"]), radix_bits=radix_bits)
     return P.AggPlan(expr(p["predicate"]), p["group_by"], aggs(p["aggs"]))
 
 

@@ -525,6 +525,10 @@ struct Gen {
     std::ostringstream& os;
     std::vector<char> done;
     std::string ind = "            ";
+    // scanned-table columns: from the chunk registers (cv/cm), or gathered at
+    // row `row` (partition join, where rows arrive one by one)
+    bool gather = false;
+    std::string row = "r";
     Gen(Plan& pp, std::ostringstream& o) : p(pp), os(o), done(pp.ir.size(), 0) {}
 
     void emit(int i) {
@@ -543,6 +547,14 @@ struct Gen {
                     os << ind << "const bool " << ok << " = " << (n.nullable ? "vq_bit(P.bvalid[" + c + "], brow)" : "true") << ";\n";
                     std::string ld = "((const " + ct + "*)P.bcol[" + c + "])[brow]";
                     if (n.type == VEXQ_TYPE_BOOL)  // a NULL bool reads false
+                        os << ind << "const bool " << x << " = " << ok << " && " << ld << " != 0;\n";
+                    else
+                        os << ind << "const " << ctype(n.type) << " " << x << " = " << ld << ";\n";
+                } else if (gather) {
+                    std::string ct = n.type == VEXQ_TYPE_BOOL ? "unsigned char" : ctype(n.type);
+                    os << ind << "const bool " << ok << " = " << (n.nullable ? "vq_bit(P.valid[" + c + "], " + row + ")" : "true") << ";\n";
+                    std::string ld = "((const " + ct + "*)P.col[" + c + "])[" + row + "]";
+                    if (n.type == VEXQ_TYPE_BOOL)
                         os << ind << "const bool " << x << " = " << ok << " && " << ld << " != 0;\n";
                     else
                         os << ind << "const " << ctype(n.type) << " " << x << " = " << ld << ";\n";
@@ -1108,7 +1120,7 @@ void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string
     if (p.path == AggPath::Dense) {
         os << ind << "const unsigned long long slot = key;\n";
     } else {
-        os << ind << "const unsigned long long slot = vq_insert(P.keys, P.cap_mask, P.cap, key, P.ngroups, P.error);\n";
+        os << ind << "const unsigned long long slot = vq_insert(P.keys, P.cap_mask, P.cap, key, nullptr, P.error);\n";
         os << ind << "if (slot == VQ_NOSLOT) continue;\n";
     }
     os << ind << "const long long stride = (long long)P.cap + 1;\n";
@@ -1257,7 +1269,7 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     const std::string in = ind + "    ";
     os << ind << "unsigned long long slot = VQ_NOSLOT;\n";
     if (p.path == AggPath::Dense) os << ind << "if (live) slot = key;\n";
-    else os << ind << "if (live) slot = vq_insert(P.keys, P.cap_mask, P.cap, key, P.ngroups, P.error);\n";
+    else os << ind << "if (live) slot = vq_insert(P.keys, P.cap_mask, P.cap, key, nullptr, P.error);\n";
     os << ind << "live = live && slot != VQ_NOSLOT;\n";
     os << ind << "const unsigned act = __ballot_sync(0xffffffffu, live);\n";
     os << ind << "if (live) {\n";
@@ -1747,6 +1759,9 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     p.bsmem = loop.smem();
     loop.prologue(os);
     os << kernel_head("vq_build", block);
+    // distinct keys counted per block, added to P.jnkeys once at the end
+    os << "    __shared__ unsigned long long vq_nkeys;\n";
+    os << "    if (threadIdx.x == 0) vq_nkeys = 0ull;\n    __syncthreads();\n";
     loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
@@ -1761,7 +1776,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
     os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
     os << "            if (P.mode == 0) {\n";
-    os << "                const unsigned long long js = vq_insert(P.jkeys, P.jmask, P.jmask + 1, jk, P.jnkeys, P.error);\n";
+    os << "                const unsigned long long js = vq_insert(P.jkeys, P.jmask, P.jmask + 1, jk, &vq_nkeys, P.error);\n";
     os << "                if (js != VQ_NOSLOT) atomicAdd(P.jcount + js, 1);\n";
     os << "            } else {\n";
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
@@ -1769,6 +1784,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            }\n";
     os << "        }\n";
     loop.close(os);
+    os << "    __syncthreads();\n";
+    os << "    if (threadIdx.x == 0 && vq_nkeys) atomicAdd(P.jnkeys, vq_nkeys);\n";
     os << "}\n";
     return os.str();
 }
@@ -1830,6 +1847,127 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     return os.str();
 }
 
+// ---- radix-partitioned join ----------------------------------------------------------
+// Partition pass over one side (build: P.col = build table, its filter and key;
+// probe: the probe table): rows that pass the filter with a non-NULL key go to
+// partition = top pbits bits of the key hash. mode 0 counts rows per (block,
+// partition) in a shared-memory histogram and stores it partition-major in
+// P.phist; mode 1 re-runs the same rows in the same blocks and scatters
+// (key, row) to the offsets the scan left in P.phist. Order inside a
+// partition is not kept: the join pass sorts each build partition.
+static std::string gen_part_kernel(Plan& p, const Table* t, int pred, int key_node, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, pred, cols);
+    collect_cols(p, key_node, cols);
+    os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") vq_part(const __grid_constant__ VQParams P) {\n";
+    os << "    extern __shared__ __align__(16) unsigned vq_hist[];\n";
+    os << "    const int np = P.nparts;\n";
+    os << "    for (int i = threadIdx.x; i < np; i += blockDim.x)\n";
+    os << "        vq_hist[i] = P.mode == 0 ? 0u : (unsigned)P.phist[(long long)i * gridDim.x + blockIdx.x];\n";
+    os << "    __syncthreads();\n";
+    // plain grid-stride chunk loop: both passes give every block the same rows
+    os << "    const int lane = threadIdx.x & 31;\n"
+          "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n"
+          "    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < P.nchunks; c += nw) {\n"
+          "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    emit_loads(os, p, t, cols, "cv", "cm", "r0", "        ", true);
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(p, os);
+    if (pred >= 0) {
+        g.emit(pred);
+        os << "            if (!(x" << pred << " && ok" << pred << ")) continue;\n";
+    }
+    g.emit(key_node);
+    std::string K = std::to_string(key_node);
+    os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
+    os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
+    os << "            const unsigned part = (unsigned)(vq_hash(jk) >> (64 - P.pbits));\n";
+    os << "            if (P.mode == 0) {\n";
+    os << "                atomicAdd(vq_hist + part, 1u);\n";
+    os << "            } else {\n";
+    os << "                const unsigned pos = atomicAdd(vq_hist + part, 1u);\n";
+    os << "                P.pkeys[pos] = jk;\n";
+    os << "                P.prows[pos] = (int)r;\n";
+    os << "            }\n";
+    os << "        }\n    }\n";
+    os << "    __syncthreads();\n";
+    os << "    if (P.mode == 0)\n";
+    os << "        for (int i = threadIdx.x; i < np; i += blockDim.x) P.phist[(long long)i * gridDim.x + blockIdx.x] = (int)vq_hist[i];\n";
+    os << "}\n";
+    return os.str();
+}
+
+// Join pass: each block takes whole partitions. The partition's build entries
+// (at most kRadixCap) are loaded into shared memory and bitonic-sorted by
+// (key, build row), so equal keys form a run in build-row order, the chain
+// order joinHashTable keeps (exec/join_table.go:496-517). Each probe entry
+// binary-searches its run; every match runs the residual filter and is folded
+// into the aggregate with order key (probe row << 16 | position in the run).
+static const int kRadixCap = VQ_RADIX_CAP;
+static const int kRadixMaxBits = VQ_RADIX_MAX_BITS;
+
+static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
+    std::ostringstream os;
+    os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") vq_rjoin(const __grid_constant__ VQParams P) {\n";
+    os << "    extern __shared__ __align__(16) unsigned char vq_sm[];\n";
+    os << "    unsigned long long* sk = (unsigned long long*)vq_sm;\n";
+    os << "    int* sr = (int*)(vq_sm + " << kRadixCap * 8 << ");\n";
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    os << "    for (int part = blockIdx.x; part < P.nparts; part += gridDim.x) {\n";
+    os << "        const long long b0 = P.bstart[part];\n";
+    os << "        const int nb = (int)(P.bstart[part + 1] - b0);\n";
+    os << "        int M = 1;\n        while (M < nb) M <<= 1;\n";
+    os << "        __syncthreads();\n";
+    os << "        for (int i = threadIdx.x; i < M; i += blockDim.x) {\n";
+    os << "            if (i < nb) { sk[i] = P.bkeys[b0 + i]; sr[i] = P.brows[b0 + i]; }\n";
+    os << "            else { sk[i] = 0xFFFFFFFFFFFFFFFFull; sr[i] = 0x7FFFFFFF; }  // pads sort after every entry\n";
+    os << "        }\n";
+    os << "        __syncthreads();\n";
+    os << "        for (int kk = 2; kk <= M; kk <<= 1)\n";
+    os << "            for (int j = kk >> 1; j > 0; j >>= 1) {\n";
+    os << "                for (int i = threadIdx.x; i < M; i += blockDim.x) {\n";
+    os << "                    const int ij = i ^ j;\n";
+    os << "                    if (ij > i) {\n";
+    os << "                        const unsigned long long ka = sk[i], kb = sk[ij];\n";
+    os << "                        const int ra = sr[i], rb = sr[ij];\n";
+    os << "                        const bool gt = ka > kb || (ka == kb && ra > rb);\n";
+    os << "                        if (gt == ((i & kk) == 0)) { sk[i] = kb; sk[ij] = ka; sr[i] = rb; sr[ij] = ra; }\n";
+    os << "                    }\n";
+    os << "                }\n";
+    os << "                __syncthreads();\n";
+    os << "            }\n";
+    os << "        const long long q1 = P.qstart[part + 1];\n";
+    os << "        for (long long e = P.qstart[part] + threadIdx.x; e < q1; e += blockDim.x) {\n";
+    os << "            const unsigned long long jkey = P.qkeys[e];\n";
+    os << "            const long long r = P.qrows[e];\n";
+    os << "            int lo = 0, hi = nb;\n";
+    os << "            while (lo < hi) { const int mid = (lo + hi) >> 1; if (sk[mid] < jkey) lo = mid + 1; else hi = mid; }\n";
+    os << "            for (int ji = lo; ji < nb && sk[ji] == jkey; ji++) {\n";
+    os << "                const long long brow = sr[ji];\n";
+    Gen g(p, os);
+    g.gather = true;
+    g.row = "r";
+    g.ind = "                ";
+    if (p.resid >= 0) {
+        g.emit(p.resid);
+        os << "                if (!(x" << p.resid << " && ok" << p.resid << ")) continue;\n";
+    }
+    for (int k : key_nodes) g.emit(k);
+    for (auto& s : p.slots) if (s.input >= 0) g.emit(s.input);
+    emit_key(os, p, key_nodes, "                ");
+    emit_slot_values(os, p, "                ");
+    std::string order = order_expr(p, "((r << 16) | (long long)min(ji - lo, 65535))");
+    if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
+    else emit_atomic_update(os, p, "                ", order);
+    os << "            }\n        }\n    }\n";
+    if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
+    os << "}\n";
+    return os.str();
+}
+
 // Kind tables used by the register-path flush (per bank entry).
 static std::string gen_kind_tables(const Plan& p, const std::string& prefix) {
     std::ostringstream os;
@@ -1860,7 +1998,9 @@ static void choose_tunables(Plan& p) {
     p.block = acc > 24 ? 128 : 256;
     // measured: software prefetch costs registers the register-accumulator path
     // needs (6M-row Q1: 74.9 µs without, 87.0 µs with); neutral for Q6
-    p.pipeline = p.path != AggPath::Regs;
+    // joins (measured, 6M-row probe): prefetch helps the register path and
+    // costs the atomic path registers it needs for the table walk
+    p.pipeline = p.is_join ? p.path == AggPath::Regs : p.path != AggPath::Regs;
     p.staged = false;  // measured: TMA staging is not faster for these scans yet
     p.regs_pred = true;
     // measured on Zipf(1.1) keys: per-lane shared-memory atomics beat folding
@@ -1923,7 +2063,12 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
     std::string body = join ? gen_probe_kernel(p, key_nodes, p.block) : gen_agg_kernel(p, key_nodes, p.block);
     p.src_main = src.str() + body;
-    if (join) p.src_build = std::string(prelude_source()) + "\n" + gen_build_kernel(p, build_key_node, kBlock);
+    if (join) {
+        p.src_build = std::string(prelude_source()) + "\n" + gen_build_kernel(p, build_key_node, kBlock);
+        p.src_part_b = std::string(prelude_source()) + "\n" + gen_part_kernel(p, p.bt, p.bpred, build_key_node, kBlock);
+        p.src_part_p = std::string(prelude_source()) + "\n" + gen_part_kernel(p, p.t, p.pred, p.probe_key, kBlock);
+        p.src_rjoin = std::string(prelude_source()) + "\n" + gen_kind_tables(p) + "\n" + gen_rjoin_kernel(p, key_nodes, p.block);
+    }
     std::ostringstream ex;
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
@@ -1931,7 +2076,16 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
     p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
-    if (join) p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);
+    if (join) {
+        p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);
+        // radix-partitioned join (exec/parallel_join.go:72-109): the partition
+        // histogram takes 4 bytes of shared memory per partition (set at launch)
+        p.k_part_b = jit_get(p.src_part_b, "vq_part", kBlock, 4 << kRadixMaxBits);
+        p.k_part_p = jit_get(p.src_part_p, "vq_part", kBlock, 4 << kRadixMaxBits);
+        // 48 KB of keys and rows plus an opt-in margin for the register path's static staging
+        p.k_rjoin = jit_get(p.src_rjoin, "vq_rjoin", p.block, kRadixCap * 12 + 8192);
+        p.radix = p.radix_bits != 0;
+    }
     // device-side tables of the plan
     if (!p.sets.empty()) {
         size_t tot = 0;

@@ -305,11 +305,13 @@ __device__ __host__ inline double vq_fx_value(const vq_i64* c, int lsb) {
 // Open-addressing insert (linear probing, atomicCAS on the key). The key equal
 // to the empty sentinel lives in the extra slot `cap`, whose key word is a
 // used-flag. Returns VQ_NOSLOT and raises err bit 0 when the probe limit is
-// reached, so a full table ends the kernel's work instead of spinning.
+// reached, so a full table ends the kernel's work instead of spinning. New
+// keys are counted in *nkeys when it is not null (a block-local counter: one
+// global word taking an atomic per key serialises the whole insert).
 __device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key,
                                             vq_u64* nkeys, int* err) {
     if (key == VQ_EMPTY_KEY) {
-        if (atomicCAS(keys + cap, 0ull, 1ull) == 0ull) atomicAdd(nkeys, 1ull);
+        if (atomicCAS(keys + cap, 0ull, 1ull) == 0ull && nkeys) atomicAdd(nkeys, 1ull);
         return cap;
     }
     vq_u64 i = vq_hash(key) & mask;
@@ -317,7 +319,10 @@ __device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 ca
     for (vq_u64 n = 0; n < limit; n++) {
         // one round trip: claim the slot or learn its key
         vq_u64 old = atomicCAS(keys + i, VQ_EMPTY_KEY, key);
-        if (old == VQ_EMPTY_KEY) { atomicAdd(nkeys, 1ull); return i; }
+        if (old == VQ_EMPTY_KEY) {
+            if (nkeys) atomicAdd(nkeys, 1ull);  // callers count in shared memory, not one global word
+            return i;
+        }
         if (old == key) return i;
         i = (i + 1) & mask;
     }

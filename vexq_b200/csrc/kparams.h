@@ -7,6 +7,8 @@
 #define VQ_MAXSETS 16
 #define VQ_FX_DIGITS 4  // 32-bit digits of the exact fixed-point float sums
 #define VQ_MAXLITS 32   // numeric literals passed at launch (raw 8-byte images)
+#define VQ_RADIX_CAP 4096      // radix join: build entries of one partition held in shared memory
+#define VQ_RADIX_MAX_BITS 12   // radix join: at most 4,096 partitions
 
 struct VQParams {
     // ---- scanned table (aggregate: the table; join: probe or build side) ----
@@ -41,6 +43,16 @@ struct VQParams {
     int* jrows;                // build row ids, grouped by slot in row order
     int2* jmeta;               // [jcap + 1] {first row position, row count} per slot
     unsigned long long* jnkeys;
+    // ---- radix-partitioned join ----
+    unsigned long long* pkeys;     // partition pass: keys written per partition
+    int* prows;                    //                 their row ids
+    int* phist;                    // [nparts][grid] row counts (histogram) / offsets (scatter)
+    const long long* bstart;       // join: [nparts + 1] build partition starts in bkeys/brows
+    const unsigned long long* bkeys;
+    const int* brows;
+    const long long* qstart;       // join: [nparts + 1] probe partition starts in qkeys/qrows
+    const unsigned long long* qkeys;
+    const int* qrows;
     // ---- numeric literals of the plan's expressions (int64, date, float64 bits):
     //      plans that differ only in constants share one compiled kernel ----
     long long lit[VQ_MAXLITS];
@@ -55,6 +67,8 @@ struct VQParams {
     int n_rg;
     int mode;                  // join build: 0 = insert/count, 1 = fill
     int cache_n;               // dense path: groups held in the block's shared-memory cache
+    int nparts;                // radix join: partitions (a power of two)
+    int pbits;                 // radix join: partition = top pbits bits of the key hash
     int fx_lsb[16];            // per float-sum slot: exponent of the window's LSB
 };
 

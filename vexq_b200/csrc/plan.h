@@ -139,7 +139,12 @@ struct Plan {
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
     // scratch reused across runs
     DevBuf scratch_a, scratch_b, scratch_c, scratch_d, scratch_e, scratch_f, scratch_g;
-    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta;
+    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta, jt_long, jt_sort;
+    // radix-partitioned join: kernels and buffers
+    bool radix = false;
+    std::string src_part_b, src_part_p, src_rjoin;
+    JitKernel k_part_b, k_part_p, k_rjoin;
+    DevBuf rp_bkeys, rp_brows, rp_qkeys, rp_qrows, rp_hist, rp_off, rp_start, rp_scalar;
     ~Plan();
 };
 

@@ -114,14 +114,13 @@ __global__ void k_init_table(unsigned long long* keys, long long* first, long lo
 }
 
 // Compacts occupied slots (count > 0) and turns exact fixed-point sums into
-// correctly rounded doubles (NaN / ±inf flags applied IEEE-style).
-__device__ __forceinline__ void finalize_slot(long long i, const unsigned long long* keys, const long long* first,
-                                              const long long* acc_i, const long long* acc_fx, const unsigned* special,
-                                              long long nslots, int ni, int nf, const int* fx_lsb, int hash,
-                                              unsigned long long* n_out, unsigned long long* o_key, long long* o_first,
-                                              long long* o_i, double* o_f, long long cap_out) {
-    if (acc_i[i] == 0) return;  // slot 0 of the int bank is the row count
-    unsigned long long pos = atomicAdd(n_out, 1ull);
+// correctly rounded doubles (NaN / ±inf flags applied IEEE-style). Output
+// positions are taken one atomic per warp (per table within a warp).
+__device__ __forceinline__ void finalize_write(long long i, unsigned long long pos, const unsigned long long* keys,
+                                               const long long* first, const long long* acc_i, const long long* acc_fx,
+                                               const unsigned* special, long long nslots, int ni, int nf,
+                                               const int* fx_lsb, int hash, unsigned long long* o_key,
+                                               long long* o_first, long long* o_i, double* o_f, long long cap_out) {
     if ((long long)pos >= cap_out) return;
     o_key[pos] = hash ? (i == nslots - 1 ? VQ_EMPTY_KEY : keys[i]) : (unsigned long long)i;
     o_first[pos] = first[i];
@@ -137,13 +136,30 @@ __device__ __forceinline__ void finalize_slot(long long i, const unsigned long l
     }
 }
 
+// Position of an occupied lane among the occupied lanes of its peer group
+// (lanes of one table), with one atomicAdd on that table's counter per group.
+__device__ __forceinline__ unsigned long long vq_claim(bool occ, unsigned peers, unsigned long long* n_out) {
+    const int lane = threadIdx.x & 31;
+    const unsigned b = __ballot_sync(0xffffffffu, occ) & peers;
+    const int leader = __ffs(peers) - 1;
+    unsigned long long base = 0;
+    if (lane == leader && b) base = atomicAdd(n_out, (unsigned long long)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(b & ((1u << lane) - 1u));
+}
+
 __global__ void k_finalize(const unsigned long long* keys, const long long* first, const long long* acc_i,
                            const long long* acc_fx, const unsigned* special, long long nslots, int ni, int nf,
                            const int* fx_lsb, int hash, unsigned long long* n_out, unsigned long long* o_key,
                            long long* o_first, long long* o_i, double* o_f, long long cap_out) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x)
-        finalize_slot(i, keys, first, acc_i, acc_fx, special, nslots, ni, nf, fx_lsb, hash, n_out, o_key, o_first, o_i,
-                      o_f, cap_out);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < nslots; b0 += stride) {  // warp-uniform trip count
+        const long long i = b0 + threadIdx.x;
+        const bool occ = i < nslots && acc_i[i] != 0;  // slot 0 of the int bank is the row count
+        const unsigned long long pos = vq_claim(occ, 0xffffffffu, n_out);
+        if (occ) finalize_write(i, pos, keys, first, acc_i, acc_fx, special, nslots, ni, nf, fx_lsb, hash, o_key, o_first,
+                                o_i, o_f, cap_out);
+    }
 }
 
 // Batched group tables: global slot g belongs to the table whose slot0 is the
@@ -177,10 +193,24 @@ __global__ void k_init_batch(const VQTableDesc* d, int n, long long total) {
 }
 
 __global__ void k_finalize_batch(const VQTableDesc* d, int n, long long total) {
-    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
-        const VQTableDesc& t = d[table_of(d, n, g)];
-        finalize_slot(g - t.slot0, t.keys, t.first, t.acc_i, t.acc_fx, t.special, t.nslots, t.ni, t.nf, t.fx_lsb, t.hash,
-                      t.n_out, t.o_key, t.o_first, t.o_i, t.o_f, t.cap_out);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < total; b0 += stride) {  // warp-uniform trip count
+        const long long g = b0 + threadIdx.x;
+        const int ti = g < total ? table_of(d, n, g) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, ti);
+        bool occ = false;
+        if (ti >= 0) {
+            const VQTableDesc& t = d[ti];
+            occ = t.acc_i[g - t.slot0] != 0;
+        }
+        unsigned long long* cnt = ti >= 0 ? d[ti].n_out : nullptr;
+        // every peer group claims from its own table's counter (a group without a table claims nothing)
+        const unsigned long long pos = vq_claim(occ, peers, cnt ? cnt : (unsigned long long*)nullptr);
+        if (occ) {
+            const VQTableDesc& t = d[ti];
+            finalize_write(g - t.slot0, pos, t.keys, t.first, t.acc_i, t.acc_fx, t.special, t.nslots, t.ni, t.nf,
+                           t.fx_lsb, t.hash, t.o_key, t.o_first, t.o_i, t.o_f, t.cap_out);
+        }
     }
 }
 
@@ -235,6 +265,17 @@ __global__ void k_scan_add(int* out, long long n, const int* sums) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += sums[i / 4096];
 }
+// Radix join: partition starts [np + 1] from the partition-major exclusive
+// scan of the (partition, block) histogram.
+__global__ void k_part_starts(const int* off, const int* hist, int np, int grid, long long* starts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < np) starts[i] = off[(long long)i * grid];
+    if (i == np) {
+        const long long n = (long long)np * grid;
+        starts[np] = (long long)off[n - 1] + hist[n - 1];
+    }
+}
+
 // Packs each slot's chain start and length into one 8-byte probe read.
 __global__ void k_pack_meta(const int* start, const int* count, int2* meta, long long n) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,11 +284,19 @@ __global__ void k_pack_meta(const int* start, const int* count, int2* meta, long
 
 // Restores build-row order inside each key's chain (joinHashTable.insert keeps
 // insertion order, exec/join_table.go:496-517): one thread per slot.
-__global__ void k_sort_chains(const int* start, const int* count, int* rows, long long nslots, int* unsorted) {
+// Chains longer than kShortChain are listed (slot, length) for k_sort_long.
+constexpr int kShortChain = 64;
+__global__ void k_sort_chains(const int* start, const int* count, int* rows, long long nslots, int* unsorted,
+                              int2* long_list, int* long_count, int long_cap) {
     for (long long sl = (long long)blockIdx.x * blockDim.x + threadIdx.x; sl < nslots; sl += (long long)gridDim.x * blockDim.x) {
         int c = count[sl];
         if (c < 2) continue;
-        if (c > 4096) { atomicOr(unsorted, 4); continue; }  // chain left in fill order
+        if (c > kShortChain) {
+            const int at = atomicAdd(long_count, 1);
+            if (at < long_cap) long_list[at] = make_int2((int)sl, c);
+            else atomicOr(unsorted, 4);
+            continue;
+        }
         int* r = rows + start[sl];
         for (int i = 1; i < c; i++) {
             int x = r[i], j = i - 1;
@@ -255,6 +304,32 @@ __global__ void k_sort_chains(const int* start, const int* count, int* rows, lon
             r[j + 1] = x;
         }
     }
+}
+
+// One block per long chain: bitonic sort of its row ids (padded to a power of
+// two in scratch at soff[b]) back into build-row order.
+__global__ void __launch_bounds__(1024) k_sort_long(const int2* list, const int* start, int* rows, int* scratch,
+                                                    const long long* soff) {
+    const int2 e = list[blockIdx.x];
+    const int c = e.y;
+    int M = 1;
+    while (M < c) M <<= 1;
+    int* w = scratch + soff[blockIdx.x];
+    int* r = rows + start[e.x];
+    for (int i = threadIdx.x; i < M; i += blockDim.x) w[i] = i < c ? r[i] : 0x7FFFFFFF;
+    __syncthreads();
+    for (int k = 2; k <= M; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < M; i += blockDim.x) {
+                const int ij = i ^ j;
+                if (ij > i) {
+                    const int a = w[i], b = w[ij];
+                    if ((a > b) == ((i & k) == 0)) { w[i] = b; w[ij] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < c; i += blockDim.x) r[i] = w[i];
 }
 
 // Top-k support: order-preserving "better is larger" transform of a sort key.
@@ -385,6 +460,8 @@ struct RunCtx {
     float kernel_ms = 0;
     float scan_ms = 0;
     int launches = 0;
+    const JitKernel* k = nullptr;  // main kernel other than p.k_main (partition join)
+    int grid = 0;                  // and its grid
 };
 
 void ensure_events(Plan& p) {
@@ -404,7 +481,8 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     Groups g;
     int G = (int)p.domain, nf = p.nf, ni = p.ni;
     int nfb = std::max(nf, 1);
-    int grid = grid_for(p.k_main, nchunks, p.staged);
+    const JitKernel& K = rc.k ? *rc.k : p.k_main;
+    int grid = rc.k ? rc.grid : grid_for(p.k_main, nchunks, p.staged);
     size_t pf = (size_t)grid * G * nfb, pi = (size_t)grid * G * (ni + 1);
     p.scratch_a.ensure(pf * 8);
     p.scratch_b.ensure(pi * 8);
@@ -431,7 +509,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     ensure_events(p);
     VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
-    jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+    jit_launch(K, grid, &P, sizeof P, rc.s);
     launch_check(rc.s, "p.k_main");
     VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
     int tot = G * nf + G * (ni + 1);
@@ -528,9 +606,10 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
         launch_check(rc.s, "k_init_table");
         VQ_CUDA(cudaGetLastError());
-        int grid = grid_for(p.k_main, nchunks, p.staged);
+        const JitKernel& K = rc.k ? *rc.k : p.k_main;
+        int grid = rc.k ? rc.grid : grid_for(p.k_main, nchunks, p.staged);
         VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
-        jit_launch(p.k_main, grid, &P, sizeof P, rc.s);
+        jit_launch(K, grid, &P, sizeof P, rc.s);
         launch_check(rc.s, "p.k_main");
         VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
         int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
@@ -878,6 +957,61 @@ cudaStream_t plan_stream(Plan& p) {
     return p.stream;
 }
 
+// One radix partition pass over a side (Q: its columns, row ranges, filter
+// inputs): histogram, partition-major scan, starts, then — unless a
+// partition exceeds the shared-memory capacity and *maxpart is asked for —
+// the scatter of (key, row) into keys/rows. Returns the entries written.
+static long long radix_pass(RunCtx& rc, const JitKernel& kp, VQParams Q, int pbits, long long* d_starts, DevBuf& keys,
+                            DevBuf& rows, long long* maxpart) {
+    Plan& p = rc.p;
+    const int np = 1 << pbits;
+    const int grid = grid_for(kp, Q.nchunks, false);
+    const long long n = (long long)np * grid;
+    p.rp_hist.ensure(n * 4);
+    p.rp_off.ensure(n * 4);
+    const int nbk = (int)((n + 4095) / 4096);
+    p.rp_scalar.ensure((size_t)(nbk + 16) * 4);
+    Q.nparts = np;
+    Q.pbits = pbits;
+    Q.mode = 0;
+    Q.phist = p.rp_hist.as<int>();
+    JitKernel k = kp;
+    k.smem = np * 4;
+    jit_launch(k, grid, &Q, sizeof Q, rc.s);
+    launch_check(rc.s, "vq_part (histogram)");
+    int* off = p.rp_off.as<int>();
+    int* bsums = p.rp_scalar.as<int>();
+    k_scan_blocks<<<nbk, 1024, 0, rc.s>>>(Q.phist, off, n, bsums);
+    launch_check(rc.s, "k_scan_blocks");
+    k_scan_sums<<<1, 1024, 0, rc.s>>>(bsums, nbk);
+    launch_check(rc.s, "k_scan_sums");
+    k_scan_add<<<(int)((n + 255) / 256), 256, 0, rc.s>>>(off, n, bsums);
+    launch_check(rc.s, "k_scan_add");
+    k_part_starts<<<(np + 1 + 255) / 256, 256, 0, rc.s>>>(off, Q.phist, np, grid, d_starts);
+    launch_check(rc.s, "k_part_starts");
+    std::vector<long long> hs(np + 1);
+    VQ_CUDA(cudaMemcpyAsync(hs.data(), d_starts, (size_t)(np + 1) * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    rc.launches += 5;
+    const long long total = hs[np];
+    if (maxpart) {
+        long long mx = 0;
+        for (int i = 0; i < np; i++) mx = std::max(mx, hs[i + 1] - hs[i]);
+        *maxpart = mx;
+        if (mx > VQ_RADIX_CAP) return total;
+    }
+    keys.ensure((size_t)std::max<long long>(total, 1) * 8);
+    rows.ensure((size_t)std::max<long long>(total, 1) * 4);
+    Q.mode = 1;
+    Q.phist = off;
+    Q.pkeys = keys.as<unsigned long long>();
+    Q.prows = rows.as<int>();
+    jit_launch(k, grid, &Q, sizeof Q, rc.s);
+    launch_check(rc.s, "vq_part (scatter)");
+    rc.launches += 1;
+    return total;
+}
+
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
     RunCtx rc{p, plan_stream(p)};
@@ -889,9 +1023,81 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     int rgs = std::max(0, rg_start);
     long long join_keys = 0;
     int64_t bytes = 0, rows_scanned = 0;
+    bool use_radix = false;
+    int pbits = 0;
     if (p.is_join) {
         Table& bt = *p.bt;
         // ---- build phase ----
+        std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
+        ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
+        // radix partitioning (RadixBitsFor, exec/parallel_join.go:72-89): none
+        // below 65,536 build rows; partitions sized to fit shared memory
+        // automatic choice: the global table until partitioning measures faster
+        use_radix = p.radix && !p.staged && p.btile == 128 && p.tile == 128 && p.radix_bits > 0;
+        if (use_radix) {
+            VQParams B;
+            std::memset(&B, 0, sizeof B);
+            set_plan_constants(p, B);
+            set_columns(B, bt, false);
+            if (bs.seg != p.bseg_cache || !p.d_bseg.p) {
+                p.d_bseg.ensure(std::max<size_t>(bs.seg.size(), 3) * 8);
+                if (!bs.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice));
+                p.bseg_cache = bs.seg;
+            }
+            B.seg = p.d_bseg.as<long long>();
+            B.nseg = (int)bs.seg.size() / 3;
+            B.nchunks = bs.nchunks;
+            B.rg_rows = bt.rg_rows;
+            B.n_rg = bt.n_rg;
+            B.present = p.d_bpresent.as<unsigned char>();
+            for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
+            if (p.radix_bits > 0) {
+                pbits = std::min(p.radix_bits, VQ_RADIX_MAX_BITS);
+            } else {
+                pbits = 1;
+                while (pbits < VQ_RADIX_MAX_BITS && (bs.rows >> pbits) > VQ_RADIX_CAP / 2) pbits++;
+            }
+            p.rp_start.ensure((size_t)2 * ((1 << VQ_RADIX_MAX_BITS) + 1) * 8);
+            long long* bstart = p.rp_start.as<long long>();
+            ensure_events(p);
+            VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
+            long long total = 0;
+            for (;;) {
+                long long mx = 0;
+                total = bs.nchunks > 0 ? radix_pass(rc, p.k_part_b, B, pbits, bstart, p.rp_bkeys, p.rp_brows, &mx) : 0;
+                if (mx <= VQ_RADIX_CAP) break;
+                if (pbits >= VQ_RADIX_MAX_BITS) { use_radix = false; break; }  // one key's chain is too long: global table
+                while (pbits < VQ_RADIX_MAX_BITS && mx > VQ_RADIX_CAP) { pbits++; mx = (mx + 1) / 2; }
+            }
+            VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+            VQ_CUDA(cudaEventSynchronize(p.ev[5]));
+            rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
+            if (use_radix) {
+                bytes += scanned_bytes(p, bt, bs.rows, true);
+                rows_scanned += bs.rows;
+                join_keys = total;  // at least the distinct build keys
+                set_columns(P, bt, true);
+                P.bstart = bstart;
+                P.bkeys = p.rp_bkeys.as<unsigned long long>();
+                P.brows = p.rp_brows.as<int>();
+                P.nparts = 1 << pbits;
+                P.pbits = pbits;
+                if (total == 0 || bs.nchunks == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
+                    Groups g;
+                    g.ival.assign(p.ni, {});
+                    g.fval.assign(p.nf, {});
+                    vexq_result_s* r = build_result(p, g);
+                    r->kernel_ms = rc.kernel_ms;
+                    r->launches = rc.launches;
+                    r->rows_scanned = rows_scanned;
+                    r->bytes_scanned = bytes;
+                    return r;
+                }
+            }
+        }
+    }
+    if (p.is_join && !use_radix) {
+        Table& bt = *p.bt;
         std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
         ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
         long long jcap = 16;
@@ -933,7 +1139,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         {
             ensure_events(p);
             VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
-            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 16, rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 24, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
             int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
@@ -954,21 +1160,45 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             B.mode = 1;
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
             if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
-            k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error);
+            const int long_cap = (int)(bs.rows / (kShortChain + 1) + 2);
+            p.jt_long.ensure((size_t)long_cap * 8);
+            int* long_count = (int*)(p.jt_scalar.as<char>() + 16);
+            k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error, p.jt_long.as<int2>(),
+                                                long_count, long_cap);
             launch_check(rc.s, "k_sort_chains");
             k_pack_meta<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, B.jcount, p.jt_meta.as<int2>(), nslots);
             launch_check(rc.s, "k_pack_meta");
             VQ_CUDA(cudaGetLastError());
-            int herr = 0;
+            int herr = 0, nlong = 0;
             unsigned long long nk = 0;
             VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
             VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&nlong, long_count, 4, cudaMemcpyDeviceToHost, rc.s));
+            if (nlong > 0 && !(herr & 4)) {  // long chains: one block each, scratch for the power-of-two pad
+                std::vector<int2> lst(nlong);
+                VQ_CUDA(cudaMemcpyAsync(lst.data(), p.jt_long.p, (size_t)nlong * 8, cudaMemcpyDeviceToHost, rc.s));
+                std::vector<long long> soff(nlong);
+                long long tot = 0;
+                for (int i = 0; i < nlong; i++) {
+                    long long m = 1;
+                    while (m < lst[i].y) m <<= 1;
+                    soff[i] = tot;
+                    tot += m;
+                }
+                p.jt_sort.ensure((size_t)tot * 4 + (size_t)nlong * 8);
+                long long* d_soff = (long long*)(p.jt_sort.as<char>() + (size_t)tot * 4);
+                VQ_CUDA(cudaMemcpyAsync(d_soff, soff.data(), (size_t)nlong * 8, cudaMemcpyHostToDevice, rc.s));
+                k_sort_long<<<nlong, 1024, 0, rc.s>>>(p.jt_long.as<int2>(), B.jstart, B.jrows, p.jt_sort.as<int>(), d_soff);
+                launch_check(rc.s, "k_sort_long");
+                rc.launches += 1;
+            }
             VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
             VQ_CUDA(cudaEventSynchronize(p.ev[5]));
             rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
             rc.launches += 8;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");
+            if (herr & 4) fail(VEXQ_EDEVICE, "join build: more long chains than the sort list holds");
             join_keys = (long long)nk;
         }
         bytes += scanned_bytes(p, bt, bs.rows, true);
@@ -1011,6 +1241,21 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
 
     bytes += scanned_bytes(p, t, ss.rows, false);
     rows_scanned += ss.rows;
+    if (use_radix && ss.nchunks > 0) {
+        // probe side: the same partitions, then one block per partition joins
+        ensure_events(p);
+        VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
+        long long* qstart = p.rp_start.as<long long>() + ((1 << VQ_RADIX_MAX_BITS) + 1);
+        radix_pass(rc, p.k_part_p, P, pbits, qstart, p.rp_qkeys, p.rp_qrows, nullptr);
+        VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+        VQ_CUDA(cudaEventSynchronize(p.ev[5]));
+        rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
+        P.qstart = qstart;
+        P.qkeys = p.rp_qkeys.as<unsigned long long>();
+        P.qrows = p.rp_qrows.as<int>();
+        rc.k = &p.k_rjoin;
+        rc.grid = (int)std::min<long long>(P.nparts, (long long)sm_count() * std::max(1, p.k_rjoin.max_blocks_per_sm));
+    }
     vexq_result_s* r;
     if (ss.nchunks == 0) {
         Groups g;

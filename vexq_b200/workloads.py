@@ -41,7 +41,7 @@ def q6_plan(lo: str = Q6_LO, hi: str = Q6_HI) -> AggPlan:
 NB = 3
 
 
-def q3_plan(build_frac: float = 0.48, probe_frac: float = 0.46, limit: int = 10) -> JoinPlan:
+def q3_plan(build_frac: float = 0.48, probe_frac: float = 0.46, limit: int = 10, radix_bits: int = -1) -> JoinPlan:
     """orders (date < mid, ~48%) ⋈ items (shipdate > mid, ~54%) GROUP BY key,
     SUM(price*(1-disc)) ORDER BY revenue DESC LIMIT 10."""
     bmid, pmid = D.join_mid(build_frac), D.join_mid(probe_frac)
@@ -53,10 +53,10 @@ def q3_plan(build_frac: float = 0.48, probe_frac: float = 0.46, limit: int = 10)
         residual=None,
         group_by=[D.O_KEY],
         aggs=[sum_(price * (1 - disc), "revenue")],
-        order_col=1, descending=True, limit=limit)
+        order_col=1, descending=True, limit=limit, radix_bits=radix_bits)
 
 
-def q12_plan() -> JoinPlan:
+def q12_plan(radix_bits: int = -1) -> JoinPlan:
     prio = col(D.O_PRIORITY)
     high = or_(prio == lit("1-URGENT"), prio == lit("2-HIGH"))
     low = and_(prio != lit("1-URGENT"), prio != lit("2-HIGH"))
@@ -70,7 +70,7 @@ def q12_plan() -> JoinPlan:
         group_by=[NB + D.I_MODE],
         aggs=[sum_(case([(high, 1)], 0), "high_line_count"),
               sum_(case([(low, 1)], 0), "low_line_count")],
-        order_col=0)
+        order_col=0, radix_bits=radix_bits)
 
 
 def batch_plan() -> AggPlan:
