@@ -43,7 +43,179 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling driver: three Q1 and three Q6 runs on the 6M-row table, no timing")
+    ap.add_argument("--workload", default="lineitem", choices=["lineitem", "batch", "serve"],
+                    help="lineitem: Q1+Q6 step (default); batch: 256 Zipf GROUP BYs, batched vs one by one; "
+                         "serve: Poisson arrivals of a Q1/Q6/Q3 mix over resident tables, p50/p99")
+    ap.add_argument("--fact-rows", type=int, default=60_000_000, help="serve workload: fact and probe rows")
+    ap.add_argument("--queries", type=int, default=400, help="serve workload: queries per arm")
+    ap.add_argument("--plans", type=int, default=256, help="batch workload: number of GROUP BY plans")
     return ap.parse_args()
+
+
+def serve_workload(args):
+    """Serving: lineitem (fact) rows, orders (build) = fact/4 and items (probe)
+    = fact rows resident in HBM; a 50/20/30 mix of the Q1-shape GROUP BY,
+    the Q6-shape range SUM and the Q3-shape join with randomised date
+    cutoffs, prepared once (64 plans); queries submitted to the serving loop.
+    Arms: plain (one query per launch, one worker) and batched (continuous
+    batching, two workers), closed loop (all queued at once: throughput) and
+    open loop (Poisson arrivals at 70% of the plain arm's closed-loop rate:
+    p50/p99 latency, submit to result ready)."""
+    import ctypes as C
+    import datetime
+
+    import numpy as np
+
+    from vexq_b200 import abi, build, datagen as D, exec as X, workloads as W
+    build.build()
+    X.init(0)
+    fact = args.fact_rows
+    li = X.GpuTable(D.lineitem(fact, seed=77, rg_rows=RG_ROWS))
+    o = X.GpuTable(D.orders(fact // 4, seed=78))
+    it = X.GpuTable(D.items(fact, fact // 4, seed=79))
+
+    def day(n):
+        return (datetime.date(1970, 1, 1) + datetime.timedelta(days=int(n))).isoformat()
+
+    rng = np.random.default_rng(5)
+    ops, kinds = [], []
+    for _ in range(64):
+        u = rng.random()
+        if u < 0.5:
+            ops.append(X.GpuHashAggregate(li, W.q1_plan(day(8036 + rng.integers(1500, 2526)))))
+            kinds.append("q1")
+        elif u < 0.7:
+            lo = 8036 + int(rng.integers(0, 2000))
+            ops.append(X.GpuHashAggregate(li, W.q6_plan(day(lo), day(lo + 365))))
+            kinds.append("q6")
+        else:
+            ops.append(X.GpuParallelHashJoinAggregate(o, it, W.q3_plan(float(rng.uniform(0.3, 0.6)), float(rng.uniform(0.3, 0.6)))))
+            kinds.append("q3")
+    alone = {}
+    for op, k in zip(ops, kinds):
+        op.run().close()
+        t0 = time.perf_counter()
+        op.run().close()
+        alone.setdefault(k, []).append((time.perf_counter() - t0) * 1e3)
+    L = abi.load()
+
+    def arm(arrivals, workers, flags):
+        srv = C.c_void_p()
+        abi.check(L.vexq_server_start(1 << 37, 16, workers, flags, C.byref(srv)))
+        order = rng.integers(0, len(ops), len(arrivals))
+        tickets = []
+        start = time.perf_counter()
+        for a, qi in zip(arrivals, order):
+            now = time.perf_counter() - start
+            if a > now:
+                time.sleep(a - now)
+            tk = C.c_int64()
+            abi.check(L.vexq_server_submit(srv, ops[qi].h, C.byref(tk)))
+            tickets.append(tk.value)
+        lat = []
+        for tk in tickets:
+            h = C.c_void_p()
+            abi.check(L.vexq_server_wait(srv, tk, 600000, C.byref(h)))
+            L.vexq_result_free(h)
+            ms = C.c_double()
+            abi.check(L.vexq_server_latency(srv, tk, C.byref(ms)))
+            lat.append(ms.value)
+        total = time.perf_counter() - start
+        la, q, mb, mc = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        abi.check(L.vexq_server_stats(srv, C.byref(la), C.byref(q), C.byref(mb), C.byref(mc)))
+        abi.check(L.vexq_server_stop(srv))
+        lat = np.array(lat)
+        return {"qps": round(len(arrivals) / total, 2), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat, 99)), 3), "launches": la.value, "max_batch": mb.value,
+                "max_concurrent": mc.value}
+
+    n = args.queries
+    closed_plain = arm(np.zeros(n), 1, abi.SERVE_NO_BATCH)
+    closed_batched = arm(np.zeros(n), 2, 0)
+    qps = 0.7 * closed_plain["qps"]
+    arrivals = np.cumsum(rng.exponential(1.0 / qps, n))
+    poisson_plain = arm(arrivals, 1, abi.SERVE_NO_BATCH)
+    poisson_batched = arm(arrivals, 2, 0)
+    line = {"metric": "queries/s", "value": closed_batched["qps"], "unit": "queries/s", "n_gpus": 1,
+            "steps": n, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded lineitem / orders / items generators)",
+            "config": {"workload": f"serving: {fact} fact rows, {fact // 4} build rows, {fact} probe rows; "
+                                   "50% Q1 / 20% Q6 / 30% Q3 with randomised cutoffs"},
+            "alone_ms_median": {k: round(float(statistics.median(v)), 3) for k, v in alone.items()},
+            "closed_plain": closed_plain, "closed_batched": closed_batched,
+            "poisson_qps": round(qps, 2), "poisson_plain": poisson_plain, "poisson_batched": poisson_batched}
+    print(json.dumps(line), flush=True)
+
+
+def batch_workload(args):
+    """256 independent GROUP BYs: rows log-uniform over 10K-4M, key
+    cardinality log-uniform over 2-65,536 with Zipf(1.1) frequencies as
+    dictionary codes, float64 values U(0,1e5) at 2 decimals, mixed
+    SUM/COUNT/MIN/MAX/AVG. One step = all plans; the batched arm (one
+    persistent launch per path class, graph replay, autotuned) is the line's
+    value, the same plans one by one through vexq_plan_run are beside it.
+    Device time: CUDA events, kernels only (before the copy back)."""
+    import math
+
+    import numpy as np
+
+    from vexq_b200 import build, datagen as D, exec as X, plan as P
+    build.build()
+    X.init(0)
+    rng = np.random.default_rng(2024)
+    mixes = [lambda v: [P.sum_(v, "sum"), P.count_star("count")],
+             lambda v: [P.min_(v, "min"), P.max_(v, "max"), P.count_star("count")],
+             lambda v: [P.avg(v, "avg"), P.sum_(v, "sum")],
+             lambda v: [P.sum_(v, "sum"), P.count_star("count"), P.min_(v, "min"), P.max_(v, "max"), P.avg(v, "avg")]]
+    tabs, ops = [], []
+    for i in range(args.plans):
+        rows = int(math.exp(rng.uniform(math.log(1e4), math.log(4e6))))
+        card = int(round(math.exp(rng.uniform(math.log(2), math.log(65536)))))
+        mix = int(rng.integers(4))
+        g = X.GpuTable(D.zipf_groups(rows, card, seed=i))
+        tabs.append(g)
+        ops.append(X.GpuHashAggregate(g, P.AggPlan(None, [0], mixes[mix](P.col(1)))))
+
+    def plain():
+        ms, nbytes = 0.0, 0
+        for op in ops:
+            r = op.run()
+            ms += r.kernel_ms
+            nbytes += r.bytes_scanned
+            r.close()
+        return ms, nbytes
+
+    for _ in range(max(args.warmup, 3)):
+        plain()
+    pms = []
+    for _ in range(args.steps):
+        ms, nbytes = plain()
+        pms.append(ms)
+    b = X.GpuBatch(ops, autotune=True)
+    for _ in range(max(args.warmup, 3)):
+        for r in b.exec():
+            r.close()
+    bms, walls = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = b.exec()
+        walls.append(time.perf_counter() - t0)
+        for r in res:
+            r.close()
+        bms.append(b.stats()[1])
+    explain = b.explain()
+    b.close()
+    p_ms, b_ms = statistics.median(pms), statistics.median(bms)
+    line = {"metric": "GB/s scanned", "value": round(nbytes / b_ms / 1e6, 3), "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(b_ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Zipf(1.1) dictionary codes, 2-decimal values)",
+            "config": {"workload": f"{args.plans} GROUP BYs, 10K-4M rows, 2-65,536 groups, Zipf(1.1)",
+                       "bytes_per_step": nbytes, "batch": explain},
+            "plain_one_by_one": {"value": round(nbytes / p_ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(p_ms, 4)},
+            "batched_over_plain": round(p_ms / b_ms, 3),
+            "batched_wall_ms_per_step": round(statistics.median(walls) * 1e3, 3)}
+    print(json.dumps(line), flush=True)
 
 
 def profile_driver():
@@ -181,6 +353,10 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload in ("batch", "serve"):
+        if rank == 0:
+            (batch_workload if args.workload == "batch" else serve_workload)(args)
         return
     import datetime
 

@@ -529,6 +529,9 @@ struct Gen {
     // row `row` (partition join, where rows arrive one by one)
     bool gather = false;
     std::string row = "r";
+    // partition join: probe columns carried in the payload, read at entry `pay_row`
+    const std::vector<int>* pay_slot = nullptr;
+    std::string pay_row = "e";
     Gen(Plan& pp, std::ostringstream& o) : p(pp), os(o), done(pp.ir.size(), 0) {}
 
     void emit(int i) {
@@ -550,6 +553,17 @@ struct Gen {
                         os << ind << "const bool " << x << " = " << ok << " && " << ld << " != 0;\n";
                     else
                         os << ind << "const " << ctype(n.type) << " " << x << " = " << ld << ";\n";
+                } else if (gather && pay_slot && n.col < (int)pay_slot->size() && (*pay_slot)[n.col] >= 0) {
+                    const std::string j = std::to_string((*pay_slot)[n.col]);
+                    os << ind << "const bool " << ok << " = " << (n.nullable ? "P.qpayv[" + j + "][" + pay_row + "] != 0" : "true") << ";\n";
+                    const std::string w = "P.qpay[" + j + "][" + pay_row + "]";
+                    switch (n.type) {
+                        case VEXQ_TYPE_FLOAT64: os << ind << "const double " << x << " = __longlong_as_double((long long)" << w << ");\n"; break;
+                        case VEXQ_TYPE_INT64: os << ind << "const long long " << x << " = (long long)" << w << ";\n"; break;
+                        case VEXQ_TYPE_DATE: os << ind << "const int " << x << " = (int)(long long)" << w << ";\n"; break;
+                        case VEXQ_TYPE_STRING: os << ind << "const unsigned " << x << " = (unsigned)" << w << ";\n"; break;
+                        default: os << ind << "const bool " << x << " = " << ok << " && " << w << " != 0ull;\n"; break;
+                    }
                 } else if (gather) {
                     std::string ct = n.type == VEXQ_TYPE_BOOL ? "unsigned char" : ctype(n.type);
                     os << ind << "const bool " << ok << " = " << (n.nullable ? "vq_bit(P.valid[" + c + "], " + row + ")" : "true") << ";\n";
@@ -1855,11 +1869,13 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
 // P.phist; mode 1 re-runs the same rows in the same blocks and scatters
 // (key, row) to the offsets the scan left in P.phist. Order inside a
 // partition is not kept: the join pass sorts each build partition.
-static std::string gen_part_kernel(Plan& p, const Table* t, int pred, int key_node, int block) {
+static std::string gen_part_kernel(Plan& p, const Table* t, int pred, int key_node, int block,
+                                   const std::vector<int>& pay_cols = {}) {
     std::ostringstream os;
     std::set<int> cols;
     collect_cols(p, pred, cols);
     collect_cols(p, key_node, cols);
+    for (int c : pay_cols) cols.insert(c);
     os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") vq_part(const __grid_constant__ VQParams P) {\n";
     os << "    extern __shared__ __align__(16) unsigned vq_hist[];\n";
     os << "    const int np = P.nparts;\n";
@@ -1891,6 +1907,19 @@ static std::string gen_part_kernel(Plan& p, const Table* t, int pred, int key_no
     os << "                const unsigned pos = atomicAdd(vq_hist + part, 1u);\n";
     os << "                P.pkeys[pos] = jk;\n";
     os << "                P.prows[pos] = (int)r;\n";
+    for (size_t j = 0; j < pay_cols.size(); j++) {
+        const int c = pay_cols[j];
+        const Column& col = t->cols[c];
+        const std::string C = std::to_string(c), J = std::to_string(j);
+        std::string w;
+        switch (col.type) {
+            case VEXQ_TYPE_FLOAT64: w = "(unsigned long long)__double_as_longlong(cv" + C + "[k])"; break;
+            case VEXQ_TYPE_DATE: w = "(unsigned long long)(long long)cv" + C + "[k]"; break;
+            default: w = "(unsigned long long)cv" + C + "[k]"; break;
+        }
+        os << "                P.qpay[" << J << "][pos] = " << w << ";\n";
+        if (col.nullable) os << "                P.qpayv[" << J << "][pos] = (unsigned char)((cm" << C << " >> k) & 1u);\n";
+    }
     os << "            }\n";
     os << "        }\n    }\n";
     os << "    __syncthreads();\n";
@@ -1909,12 +1938,25 @@ static std::string gen_part_kernel(Plan& p, const Table* t, int pred, int key_no
 static const int kRadixCap = VQ_RADIX_CAP;
 static const int kRadixMaxBits = VQ_RADIX_MAX_BITS;
 
+// Partition-local aggregation (GROUP BY the join key): per build entry the
+// accumulators of the group whose run starts there, in shared memory after the
+// keys and rows: [first][int bank][fixed-point digits][flags] × rcap entries.
+static int rlocal_bytes_per_entry(const Plan& p) { return 12 + 8 + 8 * p.ni + 36 * p.nf; }
+
 static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
     std::ostringstream os;
+    const int cap = p.rcap;
+    const std::string CAP = std::to_string(cap);
     os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") vq_rjoin(const __grid_constant__ VQParams P) {\n";
     os << "    extern __shared__ __align__(16) unsigned char vq_sm[];\n";
     os << "    unsigned long long* sk = (unsigned long long*)vq_sm;\n";
-    os << "    int* sr = (int*)(vq_sm + " << kRadixCap * 8 << ");\n";
+    os << "    int* sr = (int*)(vq_sm + " << cap * 8 << ");\n";
+    if (p.rlocal) {
+        os << "    long long* LF = (long long*)(vq_sm + " << cap * 12 << ");\n";
+        os << "    long long* LI = LF + " << cap << ";\n";
+        os << "    long long* LX = LI + " << (long long)cap * p.ni << ";\n";
+        os << "    unsigned* LS = (unsigned*)(LX + " << (long long)cap * 4 * p.nf << ");\n";
+    }
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     os << "    for (int part = blockIdx.x; part < P.nparts; part += gridDim.x) {\n";
     os << "        const long long b0 = P.bstart[part];\n";
@@ -1939,6 +1981,15 @@ static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, 
     os << "                }\n";
     os << "                __syncthreads();\n";
     os << "            }\n";
+    if (p.rlocal) {  // identities for every entry's group accumulators
+        std::vector<long long> iv = init_values(p);
+        os << "        for (int i = threadIdx.x; i < nb; i += blockDim.x) {\n";
+        os << "            LF[i] = 0x7FFFFFFFFFFFFFFFLL;\n";
+        for (int s = 0; s < p.ni; s++) os << "            LI[" << s << " * " << CAP << " + i] = " << ilit(iv[s]) << ";\n";
+        os << "            for (int d = 0; d < " << 4 * p.nf << "; d++) LX[(long long)i * " << 4 * p.nf << " + d] = 0;\n";
+        for (int f = 0; f < p.nf; f++) os << "            LS[" << f << " * " << CAP << " + i] = 0u;\n";
+        os << "        }\n        __syncthreads();\n";
+    }
     os << "        const long long q1 = P.qstart[part + 1];\n";
     os << "        for (long long e = P.qstart[part] + threadIdx.x; e < q1; e += blockDim.x) {\n";
     os << "            const unsigned long long jkey = P.qkeys[e];\n";
@@ -1951,6 +2002,10 @@ static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, 
     g.gather = true;
     g.row = "r";
     g.ind = "                ";
+    std::vector<int> pay_slot(p.t->cols.size(), -1);
+    for (size_t j = 0; j < p.qpay_cols.size(); j++) pay_slot[p.qpay_cols[j]] = (int)j;
+    g.pay_slot = &pay_slot;
+    g.pay_row = "e";
     if (p.resid >= 0) {
         g.emit(p.resid);
         os << "                if (!(x" << p.resid << " && ok" << p.resid << ")) continue;\n";
@@ -1960,9 +2015,68 @@ static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, 
     emit_key(os, p, key_nodes, "                ");
     emit_slot_values(os, p, "                ");
     std::string order = order_expr(p, "((r << 16) | (long long)min(ji - lo, 65535))");
-    if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
-    else emit_atomic_update(os, p, "                ", order);
-    os << "            }\n        }\n    }\n";
+    if (p.rlocal) {
+        // the group is the key's run: shared-memory atomics on the run head `lo`
+        const std::string in = "                ";
+        os << in << "{ const long long ord = " << order << ";\n";
+        os << in << "  if (ord < LF[lo]) atomicMin(LF + lo, ord);\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            const std::string S = std::to_string(s);
+            const int pos = p.slot_pos[s];
+            const std::string li = "LI + " + std::to_string(pos) + " * " + CAP + " + lo";
+            switch (p.slots[s].kind) {
+                case S_CNT: os << in << "  atomicAdd((unsigned long long*)(" << li << "), 1ull);\n"; break;
+                case S_NN: os << in << "  if (sok" << S << ") atomicAdd((unsigned long long*)(" << li << "), 1ull);\n"; break;
+                case S_ISUM: os << in << "  if (sok" << S << ") atomicAdd((unsigned long long*)(" << li << "), (unsigned long long)sv" << S << ");\n"; break;
+                case S_IMIN: os << in << "  if (sok" << S << " && sv" << S << " < *(" << li << ")) atomicMin(" << li << ", sv" << S << ");\n"; break;
+                case S_IMAX: os << in << "  if (sok" << S << " && sv" << S << " > *(" << li << ")) atomicMax(" << li << ", sv" << S << ");\n"; break;
+                case S_FMIN:
+                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) atomicMin((unsigned long long*)(" << li << "), vq_fkey(sv" << S << "));\n";
+                    break;
+                case S_FMAX:
+                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) atomicMax((unsigned long long*)(" << li << "), vq_fkey(sv" << S << "));\n";
+                    break;
+                case S_FSUM:
+                    os << in << "  if (sok" << S << ") vq_fx_add<true>(LX + ((long long)lo * " << p.nf << " + " << pos << ") * 4, sv" << S
+                       << ", P.fx_lsb[" << pos << "], LS + " << pos << " * " << CAP << " + lo, P.error);\n";
+                    break;
+            }
+        }
+        os << in << "}\n";
+    } else if (p.path == AggPath::Regs) {
+        emit_regs_update(os, p, "                ", order);
+    } else {
+        emit_atomic_update(os, p, "                ", order);
+    }
+    os << "            }\n        }\n";
+    if (p.rlocal) {
+        // each group lives in one partition only: its totals go to the global
+        // table with plain stores (the table starts at the identities)
+        os << "        __syncthreads();\n";
+        os << "        for (int i = threadIdx.x; i < nb; i += blockDim.x) {\n";
+        os << "            if ((i > 0 && sk[i] == sk[i - 1]) || LI[" << p.slot_pos[0] << " * " << CAP << " + i] == 0) continue;\n";
+        const int kn = key_nodes[0];
+        const INode& kx = p.ir[kn];
+        os << "            const bool ok" << kn << " = true;\n";
+        os << "            const " << ctype(kx.type) << " x" << kn << " = (" << ctype(kx.type) << ")(long long)sk[i];\n";
+        emit_key(os, p, key_nodes, "            ");
+        if (p.path == AggPath::Dense) os << "            const unsigned long long slot = key;\n";
+        else {
+            os << "            const unsigned long long slot = vq_insert(P.keys, P.cap_mask, P.cap, key, nullptr, P.error);\n";
+            os << "            if (slot == VQ_NOSLOT) continue;\n";
+        }
+        os << "            const long long stride = (long long)P.cap + 1;\n";
+        os << "            P.first[slot] = LF[i];\n";
+        for (int s = 0; s < p.ni; s++)
+            os << "            P.acc_i[" << s << " * stride + slot] = LI[" << s << " * " << CAP << " + i];\n";
+        for (int f = 0; f < p.nf; f++) {
+            os << "            for (int d = 0; d < 4; d++) P.acc_fx[((long long)" << f << " * stride + slot) * 4 + d] = LX[((long long)i * "
+               << p.nf << " + " << f << ") * 4 + d];\n";
+            os << "            P.special[" << f << " * stride + slot] = LS[" << f << " * " << CAP << " + i];\n";
+        }
+        os << "        }\n";
+    }
+    os << "    }\n";
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
     return os.str();
@@ -2066,7 +2180,38 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     if (join) {
         p.src_build = std::string(prelude_source()) + "\n" + gen_build_kernel(p, build_key_node, kBlock);
         p.src_part_b = std::string(prelude_source()) + "\n" + gen_part_kernel(p, p.bt, p.bpred, build_key_node, kBlock);
-        p.src_part_p = std::string(prelude_source()) + "\n" + gen_part_kernel(p, p.t, p.pred, p.probe_key, kBlock);
+        // probe columns read above the join travel with the partitioned entries
+        {
+            std::set<int> above;
+            std::function<void(int)> walk = [&](int i) {
+                if (i < 0) return;
+                const INode& n = p.ir[i];
+                if (n.k == NK::Col && !n.build && n.tab == p.t) above.insert(n.col);
+                for (int ch : n.ch) walk(ch);
+            };
+            walk(p.resid);
+            for (int k : key_nodes) walk(k);
+            for (auto& sl : p.slots) walk(sl.input);
+            p.qpay_cols.clear();
+            for (int c : above)
+                if (p.qpay_cols.size() < 8) p.qpay_cols.push_back(c);
+        }
+        p.src_part_p = std::string(prelude_source()) + "\n" + gen_part_kernel(p, p.t, p.pred, p.probe_key, kBlock, p.qpay_cols);
+        // GROUP BY exactly the join key on a group-table path: aggregate per partition
+        p.rlocal = false;
+        p.rcap = kRadixCap;
+        if (p.path != AggPath::Regs && p.keys.size() == 1 && !p.keys[0].nullable) {
+            const KeyCol& k = p.keys[0];
+            const bool jk = (k.build && k.col == p.build_key) || (!k.build && k.col == p.ir[p.probe_key].col);
+            const int per = rlocal_bytes_per_entry(p);
+            int cap = kRadixCap;
+            // ≤ 96 KB a block keeps two or more blocks per SM
+            while (cap > 256 && (long long)cap * per > 96 * 1024) cap >>= 1;
+            if (jk && (long long)cap * per <= 96 * 1024 && std::getenv("VEXQ_NO_RLOCAL") == nullptr) {
+                p.rlocal = true;
+                p.rcap = cap;
+            }
+        }
         p.src_rjoin = std::string(prelude_source()) + "\n" + gen_kind_tables(p) + "\n" + gen_rjoin_kernel(p, key_nodes, p.block);
     }
     std::ostringstream ex;
@@ -2083,7 +2228,8 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         p.k_part_b = jit_get(p.src_part_b, "vq_part", kBlock, 4 << kRadixMaxBits);
         p.k_part_p = jit_get(p.src_part_p, "vq_part", kBlock, 4 << kRadixMaxBits);
         // 48 KB of keys and rows plus an opt-in margin for the register path's static staging
-        p.k_rjoin = jit_get(p.src_rjoin, "vq_rjoin", p.block, kRadixCap * 12 + 8192);
+        p.k_rjoin = jit_get(p.src_rjoin, "vq_rjoin", p.block,
+                            (p.rlocal ? p.rcap * rlocal_bytes_per_entry(p) : kRadixCap * 12) + 8192);
         p.radix = p.radix_bits != 0;
     }
     // device-side tables of the plan

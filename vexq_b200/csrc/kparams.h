@@ -53,6 +53,8 @@ struct VQParams {
     const long long* qstart;       // join: [nparts + 1] probe partition starts in qkeys/qrows
     const unsigned long long* qkeys;
     const int* qrows;
+    unsigned long long* qpay[8];   // probe columns used above the join, per probe entry (raw 8-byte words)
+    unsigned char* qpayv[8];       // their validity (nullable columns)
     // ---- numeric literals of the plan's expressions (int64, date, float64 bits):
     //      plans that differ only in constants share one compiled kernel ----
     long long lit[VQ_MAXLITS];

@@ -145,6 +145,10 @@ struct Plan {
     std::string src_part_b, src_part_p, src_rjoin;
     JitKernel k_part_b, k_part_p, k_rjoin;
     DevBuf rp_bkeys, rp_brows, rp_qkeys, rp_qrows, rp_hist, rp_off, rp_start, rp_scalar;
+    std::vector<int> qpay_cols;    // probe columns carried in the partition payload (≤ 8)
+    bool rlocal = false;           // GROUP BY the join key: groups aggregated per partition in shared memory
+    int rcap = VQ_RADIX_CAP;       // build entries a partition may hold
+    DevBuf rp_qpay[8], rp_qpayv[8];
     ~Plan();
 };
 

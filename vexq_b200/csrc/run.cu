@@ -962,7 +962,7 @@ cudaStream_t plan_stream(Plan& p) {
 // partition exceeds the shared-memory capacity and *maxpart is asked for —
 // the scatter of (key, row) into keys/rows. Returns the entries written.
 static long long radix_pass(RunCtx& rc, const JitKernel& kp, VQParams Q, int pbits, long long* d_starts, DevBuf& keys,
-                            DevBuf& rows, long long* maxpart) {
+                            DevBuf& rows, long long* maxpart, int cap) {
     Plan& p = rc.p;
     const int np = 1 << pbits;
     const int grid = grid_for(kp, Q.nchunks, false);
@@ -998,7 +998,7 @@ static long long radix_pass(RunCtx& rc, const JitKernel& kp, VQParams Q, int pbi
         long long mx = 0;
         for (int i = 0; i < np; i++) mx = std::max(mx, hs[i + 1] - hs[i]);
         *maxpart = mx;
-        if (mx > VQ_RADIX_CAP) return total;
+        if (mx > cap) return total;
     }
     keys.ensure((size_t)std::max<long long>(total, 1) * 8);
     rows.ensure((size_t)std::max<long long>(total, 1) * 4);
@@ -1033,7 +1033,10 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         // radix partitioning (RadixBitsFor, exec/parallel_join.go:72-89): none
         // below 65,536 build rows; partitions sized to fit shared memory
         // automatic choice: the global table until partitioning measures faster
-        use_radix = p.radix && !p.staged && p.btile == 128 && p.tile == 128 && p.radix_bits > 0;
+        // (VEXQ_RADIX=1 partitions with automatic bits, for measurement)
+        static const bool radix_env = std::getenv("VEXQ_RADIX") && std::getenv("VEXQ_RADIX")[0] == '1';
+        use_radix = p.radix && !p.staged && p.btile == 128 && p.tile == 128 &&
+                    (p.radix_bits > 0 || (p.radix_bits < 0 && radix_env && bs.rows >= 65536));
         if (use_radix) {
             VQParams B;
             std::memset(&B, 0, sizeof B);
@@ -1055,7 +1058,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
                 pbits = std::min(p.radix_bits, VQ_RADIX_MAX_BITS);
             } else {
                 pbits = 1;
-                while (pbits < VQ_RADIX_MAX_BITS && (bs.rows >> pbits) > VQ_RADIX_CAP / 2) pbits++;
+                while (pbits < VQ_RADIX_MAX_BITS && (bs.rows >> pbits) > p.rcap / 2) pbits++;
             }
             p.rp_start.ensure((size_t)2 * ((1 << VQ_RADIX_MAX_BITS) + 1) * 8);
             long long* bstart = p.rp_start.as<long long>();
@@ -1064,10 +1067,10 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             long long total = 0;
             for (;;) {
                 long long mx = 0;
-                total = bs.nchunks > 0 ? radix_pass(rc, p.k_part_b, B, pbits, bstart, p.rp_bkeys, p.rp_brows, &mx) : 0;
-                if (mx <= VQ_RADIX_CAP) break;
+                total = bs.nchunks > 0 ? radix_pass(rc, p.k_part_b, B, pbits, bstart, p.rp_bkeys, p.rp_brows, &mx, p.rcap) : 0;
+                if (mx <= p.rcap) break;
                 if (pbits >= VQ_RADIX_MAX_BITS) { use_radix = false; break; }  // one key's chain is too long: global table
-                while (pbits < VQ_RADIX_MAX_BITS && mx > VQ_RADIX_CAP) { pbits++; mx = (mx + 1) / 2; }
+                while (pbits < VQ_RADIX_MAX_BITS && mx > p.rcap) { pbits++; mx = (mx + 1) / 2; }
             }
             VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
             VQ_CUDA(cudaEventSynchronize(p.ev[5]));
@@ -1246,7 +1249,17 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         ensure_events(p);
         VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
         long long* qstart = p.rp_start.as<long long>() + ((1 << VQ_RADIX_MAX_BITS) + 1);
-        radix_pass(rc, p.k_part_p, P, pbits, qstart, p.rp_qkeys, p.rp_qrows, nullptr);
+        // payload columns: sized for every probe row of the scanned ranges
+        VQParams Q = P;
+        for (size_t j = 0; j < p.qpay_cols.size(); j++) {
+            p.rp_qpay[j].ensure((size_t)std::max<long long>(ss.rows, 1) * 8);
+            Q.qpay[j] = P.qpay[j] = p.rp_qpay[j].as<unsigned long long>();
+            if (t.cols[p.qpay_cols[j]].nullable) {
+                p.rp_qpayv[j].ensure((size_t)std::max<long long>(ss.rows, 1));
+                Q.qpayv[j] = P.qpayv[j] = p.rp_qpayv[j].as<unsigned char>();
+            }
+        }
+        radix_pass(rc, p.k_part_p, Q, pbits, qstart, p.rp_qkeys, p.rp_qrows, nullptr, p.rcap);
         VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
         VQ_CUDA(cudaEventSynchronize(p.ev[5]));
         rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
