@@ -1406,9 +1406,11 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
     os << in << "}\n" << ind << "}\n";
 }
 
-std::string kernel_head(const std::string& name, int block) {
+std::string kernel_head(const std::string& name, int block, int min_blocks = 0) {
     std::ostringstream os;
-    os << "extern \"C\" __global__ void __launch_bounds__(" << block << ") " << name
+    os << "extern \"C\" __global__ void __launch_bounds__(" << block;
+    if (min_blocks > 0) os << ", " << min_blocks;
+    os << ") " << name
        << "(const __grid_constant__ VQParams P) {\n";
     return os.str();
 }
@@ -1574,32 +1576,122 @@ void chunk_loop_close(std::ostringstream& os, const Plan& p, const Table* t, con
 }
 
 
-// Loop skeleton used by every scan kernel: TMA-staged tiles (default) or the
-// register-prefetch chunk loop.
+// ---- per-warp cp.async pipeline -------------------------------------------------------
+// Each warp keeps `stages` 128-row chunk buffers in shared memory: while it
+// computes chunk i from its buffer, the copies of the next stages-1 chunks are
+// in flight, so bytes in flight do not cost registers. One commit group per
+// iteration (possibly empty) keeps cp.async.wait_group's count exact.
+struct AsyncLayout {
+    int chunk_bytes = 0;
+    std::map<int, int> off, voff;
+};
+
+AsyncLayout async_layout(const Table* t, const std::set<int>& cols) {
+    AsyncLayout L;
+    int o = 0;
+    for (int c : cols) { L.off[c] = o; o += 128 * type_w(t->cols[c].type); }
+    for (int c : cols)
+        if (t->cols[c].nullable) { L.voff[c] = o; o += 16; }
+    L.chunk_bytes = (o + 15) & ~15;
+    return L;
+}
+
+void emit_async_issue_fn(std::ostringstream& os, const Table* t, const std::set<int>& cols, const AsyncLayout& L,
+                         const std::string& name) {
+    os << "__device__ __forceinline__ void " << name << "(const VQParams& P, unsigned char* dst, long long cc, int lane) {\n";
+    os << "    int lo = 0, hi = P.nseg - 1;\n";
+    os << "    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= cc) lo = mid; else hi = mid - 1; }\n";
+    os << "    const long long base = (P.seg[3 * lo] & ~127LL) + (cc - P.seg[3 * lo + 2]) * 128;\n";
+    for (int c : cols) {
+        const int w = type_w(t->cols[c].type);
+        os << "    { const unsigned char* src = (const unsigned char*)P.col[" << c << "] + base * " << w << ";\n";
+        os << "      for (int i = lane; i < " << 8 * w << "; i += 32) vq_cp16(dst + " << L.off.at(c) << " + i * 16, src + i * 16); }\n";
+    }
+    for (auto& kv : L.voff)
+        os << "    if (lane == 0) vq_cp16(dst + " << kv.second << ", P.valid[" << kv.first << "] + (base >> 3));\n";
+    os << "}\n";
+}
+
+void async_loop_open(std::ostringstream& os, const Table* t, const std::set<int>& cols, const AsyncLayout& L, int stages,
+                     const std::string& issue) {
+    os << "    extern __shared__ __align__(16) unsigned char vq_abuf[];\n";
+    os << "    const int lane = threadIdx.x & 31;\n";
+    os << "    unsigned char* const wb = vq_abuf + (threadIdx.x >> 5) * " << stages * L.chunk_bytes << ";\n";
+    os << "    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;\n";
+    os << "    const long long c0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;\n";
+    os << "    for (int s = 0; s < " << stages - 1 << "; s++) {\n";
+    os << "        const long long cc = c0 + s * nw;\n";
+    os << "        if (cc < P.nchunks) " << issue << "(P, wb + s * " << L.chunk_bytes << ", cc, lane);\n";
+    os << "        vq_cp_commit();\n    }\n";
+    os << "    long long it = 0;\n";
+    os << "    for (long long c = c0; c < P.nchunks; c += nw, it++) {\n";
+    os << "        const long long cn = c + " << stages - 1 << " * nw;\n";
+    os << "        if (cn < P.nchunks) " << issue << "(P, wb + (int)((it + " << stages - 1 << ") % " << stages << ") * " << L.chunk_bytes
+       << ", cn, lane);\n";
+    os << "        vq_cp_commit();\n";
+    os << "        vq_cp_wait<" << stages - 1 << ">();\n";
+    os << "        __syncwarp();\n";
+    os << "        const unsigned char* st = wb + (int)(it % " << stages << ") * " << L.chunk_bytes << ";\n";
+    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    for (int c : cols) {
+        const Column& col = t->cols[c];
+        std::string C = std::to_string(c);
+        const char* ty = "unsigned";
+        const char* fn = "vq_sld4_u32";
+        switch (col.type) {
+            case VEXQ_TYPE_INT64: ty = "long long"; fn = "vq_sld4_i64"; break;
+            case VEXQ_TYPE_FLOAT64: ty = "double"; fn = "vq_sld4_f64"; break;
+            case VEXQ_TYPE_DATE: ty = "int"; fn = "vq_sld4_i32"; break;
+            case VEXQ_TYPE_BOOL: ty = "unsigned"; fn = "vq_sld4_u8"; break;
+        }
+        os << "        " << ty << " cv" << C << "[4]; " << fn << "(st + " << L.off.at(c) << ", lane * 4, cv" << C << ");\n";
+        if (col.nullable) os << "        const unsigned cm" << C << " = vq_sbits4(st + " << L.voff.at(c) << ", lane * 4);\n";
+    }
+}
+
+void async_loop_close(std::ostringstream& os) {
+    os << "        __syncwarp();  // the buffer is refilled after every lane has read it\n";
+    os << "    }\n";
+    os << "    vq_cp_wait<0>();\n";
+}
+
+// Loop skeleton used by every scan kernel: TMA-staged tiles, the per-warp
+// cp.async pipeline, or the (optionally register-prefetched) chunk loop.
 struct ScanLoop {
     const Plan& p;
     const Table* t;
     std::set<int> cols;
     StageLayout L;
+    AsyncLayout A;
     std::string issue;
     bool staged;
-    ScanLoop(const Plan& pp, const Table* tt, const std::set<int>& cc, int block, const std::string& name)
+    int async_n = 0;
+    int warps = 8;
+    ScanLoop(const Plan& pp, const Table* tt, const std::set<int>& cc, int block, const std::string& name, bool allow_async = false)
         : p(pp), t(tt), cols(cc), staged(pp.staged) {
         int budget = pp.stage_budget > 0 ? pp.stage_budget : (block >= 256 ? 160 * 1024 : 96 * 1024);
         L = stage_layout(t, cols, block, budget);
         issue = "vq_issue_" + name;
+        warps = block / 32;
+        if (!staged && allow_async && pp.async_stages > 1) {
+            async_n = pp.async_stages;
+            A = async_layout(t, cols);
+        }
     }
     int tile_rows() const { return staged ? L.T : 128; }
-    int smem() const { return staged ? L.S * L.stage_bytes : 0; }
+    int smem() const { return staged ? L.S * L.stage_bytes : async_n ? warps * async_n * A.chunk_bytes : 0; }
     void prologue(std::ostringstream& os) const {
         if (staged) emit_issue_fn(os, t, cols, L, issue);
+        else if (async_n) emit_async_issue_fn(os, t, cols, A, issue);
     }
     void open(std::ostringstream& os) const {
         if (staged) staged_loop_open(os, t, cols, L, issue);
+        else if (async_n) async_loop_open(os, t, cols, A, async_n, issue);
         else chunk_loop_open(os, p, t, cols);
     }
     void close(std::ostringstream& os) const {
         if (staged) staged_loop_close(os, L, issue);
+        else if (async_n) async_loop_close(os);
         else chunk_loop_close(os, p, t, cols);
     }
 };
@@ -1642,11 +1734,12 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     collect_cols(p, p.pred, cols);
     for (int k : key_nodes) collect_cols(p, k, cols);
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
-    ScanLoop loop(p, p.t, cols, block, "agg");
+    // the cp.async pipeline owns the dynamic shared memory: register path only
+    ScanLoop loop(p, p.t, cols, block, "agg", p.path == AggPath::Regs);
     p.tile = loop.tile_rows();
     p.smem = p.smem_groups > 0 ? cache_bytes(p) : loop.smem();
     loop.prologue(os);
-    os << kernel_head("vq_agg", block);
+    os << kernel_head("vq_agg", block, p.min_blocks);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     if (p.smem_groups > 0) emit_cache_init(os, p);
     loop.open(os);
@@ -2129,7 +2222,9 @@ static void choose_tunables(Plan& p) {
         };
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
-        int ck = get("cache_kb="), wa = get("warp_agg=");
+        int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb=");
+        if (as >= 0) p.async_stages = as;
+        if (mb >= 0) p.min_blocks = mb;
         if (ck >= 0) cache_kb = ck;
         if (wa >= 0) p.warp_agg = wa != 0;
         if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
@@ -2217,7 +2312,10 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     std::ostringstream ex;
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
-       << " block=" << p.block << (p.staged ? " staged=tma" : p.pipeline ? " pipeline=1" : " pipeline=0")
+       << " block=" << p.block
+       << (p.staged ? " staged=tma" : (p.async_stages > 1 && p.path == AggPath::Regs && !join) ? " async=" + std::to_string(p.async_stages)
+           : p.pipeline ? " pipeline=1" : " pipeline=0")
+       << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
     p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);

@@ -419,6 +419,14 @@ __device__ __forceinline__ void vq_sld4_u8(const unsigned char* s, int o, unsign
     unsigned w = reinterpret_cast<const unsigned*>(s)[o >> 2];
     v[0] = w & 0xFF; v[1] = (w >> 8) & 0xFF; v[2] = (w >> 16) & 0xFF; v[3] = w >> 24;
 }
+// Per-warp asynchronous copies (cp.async, 16 bytes, L2 only) into shared memory.
+__device__ __forceinline__ void vq_cp16(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(vq_smem_addr(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void vq_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void vq_cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 __device__ __forceinline__ unsigned vq_sbits4(const unsigned char* s, int o) {
     return (s[o >> 3] >> (o & 7)) & 0xFu;
 }

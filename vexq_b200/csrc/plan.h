@@ -125,6 +125,8 @@ struct Plan {
     int smem_groups = 0;       // dense path: groups cached in block-private shared memory
     int stage_budget = 0;      // bytes of the stage ring per block (0: default)
     int tile = 128, smem = 0;  // main kernel: rows per loop unit, dynamic shared memory
+    int async_stages = 0;      // >1: per-warp cp.async pipeline of that many 128-row chunks
+    int min_blocks = 0;        // >0: __launch_bounds__ minimum resident blocks per SM
     int btile = 128, bsmem = 0;  // join build kernel
     // per-run caches (host-side overhead of a run)
     std::vector<long long> seg_cache;      // last uploaded segment list
