@@ -1,0 +1,130 @@
+"""GPU tests of the register-path accumulator forms: integer-valued sums kept
+as exact doubles (COUNT, integer SUM, AVG over an integer column sharing
+SUM's accumulator), float sums updated by FMA against the group's 0/1 hit
+when no value can be NaN/±inf, and the fallbacks when neither holds (NaN and
+±inf in a float column, integer sums that could pass 2^53). Every case is
+compared with the oracle; a table re-filled with values outside the ranges a
+plan was compiled for is refused."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import refcpu as R
+from tests.helpers import assert_float_vs_exact, assert_rows_match
+from vexq_b200 import abi, plan as P
+from vexq_b200.table import HostTable, date_column, float_column, int_column, string_column
+
+pytestmark = pytest.mark.gpu
+
+
+def key_table(n, seed, vals=None, ivals=None, valid=None, rg=8192):
+    rng = np.random.default_rng(seed)
+    keys, flag = rng.integers(0, 3, n), rng.integers(0, 2, n)
+    v = vals if vals is not None else np.rint(rng.uniform(0, 1e5, n)) / 100.0
+    iv = ivals if ivals is not None else rng.integers(1, 51, n)
+    d = (8036 + rng.integers(0, 2500, n)).astype(np.int32)
+    cols = [string_column("k", keys, ["A", "N", "R"], n, rg), string_column("f", flag, ["F", "O"], n, rg), float_column("v", v),
+            int_column("q", iv.astype(np.int64), valid), date_column("d", d)]
+    return HostTable(cols, n, rg)
+
+
+def aggs():
+    return [P.count_star("n"), P.sum_(P.col(3), "sq"), P.avg(P.col(3), "aq"), P.count(P.col(3), "cq"),
+            P.sum_(P.col(2), "sv"), P.avg(P.col(2), "av"), P.sum_(P.col(2) * (1 - P.col(2) / 1e6), "se"),
+            P.min_(P.col(2), "mn"), P.max_(P.col(3), "mx")]
+
+
+def run(X, host, plan):
+    op = X.GpuHashAggregate(X.GpuTable(host), plan)
+    try:
+        g = op.run()
+        g.collect()
+        return g, op.explain()
+    finally:
+        op.close()
+
+
+def check(X, host, plan):
+    g, ex = run(X, host, plan)
+    r = R.agg(R.RefTable(host), plan, workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_float_vs_exact(g.rows(), r)
+    return g, r, ex
+
+
+def test_exact_integer_sums_and_fma_float_sums(gpu_lib):
+    host = key_table(300_000, 1)
+    plan = P.AggPlan(P.col(4) <= P.lit("1998-09-02"), [0, 1], aggs())
+    g, r, ex = check(gpu_lib, host, plan)
+    # COUNT(*) and SUM(q) exact doubles, AVG(q) shares SUM(q); SUM(v) (which
+    # AVG(v) reuses) and the expression sum are FMA sums
+    assert "path=regs" in ex and "exact_int_sums=2" in ex and "shared_sums=1" in ex and "fma_sums=2" in ex, ex
+    # integer SUM and AVG(int) are exact: equal to the oracle bit for bit
+    for i, (a, b) in enumerate(zip(g.rows(), r.rows())):
+        assert a[3] == b[3] and a[4] == b[4] and a[5] == b[5], (i, a, b)
+
+
+def test_nullable_integer_column(gpu_lib):
+    n = 120_000
+    valid = np.random.default_rng(4).random(n) > 0.2
+    host = key_table(n, 2, valid=valid)
+    g, r, ex = check(gpu_lib, host, P.AggPlan(None, [0, 1], aggs()))
+    assert "exact_int_sums=" in ex
+    for a, b in zip(g.rows(), r.rows()):
+        assert a[3:6] == b[3:6]
+
+
+def test_nan_and_inf_take_the_selected_add(gpu_lib):
+    n = 100_000
+    rng = np.random.default_rng(3)
+    v = np.rint(rng.uniform(0, 1e5, n)) / 100.0
+    v[rng.choice(n, 5, replace=False)] = np.nan
+    v[rng.choice(np.arange(50_000, n), 3, replace=False)] = np.inf
+    host = key_table(n, 3, vals=v)
+    g, ex = run(gpu_lib, host, P.AggPlan(None, [0, 1], aggs()))
+    assert "fma_sums=0" in ex, ex
+    r = R.agg(R.RefTable(host), P.AggPlan(None, [0, 1], aggs()), workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_large_integers_keep_integer_accumulators(gpu_lib):
+    n = 40_000
+    rng = np.random.default_rng(5)
+    iv = rng.integers(-(1 << 50), 1 << 50, n)
+    host = key_table(n, 5, ivals=iv)
+    plan = P.AggPlan(None, [0], [P.sum_(P.col(3), "s"), P.avg(P.col(3), "a"), P.count_star("n")])
+    g, ex = run(gpu_lib, host, plan)
+    # |value| × rows passes 2^53: the integer SUM stays an int64 accumulator
+    assert "exact_int_sums=1" in ex and "shared_sums=0" in ex, ex
+    r = R.agg(R.RefTable(host), plan, workers=0)
+    assert [row[:2] for row in g.rows()] == [row[:2] for row in r.rows()]
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_refill_outside_compiled_range_is_refused(gpu_lib):
+    X = gpu_lib
+    host = key_table(50_000, 6)
+    gt = X.GpuTable(host)
+    plan = P.AggPlan(None, [0, 1], aggs())
+    op = X.GpuHashAggregate(gt, plan)
+    other = X.GpuHashAggregate(gt, P.AggPlan(None, [], [P.sum_(P.col(2), "s")]))
+    try:
+        same = op.run_host(host).rows()  # same values: the compiled ranges still hold
+        assert same == op.run().rows()
+        wide = key_table(50_000, 6, ivals=np.full(50_000, 10**6))
+        with pytest.raises(abi.VexqError) as e:
+            op.run_host(wide)
+        assert e.value.status == abi.EINVAL and "compile the plan again" in str(e.value)
+        with pytest.raises(abi.VexqError):
+            other.run()  # every plan compiled before the re-fill refuses
+        fresh = X.GpuHashAggregate(gt, plan)  # a plan compiled now sees the new values
+        try:
+            g = fresh.run()
+            r = R.agg(R.RefTable(wide), plan, workers=0)
+            assert_rows_match(g.rows(), r.rows(), ordered=True)
+        finally:
+            fresh.close()
+    finally:
+        op.close()
+        other.close()

@@ -381,6 +381,7 @@ struct Batch {
     }
 
     float replay() {
+        for (const Item& it : items) check_ranges(*it.p);
         if (!gexec) capture();
         VQ_CUDA(cudaEventRecord(ev[0], s));
         VQ_CUDA(cudaGraphLaunch(gexec, s));
@@ -389,6 +390,7 @@ struct Batch {
 
     // One execution launched directly, for plan sets that run once.
     float run_direct() {
+        for (const Item& it : items) check_ranges(*it.p);
         VQ_CUDA(cudaEventRecord(ev[0], s));
         enqueue();
         return finish_timing();

@@ -409,6 +409,7 @@ void analyze(Plan& p) {
                 } else if (c.type == VEXQ_TYPE_BOOL) {
                     n.bounded = true; n.lo = 0; n.hi = 1;
                 }
+                n.finite = c.type != VEXQ_TYPE_FLOAT64 || (c.finite && n.bounded);
                 break;
             }
             case NK::Lit:
@@ -416,10 +417,12 @@ void analyze(Plan& p) {
                 n.bounded = true;
                 n.lo = n.hi = n.type == VEXQ_TYPE_FLOAT64 ? n.lf : n.type == VEXQ_TYPE_DATE ? n.ld : (double)n.li;
                 if (!std::isfinite(n.lo)) n.bounded = false;
+                n.finite = n.type != VEXQ_TYPE_FLOAT64 || n.bounded;
                 break;
             case NK::Cast:
                 n.nullable = C(0).nullable;
                 n.bounded = C(0).bounded; n.lo = C(0).lo; n.hi = C(0).hi;
+                n.finite = C(0).finite || C(0).type != VEXQ_TYPE_FLOAT64;
                 break;
             case NK::Arith: {
                 n.nullable = C(0).nullable || C(1).nullable;
@@ -447,6 +450,8 @@ void analyze(Plan& p) {
                 if (n.bounded && (!std::isfinite(n.lo) || !std::isfinite(n.hi))) n.bounded = false;
                 // widen by a relative ulp margin for rounding
                 if (n.bounded) { double m = std::max(std::fabs(n.lo), std::fabs(n.hi)) * 1e-12; n.lo -= m; n.hi += m; }
+                // finite operands inside finite bounds give a finite result
+                n.finite = n.type != VEXQ_TYPE_FLOAT64 || (n.bounded && C(0).finite && C(1).finite);
                 break;
             }
             case NK::Case: {
@@ -464,19 +469,28 @@ void analyze(Plan& p) {
                     n.hi = std::max(n.hi, r.hi);
                 }
                 if (!n.has_else) { n.lo = std::min(n.lo, 0.0); n.hi = std::max(n.hi, 0.0); }
+                n.finite = true;
+                for (int w = 0; w <= nw; w++) {
+                    int ri = w < nw ? n.ch[2 * w + 1] : (n.has_else ? n.ch.back() : -1);
+                    if (ri >= 0 && !p.ir[ri].finite) n.finite = false;
+                }
+                n.finite = n.finite || n.type != VEXQ_TYPE_FLOAT64;
                 break;
             }
             case NK::IsNull:
             case NK::IsNotNull:
                 n.nullable = false;
+                n.finite = true;
                 break;
             case NK::StrEq:
                 n.nullable = C(0).nullable || n.present_idx >= 0 || n.streq_code < 0;
+                n.finite = true;
                 break;
             default: {
                 bool any = false;
                 for (int c : n.ch) any = any || p.ir[c].nullable;
                 n.nullable = any;
+                n.finite = n.type != VEXQ_TYPE_FLOAT64;
                 break;
             }
         }
@@ -990,11 +1004,100 @@ std::string acc_name(const Plan& p, int g, int s) {
     return (p.slots[s].is_float() ? "af" : "ai") + std::to_string(g) + "_" + std::to_string(p.slot_pos[s]);
 }
 
+static bool slot_rdx(const Plan& p, size_t s) { return s < p.rdx.size() && p.rdx[s]; }
+static bool slot_rfma(const Plan& p, size_t s) { return s < p.rfma.size() && p.rfma[s]; }
+static int slot_alias(const Plan& p, size_t s) { return s < p.ralias.size() ? p.ralias[s] : -1; }
+
+// Register variable holding slot s of group g during the scan: an exact-double
+// accumulator ("ad") for integer-valued sums, the aliased slot's variable for
+// a slot sharing another's sum, else the slot's own typed accumulator.
+std::string acc_var(const Plan& p, int g, int s) {
+    int t = slot_alias(p, s) >= 0 ? slot_alias(p, s) : s;
+    if (slot_rdx(p, t)) return "ad" + std::to_string(g) + "_" + std::to_string(t);
+    return acc_name(p, g, t);
+}
+
+// Integer input under a value-preserving int→float cast (the same values).
+static int strip_int_cast(const Plan& p, int i) {
+    while (i >= 0 && p.ir[i].k == NK::Cast && p.ir[i].type == VEXQ_TYPE_FLOAT64 && !p.ir[i].ch.empty() &&
+           p.ir[p.ir[i].ch[0]].type != VEXQ_TYPE_FLOAT64)
+        i = p.ir[i].ch[0];
+    return i;
+}
+
+static bool same_column(const Plan& p, int a, int b) {
+    if (a == b) return true;
+    const INode &x = p.ir[a], &y = p.ir[b];
+    return x.k == NK::Col && y.k == NK::Col && x.col == y.col && x.build == y.build && x.tab == y.tab;
+}
+
+// Chooses the register-path accumulator forms of an aggregate scan plan
+// (joins keep the plain forms: a probe row may match many build rows, so
+// no per-accumulator row bound exists). Integer-valued sums become exact
+// doubles when every partial sum stays within 2^53 (|value| bound × table
+// rows), which makes the update one FMA and lets AVG over an integer column
+// share SUM's accumulator; float sums of never-NaN/inf values use
+// fma(v, hit, acc), which equals the selected add bit for bit (v·1 and v·0
+// are exact, and the accumulator, starting at +0, is never -0).
+static void choose_regs_forms(Plan& p) {
+    const size_t n = p.slots.size();
+    p.rdx.assign(n, 0);
+    p.rfma.assign(n, 0);
+    p.ralias.assign(n, -1);
+    if (p.path != AggPath::Regs || p.is_join || !p.t) return;
+    const double rows = (double)std::max<int64_t>(p.t->nrows, 1);
+    const double lim = 9007199254740992.0;  // 2^53
+    std::vector<int> val(n, -1);
+    for (size_t s = 0; s < n; s++) {
+        const Slot& sl = p.slots[s];
+        if (sl.kind == S_CNT || sl.kind == S_NN) {
+            p.rdx[s] = rows <= lim;
+            continue;
+        }
+        if (sl.kind != S_ISUM && sl.kind != S_FSUM) continue;
+        const int v = strip_int_cast(p, sl.input);
+        const INode& x = p.ir[v];
+        if (x.type == VEXQ_TYPE_FLOAT64) {
+            if (sl.kind == S_FSUM && p.ir[sl.input].finite) p.rfma[s] = 1;
+            continue;
+        }
+        if (!x.bounded) continue;
+        const double m = std::max(std::fabs(x.lo), std::fabs(x.hi));
+        if (m * rows <= lim) {
+            p.rdx[s] = 1;
+            val[s] = v;
+        }
+    }
+    for (size_t s = 0; s < n; s++) {
+        if (!p.rdx[s] || val[s] < 0) continue;
+        for (size_t t = 0; t < s; t++)
+            if (p.rdx[t] && val[t] >= 0 && p.ralias[t] < 0 && same_column(p, val[s], val[t])) {
+                p.ralias[s] = (int)t;
+                break;
+            }
+    }
+}
+
+// The predicated update of an aggregate scan writes first-row keys only on a
+// lane's first row of each group, so they live in a per-thread array (local
+// memory, written at most once per group) instead of registers.
+static bool regs_fo_local(const Plan& p) { return p.regs_pred && !p.is_join; }
+
 // Register path: accumulators live in registers, one set per dense group.
 void emit_regs_decl(std::ostringstream& os, const Plan& p) {
+    if (regs_fo_local(p)) {
+        os << "    unsigned vq_seen = 0u;\n";
+        os << "    long long vq_fo[" << p.domain << "];\n";
+        os << "#pragma unroll\n    for (int g = 0; g < " << p.domain << "; g++) vq_fo[g] = 0x7FFFFFFFFFFFFFFFLL;\n";
+    }
     for (int64_t g = 0; g < p.domain; g++) {
-        os << "    long long fo" << g << " = 0x7FFFFFFFFFFFFFFFLL;\n";
+        if (!regs_fo_local(p)) os << "    long long fo" << g << " = 0x7FFFFFFFFFFFFFFFLL;\n";
         for (size_t s = 0; s < p.slots.size(); s++) {
+            if (slot_alias(p, s) >= 0) continue;
+            if (slot_rdx(p, s)) {
+                os << "    double " << acc_var(p, (int)g, (int)s) << " = 0.0;\n";
+                continue;
+            }
             const Slot& sl = p.slots[s];
             std::string init;
             switch (sl.kind) {
@@ -1017,7 +1120,16 @@ void emit_regs_update(std::ostringstream& os, const Plan& p, const std::string& 
         std::string in = ind + "    ";
         os << in << "fo" << g << " = min(fo" << g << ", " << order << ");\n";
         for (size_t s = 0; s < p.slots.size(); s++) {
-            std::string a = acc_name(p, (int)g, (int)s), S = std::to_string(s);
+            if (slot_alias(p, s) >= 0) continue;
+            std::string a = acc_var(p, (int)g, (int)s), S = std::to_string(s);
+            if (slot_rdx(p, s)) {
+                switch (p.slots[s].kind) {
+                    case S_CNT: os << in << a << " += 1.0;\n"; break;
+                    case S_NN: os << in << "if (sok" << S << ") " << a << " += 1.0;\n"; break;
+                    default: os << in << "if (sok" << S << ") " << a << " += (double)sv" << S << ";\n"; break;
+                }
+                continue;
+            }
             switch (p.slots[s].kind) {
                 case S_CNT: os << in << a << " += 1LL;\n"; break;
                 case S_NN: os << in << "if (sok" << S << ") " << a << " += 1LL;\n"; break;
@@ -1038,15 +1150,45 @@ void emit_regs_update(std::ostringstream& os, const Plan& p, const std::string& 
 // Branch-free register update: every group's accumulators are updated with a
 // select on (gid == g), so the four rows a lane holds form independent
 // dependency chains the scheduler can interleave (a switch serialises them).
+// A lane meets its rows in increasing row order (chunks and tiles ascend per
+// warp) and a group's order key rises with the row, so a group's first-row
+// key is recorded once, on the lane's first row of that group, in a branch
+// taken at most once per group and lane. Exact-double and finite float sums
+// are one FMA against the group's 0/1 hit.
 void emit_regs_update_pred(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
-    os << ind << "const long long ord = " << order << ";\n";
+    os << ind << "const unsigned vq_k32 = (unsigned)key;\n";
+    os << ind << "{ const unsigned vq_kb = vq_k32 < 32u ? (1u << vq_k32) : 0u;\n";
+    os << ind << "  if (key < " << p.domain << "ull && !(vq_seen & vq_kb)) {\n";
+    os << ind << "    vq_seen |= vq_kb;\n";
+    os << ind << "    vq_fo[vq_k32] = " << order << ";\n";
+    os << ind << "  } }\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        if (slot_alias(p, s) >= 0) continue;
+        std::string S = std::to_string(s);
+        const SlotKind k = p.slots[s].kind;
+        if (slot_rdx(p, s)) {
+            if (k == S_NN) os << ind << "const double vd" << S << " = sok" << S << " ? 1.0 : 0.0;\n";
+            else if (k != S_CNT) os << ind << "const double vd" << S << " = sok" << S << " ? (double)sv" << S << " : 0.0;\n";
+        } else if (slot_rfma(p, s)) {
+            os << ind << "const double vd" << S << " = sok" << S << " ? sv" << S << " : 0.0;\n";
+        }
+    }
     for (int64_t g = 0; g < p.domain; g++) {
         std::string G = std::to_string(g);
-        os << ind << "{ const bool h = key == " << g << "ull;\n";
+        os << ind << "{ const bool h = vq_k32 == " << g << "u;\n";
         std::string in = ind + "  ";
-        os << in << "fo" << G << " = (h && ord < fo" << G << ") ? ord : fo" << G << ";\n";
+        os << in << "const double hd = h ? 1.0 : 0.0;\n";
         for (size_t s = 0; s < p.slots.size(); s++) {
-            std::string a = acc_name(p, (int)g, (int)s), S = std::to_string(s);
+            if (slot_alias(p, s) >= 0) continue;
+            std::string a = acc_var(p, (int)g, (int)s), S = std::to_string(s);
+            if (slot_rdx(p, s) && p.slots[s].kind == S_CNT) {
+                os << in << a << " += hd;\n";
+                continue;
+            }
+            if (slot_rdx(p, s) || slot_rfma(p, s)) {
+                os << in << a << " = fma(vd" << S << ", hd, " << a << ");\n";
+                continue;
+            }
             switch (p.slots[s].kind) {
                 case S_CNT: os << in << a << " += h ? 1LL : 0LL;\n"; break;
                 case S_NN: os << in << a << " += (h && sok" << S << ") ? 1LL : 0LL;\n"; break;
@@ -1083,6 +1225,16 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
     int G = (int)p.domain;
     int nf = p.nf, ni = p.ni;
     const int WF = std::max(G * nf, 1), WI = std::max(G * (ni + 1), 1);
+    // first-row keys and exact-double / shared accumulators back to the
+    // variables (and types) the reduction below works on
+    if (regs_fo_local(p))
+        for (int g = 0; g < G; g++) os << "    long long fo" << g << " = vq_fo[" << g << "];\n";
+    for (int g = 0; g < G; g++)
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            if (!slot_rdx(p, s) && slot_alias(p, s) < 0) continue;
+            if (p.slots[s].is_float()) os << "    double " << acc_name(p, g, (int)s) << " = " << acc_var(p, g, (int)s) << ";\n";
+            else os << "    long long " << acc_name(p, g, (int)s) << " = (long long)" << acc_var(p, g, (int)s) << ";\n";
+        }
     if (fc.dyn_smem) {
         os << "    __syncthreads();\n";
         os << "    double (*sh_f)[" << WF << "] = (double (*)[" << WF << "])vq_smem;\n";
@@ -2242,6 +2394,8 @@ static void choose_tunables(Plan& p) {
 
 static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join, int build_key_node) {
     p.key_nodes = key_nodes;
+    p.range_epoch = p.t ? p.t->range_epoch : 0;
+    p.brange_epoch = p.bt ? p.bt->range_epoch : 0;
     analyze(p);
     // large IN/LIKE code sets go to device bitsets
     for (auto& n : p.ir) {
@@ -2255,6 +2409,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     }
     choose_path(p);
     choose_tunables(p);
+    choose_regs_forms(p);
     // numeric literals become launch-time values (first VQ_MAXLITS of them)
     p.lits.clear();
     for (auto& n : p.ir) {
@@ -2317,6 +2472,15 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
            : p.pipeline ? " pipeline=1" : " pipeline=0")
        << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
+    if (p.path == AggPath::Regs && !join) {
+        int nx = 0, nm = 0, na = 0;
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            nx += slot_rdx(p, s) && slot_alias(p, s) < 0;
+            nm += slot_rfma(p, s);
+            na += slot_alias(p, s) >= 0;
+        }
+        ex << " exact_int_sums=" << nx << " fma_sums=" << nm << " shared_sums=" << na;
+    }
     p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
     if (join) {
@@ -2542,6 +2706,7 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred) {
     std::unique_ptr<Plan> p(new Plan);
     p->t = t;
+    p->range_epoch = t->range_epoch;
     Translator tr{*p, nodes, nnodes, children, nchildren, t, nullptr};
     p->pred = tr.tr(pred);
     if (p->ir[p->pred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
@@ -2682,6 +2847,11 @@ static bool zone_rec(const Plan& p, int idx, const Table& t, int rg) {
 }
 
 bool zone_eval(const Plan& p, int root, const Table& t, int rg) { return root < 0 ? true : zone_rec(p, root, t, rg); }
+
+void check_ranges(const Plan& p) {
+    if ((p.t && p.t->range_epoch != p.range_epoch) || (p.bt && p.bt->range_epoch != p.brange_epoch))
+        fail(VEXQ_EINVAL, "table values were re-filled outside the value ranges this plan was compiled for; compile the plan again");
+}
 
 void set_plan_constants(const Plan& p, VQParams& P) {
     for (size_t i = 0; i < p.lits.size() && i < VQ_MAXLITS; i++) P.lit[i] = p.lits[i];

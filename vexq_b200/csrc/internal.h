@@ -88,6 +88,7 @@ struct Column {
     std::vector<vexq_zone_map> zones;              // per RG
     // table-wide min/max (numeric), for accumulator windows
     bool has_range = false;
+    bool finite = true;             // FLOAT64: every row group's zone sum is finite (no NaN/±inf)
     double fmin = 0, fmax = 0;      // FLOAT64
     int64_t imin = 0, imax = 0;     // INT64 / DATE
 };
@@ -98,6 +99,10 @@ struct Table {
     int32_t rg_rows = 65536;
     int32_t n_rg = 0;
     int device = 0;
+    // bumped when re-filled values leave a column's earlier range (or bring in
+    // NaN/±inf): plans compiled against the earlier ranges refuse to run
+    uint64_t range_epoch = 0;
+    bool zones_ready = false;
     int64_t rg_start(int rg) const { return (int64_t)rg * rg_rows; }
     int64_t rg_end(int rg) const { return std::min<int64_t>(nrows, (int64_t)(rg + 1) * rg_rows); }
     int64_t device_bytes() const;

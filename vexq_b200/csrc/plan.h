@@ -35,6 +35,9 @@ struct INode {
     // |value| bound from zone maps by interval arithmetic (exact-sum windows)
     bool bounded = false;
     double lo = 0, hi = 0;
+    // a valid value is never NaN or ±inf (non-float types always; floats from
+    // zone sums and bounded interval arithmetic)
+    bool finite = false;
     bool is_literal_raw = false;  // literal before coercion (SQL level)
     int lit_kind = 0;
     int lit_slot = -1;            // numeric literal passed at launch: index into VQParams::lit
@@ -127,6 +130,15 @@ struct Plan {
     int tile = 128, smem = 0;  // main kernel: rows per loop unit, dynamic shared memory
     int async_stages = 0;      // >1: per-warp cp.async pipeline of that many 128-row chunks
     int min_blocks = 0;        // >0: __launch_bounds__ minimum resident blocks per SM
+    // register-path accumulator forms, per slot (aggregate scans only):
+    //  rdx    integer-valued sum (COUNT, integer SUM, float SUM of an integer
+    //         input) kept as a double, exact while |sum| <= 2^53
+    //  ralias slot whose accumulator this slot shares (-1: its own)
+    //  rfma   float SUM of a never-NaN/inf value, updated as fma(v, hit, acc)
+    std::vector<char> rdx, rfma;
+    std::vector<int> ralias;
+    // value-range epochs of the tables the plan was compiled against
+    uint64_t range_epoch = 0, brange_epoch = 0;
     int btile = 128, bsmem = 0;  // join build kernel
     // per-run caches (host-side overhead of a run)
     std::vector<long long> seg_cache;      // last uploaded segment list
@@ -169,6 +181,9 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
 // Copies the plan's launch-time constants (literals, float-sum windows, cache size) into P.
 void set_plan_constants(const Plan& p, VQParams& P);
+// Fails when a table the plan reads was re-filled with values outside the
+// ranges (or finiteness) the plan's kernels were generated for.
+void check_ranges(const Plan& p);
 // Source of one batched launch over aggregate plans of one class: a body per
 // distinct plan shape (body_of[i] for plans[i]) and the vq_batch dispatcher;
 // smem = dynamic shared memory the bodies need beyond the dense caches.

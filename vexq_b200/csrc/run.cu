@@ -1014,6 +1014,7 @@ static long long radix_pass(RunCtx& rc, const JitKernel& kp, VQParams Q, int pbi
 
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
+    check_ranges(p);
     RunCtx rc{p, plan_stream(p)};
     VQParams P;
     std::memset(&P, 0, sizeof P);

@@ -3,6 +3,7 @@
 // remap exec/agg_intkey.go:118-134 performs per row group), and zone maps
 // with the writer's rules (storage/writer.go:205-372).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "internal.h"
@@ -258,7 +259,11 @@ void compute_zones(Table& t, cudaStream_t s) {
             }
         }
         // table-wide range for dense keys and exact-sum windows
+        const bool had = c.has_range, was_finite = c.finite;
+        const double ofmin = c.fmin, ofmax = c.fmax;
+        const int64_t oimin = c.imin, oimax = c.imax;
         c.has_range = false;
+        c.finite = true;
         for (int rg = 0; rg < t.n_rg; rg++) {
             const vexq_zone_map& zm = c.zones[rg];
             if (!zm.has_min_max || c.type == VEXQ_TYPE_STRING || c.type == VEXQ_TYPE_BOOL) continue;
@@ -268,6 +273,9 @@ void compute_zones(Table& t, cudaStream_t s) {
                 std::memcpy(&mx, &zm.max, 8);
                 if (!c.has_range) { c.fmin = mn; c.fmax = mx; }
                 else { c.fmin = std::min(c.fmin, mn); c.fmax = std::max(c.fmax, mx); }
+                double zs;  // the zone sum is NaN/±inf when the row group holds NaN or ±inf
+                std::memcpy(&zs, &zm.sum, 8);
+                if (!std::isfinite(zs)) c.finite = false;
             } else {
                 int64_t mn = c.type == VEXQ_TYPE_DATE ? (int64_t)(int32_t)(uint32_t)zm.min : (int64_t)zm.min;
                 int64_t mx = c.type == VEXQ_TYPE_DATE ? (int64_t)(int32_t)(uint32_t)zm.max : (int64_t)zm.max;
@@ -276,7 +284,15 @@ void compute_zones(Table& t, cudaStream_t s) {
             }
             c.has_range = true;
         }
+        if (t.zones_ready) {
+            bool wider = (was_finite && !c.finite);
+            if (had && c.has_range)
+                wider = wider || (c.type == VEXQ_TYPE_FLOAT64 ? (c.fmin < ofmin || c.fmax > ofmax)
+                                                             : (c.imin < oimin || c.imax > oimax));
+            if (wider) t.range_epoch++;
+        }
     }
+    t.zones_ready = true;
 }
 
 Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows) {
