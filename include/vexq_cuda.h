@@ -261,8 +261,10 @@ int32_t vexq_result_free(vexq_result_t r);
 /* Device timing of the last run: kernel milliseconds and launches. */
 int32_t vexq_result_stats(vexq_result_t r, double* kernel_ms, int32_t* launches,
                           int64_t* rows_scanned, int64_t* bytes_scanned);
-/* Duration of the run's scan kernel launches alone (CUDA events on the
- * plan's stream), in milliseconds. */
+/* Duration of the run's scan kernel launches (CUDA events on the plan's
+ * stream), in milliseconds. On the register path a scan and the partial merge
+ * launched as its programmatic dependent overlap, and the pair is timed as
+ * one span; the atomic paths time the scan alone. */
 int32_t vexq_result_scan_ms(vexq_result_t r, double* out);
 
 /* Runs a plan on a caller-owned CUDA stream (a cudaStream_t, e.g. the stream

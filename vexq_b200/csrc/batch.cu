@@ -327,7 +327,7 @@ struct Batch {
                 chk(s2, "vq_batch (register path)");
             }
             if (merge_entries > 0) {
-                k_merge_batch<<<merge_entries, 256, 0, s2>>>((const VQMergeDesc*)(D + a_mdesc), n_mdesc);
+                k_merge_batch<<<(merge_entries + 7) / 8, 256, 0, s2>>>((const VQMergeDesc*)(D + a_mdesc), n_mdesc);
                 VQ_CUDA(cudaGetLastError());
                 chk(s2, "k_merge_batch");
             }

@@ -546,6 +546,9 @@ struct Gen {
     // partition join: probe columns carried in the payload, read at entry `pay_row`
     const std::vector<int>* pay_slot = nullptr;
     std::string pay_row = "e";
+    // index of the current row in a chunk column (cv<c>[kidx]): "k" for the
+    // register arrays, "(k << 5)" for strided reads of a staged chunk
+    std::string kidx = "k";
     Gen(Plan& pp, std::ostringstream& o) : p(pp), os(o), done(pp.ir.size(), 0) {}
 
     void emit(int i) {
@@ -589,9 +592,9 @@ struct Gen {
                 } else {
                     os << ind << "const bool " << ok << " = " << (n.nullable ? "((cm" + c + " >> k) & 1u) != 0u" : "true") << ";\n";
                     if (n.type == VEXQ_TYPE_BOOL)
-                        os << ind << "const bool " << x << " = " << ok << " && cv" << c << "[k] != 0u;\n";
+                        os << ind << "const bool " << x << " = " << ok << " && cv" << c << "[" << kidx << "] != 0u;\n";
                     else
-                        os << ind << "const " << ctype(n.type) << " " << x << " = cv" << c << "[k];\n";
+                        os << ind << "const " << ctype(n.type) << " " << x << " = cv" << c << "[" << kidx << "];\n";
                 }
                 break;
             }
@@ -1225,6 +1228,9 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
     int G = (int)p.domain;
     int nf = p.nf, ni = p.ni;
     const int WF = std::max(G * nf, 1), WI = std::max(G * (ni + 1), 1);
+    // the scan is done: let the dependent merge launch while blocks flush
+    // (no effect when nothing was launched as a dependent)
+    if (!fc.dyn_smem) os << "    asm volatile(\"griddepcontrol.launch_dependents;\");\n";
     // first-row keys and exact-double / shared accumulators back to the
     // variables (and types) the reduction below works on
     if (regs_fo_local(p))
@@ -1571,12 +1577,13 @@ std::string kernel_head(const std::string& name, int block, int min_blocks = 0) 
 // handles rows r0..r0+3 with 128-bit loads. The loop is software-pipelined:
 // the loads of the warp's next chunk are issued before the current chunk is
 // processed, so a warp keeps two chunks of column data in flight.
-std::string seg_lookup(const std::string& c, const std::string& s0, const std::string& s1, const std::string& r0) {
+std::string seg_lookup(const std::string& c, const std::string& s0, const std::string& s1, const std::string& r0,
+                       const std::string& lane_term = "lane * 4") {
     return "{ int lo = 0, hi = P.nseg - 1;\n"
            "          while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (P.seg[3 * mid + 2] <= " + c +
            ") lo = mid; else hi = mid - 1; }\n"
            "          " + s0 + " = P.seg[3 * lo]; " + s1 + " = P.seg[3 * lo + 1];\n"
-           "          " + r0 + " = (" + s0 + " & ~127LL) + (" + c + " - P.seg[3 * lo + 2]) * 128 + lane * 4; }\n";
+           "          " + r0 + " = (" + s0 + " & ~127LL) + (" + c + " - P.seg[3 * lo + 2]) * 128 + " + lane_term + "; }\n";
 }
 
 void chunk_loop_open(std::ostringstream& os, const Plan& p, const Table* t, const std::set<int>& cols) {
@@ -1764,6 +1771,9 @@ void emit_async_issue_fn(std::ostringstream& os, const Table* t, const std::set<
     os << "}\n";
 }
 
+// Lanes read the staged chunk strided: lane l takes rows l, l+32, l+64, l+96,
+// each read from shared memory where it is used (consecutive lanes, consecutive
+// words: no bank conflicts), so no register holds a row before its turn.
 void async_loop_open(std::ostringstream& os, const Table* t, const std::set<int>& cols, const AsyncLayout& L, int stages,
                      const std::string& issue) {
     os << "    extern __shared__ __align__(16) unsigned char vq_abuf[];\n";
@@ -1784,20 +1794,19 @@ void async_loop_open(std::ostringstream& os, const Table* t, const std::set<int>
     os << "        vq_cp_wait<" << stages - 1 << ">();\n";
     os << "        __syncwarp();\n";
     os << "        const unsigned char* st = wb + (int)(it % " << stages << ") * " << L.chunk_bytes << ";\n";
-    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0", "lane");
     for (int c : cols) {
         const Column& col = t->cols[c];
         std::string C = std::to_string(c);
         const char* ty = "unsigned";
-        const char* fn = "vq_sld4_u32";
         switch (col.type) {
-            case VEXQ_TYPE_INT64: ty = "long long"; fn = "vq_sld4_i64"; break;
-            case VEXQ_TYPE_FLOAT64: ty = "double"; fn = "vq_sld4_f64"; break;
-            case VEXQ_TYPE_DATE: ty = "int"; fn = "vq_sld4_i32"; break;
-            case VEXQ_TYPE_BOOL: ty = "unsigned"; fn = "vq_sld4_u8"; break;
+            case VEXQ_TYPE_INT64: ty = "long long"; break;
+            case VEXQ_TYPE_FLOAT64: ty = "double"; break;
+            case VEXQ_TYPE_DATE: ty = "int"; break;
+            case VEXQ_TYPE_BOOL: ty = "unsigned char"; break;
         }
-        os << "        " << ty << " cv" << C << "[4]; " << fn << "(st + " << L.off.at(c) << ", lane * 4, cv" << C << ");\n";
-        if (col.nullable) os << "        const unsigned cm" << C << " = vq_sbits4(st + " << L.voff.at(c) << ", lane * 4);\n";
+        os << "        const " << ty << "* const cv" << C << " = (const " << ty << "*)(st + " << L.off.at(c) << ") + lane;\n";
+        if (col.nullable) os << "        const unsigned cm" << C << " = vq_sbits4_strided(st + " << L.voff.at(c) << ", lane);\n";
     }
 }
 
@@ -1831,6 +1840,8 @@ struct ScanLoop {
         }
     }
     int tile_rows() const { return staged ? L.T : 128; }
+    // lane l holds rows l + 32k of a chunk (the cp.async pipeline) rather than 4l + k
+    bool strided() const { return !staged && async_n > 0; }
     int smem() const { return staged ? L.S * L.stage_bytes : async_n ? warps * async_n * A.chunk_bytes : 0; }
     void prologue(std::ostringstream& os) const {
         if (staged) emit_issue_fn(os, t, cols, L, issue);
@@ -1853,13 +1864,15 @@ struct ScanLoop {
 static std::string gen_kind_tables(const Plan& p, const std::string& prefix = "P_");
 
 // The four rows a lane holds in the current chunk: filter, project, aggregate.
-static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool cache) {
+static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool cache,
+                          bool strided = false) {
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
-    os << "            const long long r = r0 + k;\n";
+    os << "            const long long r = r0 + " << (strided ? "(k << 5)" : "k") << ";\n";
     bool warp_sync = p.path != AggPath::Regs;  // atomic paths aggregate across the warp
     if (warp_sync) os << "            bool live = r >= s0 && r < s1;\n";
     else os << "            if (r < s0 || r >= s1) continue;\n";
     Gen g(p, os);
+    if (strided) g.kidx = "(k << 5)";
     if (p.pred >= 0) {
         g.emit(p.pred);
         if (warp_sync) os << "            live = live && x" << p.pred << " && ok" << p.pred << ";\n";
@@ -1895,7 +1908,7 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     if (p.smem_groups > 0) emit_cache_init(os, p);
     loop.open(os);
-    emit_agg_rows(os, p, key_nodes, p.smem_groups > 0);
+    emit_agg_rows(os, p, key_nodes, p.smem_groups > 0, loop.strided());
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     if (p.smem_groups > 0) emit_cache_flush(os, p);

@@ -415,6 +415,12 @@ __device__ __forceinline__ void vq_sld4_u32(const unsigned char* s, int o, unsig
     uint4 a = reinterpret_cast<const uint4*>(s)[o >> 2];
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
 }
+// Validity of rows lane, lane+32, lane+64, lane+96 of a staged 128-row chunk
+// (LSB-first bitmap: word k holds rows 32k..32k+31), as bits 0..3.
+__device__ __forceinline__ unsigned vq_sbits4_strided(const unsigned char* s, int lane) {
+    const uint4 w = *reinterpret_cast<const uint4*>(s);
+    return ((w.x >> lane) & 1u) | (((w.y >> lane) & 1u) << 1) | (((w.z >> lane) & 1u) << 2) | (((w.w >> lane) & 1u) << 3);
+}
 __device__ __forceinline__ void vq_sld4_u8(const unsigned char* s, int o, unsigned* v) {
     unsigned w = reinterpret_cast<const unsigned*>(s)[o >> 2];
     v[0] = w & 0xFF; v[1] = (w >> 8) & 0xFF; v[2] = (w >> 16) & 0xFF; v[3] = w >> 24;

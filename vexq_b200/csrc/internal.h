@@ -103,6 +103,7 @@ struct Table {
     // NaN/±inf): plans compiled against the earlier ranges refuse to run
     uint64_t range_epoch = 0;
     bool zones_ready = false;
+    uint64_t zone_version = 0;  // bumped every time the zone maps are recomputed
     int64_t rg_start(int rg) const { return (int64_t)rg * rg_rows; }
     int64_t rg_end(int rg) const { return std::min<int64_t>(nrows, (int64_t)(rg + 1) * rg_rows); }
     int64_t device_bytes() const;

@@ -173,7 +173,7 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
         P.part_i = part_i;
         P.error = d_err;
         jit_launch(k, grid, &P, sizeof P, s);
-        k_merge_regs<<<nf + ni + 1, 256, 0, s>>>(part_f, part_i, grid, 1, nf, ni, d_kinds, d_kinds + nfb, out_f, out_i);
+        k_merge_regs<<<(nf + ni + 1 + 7) / 8, 256, 0, s>>>(part_f, part_i, grid, 1, nf, ni, d_kinds, d_kinds + nfb, out_f, out_i);
         VQ_CUDA(cudaGetLastError());
         VQ_CUDA(cudaMemcpyAsync(stage, d_out, merged + 4, cudaMemcpyDeviceToHost, s));
         VQ_CUDA(cudaStreamSynchronize(s));

@@ -81,6 +81,15 @@ struct ScanSegs {
     long long rows = 0;
 };
 
+// Zone-map pruning and segment list of one row-group range of a table, kept
+// by a plan while the table's zone maps are unchanged.
+struct ScanMemo {
+    int rgs = -1, rge = -1;
+    uint64_t zone_version = ~0ull;
+    ScanSegs ss;
+    int64_t bytes = 0;  // algorithmic bytes the scan of those segments reads
+};
+
 struct Plan {
     bool is_join = false;
     Table* t = nullptr;        // aggregate table or probe table
@@ -147,6 +156,8 @@ struct Plan {
     DevBuf d_bseg;
     DevBuf d_kinds;                        // register-path combiner kinds
     PinnedBuf h_stage;                     // pinned staging for small results
+    bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
+    ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)

@@ -7,6 +7,7 @@
 // global aggregate over no rows emits one row (aggregate.go:961-982), and
 // ExternalSort's comparison on raw int64 bits with NULLs first
 // (exec/sort.go:130-163) followed by Limit (exec/limit.go:20-50).
+#include <cstdlib>
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -38,69 +39,95 @@ __device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
     hi = s;
 }
 
-// One merged output entry of the register path: a fixed-order TwoSum tree
-// over the per-block partials (floats) or a min/max/sum fold (ints).
+// One merged output entry of the register path, computed by one warp: lane l
+// folds partials l, l+32, l+64, ... in that order (a compensated TwoSum pair
+// for float sums, min/max/wrapping sum otherwise), then a fixed shuffle tree
+// combines the lanes, so the result does not depend on scheduling. Loads are
+// issued eight at a time ahead of their folds.
 __device__ void merge_entry(int e, const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
                             const int* fkind, const int* ikind, double* out_f, long long* out_i) {
-    __shared__ double sh[256], sl[256];
-    __shared__ long long si[256];
-    const int t = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     const int totf = G * nf, toti = G * (ni + 1);
     if (e < totf) {
         const int kind = fkind[e % nf];
         double hi = kind == 1 ? 1.7976931348623157e308 : kind == 2 ? -1.7976931348623157e308 : 0.0, lo = 0.0;
-        for (int b = t; b < nblocks; b += blockDim.x) {
-            const double x = part_f[(long long)b * totf + e];
-            if (kind == 0) vq_two_sum(hi, lo, x);
-            else hi = vq_fcomb(kind, hi, x);
-        }
-        sh[t] = hi;
-        sl[t] = lo;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (t < o) {
-                if (kind == 0) {
-                    double h = sh[t], l = sl[t] + sl[t + o];
-                    vq_two_sum(h, l, sh[t + o]);
-                    sh[t] = h;
-                    sl[t] = l;
-                } else {
-                    sh[t] = vq_fcomb(kind, sh[t], sh[t + o]);
-                }
+        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
+            double x[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_f[(long long)(b0 + 32 * j) * totf + e] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (b0 + 32 * j >= nblocks) break;
+                if (kind == 0) vq_two_sum(hi, lo, x[j]);
+                else hi = vq_fcomb(kind, hi, x[j]);
             }
-            __syncthreads();
         }
-        if (t == 0) out_f[e] = kind == 0 ? sh[0] + sl[0] : sh[0];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double h2 = __shfl_down_sync(0xffffffffu, hi, o), l2 = __shfl_down_sync(0xffffffffu, lo, o);
+            if (kind == 0) {
+                double h = hi, l = lo + l2;
+                vq_two_sum(h, l, h2);
+                hi = h;
+                lo = l;
+            } else {
+                hi = vq_fcomb(kind, hi, h2);
+            }
+        }
+        if (lane == 0) out_f[e] = kind == 0 ? hi + lo : hi;
     } else if (e < totf + toti) {
         const int u = e - totf;
         const int kind = ikind[u % (ni + 1)];
         long long v = kind == 1 ? 0x7FFFFFFFFFFFFFFFLL : kind == 2 ? (-0x7FFFFFFFFFFFFFFFLL - 1) : 0LL;
-        for (int b = t; b < nblocks; b += blockDim.x) v = vq_icomb(kind, v, part_i[(long long)b * toti + u]);
-        si[t] = v;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (t < o) si[t] = vq_icomb(kind, si[t], si[t + o]);
-            __syncthreads();
+        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
+            long long x[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_i[(long long)(b0 + 32 * j) * toti + u] : 0LL;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (b0 + 32 * j >= nblocks) break;
+                v = vq_icomb(kind, v, x[j]);
+            }
         }
-        if (t == 0) out_i[u] = si[0];
+        for (int o = 16; o > 0; o >>= 1) v = vq_icomb(kind, v, (long long)__shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) out_i[u] = v;
     }
 }
+
+// Entry of the calling warp: eight warps (256 threads) a block.
+__device__ __forceinline__ int merge_warp() { return (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5); }
 
 __global__ void __launch_bounds__(256) k_merge_regs(const double* part_f, const long long* part_i, int nblocks, int G,
                                                     int nf, int ni, const int* fkind, const int* ikind, double* out_f,
                                                     long long* out_i) {
-    merge_entry(blockIdx.x, part_f, part_i, nblocks, G, nf, ni, fkind, ikind, out_f, out_i);
+    merge_entry(merge_warp(), part_f, part_i, nblocks, G, nf, ni, fkind, ikind, out_f, out_i);
 }
 
-// Batched merge: block b serves entry b - e0 of the plan whose range holds b.
+// The same merge launched as a programmatic dependent of the scan kernel: its
+// blocks start while the scan drains and wait (griddepcontrol.wait) until the
+// scan grid has finished and its writes are visible. Warp 0 also hands the
+// scan's error word out with the results and clears it for the next run, so
+// no memset precedes the scan.
+__global__ void __launch_bounds__(256) k_merge_regs_dep(const double* part_f, const long long* part_i, int nblocks, int G,
+                                                        int nf, int ni, const int* fkind, const int* ikind, double* out_f,
+                                                        long long* out_i, int* err, int* err_out) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    merge_entry(merge_warp(), part_f, part_i, nblocks, G, nf, ni, fkind, ikind, out_f, out_i);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *err_out = *err;
+        *err = 0;
+    }
+}
+
+// Batched merge: global warp w serves entry w - e0 of the plan whose range holds w.
 __global__ void __launch_bounds__(256) k_merge_batch(const VQMergeDesc* d, int n) {
+    const int w = merge_warp();
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (d[mid].e0 <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        if (d[mid].e0 <= w) lo = mid; else hi = mid - 1;
     }
     const VQMergeDesc m = d[lo];
-    merge_entry((int)blockIdx.x - m.e0, m.part_f, m.part_i, m.nblocks, m.G, m.nf, m.ni, m.fkind, m.ikind, m.out_f, m.out_i);
+    merge_entry(w - m.e0, m.part_f, m.part_i, m.nblocks, m.G, m.nf, m.ni, m.fkind, m.ikind, m.out_f, m.out_i);
 }
 
 // Atomic path: per-slot initial values (counts 0, MIN/MAX identities).
@@ -501,28 +528,48 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     }
     const int* d_kinds = p.d_kinds.as<int>();
     size_t nout_f = (size_t)G * nfb * 8, nout_i = (size_t)G * (ni + 1) * 8;
+    // layout: merged floats, merged ints, the error word handed out (copied
+    // back with the results), then the error word the kernels raise
+    const size_t before = p.scratch_c.n;
     p.scratch_c.ensure(nout_f + nout_i + 16);
+    if (p.scratch_c.n != before) p.regs_err_clean = false;
     double* out_f = p.scratch_c.as<double>();
     long long* out_i = (long long*)((char*)p.scratch_c.p + nout_f);
-    P.error = (int*)((char*)p.scratch_c.p + nout_f + nout_i);
+    int* err_out = (int*)((char*)p.scratch_c.p + nout_f + nout_i);
+    P.error = err_out + 2;
     p.h_stage.ensure(nout_f + nout_i + 16);
     ensure_events(p);
-    VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
+    if (!p.regs_err_clean) VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
+    p.regs_err_clean = false;  // until the merge below has run
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(K, grid, &P, sizeof P, rc.s);
     launch_check(rc.s, "p.k_main");
-    VQ_CUDA(cudaEventRecord(p.ev[1], rc.s));
-    int tot = G * nf + G * (ni + 1);
-    k_merge_regs<<<tot, 256, 0, rc.s>>>(P.part_f, P.part_i, grid, G, nf, ni, d_kinds, d_kinds + nfb, out_f, out_i);
-    launch_check(rc.s, "k_merge_regs");
-    VQ_CUDA(cudaGetLastError());
+    // no event between the scan and its merge: an event record there stops the
+    // merge's launch from overlapping the scan's drain (measured 5-6 us a run)
+    {
+        const int tot = G * nf + G * (ni + 1);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((tot + 7) / 8);
+        cfg.blockDim = dim3(256);
+        cfg.stream = rc.s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        VQ_CUDA(cudaLaunchKernelEx(&cfg, k_merge_regs_dep, (const double*)P.part_f, (const long long*)P.part_i, grid, G, nf,
+                                   ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
+    }
+    launch_check(rc.s, "k_merge_regs_dep");
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
     VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
+    p.regs_err_clean = true;
     if (*(const int*)((const char*)p.h_stage.p + nout_f + nout_i) & 8)
         fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
-    rc.scan_ms += elapsed(p.ev[0], p.ev[1]);
-    rc.kernel_ms += elapsed(p.ev[0], p.ev[2]);
+    const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge overlapping its drain
+    rc.scan_ms += span;
+    rc.kernel_ms += span;
     rc.launches += 2;
     const double* hf = (const double*)p.h_stage.p;
     const long long* hi = (const long long*)((const char*)p.h_stage.p + nout_f);
@@ -1227,8 +1274,16 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             return r;
         }
     }
-    std::vector<uint8_t> m = prune_mask(p, t, p.zn_pred, rgs, rge);
-    ScanSegs ss = make_segments(t, m, rgs, rge, p.tile);
+    ScanMemo& sm = p.scan_memo;
+    if (sm.rgs != rgs || sm.rge != rge || sm.zone_version != t.zone_version) {
+        std::vector<uint8_t> m = prune_mask(p, t, p.zn_pred, rgs, rge);
+        sm.ss = make_segments(t, m, rgs, rge, p.tile);
+        sm.bytes = scanned_bytes(p, t, sm.ss.rows, false);
+        sm.rgs = rgs;
+        sm.rge = rge;
+        sm.zone_version = t.zone_version;
+    }
+    const ScanSegs& ss = sm.ss;
     set_columns(P, t, false);
     if (ss.seg != p.seg_cache || !p.d_seg.p) {  // segment list uploaded once per distinct pruning
         p.d_seg.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
@@ -1243,7 +1298,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     P.present = p.d_present.as<unsigned char>();
     for (size_t i = 0, off = 0; i < p.sets.size(); i++) { P.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
 
-    bytes += scanned_bytes(p, t, ss.rows, false);
+    bytes += sm.bytes;
     rows_scanned += ss.rows;
     if (use_radix && ss.nchunks > 0) {
         // probe side: the same partitions, then one block per partition joins

@@ -235,6 +235,7 @@ void fill_column(Table& t, int ci, const vexq_column_desc& d, cudaStream_t s, De
 }
 
 void compute_zones(Table& t, cudaStream_t s) {
+    t.zone_version++;
     if (t.n_rg == 0) return;
     DevBuf z(sizeof(vexq_zone_map) * t.n_rg * t.cols.size());
     for (size_t ci = 0; ci < t.cols.size(); ci++) {
