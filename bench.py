@@ -41,8 +41,12 @@ def parse():
     ap.add_argument("--impl", default="vexq", choices=["vexq", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--profile", action="store_true",
-                    help="profiling driver: three Q1 and three Q6 runs on the 6M-row table, no timing")
+    ap.add_argument("--profile", nargs="?", const="lineitem", default=None,
+                    choices=["lineitem", "groupby", "join", "radix", "batch", "filter"],
+                    help="profiling driver, no timing: a short fixed launch sequence of one workload for ncu "
+                         "(lineitem: 3 x Q1 and 3 x Q6 over 6M rows; groupby: dense and hash GROUP BY over 4M "
+                         "rows; join: Q3/Q12 global-table joins; radix: the same partitioned; batch: 64 plans "
+                         "batched; filter: selection bitmaps)")
     ap.add_argument("--workload", default="lineitem", choices=["lineitem", "batch", "serve"],
                     help="lineitem: Q1+Q6 step (default); batch: 256 Zipf GROUP BYs, batched vs one by one; "
                          "serve: Poisson arrivals of a Q1/Q6/Q3 mix over resident tables, p50/p99")
@@ -218,17 +222,62 @@ def batch_workload(args):
     print(json.dumps(line), flush=True)
 
 
-def profile_driver():
-    """Small fixed launch sequence for ncu: upload, 3 × Q1, 3 × Q6."""
-    from vexq_b200 import build, datagen as D, exec as X, workloads as W
+def profile_driver(kind="lineitem"):
+    """Small fixed launch sequence for ncu (no timing): tables uploaded once,
+    then a few runs of each plan of the chosen workload."""
+    import numpy as np
+
+    from vexq_b200 import build, datagen as D, exec as X, plan as P, workloads as W
+    from vexq_b200.table import HostTable, float_column, int_column
     build.build()
     X.init(0)
-    gt = X.GpuTable(D.lineitem(NROWS, seed=43, rg_rows=RG_ROWS))
-    for mk in (W.q1_plan, W.q6_plan):
-        op = X.GpuHashAggregate(gt, mk())
-        for _ in range(3):
+
+    def runs(op, n):
+        for _ in range(n):
             op.run().close()
         print(op.explain(), flush=True)
+        op.close()
+
+    if kind == "lineitem":
+        gt = X.GpuTable(D.lineitem(NROWS, seed=43, rg_rows=RG_ROWS))
+        for mk in (W.q1_plan, W.q6_plan):
+            runs(X.GpuHashAggregate(gt, mk()), 3)
+    elif kind == "groupby":
+        # dense table over 65,536 and 1,000 Zipf(1.1) groups, then a hash table
+        # over 200,000 distinct int64 keys (4M rows each)
+        for card in (65536, 1000):
+            runs(X.GpuHashAggregate(X.GpuTable(D.zipf_groups(4_000_000, card, seed=7)), W.batch_plan()), 3)
+        rng = np.random.default_rng(3)
+        keys = rng.integers(0, 1 << 40, 200_000)[rng.integers(0, 200_000, 4_000_000)]
+        vals = np.rint(rng.uniform(0, 1e7, 4_000_000)) / 100.0
+        ht = HostTable([int_column("k", keys), float_column("v", vals)], 4_000_000, 65536)
+        runs(X.GpuHashAggregate(X.GpuTable(ht), W.batch_plan()), 3)
+    elif kind in ("join", "radix"):
+        go, gi = X.GpuTable(D.orders(1_500_000, seed=5)), X.GpuTable(D.items(6_000_000, 1_500_000, seed=6))
+        bits = 8 if kind == "radix" else 0
+        runs(X.GpuParallelHashJoinAggregate(go, gi, W.q3_plan(radix_bits=bits)), 2)
+        runs(X.GpuParallelHashJoinAggregate(go, gi, W.q12_plan(radix_bits=bits)), 2)
+    elif kind == "batch":
+        rng = np.random.default_rng(2024)
+        ops = []
+        for i in range(64):
+            rows = int(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
+            card = int(round(np.exp(rng.uniform(np.log(2), np.log(65536)))))
+            ops.append(X.GpuHashAggregate(X.GpuTable(D.zipf_groups(rows, card, seed=i)), W.batch_plan()))
+        b = X.GpuBatch(ops)
+        for _ in range(2):
+            for r in b.exec():
+                r.close()
+        print(b.explain(), flush=True)
+        b.close()
+        for op in ops:
+            op.close()
+    elif kind == "filter":
+        gt = X.GpuTable(D.lineitem(NROWS, seed=43, rg_rows=RG_ROWS))
+        for pred in (W.q6_plan().predicate, W.q1_plan().predicate):
+            f = X.GpuFilter(gt, pred)
+            for _ in range(3):
+                f.bitmap()
 
 
 def measured_peaks():
@@ -349,7 +398,7 @@ def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.profile:
-        profile_driver()
+        profile_driver(args.profile)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

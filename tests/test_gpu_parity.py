@@ -290,3 +290,21 @@ def test_batch_and_server_equal_single_runs(gpu_lib, lineitem_1m):
         abi.check(L.vexq_server_wait(srv, tk, 60000, C.byref(h)))
         assert_rows_match(X.Result(h).rows(), single[k % 2], ordered=True, rtol=1e-13)
     abi.check(L.vexq_server_stop(srv))
+
+
+@pytest.mark.parametrize("lo,hi", [(0, -1), (5, -1), (1237, 40001), (8, 16), (3, 4), (777, 777), (49_999, 50_000)])
+def test_filter_row_subranges(gpu_lib, lo, hi):
+    """Bitmaps of row sub-ranges at every bit offset: bit i of the output is
+    row lo + i, and bits past the range stay clear."""
+    t = nullable_table(50_000, seed=6)
+    X = gpu_lib
+    pred = EXPRS[0][0]
+    rbits, _ = R.filter_bits(R.RefTable(t), pred)
+    allrows = np.unpackbits(np.frombuffer(rbits, np.uint8), bitorder="little", count=t.nrows)
+    end = t.nrows if hi < 0 else hi
+    bits, cnt = X.GpuFilter(X.GpuTable(t), pred).bitmap(lo, hi)
+    n = end - lo
+    got = np.unpackbits(np.frombuffer(bits, np.uint8), bitorder="little")
+    assert np.array_equal(got[:n], allrows[lo:end])
+    assert not got[n:].any()
+    assert cnt == int(allrows[lo:end].sum())

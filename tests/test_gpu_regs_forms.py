@@ -128,3 +128,35 @@ def test_refill_outside_compiled_range_is_refused(gpu_lib):
     finally:
         op.close()
         other.close()
+
+
+def test_hash_table_sized_from_the_last_run(gpu_lib):
+    """The hash path sizes a rerun's table from the groups the last run
+    found. A first run over one row group (100 keys) then a run over the
+    whole table (about 100,000 keys): the small table hits its probe limit,
+    the rerun takes the row-bounded size, and results match the oracle; a
+    third run reuses the right size."""
+    X = gpu_lib
+    rg, nrg = 65536, 5
+    n = rg * nrg
+    rng = np.random.default_rng(11)
+    keys = rng.integers(0, 1 << 40, 100_000)[rng.integers(0, 100_000, n)]
+    keys[:rg] = rng.integers(0, 1 << 40, 100)[rng.integers(0, 100, rg)]
+    vals = np.rint(rng.uniform(0, 1e7, n)) / 100.0
+    host = HostTable([int_column("k", keys), float_column("v", vals)], n, rg)
+    plan = P.AggPlan(None, [0], [P.sum_(P.col(1), "s"), P.count_star("n"), P.max_(P.col(1), "m")])
+    op = X.GpuHashAggregate(X.GpuTable(host), plan)
+    try:
+        assert "path=hash" in op.explain()
+        first = op.run(0, 1)
+        first.collect()
+        sub = HostTable([int_column("k", keys[:rg]), float_column("v", vals[:rg])], rg, rg)
+        assert_rows_match(first.rows(), R.agg(R.RefTable(sub), plan, workers=0).rows(), ordered=True)
+        ref = R.agg(R.RefTable(host), plan, workers=0)
+        for _ in range(2):
+            g = op.run()
+            g.collect()
+            assert_rows_match(g.rows(), ref.rows(), ordered=True)
+            assert_float_vs_exact(g.rows(), ref)
+    finally:
+        op.close()

@@ -280,12 +280,18 @@ int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes, 
         VQ_CUDA(cudaStreamSynchronize(s));
         unsigned long long cnt = sc[0];
         if ((int)(sc[2] & 0xFFFFFFFF) & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+        // the device words are LSB-first, so byte k of the (little-endian)
+        // word array holds rows 8k..8k+7: shift bytes by row_start's bit offset
         int64_t n = row_end - row_start;
-        std::memset(out_bits, 0, (size_t)(n + 7) / 8);
-        for (int64_t i = 0; i < n; i++) {
-            int64_t r = row_start + i;
-            if ((h[r >> 5] >> (r & 31)) & 1) out_bits[i >> 3] |= (uint8_t)(1u << (i & 7));
+        const uint8_t* hb = (const uint8_t*)h.data();
+        const int64_t b0 = row_start >> 3, nb = (n + 7) / 8;
+        const int sh = (int)(row_start & 7);
+        for (int64_t i = 0; i < nb; i++) {
+            unsigned v = (unsigned)hb[b0 + i] >> sh;
+            if (sh) v |= (unsigned)hb[b0 + i + 1] << (8 - sh);  // the word array has 8 words of padding
+            out_bits[i] = (uint8_t)v;
         }
+        if (n & 7) out_bits[nb - 1] &= (uint8_t)((1u << (n & 7)) - 1u);
         *count = (int64_t)cnt;
         return VEXQ_OK;
     });

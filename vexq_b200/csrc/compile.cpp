@@ -2733,6 +2733,10 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
             p->sets.push_back(std::move(bits));
         }
     }
+    // the register chunk loop: the TMA stage ring (160 KB a block) would
+    // leave one block per SM for a kernel that holds almost no state
+    p->staged = false;
+    p->pipeline = false;
     std::ostringstream os;
     std::set<int> cols;
     collect_cols(*p, p->pred, cols);
@@ -2742,6 +2746,9 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     os << prelude_source() << "\n";
     loop.prologue(os);
     os << kernel_head("vq_filter", kBlock);
+    // selected rows are counted in a register and added once per warp (one
+    // global counter taking an atomic per bitmap word serialises the kernel)
+    os << "    unsigned long long vq_cnt = 0ull;\n";
     loop.open(os);
     os << "        unsigned nib = 0u;\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
@@ -2758,9 +2765,11 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     os << "        if ((lane & 7) == 0 && word) {\n";
     os << "            const long long wi = (r0 - lane * 4) / 32 + (lane >> 3);\n";
     os << "            atomicOr(reinterpret_cast<unsigned*>(P.acc_i) + wi, word);\n";
-    os << "            atomicAdd(P.ngroups, (unsigned long long)__popc(word));\n";
+    os << "            vq_cnt += (unsigned long long)__popc(word);\n";
     os << "        }\n";
     loop.close(os);
+    os << "    for (int o = 16; o > 0; o >>= 1) vq_cnt += __shfl_xor_sync(0xffffffffu, vq_cnt, o);\n";
+    os << "    if ((threadIdx.x & 31) == 0 && vq_cnt) atomicAdd(P.ngroups, vq_cnt);\n";
     os << "}\n";
     p->src_main = os.str();
     p->k_main = jit_get(p->src_main, "vq_filter", kBlock, p->smem);

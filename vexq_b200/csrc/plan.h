@@ -158,6 +158,8 @@ struct Plan {
     PinnedBuf h_stage;                     // pinned staging for small results
     bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
     ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
+    long long hash_groups_seen = -1;       // hash path: groups the last run found (sizes the next table)
+    long long hash_rows_seen = 0;          //   and the rows that run scanned
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)

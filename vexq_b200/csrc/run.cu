@@ -597,11 +597,21 @@ struct Compacted {
     double* fval = nullptr;
 };
 
-Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate) {
+Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows) {
     Plan& p = rc.p;
     bool hash = p.path == AggPath::Hash;
-    long long cap;
+    long long cap, safe_cap = 16;
     if (hash) {
+        while (safe_cap < 2 * std::max<long long>(estimate, 8)) safe_cap <<= 1;
+        // a rerun sizes its table from the groups the last run found, scaled
+        // up by the rows scanned (the row-count bound is usually far above the
+        // distinct keys, and a table sized by rows leaves L2, sending every
+        // atomic to DRAM); if that is too small, the probe limit is hit and
+        // the rerun below takes the row-bounded size
+        if (p.hash_groups_seen >= 0) {
+            const double scale = std::max(1.0, (double)rows / (double)std::max<long long>(p.hash_rows_seen, 1));
+            estimate = std::min<long long>(estimate, std::max<long long>((long long)(p.hash_groups_seen * scale), 1024));
+        }
         cap = 16;
         while (cap < 2 * std::max<long long>(estimate, 8)) cap <<= 1;
     } else {
@@ -678,10 +688,14 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
         if (herr & 1) {  // probe limit: grow the table and rerun
             if (!hash) fail(VEXQ_EDEVICE, "dense group table reported a probe failure");
-            cap <<= 1;
+            cap = std::max(cap << 1, safe_cap);
             continue;
         }
         c.n = (long long)std::min<unsigned long long>(nn, (unsigned long long)cap_out);
+        if (hash) {
+            p.hash_groups_seen = c.n;
+            p.hash_rows_seen = rows;
+        }
         return c;
     }
     fail(VEXQ_ENOMEM, "group table could not be sized");
@@ -934,13 +948,13 @@ std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs
 
 // Runs the scan kernel over prepared params and returns host groups plus the
 // compacted device arrays (atomic path) for top-k.
-static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, long long estimate) {
+static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows) {
     Plan& p = rc.p;
     Groups g;
     if (p.path == AggPath::Regs) {
         g = run_regs(rc, P, nchunks);
     } else {
-        Compacted c = run_atomic(rc, P, nchunks, estimate);
+        Compacted c = run_atomic(rc, P, nchunks, estimate, rows);
         std::vector<long long> sel;
         if (topk_candidates(rc, c, sel)) g = fetch_groups(rc, c, &sel);
         else g = fetch_groups(rc, c, nullptr);
@@ -1335,7 +1349,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         r->launches = rc.launches;
     } else {
         long long est = estimate_groups(p, ss.rows, join_keys);
-        r = finish_groups(rc, P, ss.nchunks, est);
+        r = finish_groups(rc, P, ss.nchunks, est, ss.rows);
     }
     r->rows_scanned = rows_scanned;
     r->bytes_scanned = bytes;
