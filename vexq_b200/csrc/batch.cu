@@ -568,6 +568,7 @@ static void collect(Batch& b, vexq_result_s** out) {
                     for (int s = 0; s < it.ni; s++) g.ival[s].assign(oi + (size_t)s * it.cap_out, oi + (size_t)s * it.cap_out + m);
                     for (int s = 0; s < it.nf; s++) g.fval[s].assign(odf + (size_t)s * it.cap_out, odf + (size_t)s * it.cap_out + m);
                 }
+                if (it.cls == 1) note_hot_groups(p, g);
                 vexq_result_s* r = build_result(p, g);
                 r->kernel_ms = b.kernel_ms;
                 r->scan_ms = b.kernel_ms;

@@ -1363,8 +1363,8 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
             case S_FMIN: os << in << "if (ah" << S << " && ag" << S << " < *" << aiu << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
             case S_FMAX: os << in << "if (ah" << S << " && ag" << S << " > *" << aiu << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
             case S_FSUM:
-                os << in << "if (ah" << S << ") { vq_fx_add_digits<true>(" << L.fx << " + (" << pos << " * " << C
-                   << " + (long long)slot) * 4, fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
+                os << in << "if (ah" << S << ") { vq_fx_add_digits_s(" << L.fx << " + (long long)" << pos << " * 4 * " << C
+                   << " + (long long)slot, " << C << ", fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
                    << ") atomicOr(" << L.sp << " + " << pos << " * " << C << " + slot, fsp" << S << "); }\n";
                 break;
         }
@@ -1383,7 +1383,7 @@ void emit_cache_init(std::ostringstream& os, const Plan& p, bool declare_smem = 
         const Slot& sl = p.slots[s];
         if (sl.kind == S_FSUM) {
             std::string pos = std::to_string(p.slot_pos[s]);
-            os << "        for (int d = 0; d < 4; d++) " << L.fx << "[(" << pos << " * " << C << " + i) * 4 + d] = 0;\n";
+            os << "        for (int d = 0; d < 4; d++) " << L.fx << "[(" << pos << " * 4 + d) * " << C << " + i] = 0;\n";
             os << "        " << L.sp << "[" << pos << " * " << C << " + i] = 0u;\n";
             continue;
         }
@@ -1419,8 +1419,8 @@ void emit_cache_flush(std::ostringstream& os, const Plan& p) {
             case S_FMIN: os << "        atomicMin((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
             case S_FMAX: os << "        atomicMax((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
             case S_FSUM:
-                os << "        for (int d = 0; d < 4; d++) { const long long x = " << L.fx << "[(" << P_ << " * " << C
-                   << " + i) * 4 + d]; if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_ << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
+                os << "        for (int d = 0; d < 4; d++) { const long long x = " << L.fx << "[(" << P_ << " * 4 + d) * " << C
+                   << " + i]; if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_ << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
                 os << "        if (" << L.sp << "[" << P_ << " * " << C << " + i]) atomicOr(&P.special[" << P_ << " * stride + i], "
                    << L.sp << "[" << P_ << " * " << C << " + i]);\n";
                 break;
@@ -1436,6 +1436,38 @@ void emit_cache_flush(std::ostringstream& os, const Plan& p) {
 // keys, and float sums fold 128-bit fixed-point images of the values (the
 // same integers the single-row update would add). When no two lanes of the
 // warp share a group every lane updates its own row without reducing.
+// Whether the dense path's hot-group registers are generated.
+bool hot_on(const Plan& p) { return p.hot_n > 0 && p.path == AggPath::Dense && !p.is_join && !p.warp_agg; }
+
+// One group's update from values in scope (slot, stride, ag_first, ag<s>,
+// ah<s>, fd<s>_<k>, fsp<s>): the block's shared-memory cache when the slot is
+// cached, else the global table.
+void emit_lead_update(std::ostringstream& os, const Plan& p, const std::string& in3, bool cache) {
+    if (cache) emit_cache_update(os, p, in3);
+    os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        std::string S = std::to_string(s);
+        int pos = p.slot_pos[s];
+        std::string ai = "P.acc_i[" + std::to_string(pos) + " * stride + slot]";
+        std::string aiu = "(unsigned long long*)&" + ai;
+        switch (p.slots[s].kind) {
+            case S_CNT:
+            case S_NN: os << in3 << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_ISUM: os << in3 << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_IMIN: os << in3 << "if (ah" << S << ") atomicMin(&" << ai << ", ag" << S << ");\n"; break;
+            case S_IMAX: os << in3 << "if (ah" << S << ") atomicMax(&" << ai << ", ag" << S << ");\n"; break;
+            case S_FMIN: os << in3 << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FMAX: os << in3 << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
+            case S_FSUM:
+                os << in3 << "if (ah" << S << ") { vq_fx_add_digits<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, fd"
+                   << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S << ") atomicOr(P.special + (long long)" << pos
+                   << " * stride + slot, fsp" << S << "); }\n";
+                break;
+        }
+    }
+    if (cache) os << in3 << "}\n";  // closes the global branch opened by emit_cache_update
+}
+
 void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order,
                              bool cache) {
     const std::string in = ind + "    ";
@@ -1536,32 +1568,101 @@ void emit_atomic_update_warp(std::ostringstream& os, const Plan& p, const std::s
         }
     }
     os << in << "}\n";
-    os << in << "if (lead) {\n";
-    std::string in3 = in + "    ";
-    if (cache) emit_cache_update(os, p, in3);
-    os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
-    for (size_t s = 0; s < p.slots.size(); s++) {
-        std::string S = std::to_string(s);
-        int pos = p.slot_pos[s];
-        std::string ai = "P.acc_i[" + std::to_string(pos) + " * stride + slot]";
-        std::string aiu = "(unsigned long long*)&" + ai;
-        switch (p.slots[s].kind) {
-            case S_CNT:
-            case S_NN: os << in3 << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
-            case S_ISUM: os << in3 << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
-            case S_IMIN: os << in3 << "if (ah" << S << ") atomicMin(&" << ai << ", ag" << S << ");\n"; break;
-            case S_IMAX: os << in3 << "if (ah" << S << ") atomicMax(&" << ai << ", ag" << S << ");\n"; break;
-            case S_FMIN: os << in3 << "if (ah" << S << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
-            case S_FMAX: os << in3 << "if (ah" << S << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
-            case S_FSUM:
-                os << in3 << "if (ah" << S << ") { vq_fx_add_digits<true>(P.acc_fx + ((long long)" << pos << " * stride + (long long)slot) * 4, fd"
-                   << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S << ") atomicOr(P.special + (long long)" << pos
-                   << " * stride + slot, fsp" << S << "); }\n";
-                break;
+    if (hot_on(p)) {
+        // the plan's hottest groups accumulate in this thread's registers
+        os << in << "int vq_h = -1;\n";
+        for (int h = 0; h < p.hot_n; h++)
+            os << in << (h ? "else " : "") << "if (slot == P.hot[" << h << "]) vq_h = " << h << ";\n";
+        os << in << "if (vq_h >= 0) {\n";
+        os << in << "    switch (vq_h) {\n";
+        for (int h = 0; h < p.hot_n; h++) {
+            std::string H = std::to_string(h), i4 = in + "        ";
+            os << in << "    case " << h << ": {\n";
+            // a lane meets its rows in increasing order: its first row of the group holds the smallest order key
+            os << i4 << "if (!hs" << H << ") { hs" << H << " = true; hf" << H << " = ag_first; }\n";
+            for (size_t s = 0; s < p.slots.size(); s++) {
+                std::string S = std::to_string(s), v = "hv" + H + "_" + S, hh = "hh" + H + "_" + S;
+                switch (p.slots[s].kind) {
+                    case S_CNT: case S_NN: os << i4 << v << " += ag" << S << ";\n"; break;
+                    case S_ISUM:
+                        os << i4 << "if (ah" << S << ") { " << v << " = (long long)((unsigned long long)" << v << " + (unsigned long long)ag" << S
+                           << "); " << hh << " = true; }\n";
+                        break;
+                    case S_IMIN: case S_FMIN:
+                        os << i4 << "if (ah" << S << " && ag" << S << " < " << v << ") " << v << " = ag" << S << "; " << hh << " = " << hh << " || ah" << S << ";\n";
+                        break;
+                    case S_IMAX: case S_FMAX:
+                        os << i4 << "if (ah" << S << " && ag" << S << " > " << v << ") " << v << " = ag" << S << "; " << hh << " = " << hh << " || ah" << S << ";\n";
+                        break;
+                    case S_FSUM: {
+                        std::string d = "hd" + H + "_" + S + "_";
+                        os << i4 << "if (ah" << S << ") { " << d << "0 += fd" << S << "_0; " << d << "1 += fd" << S << "_1; " << d << "2 += fd" << S << "_2; "
+                           << d << "3 += fd" << S << "_3; hp" << H << "_" << S << " |= fsp" << S << "; " << hh << " = true; }\n";
+                        break;
+                    }
+                }
+            }
+            os << i4 << "break;\n" << in << "    }\n";
+        }
+        os << in << "    }\n" << in << "} else if (lead) {\n";
+    } else {
+        os << in << "if (lead) {\n";
+    }
+    emit_lead_update(os, p, in + "    ", cache);
+    os << in << "}\n" << ind << "}\n";
+}
+
+// The dense path's hot groups: register accumulators (declared at kernel or
+// body scope) and their flush into the cache or the table after the scan.
+void emit_hot_decl(std::ostringstream& os, const Plan& p) {
+    for (int h = 0; h < p.hot_n; h++) {
+        std::string H = std::to_string(h);
+        os << "    bool hs" << H << " = false; long long hf" << H << " = 0x7FFFFFFFFFFFFFFFLL;\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string S = std::to_string(s), v = "hv" + H + "_" + S, hh = "bool hh" + H + "_" + S + " = false;";
+            switch (p.slots[s].kind) {
+                case S_CNT: case S_NN: os << "    long long " << v << " = 0;\n"; break;
+                case S_ISUM: os << "    long long " << v << " = 0; " << hh << "\n"; break;
+                case S_IMIN: os << "    long long " << v << " = 0x7FFFFFFFFFFFFFFFLL; " << hh << "\n"; break;
+                case S_IMAX: os << "    long long " << v << " = (-0x7FFFFFFFFFFFFFFFLL - 1LL); " << hh << "\n"; break;
+                case S_FMIN: os << "    unsigned long long " << v << " = 0xFFFFFFFFFFFFFFFFull; " << hh << "\n"; break;
+                case S_FMAX: os << "    unsigned long long " << v << " = 0ull; " << hh << "\n"; break;
+                case S_FSUM: {
+                    std::string d = "hd" + H + "_" + S + "_";
+                    os << "    long long " << d << "0 = 0, " << d << "1 = 0, " << d << "2 = 0, " << d << "3 = 0; unsigned hp" << H << "_" << S
+                       << " = 0u; " << hh << "\n";
+                    break;
+                }
+            }
         }
     }
-    if (cache) os << in3 << "}\n";  // closes the global branch opened by emit_cache_update
-    os << in << "}\n" << ind << "}\n";
+}
+
+void emit_hot_flush(std::ostringstream& os, const Plan& p, bool cache) {
+    os << "    {\n        const long long stride = (long long)P.cap + 1;\n";
+    for (int h = 0; h < p.hot_n; h++) {
+        std::string H = std::to_string(h), in = "            ";
+        os << "        if (hs" << H << ") {\n";
+        os << in << "const unsigned long long slot = P.hot[" << h << "];\n";
+        os << in << "const long long ag_first = hf" << H << ";\n";
+        for (size_t s = 0; s < p.slots.size(); s++) {
+            std::string S = std::to_string(s), v = "hv" + H + "_" + S, hh = "hh" + H + "_" + S;
+            switch (p.slots[s].kind) {
+                case S_CNT: case S_NN: os << in << "const long long ag" << S << " = " << v << ";\n"; break;
+                case S_ISUM: case S_IMIN: case S_IMAX: os << in << "const long long ag" << S << " = " << v << "; const bool ah" << S << " = " << hh << ";\n"; break;
+                case S_FMIN: case S_FMAX: os << in << "const unsigned long long ag" << S << " = " << v << "; const bool ah" << S << " = " << hh << ";\n"; break;
+                case S_FSUM: {
+                    std::string d = "hd" + H + "_" + S + "_";
+                    os << in << "const long long fd" << S << "_0 = " << d << "0, fd" << S << "_1 = " << d << "1, fd" << S << "_2 = " << d << "2, fd" << S
+                       << "_3 = " << d << "3; const unsigned fsp" << S << " = hp" << H << "_" << S << "; const bool ah" << S << " = " << hh << ";\n";
+                    break;
+                }
+            }
+        }
+        emit_lead_update(os, p, in, cache);
+        os << "        }\n";
+    }
+    os << "    }\n";
 }
 
 std::string kernel_head(const std::string& name, int block, int min_blocks = 0) {
@@ -1907,10 +2008,12 @@ static std::string gen_agg_kernel(Plan& p, const std::vector<int>& key_nodes, in
     os << kernel_head("vq_agg", block, p.min_blocks);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     if (p.smem_groups > 0) emit_cache_init(os, p);
+    if (hot_on(p)) emit_hot_decl(os, p);
     loop.open(os);
     emit_agg_rows(os, p, key_nodes, p.smem_groups > 0, loop.strided());
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
+    if (hot_on(p)) emit_hot_flush(os, p, p.smem_groups > 0);
     if (p.smem_groups > 0) emit_cache_flush(os, p);
     os << "}\n";
     return os.str();
@@ -1932,6 +2035,7 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
        << "(const VQParams& P, const long long cbeg, const long long cend, const long long pslot, unsigned char* vq_smem) {\n";
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     if (cache) emit_cache_init(os, p, false);
+    if (hot_on(p)) emit_hot_decl(os, p);
     os << "    const int lane = threadIdx.x & 31;\n";
     os << "    for (long long c = cbeg + (threadIdx.x >> 5); c < cend; c += " << block / 32 << ") {\n";
     os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
@@ -1945,6 +2049,7 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
         fc.dyn_smem = true;
         emit_regs_flush(os, p, block, fc);
     }
+    if (hot_on(p)) emit_hot_flush(os, p, cache);
     if (cache) emit_cache_flush(os, p);
     os << "}\n";
     return os.str();
@@ -2378,6 +2483,11 @@ static void choose_tunables(Plan& p) {
     // measured on Zipf(1.1) keys: per-lane shared-memory atomics beat folding
     // the peers of a warp first (the fold serialises over distinct groups)
     p.warp_agg = false;
+    // dense path: the largest group of the last run accumulates in each
+    // thread's registers (measured on 4M Zipf(1.1) rows: one hot group 122 /
+    // 140 us at 1,000 / 65,536 groups, none 144 / 157, two 145 / 148 — more
+    // registers cost more occupancy than the atomics they save)
+    p.hot_n = (p.path == AggPath::Dense && !p.is_join) ? 1 : 0;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -2387,7 +2497,8 @@ static void choose_tunables(Plan& p) {
         };
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
-        int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb=");
+        int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb="), ho = get("hot=");
+        if (ho >= 0 && p.path == AggPath::Dense && !p.is_join) p.hot_n = std::min(ho, VQ_MAXHOT);
         if (as >= 0) p.async_stages = as;
         if (mb >= 0) p.min_blocks = mb;
         if (ck >= 0) cache_kb = ck;
@@ -2485,6 +2596,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
            : p.pipeline ? " pipeline=1" : " pipeline=0")
        << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
+    if (hot_on(p)) ex << " hot_groups=" << p.hot_n;
     if (p.path == AggPath::Regs && !join) {
         int nx = 0, nm = 0, na = 0;
         for (size_t s = 0; s < p.slots.size(); s++) {
@@ -2876,6 +2988,10 @@ void check_ranges(const Plan& p) {
 }
 
 void set_plan_constants(const Plan& p, VQParams& P) {
+    {
+        std::lock_guard<std::mutex> lk(p.hot_mu);
+        for (int h = 0; h < VQ_MAXHOT; h++) P.hot[h] = h < (int)p.hot_keys.size() ? p.hot_keys[h] : ~0ull;
+    }
     for (size_t i = 0; i < p.lits.size() && i < VQ_MAXLITS; i++) P.lit[i] = p.lits[i];
     for (size_t f = 0; f < p.fx_lsb.size() && f < 16; f++) P.fx_lsb[f] = p.fx_lsb[f];
     P.cache_n = p.smem_groups;

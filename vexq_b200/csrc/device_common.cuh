@@ -153,6 +153,16 @@ __device__ __forceinline__ void vq_fx_add_digits(vq_i64* c, vq_i64 d0, vq_i64 d1
     }
 }
 
+// The same with the four counters `stride` words apart: the shared-memory
+// group cache keeps digit d of every group contiguous, so the lanes of a warp
+// updating different groups spread over the banks.
+__device__ __forceinline__ void vq_fx_add_digits_s(vq_i64* c, long long stride, vq_i64 d0, vq_i64 d1, vq_i64 d2, vq_i64 d3) {
+    if (d0) atomicAdd(reinterpret_cast<unsigned long long*>(c), (unsigned long long)d0);
+    if (d1) atomicAdd(reinterpret_cast<unsigned long long*>(c + stride), (unsigned long long)d1);
+    if (d2) atomicAdd(reinterpret_cast<unsigned long long*>(c + 2 * stride), (unsigned long long)d2);
+    if (d3) atomicAdd(reinterpret_cast<unsigned long long*>(c + 3 * stride), (unsigned long long)d3);
+}
+
 // ---- warp reductions over a peer mask (redux.sync; every lane named in the
 // mask executes the same call with the same mask) ----
 __device__ __forceinline__ unsigned vq_redux_add(unsigned mask, unsigned v) {

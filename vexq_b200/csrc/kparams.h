@@ -7,6 +7,7 @@
 #define VQ_MAXSETS 16
 #define VQ_FX_DIGITS 4  // 32-bit digits of the exact fixed-point float sums
 #define VQ_MAXLITS 32   // numeric literals passed at launch (raw 8-byte images)
+#define VQ_MAXHOT 4     // dense path: hottest groups accumulated in registers
 #define VQ_RADIX_CAP 4096      // radix join: build entries of one partition held in shared memory
 #define VQ_RADIX_MAX_BITS 12   // radix join: at most 4,096 partitions
 
@@ -64,6 +65,7 @@ struct VQParams {
     unsigned long long cap_mask;   // atomic path: capacity - 1 (hash) or unused (dense)
     unsigned long long cap;        // slots (hash: power of two; dense: domain)
     unsigned long long jmask;      // join table capacity - 1
+    unsigned long long hot[VQ_MAXHOT];  // dense path: groups a thread accumulates in registers (~0 = none)
     // ---- 4-byte scalars ----
     int nseg;
     int n_rg;

@@ -159,6 +159,11 @@ struct Plan {
     bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
     ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
     long long hash_groups_seen = -1;       // hash path: groups the last run found (sizes the next table)
+    // dense path: the kernel accumulates hot_n groups per thread in registers;
+    // which groups is a launch value, the largest-count groups of the last run
+    int hot_n = 0;
+    std::vector<unsigned long long> hot_keys;
+    mutable std::mutex hot_mu;
     long long hash_rows_seen = 0;          //   and the rows that run scanned
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
@@ -216,6 +221,9 @@ struct Groups {
 };
 std::vector<long long> init_values(const Plan& p);
 vexq_result_s* build_result(Plan& p, Groups& g);
+// Dense path: the groups with the largest counts of a finished run become the
+// groups the next run accumulates in registers.
+void note_hot_groups(Plan& p, const Groups& g);
 int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build);
 long long estimate_groups(const Plan& p, long long rows, long long join_keys);
 void set_columns(VQParams& P, const Table& t, bool build_side);

@@ -959,11 +959,31 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
         if (topk_candidates(rc, c, sel)) g = fetch_groups(rc, c, &sel);
         else g = fetch_groups(rc, c, nullptr);
     }
+    note_hot_groups(p, g);
     vexq_result_s* r = build_result(p, g);
     r->kernel_ms = rc.kernel_ms;
     r->scan_ms = rc.scan_ms;
     r->launches = rc.launches;
     return r;
+}
+
+void note_hot_groups(Plan& p, const Groups& g) {
+    if (p.hot_n <= 0 || p.path != AggPath::Dense || p.is_join || g.key.empty()) return;
+    int cs = -1;
+    for (size_t s = 0; s < p.slots.size(); s++)
+        if (p.slots[s].kind == S_CNT) { cs = (int)s; break; }
+    if (cs < 0) return;
+    const std::vector<int64_t>& cnt = g.ival[p.slot_pos[cs]];
+    std::vector<size_t> idx(g.key.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    const size_t k = std::min<size_t>((size_t)p.hot_n, idx.size());
+    std::partial_sort(idx.begin(), idx.begin() + k, idx.end(), [&](size_t a, size_t b) {
+        return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : g.key[a] < g.key[b];
+    });
+    std::vector<unsigned long long> hot;
+    for (size_t i = 0; i < k; i++) hot.push_back((unsigned long long)g.key[idx[i]]);
+    std::lock_guard<std::mutex> lk(p.hot_mu);
+    p.hot_keys = hot;
 }
 
 int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build) {

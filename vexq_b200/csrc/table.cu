@@ -100,7 +100,11 @@ __global__ void k_remap(unsigned* codes, const unsigned char* valid, long long n
     }
 }
 
-// Per (row group, column) min / max / null count / sum.
+// Per (row group, column) min / max / null count / sum. A row group is split
+// into slices, one block each, so every SM works on the upload (one block per
+// row group left most of the GPU idle); the slices' partials are then combined
+// in slice order by one thread per row group, so the float sum does not depend
+// on scheduling.
 struct ZoneAcc {
     long long nulls;
     long long isum;
@@ -110,9 +114,50 @@ struct ZoneAcc {
     int has;
 };
 
+__device__ __forceinline__ void zone_comb(ZoneAcc& a, const ZoneAcc& b) {
+    a.nulls += b.nulls;
+    a.isum = (long long)((unsigned long long)a.isum + (unsigned long long)b.isum);
+    a.imin = min(a.imin, b.imin);
+    a.imax = max(a.imax, b.imax);
+    a.fsum += b.fsum;
+    a.fmin = fmin(a.fmin, b.fmin);
+    a.fmax = fmax(a.fmax, b.fmax);
+    a.has |= b.has;
+}
+
+__device__ __forceinline__ ZoneAcc zone_shfl(const ZoneAcc& a, int o) {
+    ZoneAcc b;
+    b.nulls = __shfl_down_sync(0xffffffffu, a.nulls, o);
+    b.isum = __shfl_down_sync(0xffffffffu, a.isum, o);
+    b.fsum = __shfl_down_sync(0xffffffffu, a.fsum, o);
+    b.imin = __shfl_down_sync(0xffffffffu, a.imin, o);
+    b.imax = __shfl_down_sync(0xffffffffu, a.imax, o);
+    b.fmin = __shfl_down_sync(0xffffffffu, a.fmin, o);
+    b.fmax = __shfl_down_sync(0xffffffffu, a.fmax, o);
+    b.has = __shfl_down_sync(0xffffffffu, a.has, o);
+    return b;
+}
+
+// Fixed-order block reduction (warp shuffle tree, then warps in order).
+__device__ void zone_block_reduce(ZoneAcc a, ZoneAcc* out) {
+    for (int o = 16; o > 0; o >>= 1) {
+        ZoneAcc b = zone_shfl(a, o);
+        zone_comb(a, b);
+    }
+    __shared__ ZoneAcc w[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) w[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ZoneAcc z = w[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) zone_comb(z, w[k]);
+        *out = z;
+    }
+}
+
 template <class T>
-__device__ void zone_block(const T* v, const unsigned char* valid, long long s, long long e, int type, vexq_zone_map* out) {
-    ZoneAcc a{0, 0, 0.0, 0x7FFFFFFFFFFFFFFFLL, (-0x7FFFFFFFFFFFFFFFLL - 1), 1.7976931348623157e308, -1.7976931348623157e308, 0};
+__device__ void zone_part(const T* v, const unsigned char* valid, long long s, long long e, int type, ZoneAcc* out) {
+    ZoneAcc a{0, 0, 0.0, 0x7FFFFFFFFFFFFFFFLL, (-0x7FFFFFFFFFFFFFFFLL - 1), 0.0, 0.0, 0};
     double fmn = __longlong_as_double(0x7FF0000000000000LL), fmx = -fmn;
     for (long long r = s + threadIdx.x; r < e; r += blockDim.x) {
         if (valid && !vq_bit(valid, r)) { a.nulls++; continue; }
@@ -120,79 +165,76 @@ __device__ void zone_block(const T* v, const unsigned char* valid, long long s, 
         if (type == VEXQ_TYPE_FLOAT64) {
             double d = (double)v[r];
             a.fsum += d;
-            if (d < fmn) fmn = d;
+            if (d < fmn) fmn = d;  // NaN never replaces a bound
             if (d > fmx) fmx = d;
-        } else {
+        } else if (type != VEXQ_TYPE_STRING && type != VEXQ_TYPE_BOOL) {
             long long x = (long long)v[r];
             a.isum = (long long)((unsigned long long)a.isum + (unsigned long long)x);
             a.imin = min(a.imin, x);
             a.imax = max(a.imax, x);
         }
     }
-    __shared__ long long s_n[256], s_s[256], s_mn[256], s_mx[256];
-    __shared__ double s_fs[256], s_fmn[256], s_fmx[256];
-    __shared__ int s_h[256];
-    int t = threadIdx.x;
-    s_n[t] = a.nulls; s_s[t] = a.isum; s_mn[t] = a.imin; s_mx[t] = a.imax;
-    s_fs[t] = a.fsum; s_fmn[t] = fmn; s_fmx[t] = fmx; s_h[t] = a.has;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (t < o) {
-            s_n[t] += s_n[t + o];
-            s_s[t] = (long long)((unsigned long long)s_s[t] + (unsigned long long)s_s[t + o]);
-            s_mn[t] = min(s_mn[t], s_mn[t + o]);
-            s_mx[t] = max(s_mx[t], s_mx[t + o]);
-            s_fs[t] += s_fs[t + o];
-            s_fmn[t] = fmin(s_fmn[t], s_fmn[t + o]);
-            s_fmx[t] = fmax(s_fmx[t], s_fmx[t + o]);
-            s_h[t] |= s_h[t + o];
-        }
-        __syncthreads();
-    }
-    if (t == 0) {
-        vexq_zone_map z{};
-        z.null_count = s_n[0];
-        z.has_min_max = s_h[0];
-        if (type == VEXQ_TYPE_FLOAT64) {
-            z.sum = __double_as_longlong(s_fs[0]);
-            if (z.has_min_max) {
-                z.min = (unsigned long long)__double_as_longlong(s_fmn[0]);
-                z.max = (unsigned long long)__double_as_longlong(s_fmx[0]);
-            }
-        } else if (type == VEXQ_TYPE_DATE) {  // zero-extended raw bits (writer.go:319)
-            if (z.has_min_max) {
-                z.min = (unsigned long long)(unsigned)(int)s_mn[0];
-                z.max = (unsigned long long)(unsigned)(int)s_mx[0];
-            }
-        } else {
-            z.sum = s_s[0];
-            if (z.has_min_max) { z.min = (unsigned long long)s_mn[0]; z.max = (unsigned long long)s_mx[0]; }
-        }
-        *out = z;
+    a.fmin = fmn;
+    a.fmax = fmx;
+    zone_block_reduce(a, out);
+}
+
+// Block (row group, slice): the slice's partial into part[rg * gridDim.y + slice].
+__global__ void k_zones_part(const void* values, const unsigned char* valid, int type, long long nrows, long long rg_rows,
+                             ZoneAcc* part) {
+    const int rg = blockIdx.x, sl = blockIdx.y, ns = gridDim.y;
+    const long long s = (long long)rg * rg_rows, e = min(nrows, s + rg_rows);
+    const long long len = (e - s + ns - 1) / ns;
+    const long long a = min(e, s + (long long)sl * len), b = min(e, a + len);
+    ZoneAcc* out = part + (long long)rg * ns + sl;
+    switch (type) {
+        case VEXQ_TYPE_INT64: zone_part((const long long*)values, valid, a, b, type, out); break;
+        case VEXQ_TYPE_FLOAT64: zone_part((const double*)values, valid, a, b, type, out); break;
+        case VEXQ_TYPE_DATE: zone_part((const int*)values, valid, a, b, type, out); break;
+        default: zone_part((const unsigned char*)values, valid, a, b, type, out); break;  // STRING / BOOL: null count
     }
 }
 
-__global__ void k_zones(const void* values, const unsigned char* valid, int type, long long nrows, long long rg_rows,
-                        vexq_zone_map* out) {
-    const int rg = blockIdx.x;
-    const long long s = (long long)rg * rg_rows, e = min(nrows, s + rg_rows);
-    switch (type) {
-        case VEXQ_TYPE_INT64: zone_block((const long long*)values, valid, s, e, type, out + rg); break;
-        case VEXQ_TYPE_FLOAT64: zone_block((const double*)values, valid, s, e, type, out + rg); break;
-        case VEXQ_TYPE_DATE: zone_block((const int*)values, valid, s, e, type, out + rg); break;
-        default: {  // STRING / BOOL: null count only
-            long long n = 0;
-            if (valid) for (long long r = s + threadIdx.x; r < e; r += blockDim.x) n += !vq_bit(valid, r);
-            __shared__ long long sn[256];
-            sn[threadIdx.x] = n;
-            __syncthreads();
-            for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-                if ((int)threadIdx.x < o) sn[threadIdx.x] += sn[threadIdx.x + o];
-                __syncthreads();
-            }
-            if (threadIdx.x == 0) { vexq_zone_map z{}; z.null_count = sn[0]; out[rg] = z; }
-        }
+// One warp per (column, row group): lane l folds slices l, l+32 in order, a
+// fixed shuffle tree combines the lanes → the zone map, with the writer's
+// rules for each type. All columns in one launch.
+__global__ void k_zones_fin(const ZoneAcc* part, int ns, int n_rg, int ncols, const int* types, vexq_zone_map* out) {
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (long long)n_rg * ncols) return;  // whole warps leave together
+    const int c = (int)(w / n_rg), rg = (int)(w % n_rg), type = types[c];
+    const ZoneAcc* pp = part + ((long long)c * n_rg + rg) * ns;
+    ZoneAcc a{0, 0, 0.0, 0x7FFFFFFFFFFFFFFFLL, (-0x7FFFFFFFFFFFFFFFLL - 1), __longlong_as_double(0x7FF0000000000000LL),
+              -__longlong_as_double(0x7FF0000000000000LL), 0};
+    for (int k = lane; k < ns; k += 32) zone_comb(a, pp[k]);
+    for (int o = 16; o > 0; o >>= 1) {
+        ZoneAcc b = zone_shfl(a, o);
+        zone_comb(a, b);
     }
+    if (lane != 0) return;
+    vexq_zone_map z{};
+    z.null_count = a.nulls;
+    if (type == VEXQ_TYPE_STRING || type == VEXQ_TYPE_BOOL) {  // null count only
+        out[w] = z;
+        return;
+    }
+    z.has_min_max = a.has;
+    if (type == VEXQ_TYPE_FLOAT64) {
+        z.sum = __double_as_longlong(a.fsum);
+        if (z.has_min_max) {
+            z.min = (unsigned long long)__double_as_longlong(a.fmin);
+            z.max = (unsigned long long)__double_as_longlong(a.fmax);
+        }
+    } else if (type == VEXQ_TYPE_DATE) {  // zero-extended raw bits (writer.go:319)
+        if (z.has_min_max) {
+            z.min = (unsigned long long)(unsigned)(int)a.imin;
+            z.max = (unsigned long long)(unsigned)(int)a.imax;
+        }
+    } else {
+        z.sum = a.isum;
+        if (z.has_min_max) { z.min = (unsigned long long)a.imin; z.max = (unsigned long long)a.imax; }
+    }
+    out[w] = z;
 }
 
 // ---- upload -------------------------------------------------------------------------
@@ -238,10 +280,26 @@ void compute_zones(Table& t, cudaStream_t s) {
     t.zone_version++;
     if (t.n_rg == 0) return;
     DevBuf z(sizeof(vexq_zone_map) * t.n_rg * t.cols.size());
-    for (size_t ci = 0; ci < t.cols.size(); ci++) {
+    // slices per row group: about eight blocks per SM over the table, each at
+    // least 8,192 rows
+    int ns = (int)std::max<long long>(1, std::min<long long>((long long)sm_count() * 8 / t.n_rg, ((long long)t.rg_rows + 8191) / 8192));
+    ns = std::min(ns, 64);
+    const int ncols = (int)t.cols.size();
+    DevBuf part(sizeof(ZoneAcc) * (size_t)t.n_rg * ns * ncols + 4 * (size_t)ncols + 16);
+    int* d_types = (int*)(part.as<char>() + sizeof(ZoneAcc) * (size_t)t.n_rg * ns * ncols);
+    std::vector<int> types(ncols);
+    for (int ci = 0; ci < ncols; ci++) {
         Column& c = t.cols[ci];
-        k_zones<<<t.n_rg, 256, 0, s>>>(c.values.p, c.nullable ? c.validity.as<unsigned char>() : nullptr, c.type, t.nrows,
-                                       t.rg_rows, z.as<vexq_zone_map>() + ci * t.n_rg);
+        types[ci] = c.type;
+        k_zones_part<<<dim3(t.n_rg, ns), 256, 0, s>>>(c.values.p, c.nullable ? c.validity.as<unsigned char>() : nullptr, c.type,
+                                                     t.nrows, t.rg_rows, part.as<ZoneAcc>() + (size_t)ci * t.n_rg * ns);
+        VQ_CUDA(cudaGetLastError());
+    }
+    if (ncols > 0) {
+        VQ_CUDA(cudaMemcpyAsync(d_types, types.data(), 4 * (size_t)ncols, cudaMemcpyHostToDevice, s));
+        const long long warps = (long long)t.n_rg * ncols;
+        k_zones_fin<<<(unsigned)((warps + 7) / 8), 256, 0, s>>>(part.as<ZoneAcc>(), ns, t.n_rg, ncols, d_types,
+                                                               z.as<vexq_zone_map>());
         VQ_CUDA(cudaGetLastError());
     }
     std::vector<vexq_zone_map> h(t.n_rg * t.cols.size());
