@@ -95,3 +95,41 @@ def test_join_known_answers_with_partitioning(gpu_lib, case):
         assert normalize(res.rows(), ordered) == normalize(case["expect"]["rows"], ordered)
     finally:
         op.close()
+
+
+def test_build_table_sized_from_the_last_build(gpu_lib):
+    """The build table is sized from the keys the plan's last build inserted.
+    The plan first runs with a build filter that keeps 500 rows; the build
+    table is then re-filled (through an aggregate plan's host-buffer run,
+    values inside the original ranges) so that every row passes: the small
+    table hits its probe limit and the build reruns at the row-bounded size."""
+    X = gpu_lib
+    rng = np.random.default_rng(21)
+    nb = 200_000
+    keys = rng.permutation(nb).astype(np.int64) + 1
+    d = np.full(nb, 9000, np.int32)
+    d[:500] = 8000  # only 500 build rows pass date < 8500
+    bt = HostTable([int_column("k", keys), date_column("d", d)], nb, 65536)
+    npr = 400_000
+    fk = rng.integers(1, nb + 1, npr).astype(np.int64)
+    val = np.rint(rng.uniform(0, 1e5, npr)) / 100.0
+    pt = HostTable([int_column("fk", fk), float_column("v", val)], npr, 65536)
+    plan = P.JoinPlan(0, 0, P.col(1) < P.lit("1993-04-10"), None, None, [], [P.count_star("n"), P.sum_(P.col(3), "s")])
+    gb, gp = X.GpuTable(bt), X.GpuTable(pt)
+    op = X.GpuParallelHashJoinAggregate(gb, gp, plan)
+    filler = X.GpuHashAggregate(gb, P.AggPlan(None, [], [P.count_star("n")]))
+    try:
+        ref = R.join(R.RefTable(bt), R.RefTable(pt), plan, workers=0)
+        for _ in range(2):
+            assert_rows_match(op.run().rows(), ref.rows(), ordered=True)
+        bt2 = HostTable([int_column("k", keys), date_column("d", np.full(nb, 8000, np.int32))], nb, 65536)
+        filler.run_host(bt2).close()
+        ref2 = R.join(R.RefTable(bt2), R.RefTable(pt), plan, workers=0)
+        for _ in range(2):
+            g = op.run()
+            g.collect()
+            assert_rows_match(g.rows(), ref2.rows(), ordered=True)
+            assert_sums_exact(g, ref2)
+    finally:
+        op.close()
+        filler.close()

@@ -2196,12 +2196,13 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     g.emit(p.probe_key);
     std::string K = std::to_string(p.probe_key);
     os << "            if (!ok" << K << ") continue;\n";
-    os << "            const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, (unsigned long long)(long long)x" << K << ");\n";
-    os << "            if (js == VQ_NOSLOT) continue;\n";
-    os << "            const int2 jm = P.jmeta[js];\n";
-    os << "            const int jb = jm.x, je = jb + jm.y;\n";
+    os << "            unsigned long long jc;\n";
+    os << "            if (!vq_find_slot(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", jc)) continue;\n";
+    // a single-row chain carries its build row in the slot (count word -1)
+    os << "            const int ja = (int)(unsigned)jc, jn = (int)(jc >> 32);\n";
+    os << "            const int jb = jn < 0 ? 0 : ja, je = jn < 0 ? 1 : ja + jn;\n";
     os << "            for (int ji = jb; ji < je; ji++) {\n";
-    os << "                const long long brow = P.jrows[ji];\n";
+    os << "                const long long brow = jn < 0 ? (long long)ja : (long long)P.jrows[ji];\n";
     // above-join expressions: a fresh memo scope per match for build-side reads
     Gen g2(p, os);
     g2.done = g.done;

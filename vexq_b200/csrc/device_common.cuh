@@ -340,6 +340,24 @@ __device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 ca
     return VQ_NOSLOT;
 }
 
+// Probe of the packed build table (key + chain in one 16-byte slot). Returns
+// whether the key is present and its chain word.
+__device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain) {
+    if (key == VQ_EMPTY_KEY) {
+        const ulonglong2 s = __ldg(slots + mask + 1);
+        chain = s.y;
+        return s.x != 0ull;
+    }
+    vq_u64 i = vq_hash(key) & mask;
+    for (vq_u64 n = 0; n <= mask; n++) {
+        const ulonglong2 s = __ldg(slots + i);
+        if (s.x == key) { chain = s.y; return true; }
+        if (s.x == VQ_EMPTY_KEY) return false;
+        i = (i + 1) & mask;
+    }
+    return false;
+}
+
 // Read-only lookup in a table no kernel is writing any more.
 __device__ __forceinline__ vq_u64 vq_find(const vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key) {
     if (key == VQ_EMPTY_KEY) return __ldg(keys + cap) ? cap : VQ_NOSLOT;

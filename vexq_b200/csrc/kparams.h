@@ -42,7 +42,11 @@ struct VQParams {
     int* jstart;               // [jcap + 1]
     int* jfill;                // [jcap + 1]
     int* jrows;                // build row ids, grouped by slot in row order
-    int2* jmeta;               // [jcap + 1] {first row position, row count} per slot
+    // [jcap + 1] probe view of the build table, one 16-byte load a probe step:
+    // .x the slot's key (slot jcap: used flag of the empty-sentinel key), .y the
+    // chain: low 32 bits the first row position and high 32 bits the row count,
+    // or, for a key with one build row, the build row id and -1
+    const ulonglong2* jslot;
     unsigned long long* jnkeys;
     // ---- radix-partitioned join ----
     unsigned long long* pkeys;     // partition pass: keys written per partition

@@ -165,6 +165,8 @@ struct Plan {
     std::vector<unsigned long long> hot_keys;
     mutable std::mutex hot_mu;
     long long hash_rows_seen = 0;          //   and the rows that run scanned
+    long long join_keys_seen = -1;         // join build: distinct keys the last build inserted
+    long long join_rows_seen = 0;          //   from this many build rows
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)

@@ -24,14 +24,8 @@ void refill_table(Table& t, const vexq_column_desc* cols, int32_t ncols, cudaStr
 
 // ---- static kernels ----------------------------------------------------------------
 
-__global__ void k_fill_u64(unsigned long long* p, long long n, unsigned long long v) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
-}
-
-// Register path: merges the per-block partials. One block per output entry;
-// each thread folds a fixed stride of blocks, then a fixed-shape shared-memory
-// tree combines the threads, so the result does not depend on scheduling.
-// Float sums carry a (hi, lo) compensated pair through both stages.
+// Compensated addition (Knuth's TwoSum): hi + lo carries the running sum, lo
+// the rounding error of each step.
 __device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
     double s = hi + x;
     double bb = s - hi;
@@ -175,15 +169,40 @@ __device__ __forceinline__ unsigned long long vq_claim(bool occ, unsigned peers,
     return base + __popc(b & ((1u << lane) - 1u));
 }
 
+// Output positions claimed per block: warp counts prefixed in shared memory,
+// one atomic per block (a single counter taking an atomic per warp serialised
+// large compactions). Every thread of the block calls it.
+__device__ __forceinline__ unsigned long long vq_claim_block(bool occ, unsigned long long* n_out) {
+    __shared__ unsigned wcnt[32];
+    __shared__ unsigned long long base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    const unsigned b = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0) wcnt[warp] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned tot = 0;
+        for (int w = 0; w < nw; w++) {
+            const unsigned c = wcnt[w];
+            wcnt[w] = tot;
+            tot += c;
+        }
+        base = tot ? atomicAdd(n_out, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    const unsigned long long pos = base + wcnt[warp] + __popc(b & ((1u << lane) - 1u));
+    __syncthreads();  // wcnt and base are rewritten by the next call
+    return pos;
+}
+
 __global__ void k_finalize(const unsigned long long* keys, const long long* first, const long long* acc_i,
                            const long long* acc_fx, const unsigned* special, long long nslots, int ni, int nf,
                            const int* fx_lsb, int hash, unsigned long long* n_out, unsigned long long* o_key,
                            long long* o_first, long long* o_i, double* o_f, long long cap_out) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < nslots; b0 += stride) {  // warp-uniform trip count
+    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < nslots; b0 += stride) {  // block-uniform trip count
         const long long i = b0 + threadIdx.x;
         const bool occ = i < nslots && acc_i[i] != 0;  // slot 0 of the int bank is the row count
-        const unsigned long long pos = vq_claim(occ, 0xffffffffu, n_out);
+        const unsigned long long pos = vq_claim_block(occ, n_out);
         if (occ) finalize_write(i, pos, keys, first, acc_i, acc_fx, special, nslots, ni, nf, fx_lsb, hash, o_key, o_first,
                                 o_i, o_f, cap_out);
     }
@@ -304,9 +323,17 @@ __global__ void k_part_starts(const int* off, const int* hist, int np, int grid,
 }
 
 // Packs each slot's chain start and length into one 8-byte probe read.
-__global__ void k_pack_meta(const int* start, const int* count, int2* meta, long long n) {
+// The probe's view of the build table: key and chain of a slot in one 16-byte
+// word pair; a key with a single build row carries the row id itself (count
+// word -1), which saves the probe its read of the row list.
+__global__ void k_pack_slots(const unsigned long long* keys, const int* start, const int* count, const int* rows,
+                             ulonglong2* slots, long long n) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) meta[i] = make_int2(start[i], count[i]);
+    if (i >= n) return;
+    const int c = count[i];
+    const int a = c == 1 ? rows[start[i]] : start[i];
+    const int b = c == 1 ? -1 : c;
+    slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
 }
 
 // Restores build-row order inside each key's chain (joinHashTable.insert keeps
@@ -1185,8 +1212,19 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         Table& bt = *p.bt;
         std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
         ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
-        long long jcap = 16;
-        while (jcap < 2 * std::max<long long>(bs.rows, 8)) jcap <<= 1;
+        // build table: twice the distinct keys the last build found (scaled by
+        // the rows scanned), else twice the rows; a build that hits the probe
+        // limit reruns at the row-bounded size (a table sized by rows leaves
+        // most slots empty, and every per-slot pass pays for them)
+        long long jsafe = 16;
+        while (jsafe < 2 * std::max<long long>(bs.rows, 8)) jsafe <<= 1;
+        long long jcap = jsafe;
+        if (p.join_keys_seen >= 0) {
+            const double scale = std::max(1.0, (double)bs.rows / (double)std::max<long long>(p.join_rows_seen, 1));
+            const long long est = std::min<long long>(bs.rows, std::max<long long>((long long)(p.join_keys_seen * scale), 1024));
+            jcap = 16;
+            while (jcap < 2 * std::max<long long>(est, 8)) jcap <<= 1;
+        }
         VQParams B;
         std::memset(&B, 0, sizeof B);
         set_plan_constants(p, B);
@@ -1204,13 +1242,14 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         B.present = p.d_bpresent.as<unsigned char>();
         B.sets[0] = nullptr;
         for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
+        for (;;) {
         long long nslots = jcap + 1;
         p.jt_keys.ensure(nslots * 8);
         p.jt_count.ensure(nslots * 4);
         p.jt_start.ensure(nslots * 4);
         p.jt_fill.ensure(nslots * 4);
         p.jt_rows.ensure(std::max<long long>(bs.rows, 1) * 4);
-        p.jt_meta.ensure(nslots * 8);
+        p.jt_meta.ensure(nslots * 16);
         p.jt_scalar.ensure(64 + ((nslots + 4095) / 4096 + 1) * 4);
         B.jkeys = p.jt_keys.as<unsigned long long>();
         B.jcount = p.jt_count.as<int>();
@@ -1228,8 +1267,8 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
             int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
-            k_fill_u64<<<ig, 256, 0, rc.s>>>(B.jkeys, jcap, VQ_EMPTY_KEY);
-            launch_check(rc.s, "k_fill_u64");
+            static_assert(VQ_EMPTY_KEY == ~0ull, "the empty-key fill is a byte memset");
+            VQ_CUDA(cudaMemsetAsync(B.jkeys, 0xFF, (size_t)jcap * 8, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jkeys + jcap, 0, 8, rc.s));
             B.mode = 0;
             int grid = grid_for(p.k_build, bs.nchunks, p.staged);
@@ -1251,8 +1290,9 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error, p.jt_long.as<int2>(),
                                                 long_count, long_cap);
             launch_check(rc.s, "k_sort_chains");
-            k_pack_meta<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, B.jcount, p.jt_meta.as<int2>(), nslots);
-            launch_check(rc.s, "k_pack_meta");
+            k_pack_slots<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jkeys, B.jstart, B.jcount, B.jrows,
+                                                                         p.jt_meta.as<ulonglong2>(), nslots);
+            launch_check(rc.s, "k_pack_slots");
             VQ_CUDA(cudaGetLastError());
             int herr = 0, nlong = 0;
             unsigned long long nk = 0;
@@ -1282,9 +1322,17 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
             rc.launches += 8;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
-            if (herr & 1) fail(VEXQ_EDEVICE, "join build table probe limit reached");
+            if (herr & 1) {
+                if (jcap >= jsafe) fail(VEXQ_EDEVICE, "join build table probe limit reached");
+                jcap = jsafe;  // the last build's key count was too small a guess
+                continue;
+            }
             if (herr & 4) fail(VEXQ_EDEVICE, "join build: more long chains than the sort list holds");
             join_keys = (long long)nk;
+            p.join_keys_seen = join_keys;
+            p.join_rows_seen = bs.rows;
+        }
+        break;
         }
         bytes += scanned_bytes(p, bt, bs.rows, true);
         rows_scanned += bs.rows;
@@ -1294,7 +1342,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         P.jcount = B.jcount;
         P.jstart = B.jstart;
         P.jrows = B.jrows;
-        P.jmeta = p.jt_meta.as<int2>();
+        P.jslot = p.jt_meta.as<ulonglong2>();
         P.jmask = B.jmask;
         if (join_keys == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
             Groups g;
