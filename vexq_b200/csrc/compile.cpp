@@ -2138,6 +2138,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << kernel_head("vq_build", block);
     // distinct keys counted per block, added to P.jnkeys once at the end
     os << "    __shared__ unsigned long long vq_nkeys;\n";
+    os << "    unsigned long long vq_nrows = 0ull;\n";
     os << "    if (threadIdx.x == 0) vq_nkeys = 0ull;\n    __syncthreads();\n";
     loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
@@ -2153,8 +2154,15 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
     os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
     os << "            if (P.mode == 0) {\n";
-    os << "                const unsigned long long js = vq_insert(P.jkeys, P.jmask, P.jmask + 1, jk, &vq_nkeys, P.error);\n";
-    os << "                if (js != VQ_NOSLOT) atomicAdd(P.jcount + js, 1);\n";
+    // pass 0 also keeps each slot's first row: a key with one build row needs
+    // no row list, and a build whose keys never repeat skips pass 1
+    os << "                bool fresh;\n";
+    os << "                const unsigned long long js = vq_insert_fresh(P.jkeys, P.jmask, P.jmask + 1, jk, fresh, P.error);\n";
+    os << "                if (js != VQ_NOSLOT) {\n";
+    os << "                    atomicAdd(P.jcount + js, 1);\n";
+    os << "                    vq_nrows++;\n";
+    os << "                    if (fresh) { P.jfirst[js] = (int)r; atomicAdd(&vq_nkeys, 1ull); }\n";
+    os << "                }\n";
     os << "            } else {\n";
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
@@ -2163,6 +2171,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     loop.close(os);
     os << "    __syncthreads();\n";
     os << "    if (threadIdx.x == 0 && vq_nkeys) atomicAdd(P.jnkeys, vq_nkeys);\n";
+    os << "    for (int o = 16; o > 0; o >>= 1) vq_nrows += __shfl_xor_sync(0xffffffffu, vq_nrows, o);\n";
+    os << "    if ((threadIdx.x & 31) == 0 && vq_nrows) atomicAdd(P.jtotal, vq_nrows);\n";
     os << "}\n";
     return os.str();
 }

@@ -340,6 +340,25 @@ __device__ __forceinline__ vq_u64 vq_insert(vq_u64* keys, vq_u64 mask, vq_u64 ca
     return VQ_NOSLOT;
 }
 
+// Insert that also reports whether this call claimed the key's slot.
+__device__ __forceinline__ vq_u64 vq_insert_fresh(vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key, bool& fresh, int* err) {
+    fresh = false;
+    if (key == VQ_EMPTY_KEY) {
+        fresh = atomicCAS(keys + cap, 0ull, 1ull) == 0ull;
+        return cap;
+    }
+    vq_u64 i = vq_hash(key) & mask;
+    const vq_u64 limit = mask < (vq_u64)VQ_MAX_PROBES ? mask + 1 : (vq_u64)VQ_MAX_PROBES;
+    for (vq_u64 n = 0; n < limit; n++) {
+        const vq_u64 old = atomicCAS(keys + i, VQ_EMPTY_KEY, key);
+        if (old == VQ_EMPTY_KEY) { fresh = true; return i; }
+        if (old == key) return i;
+        i = (i + 1) & mask;
+    }
+    atomicOr(err, 1);
+    return VQ_NOSLOT;
+}
+
 // Probe of the packed build table (key + chain in one 16-byte slot). Returns
 // whether the key is present and its chain word.
 __device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain) {

@@ -46,6 +46,8 @@ struct VQParams {
     // .x the slot's key (slot jcap: used flag of the empty-sentinel key), .y the
     // chain: low 32 bits the first row position and high 32 bits the row count,
     // or, for a key with one build row, the build row id and -1
+    int* jfirst;               // [jcap + 1] build row of the slot's first insert (pass 0)
+    unsigned long long* jtotal;    // build rows inserted (pass 0)
     const ulonglong2* jslot;
     unsigned long long* jnkeys;
     // ---- radix-partitioned join ----

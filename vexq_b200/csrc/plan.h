@@ -173,7 +173,7 @@ struct Plan {
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
     // scratch reused across runs
     DevBuf scratch_a, scratch_b, scratch_c, scratch_d, scratch_e, scratch_f, scratch_g;
-    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta, jt_long, jt_sort;
+    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta, jt_long, jt_sort, jt_first;
     // radix-partitioned join: kernels and buffers
     bool radix = false;
     std::string src_part_b, src_part_p, src_rjoin;

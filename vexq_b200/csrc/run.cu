@@ -326,12 +326,12 @@ __global__ void k_part_starts(const int* off, const int* hist, int np, int grid,
 // The probe's view of the build table: key and chain of a slot in one 16-byte
 // word pair; a key with a single build row carries the row id itself (count
 // word -1), which saves the probe its read of the row list.
-__global__ void k_pack_slots(const unsigned long long* keys, const int* start, const int* count, const int* rows,
+__global__ void k_pack_slots(const unsigned long long* keys, const int* start, const int* count, const int* first,
                              ulonglong2* slots, long long n) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = count[i];
-    const int a = c == 1 ? rows[start[i]] : start[i];
+    const int a = c == 1 ? first[i] : start[i];  // start is computed only when some key repeats
     const int b = c == 1 ? -1 : c;
     slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
 }
@@ -1250,20 +1250,23 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         p.jt_fill.ensure(nslots * 4);
         p.jt_rows.ensure(std::max<long long>(bs.rows, 1) * 4);
         p.jt_meta.ensure(nslots * 16);
+        p.jt_first.ensure(nslots * 4);
         p.jt_scalar.ensure(64 + ((nslots + 4095) / 4096 + 1) * 4);
         B.jkeys = p.jt_keys.as<unsigned long long>();
         B.jcount = p.jt_count.as<int>();
         B.jstart = p.jt_start.as<int>();
         B.jfill = p.jt_fill.as<int>();
         B.jrows = p.jt_rows.as<int>();
+        B.jfirst = p.jt_first.as<int>();
         B.jnkeys = p.jt_scalar.as<unsigned long long>();
         B.error = (int*)(p.jt_scalar.as<char>() + 8);
+        B.jtotal = (unsigned long long*)(p.jt_scalar.as<char>() + 24);
         int* bsums = (int*)(p.jt_scalar.as<char>() + 64);
         B.jmask = (unsigned long long)(jcap - 1);
         {
             ensure_events(p);
             VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
-            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 24, rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 32, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
             int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
@@ -1274,53 +1277,64 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             int grid = grid_for(p.k_build, bs.nchunks, p.staged);
             if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
             if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
-            int nb = (int)((nslots + 4095) / 4096);
-            k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);
-            launch_check(rc.s, "k_scan_blocks");
-            k_scan_sums<<<1, 1024, 0, rc.s>>>(bsums, nb);
-            launch_check(rc.s, "k_scan_sums");
-            k_scan_add<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, nslots, bsums);
-            launch_check(rc.s, "k_scan_add");
-            B.mode = 1;
-            if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
-            if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
-            const int long_cap = (int)(bs.rows / (kShortChain + 1) + 2);
-            p.jt_long.ensure((size_t)long_cap * 8);
-            int* long_count = (int*)(p.jt_scalar.as<char>() + 16);
-            k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error, p.jt_long.as<int2>(),
-                                                long_count, long_cap);
-            launch_check(rc.s, "k_sort_chains");
-            k_pack_slots<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jkeys, B.jstart, B.jcount, B.jrows,
+            // keys, inserted rows and errors of pass 0; a build whose keys never
+            // repeat needs no row lists: every chain is its slot's first row
+            int herr = 0, nlong = 0;
+            unsigned long long nk = 0, ntot = 0;
+            VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&ntot, B.jtotal, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaStreamSynchronize(rc.s));
+            const bool unique = nk == ntot && !(herr & 1);
+            if (!unique && !(herr & 1)) {
+                int nb = (int)((nslots + 4095) / 4096);
+                k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);
+                launch_check(rc.s, "k_scan_blocks");
+                k_scan_sums<<<1, 1024, 0, rc.s>>>(bsums, nb);
+                launch_check(rc.s, "k_scan_sums");
+                k_scan_add<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jstart, nslots, bsums);
+                launch_check(rc.s, "k_scan_add");
+                B.mode = 1;
+                if (bs.nchunks > 0) jit_launch(p.k_build, grid, &B, sizeof B, rc.s);
+                if (bs.nchunks > 0) launch_check(rc.s, "p.k_build");
+                const int long_cap = (int)(bs.rows / (kShortChain + 1) + 2);
+                p.jt_long.ensure((size_t)long_cap * 8);
+                int* long_count = (int*)(p.jt_scalar.as<char>() + 16);
+                k_sort_chains<<<ig, 256, 0, rc.s>>>(B.jstart, B.jcount, B.jrows, nslots, B.error, p.jt_long.as<int2>(),
+                                                    long_count, long_cap);
+                launch_check(rc.s, "k_sort_chains");
+                VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
+                VQ_CUDA(cudaMemcpyAsync(&nlong, long_count, 4, cudaMemcpyDeviceToHost, rc.s));
+                VQ_CUDA(cudaStreamSynchronize(rc.s));
+                if (nlong > 0 && !(herr & 4)) {  // long chains: one block each, scratch for the power-of-two pad
+                    std::vector<int2> lst(nlong);
+                    VQ_CUDA(cudaMemcpyAsync(lst.data(), p.jt_long.p, (size_t)nlong * 8, cudaMemcpyDeviceToHost, rc.s));
+                    VQ_CUDA(cudaStreamSynchronize(rc.s));
+                    std::vector<long long> soff(nlong);
+                    long long tot = 0;
+                    for (int i = 0; i < nlong; i++) {
+                        long long m = 1;
+                        while (m < lst[i].y) m <<= 1;
+                        soff[i] = tot;
+                        tot += m;
+                    }
+                    p.jt_sort.ensure((size_t)tot * 4 + (size_t)nlong * 8);
+                    long long* d_soff = (long long*)(p.jt_sort.as<char>() + (size_t)tot * 4);
+                    VQ_CUDA(cudaMemcpyAsync(d_soff, soff.data(), (size_t)nlong * 8, cudaMemcpyHostToDevice, rc.s));
+                    k_sort_long<<<nlong, 1024, 0, rc.s>>>(p.jt_long.as<int2>(), B.jstart, B.jrows, p.jt_sort.as<int>(), d_soff);
+                    launch_check(rc.s, "k_sort_long");
+                    rc.launches += 1;
+                }
+                rc.launches += 5;
+            }
+            k_pack_slots<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jkeys, B.jstart, B.jcount, B.jfirst,
                                                                          p.jt_meta.as<ulonglong2>(), nslots);
             launch_check(rc.s, "k_pack_slots");
             VQ_CUDA(cudaGetLastError());
-            int herr = 0, nlong = 0;
-            unsigned long long nk = 0;
-            VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
-            VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
-            VQ_CUDA(cudaMemcpyAsync(&nlong, long_count, 4, cudaMemcpyDeviceToHost, rc.s));
-            if (nlong > 0 && !(herr & 4)) {  // long chains: one block each, scratch for the power-of-two pad
-                std::vector<int2> lst(nlong);
-                VQ_CUDA(cudaMemcpyAsync(lst.data(), p.jt_long.p, (size_t)nlong * 8, cudaMemcpyDeviceToHost, rc.s));
-                std::vector<long long> soff(nlong);
-                long long tot = 0;
-                for (int i = 0; i < nlong; i++) {
-                    long long m = 1;
-                    while (m < lst[i].y) m <<= 1;
-                    soff[i] = tot;
-                    tot += m;
-                }
-                p.jt_sort.ensure((size_t)tot * 4 + (size_t)nlong * 8);
-                long long* d_soff = (long long*)(p.jt_sort.as<char>() + (size_t)tot * 4);
-                VQ_CUDA(cudaMemcpyAsync(d_soff, soff.data(), (size_t)nlong * 8, cudaMemcpyHostToDevice, rc.s));
-                k_sort_long<<<nlong, 1024, 0, rc.s>>>(p.jt_long.as<int2>(), B.jstart, B.jrows, p.jt_sort.as<int>(), d_soff);
-                launch_check(rc.s, "k_sort_long");
-                rc.launches += 1;
-            }
             VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
             VQ_CUDA(cudaEventSynchronize(p.ev[5]));
             rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
-            rc.launches += 8;
+            rc.launches += 2;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (herr & 1) {
                 if (jcap >= jsafe) fail(VEXQ_EDEVICE, "join build table probe limit reached");
