@@ -266,6 +266,19 @@ int32_t vexq_result_stats(vexq_result_t r, double* kernel_ms, int32_t* launches,
  * launched as its programmatic dependent overlap, and the pair is timed as
  * one span; the atomic paths time the scan alone. */
 int32_t vexq_result_scan_ms(vexq_result_t r, double* out);
+/* Everything above in one call (rows, columns, kernel and scan milliseconds,
+ * launches, rows and bytes scanned); any pointer may be NULL. No reference
+ * counterpart: it saves a binding one crossing per accessor. */
+typedef struct {
+    int64_t nrows;
+    int32_t ncols;
+    int32_t launches;
+    double  kernel_ms;
+    double  scan_ms;
+    int64_t rows_scanned;
+    int64_t bytes_scanned;
+} vexq_result_summary;
+int32_t vexq_result_info(vexq_result_t r, vexq_result_summary* out);
 
 /* Runs a plan on a caller-owned CUDA stream (a cudaStream_t, e.g. the stream
  * the caller times with events); NULL restores the plan's own stream.

@@ -70,6 +70,11 @@ class AggDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("input", C.c_int32), ("out_name", C.c_char_p)]
 
 
+class ResultSummary(C.Structure):
+    _fields_ = [("nrows", C.c_int64), ("ncols", C.c_int32), ("launches", C.c_int32), ("kernel_ms", C.c_double),
+                ("scan_ms", C.c_double), ("rows_scanned", C.c_int64), ("bytes_scanned", C.c_int64)]
+
+
 class OrderDesc(C.Structure):
     _fields_ = [("sort_col", C.c_int32), ("descending", C.c_int32), ("limit", C.c_int64)]
 
@@ -127,7 +132,7 @@ EXPORTS = [
     "vexq_agg_plan_create", "vexq_join_plan_create", "vexq_plan_destroy",
     "vexq_plan_explain", "vexq_zone_prune", "vexq_plan_run", "vexq_plan_run_host",
     "vexq_result_num_rows", "vexq_result_num_cols", "vexq_result_next",
-    "vexq_result_free", "vexq_result_stats", "vexq_result_scan_ms", "vexq_plan_set_stream",
+    "vexq_result_free", "vexq_result_stats", "vexq_result_scan_ms", "vexq_result_info", "vexq_plan_set_stream",
     "vexq_filter_run", "vexq_selvec_from_bits",
     "vexq_batch_run",
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
@@ -186,6 +191,7 @@ def load() -> C.CDLL:
         "vexq_result_free": (i32, [vp]),
         "vexq_result_stats": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]),
         "vexq_result_scan_ms": (i32, [vp, C.POINTER(C.c_double)]),
+        "vexq_result_info": (i32, [vp, C.POINTER(ResultSummary)]),
         "vexq_plan_set_stream": (i32, [vp, vp]),
         "vexq_filter_run": (i32, [vp, C.POINTER(Expr), i32, C.POINTER(i32), i32, i32, i64, i64,
                                   C.POINTER(C.c_uint8), C.POINTER(i64)]),

@@ -223,6 +223,18 @@ int32_t vexq_result_scan_ms(vexq_result_t r, double* out) {
     return VEXQ_OK;
 }
 
+int32_t vexq_result_info(vexq_result_t r, vexq_result_summary* out) {
+    if (!r || !out) return VEXQ_EINVAL;
+    out->nrows = r->nrows;
+    out->ncols = (int32_t)r->cols.size();
+    out->launches = r->launches;
+    out->kernel_ms = r->kernel_ms;
+    out->scan_ms = r->scan_ms;
+    out->rows_scanned = r->rows_scanned;
+    out->bytes_scanned = r->bytes_scanned;
+    return VEXQ_OK;
+}
+
 int32_t vexq_plan_set_stream(vexq_plan_t p, void* stream) {
     if (!p) return VEXQ_EINVAL;
     p->p->ext_stream = (cudaStream_t)stream;

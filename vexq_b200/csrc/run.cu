@@ -393,17 +393,33 @@ __device__ __forceinline__ unsigned long long vq_rank(long long bits, bool isnul
     u = desc ? u : ~u;
     return u == 0xFFFFFFFFFFFFFFFFull ? u - 1 : u;
 }
-__global__ void k_rank(const long long* keyv, const unsigned char* keynull, long long n, int desc,
-                       unsigned long long* rank) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        rank[i] = vq_rank(keyv[i], keynull[i], desc);
-}
 __global__ void k_sample(const unsigned long long* rank, long long n, int S, unsigned long long* out) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < S) out[j] = rank[(long long)j * n / S];
 }
-__global__ void k_select(const unsigned long long* rank, long long n, unsigned long long thr, unsigned long long* nsel,
+// One block sorts the S samples (a power of two, at most 4096) descending in
+// shared memory (bitonic network) and stores the q-th as the selection
+// threshold, so the host needs no copy of the samples.
+__global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* samp, int S, int q, unsigned long long* thr) {
+    extern __shared__ unsigned long long sv[];
+    for (int i = threadIdx.x; i < S; i += blockDim.x) sv[i] = samp[i];
+    __syncthreads();
+    for (int k = 2; k <= S; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < S; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = sv[i], b = sv[l];
+                    if ((i & k) == 0 ? a < b : a > b) { sv[i] = b; sv[l] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    if (threadIdx.x == 0) *thr = q < S ? sv[q] : 0ull;
+}
+__global__ void k_select(const unsigned long long* rank, long long n, const unsigned long long* thrp, unsigned long long* nsel,
                          long long* sel, long long cap) {
+    const unsigned long long thr = *thrp;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (rank[i] >= thr) {
             unsigned long long p = atomicAdd(nsel, 1ull);
@@ -411,9 +427,10 @@ __global__ void k_select(const unsigned long long* rank, long long n, unsigned l
         }
     }
 }
-// Sort key of one aggregate output per compacted group (bits + NULL flag).
-__global__ void k_sortkey(const long long* o_i, const double* o_f, long long cap_out, long long n, int kind, int vbank,
-                          int vpos, int nnpos, long long* keyv, unsigned char* keynull, int fmin_key) {
+// Rank of one aggregate output per compacted group: its sort key's raw bits
+// (NULL flag) mapped by vq_rank so that a larger rank sorts first.
+__global__ void k_sortrank(const long long* o_i, const double* o_f, long long cap_out, long long n, int kind, int vbank,
+                           int vpos, int nnpos, int fmin_key, int desc, unsigned long long* rank) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         long long nn = o_i[(long long)nnpos * cap_out + i];
         bool isnull = kind != VEXQ_AGG_COUNT && nn == 0;
@@ -426,15 +443,16 @@ __global__ void k_sortkey(const long long* o_i, const double* o_f, long long cap
             bits = o_i[(long long)vpos * cap_out + i];
             if (fmin_key) bits = __double_as_longlong(vq_fkey_inv((unsigned long long)bits));
         }
-        keyv[i] = bits;
-        keynull[i] = isnull;
+        rank[i] = vq_rank(bits, isnull, desc);
     }
 }
 
 // Gathers the selected compacted groups into a dense staging block.
-__global__ void k_gather(const long long* sel, long long n, const unsigned long long* key, const long long* first,
-                         const long long* ival, const double* fval, long long cap_out, int ni, int nf, long long* out) {
+__global__ void k_gather(const long long* sel, const unsigned long long* nsel, long long cap, const unsigned long long* key,
+                         const long long* first, const long long* ival, const double* fval, long long cap_out, int ni, int nf,
+                         long long* out) {
     long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)min(*nsel, (unsigned long long)cap);
     if (j >= n) return;
     long long i = sel[j];
     long long w = 2 + ni + nf;
@@ -728,51 +746,32 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
     fail(VEXQ_ENOMEM, "group table could not be sized");
 }
 
-Groups fetch_groups(RunCtx& rc, const Compacted& c, const std::vector<long long>* subset) {
+Groups fetch_groups(RunCtx& rc, const Compacted& c) {
     Plan& p = rc.p;
     Groups g;
-    long long n = subset ? (long long)subset->size() : c.n;
+    const long long n = c.n;
     g.key.resize(n);
     g.first.resize(n);
     g.ival.assign(p.ni, std::vector<int64_t>(n));
     g.fval.assign(p.nf, std::vector<double>(n));
     if (n == 0) return g;
-    if (!subset) {
-        VQ_CUDA(cudaMemcpyAsync(g.key.data(), c.key, n * 8, cudaMemcpyDeviceToHost, rc.s));
-        VQ_CUDA(cudaMemcpyAsync(g.first.data(), c.first, n * 8, cudaMemcpyDeviceToHost, rc.s));
-        for (int s = 0; s < p.ni; s++) VQ_CUDA(cudaMemcpyAsync(g.ival[s].data(), c.ival + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
-        for (int s = 0; s < p.nf; s++) VQ_CUDA(cudaMemcpyAsync(g.fval[s].data(), c.fval + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
-        VQ_CUDA(cudaStreamSynchronize(rc.s));
-        return g;
-    }
-    // gather the selected rows on the device, then one copy
-    long long w = 2 + p.ni + p.nf;
-    p.scratch_g.ensure((size_t)n * 8 + (size_t)n * w * 8);
-    long long* dsel = p.scratch_g.as<long long>();
-    long long* dout = dsel + n;
-    VQ_CUDA(cudaMemcpyAsync(dsel, subset->data(), n * 8, cudaMemcpyHostToDevice, rc.s));
-    k_gather<<<(int)((n + 127) / 128), 128, 0, rc.s>>>(dsel, n, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni, p.nf, dout);
-    launch_check(rc.s, "k_gather");
-    VQ_CUDA(cudaGetLastError());
-    std::vector<long long> h((size_t)n * w);
-    VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(g.key.data(), c.key, n * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(g.first.data(), c.first, n * 8, cudaMemcpyDeviceToHost, rc.s));
+    for (int s = 0; s < p.ni; s++) VQ_CUDA(cudaMemcpyAsync(g.ival[s].data(), c.ival + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
+    for (int s = 0; s < p.nf; s++) VQ_CUDA(cudaMemcpyAsync(g.fval[s].data(), c.fval + (long long)s * c.cap_out, n * 8, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
-    for (long long j = 0; j < n; j++) {
-        const long long* o = h.data() + j * w;
-        g.key[j] = (uint64_t)o[0];
-        g.first[j] = o[1];
-        for (int s = 0; s < p.ni; s++) g.ival[s][j] = o[2 + s];
-        for (int f = 0; f < p.nf; f++) std::memcpy(&g.fval[f][j], &o[2 + p.ni + f], 8);
-    }
     return g;
 }
 
 // Device top-k candidates for ORDER BY <aggregate> LIMIT k: every group's sort
 // rank (raw int64 bits in the ExternalSort order, NULLs first) is computed on
-// the device; a 4096-point sample gives a threshold that keeps a few hundred
-// groups per LIMIT row; groups at or above it (ties included) are the
-// candidates, and the host finishes the stable sort on them.
-bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel) {
+// the device; the q-th largest of a 4096-point sample, sorted on the device,
+// is a threshold that keeps about 4·LIMIT + 64 groups; the groups at or above
+// it (ties included) are gathered, and the host finishes the stable sort on
+// them. Two copies back: the count, then the gathered groups. Returns false
+// (the caller fetches every group) when the plan has no such ORDER BY, the
+// groups are few, or the sample was unlucky.
+bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
     Plan& p = rc.p;
     const vexq_order_desc& o = p.order;
     int ngb = (int)p.keys.size();
@@ -784,53 +783,57 @@ bool topk_candidates(RunCtx& rc, const Compacted& c, std::vector<long long>& sel
     int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
     if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
     const int S = 4096;
-    size_t need = c.n * 17 + 64 + S * 8 + kCap * 8 + 64;
+    const long long w = 2 + p.ni + p.nf;
+    // rank | samples | threshold, count | selected indices | gathered rows
+    size_t need = (size_t)c.n * 8 + S * 8 + 16 + kCap * 8 + (size_t)kCap * w * 8 + 64;
     p.scratch_d.ensure(need);
-    char* b = (char*)p.scratch_d.p;
-    long long* keyv = (long long*)b;
-    unsigned long long* rank = (unsigned long long*)(b + c.n * 8);
-    unsigned char* keynull = (unsigned char*)(b + c.n * 16);
-    unsigned long long* samp = (unsigned long long*)(((uintptr_t)(b + c.n * 17) + 63) & ~(uintptr_t)63);
-    unsigned long long* nsel = samp + S;
-    long long* dsel = (long long*)(nsel + 2);
-    int g = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
-    k_sortkey<<<g, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot], keyv,
-                                   keynull, fmin_key);
-    launch_check(rc.s, "k_sortkey");
-    k_rank<<<g, 256, 0, rc.s>>>(keyv, keynull, c.n, o.descending, rank);
-    launch_check(rc.s, "k_rank");
+    unsigned long long* rank = p.scratch_d.as<unsigned long long>();
+    unsigned long long* samp = rank + c.n;
+    unsigned long long* thr = samp + S;
+    unsigned long long* nsel = thr + 1;
+    long long* dsel = (long long*)(nsel + 1);
+    long long* dout = dsel + kCap;
+    int gr = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
+    k_sortrank<<<gr, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot],
+                                     fmin_key, o.descending, rank);
+    launch_check(rc.s, "k_sortrank");
     k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n, S, samp);
     launch_check(rc.s, "k_sample");
-    std::vector<unsigned long long> hs(S);
-    VQ_CUDA(cudaMemcpyAsync(hs.data(), samp, S * 8, cudaMemcpyDeviceToHost, rc.s));
-    VQ_CUDA(cudaStreamSynchronize(rc.s));
     // threshold: expected (q+1)·n/S groups at or above the q-th largest sample
-    long long q = (long long)std::ceil((4.0 * o.limit + 64.0) * S / (double)c.n) - 1;
-    unsigned long long thr = 0;
-    if (q < S) {
-        std::nth_element(hs.begin(), hs.begin() + q, hs.end(), std::greater<unsigned long long>());
-        thr = hs[q];
+    // (c.n > 4·limit + 4096 keeps q below S)
+    const int q = (int)std::ceil((4.0 * o.limit + 64.0) * S / (double)c.n) - 1;
+    k_threshold<<<1, 1024, S * 8, rc.s>>>(samp, S, q, thr);
+    launch_check(rc.s, "k_threshold");
+    VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
+    k_select<<<gr, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
+    launch_check(rc.s, "k_select");
+    k_gather<<<(int)((kCap + 127) / 128), 128, 0, rc.s>>>(dsel, nsel, kCap, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni,
+                                                          p.nf, dout);
+    launch_check(rc.s, "k_gather");
+    VQ_CUDA(cudaGetLastError());
+    p.h_stage.ensure(16);
+    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    rc.launches += 5;
+    const long long ns = (long long)*(const unsigned long long*)p.h_stage.p;
+    // an unlucky sample (fewer than LIMIT selected) or too many ties at the
+    // threshold: the caller fetches every group
+    if (ns < o.limit || ns > kCap) return false;
+    std::vector<long long> h((size_t)ns * w);
+    VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    g.key.resize(ns);
+    g.first.resize(ns);
+    g.ival.assign(p.ni, std::vector<int64_t>(ns));
+    g.fval.assign(p.nf, std::vector<double>(ns));
+    for (long long j = 0; j < ns; j++) {
+        const long long* r = h.data() + j * w;
+        g.key[j] = (uint64_t)r[0];
+        g.first[j] = r[1];
+        for (int s = 0; s < p.ni; s++) g.ival[s][j] = r[2 + s];
+        for (int f = 0; f < p.nf; f++) std::memcpy(&g.fval[f][j], &r[2 + p.ni + f], 8);
     }
-    for (int attempt = 0; attempt < 2; attempt++) {
-        VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
-        k_select<<<g, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
-        launch_check(rc.s, "k_select");
-        VQ_CUDA(cudaGetLastError());
-        unsigned long long ns = 0;
-        VQ_CUDA(cudaMemcpyAsync(&ns, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
-        VQ_CUDA(cudaStreamSynchronize(rc.s));
-        rc.launches += 1;
-        if ((long long)ns >= o.limit && (long long)ns <= kCap) {
-            sel.resize(ns);
-            VQ_CUDA(cudaMemcpy(sel.data(), dsel, ns * 8, cudaMemcpyDeviceToHost));
-            rc.launches += 3;
-            return true;
-        }
-        if ((long long)ns > kCap) return false;  // too many ties at the threshold: fetch everything
-        thr = 0;                                  // unlucky sample: every group qualifies
-        if (c.n > kCap) return false;
-    }
-    return false;
+    return true;
 }
 
 // Decodes group keys, computes aggregate outputs, orders groups, and applies
@@ -982,9 +985,7 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
         g = run_regs(rc, P, nchunks);
     } else {
         Compacted c = run_atomic(rc, P, nchunks, estimate, rows);
-        std::vector<long long> sel;
-        if (topk_candidates(rc, c, sel)) g = fetch_groups(rc, c, &sel);
-        else g = fetch_groups(rc, c, nullptr);
+        if (!topk_groups(rc, c, g)) g = fetch_groups(rc, c);
     }
     note_hot_groups(p, g);
     vexq_result_s* r = build_result(p, g);

@@ -99,17 +99,11 @@ class Result:
 
     def __init__(self, h: C.c_void_p):
         self.h = h
-        L = abi.load()
-        n, nc = C.c_int64(), C.c_int32()
-        L.vexq_result_num_rows(h, C.byref(n))
-        L.vexq_result_num_cols(h, C.byref(nc))
-        self.nrows, self.ncols = n.value, nc.value
-        ms, la, rs, bs = C.c_double(), C.c_int32(), C.c_int64(), C.c_int64()
-        L.vexq_result_stats(h, C.byref(ms), C.byref(la), C.byref(rs), C.byref(bs))
-        self.kernel_ms, self.launches, self.rows_scanned, self.bytes_scanned = ms.value, la.value, rs.value, bs.value
-        sc = C.c_double()
-        L.vexq_result_scan_ms(h, C.byref(sc))
-        self.scan_ms = sc.value
+        s = abi.ResultSummary()
+        abi.check(abi.load().vexq_result_info(h, C.byref(s)))
+        self.nrows, self.ncols = s.nrows, s.ncols
+        self.kernel_ms, self.launches, self.rows_scanned, self.bytes_scanned = s.kernel_ms, s.launches, s.rows_scanned, s.bytes_scanned
+        self.scan_ms = s.scan_ms
 
     def next(self) -> Optional[Batch]:
         """Operator.Next: ≤1024 rows, None at EOF."""
