@@ -42,7 +42,10 @@ int32_t guard(F&& f) {
 
 int64_t plan_footprint(const Plan& p) {
     // group table slots × (key + first + int bank + fixed-point digits + flags)
-    int64_t slots = p.path == AggPath::Hash ? 2 * std::max<int64_t>(p.t->nrows, 16)
+    // (a join grouping by its key numbers the build's distinct keys: at most
+    // one slot per build row)
+    int64_t slots = p.join_gid ? std::max<int64_t>(p.bt->nrows, 16) + 1
+                  : p.path == AggPath::Hash ? 2 * std::max<int64_t>(p.t->nrows, 16)
                   : p.path == AggPath::Dense ? p.domain : 64;
     int64_t per = 16 + 8 * p.ni + 36 * p.nf;
     int64_t f = slots * per;

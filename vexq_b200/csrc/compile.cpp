@@ -1288,8 +1288,13 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
 }
 
 // Atomic path: group table in global memory.
-void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order) {
-    if (p.path == AggPath::Dense) {
+// gid_slot: the global join probe's group number (vq_gid) is the slot; the
+// partitioned join, which has no build slots, inserts the packed key instead.
+void emit_atomic_update(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& order,
+                        bool gid_slot = false) {
+    if (gid_slot) {
+        os << ind << "const unsigned long long slot = vq_gid;\n";
+    } else if (p.path == AggPath::Dense) {
         os << ind << "const unsigned long long slot = key;\n";
     } else {
         os << ind << "const unsigned long long slot = vq_insert(P.keys, P.cap_mask, P.cap, key, nullptr, P.error);\n";
@@ -2206,10 +2211,11 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     g.emit(p.probe_key);
     std::string K = std::to_string(p.probe_key);
     os << "            if (!ok" << K << ") continue;\n";
-    os << "            unsigned long long jc;\n";
-    os << "            if (!vq_find_slot(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", jc)) continue;\n";
-    // a single-row chain carries its build row in the slot (count word -1)
+    os << "            unsigned long long jc, jat;\n";
+    os << "            if (!vq_find_slot(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", jc, jat)) continue;\n";
+    // a single-row chain carries its build row in the slot (count word ~group number, negative)
     os << "            const int ja = (int)(unsigned)jc, jn = (int)(jc >> 32);\n";
+    if (p.join_gid) os << "            const unsigned long long vq_gid = jn < 0 ? (unsigned long long)(unsigned)~jn : (unsigned long long)(unsigned)P.jgid[jat];\n";
     os << "            const int jb = jn < 0 ? 0 : ja, je = jn < 0 ? 1 : ja + jn;\n";
     os << "            for (int ji = jb; ji < je; ji++) {\n";
     os << "                const long long brow = jn < 0 ? (long long)ja : (long long)P.jrows[ji];\n";
@@ -2227,7 +2233,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     emit_slot_values(os, p, "                ");
     std::string order = order_expr(p, "((r << 16) | (long long)min(ji - jb, 65535))");
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
-    else emit_atomic_update(os, p, "                ", order);
+    else emit_atomic_update(os, p, "                ", order, p.join_gid);
     os << "            }\n        }\n";
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
@@ -2543,6 +2549,19 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         }
     }
     choose_path(p);
+    p.join_gid = false;
+    if (join && p.path != AggPath::Regs && p.keys.size() == 1 && !p.keys[0].nullable && p.keys[0].type == VEXQ_TYPE_INT64 &&
+        std::getenv("VEXQ_NO_GID") == nullptr) {
+        const KeyCol& k = p.keys[0];
+        const bool jk = (k.build && k.col == p.build_key) || (!k.build && p.ir[p.probe_key].k == NK::Col && k.col == p.ir[p.probe_key].col);
+        if (jk) {
+            // hash-path key decoding (one key, shift 0): the group table's
+            // key array holds the code the hash path would pack
+            p.join_gid = true;
+            p.path = AggPath::Hash;
+            p.gid_koff = k.domain > 0 ? k.vmin : 0;
+        }
+    }
     choose_tunables(p);
     choose_regs_forms(p);
     // numeric literals become launch-time values (first VQ_MAXLITS of them)
@@ -2608,6 +2627,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
        << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
     if (hot_on(p)) ex << " hot_groups=" << p.hot_n;
+    if (p.join_gid) ex << " groups=build_key_numbers";
     if (p.path == AggPath::Regs && !join) {
         int nx = 0, nm = 0, na = 0;
         for (size_t s = 0; s < p.slots.size(); s++) {

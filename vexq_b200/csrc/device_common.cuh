@@ -361,16 +361,17 @@ __device__ __forceinline__ vq_u64 vq_insert_fresh(vq_u64* keys, vq_u64 mask, vq_
 
 // Probe of the packed build table (key + chain in one 16-byte slot). Returns
 // whether the key is present and its chain word.
-__device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain) {
+__device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain, vq_u64& at) {
     if (key == VQ_EMPTY_KEY) {
         const ulonglong2 s = __ldg(slots + mask + 1);
         chain = s.y;
+        at = mask + 1;
         return s.x != 0ull;
     }
     vq_u64 i = vq_hash(key) & mask;
     for (vq_u64 n = 0; n <= mask; n++) {
         const ulonglong2 s = __ldg(slots + i);
-        if (s.x == key) { chain = s.y; return true; }
+        if (s.x == key) { chain = s.y; at = i; return true; }
         if (s.x == VQ_EMPTY_KEY) return false;
         i = (i + 1) & mask;
     }

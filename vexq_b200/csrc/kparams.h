@@ -47,6 +47,7 @@ struct VQParams {
     // chain: low 32 bits the first row position and high 32 bits the row count,
     // or, for a key with one build row, the build row id and -1
     int* jfirst;               // [jcap + 1] build row of the slot's first insert (pass 0)
+    int* jgid;                 // [jcap + 1] group number of the slot's key (GROUP BY the join key)
     unsigned long long* jtotal;    // build rows inserted (pass 0)
     const ulonglong2* jslot;
     unsigned long long* jnkeys;

@@ -165,6 +165,12 @@ struct Plan {
     std::vector<unsigned long long> hot_keys;
     mutable std::mutex hot_mu;
     long long hash_rows_seen = 0;          //   and the rows that run scanned
+    // GROUP BY exactly the (non-NULL int64) join key on a group-table path:
+    // the global join numbers the build's distinct keys (0..nk-1) and the
+    // group table is indexed by that number (gid_koff: the key's code offset)
+    bool join_gid = false;
+    long long gid_koff = 0;
+    long long gid_groups = 0;              // group numbers the last build handed out
     long long join_keys_seen = -1;         // join build: distinct keys the last build inserted
     long long join_rows_seen = 0;          //   from this many build rows
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
@@ -173,7 +179,7 @@ struct Plan {
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
     // scratch reused across runs
     DevBuf scratch_a, scratch_b, scratch_c, scratch_d, scratch_e, scratch_f, scratch_g;
-    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta, jt_long, jt_sort, jt_first;
+    DevBuf jt_keys, jt_count, jt_start, jt_fill, jt_rows, jt_scalar, jt_meta, jt_long, jt_sort, jt_first, jt_gid, jt_gkey;
     // radix-partitioned join: kernels and buffers
     bool radix = false;
     std::string src_part_b, src_part_p, src_rjoin;

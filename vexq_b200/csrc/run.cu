@@ -326,14 +326,29 @@ __global__ void k_part_starts(const int* off, const int* hist, int np, int grid,
 // The probe's view of the build table: key and chain of a slot in one 16-byte
 // word pair; a key with a single build row carries the row id itself (count
 // word -1), which saves the probe its read of the row list.
+// Each key also gets a group number (positions claimed once per block, so
+// numbers are dense in 0..keys-1) and gkey[number] = its key's code (key -
+// koff) for plans that group by the join key; a one-row chain's count word is
+// ~number (negative), so the probe finds both its row and its group in the slot.
 __global__ void k_pack_slots(const unsigned long long* keys, const int* start, const int* count, const int* first,
+                             int* gid, unsigned long long* gkey, unsigned long long* ngid, long long koff,
                              ulonglong2* slots, long long n) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int c = count[i];
-    const int a = c == 1 ? first[i] : start[i];  // start is computed only when some key repeats
-    const int b = c == 1 ? -1 : c;
-    slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < n; b0 += stride) {  // block-uniform trip count
+        const long long i = b0 + threadIdx.x;
+        const int c = i < n ? count[i] : 0;
+        const unsigned long long g = vq_claim_block(c > 0, ngid);
+        if (i >= n) continue;
+        const int a = c == 1 ? first[i] : start[i];  // start is computed only when some key repeats
+        const int b = c == 1 ? ~(int)g : c;
+        // the last slot holds the key equal to the empty sentinel (its key word is a used flag)
+        const unsigned long long key = i == n - 1 ? VQ_EMPTY_KEY : keys[i];
+        slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
+        if (c > 0) {
+            gid[i] = (int)g;
+            gkey[g] = (unsigned long long)((long long)key - koff);
+        }
+    }
 }
 
 // Restores build-row order inside each key's chain (joinHashTable.insert keeps
@@ -644,9 +659,14 @@ struct Compacted {
 
 Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows) {
     Plan& p = rc.p;
-    bool hash = p.path == AggPath::Hash;
+    // a join grouping by its key on the global table: one slot per build key
+    // number, no key inserts; the keys come from the build's number→key array
+    const bool gid = p.join_gid && !rc.k;
+    bool hash = p.path == AggPath::Hash && !gid;
     long long cap, safe_cap = 16;
-    if (hash) {
+    if (gid) {
+        cap = std::max<long long>(p.gid_groups, 1);
+    } else if (hash) {
         while (safe_cap < 2 * std::max<long long>(estimate, 8)) safe_cap <<= 1;
         // a rerun sizes its table from the groups the last run found, scaled
         // up by the rows scanned (the row-count bound is usually far above the
@@ -715,8 +735,8 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         launch_check(rc.s, "p.k_main");
         VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
         int fg = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
-        k_finalize<<<fg, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, P.acc_fx, P.special, nslots, ni, nf, d_lsb, hash, n_out,
-                                         c.key, c.first, c.ival, c.fval, cap_out);
+        k_finalize<<<fg, 256, 0, rc.s>>>(gid ? p.jt_gkey.as<unsigned long long>() : P.keys, P.first, P.acc_i, P.acc_fx, P.special,
+                                         nslots, ni, nf, d_lsb, hash || gid, n_out, c.key, c.first, c.ival, c.fval, cap_out);
         launch_check(rc.s, "k_finalize");
         VQ_CUDA(cudaGetLastError());
         VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
@@ -1252,6 +1272,8 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         p.jt_rows.ensure(std::max<long long>(bs.rows, 1) * 4);
         p.jt_meta.ensure(nslots * 16);
         p.jt_first.ensure(nslots * 4);
+        p.jt_gid.ensure(nslots * 4);
+        p.jt_gkey.ensure(nslots * 8);
         p.jt_scalar.ensure(64 + ((nslots + 4095) / 4096 + 1) * 4);
         B.jkeys = p.jt_keys.as<unsigned long long>();
         B.jcount = p.jt_count.as<int>();
@@ -1262,12 +1284,14 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         B.jnkeys = p.jt_scalar.as<unsigned long long>();
         B.error = (int*)(p.jt_scalar.as<char>() + 8);
         B.jtotal = (unsigned long long*)(p.jt_scalar.as<char>() + 24);
+        B.jgid = p.jt_gid.as<int>();
+        unsigned long long* d_ngid = (unsigned long long*)(p.jt_scalar.as<char>() + 32);
         int* bsums = (int*)(p.jt_scalar.as<char>() + 64);
         B.jmask = (unsigned long long)(jcap - 1);
         {
             ensure_events(p);
             VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
-            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 32, rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 40, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jcount, 0, nslots * 4, rc.s));
             VQ_CUDA(cudaMemsetAsync(B.jfill, 0, nslots * 4, rc.s));
             int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
@@ -1328,8 +1352,9 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
                 }
                 rc.launches += 5;
             }
-            k_pack_slots<<<(int)((nslots + 255) / 256), 256, 0, rc.s>>>(B.jkeys, B.jstart, B.jcount, B.jfirst,
-                                                                         p.jt_meta.as<ulonglong2>(), nslots);
+            k_pack_slots<<<(int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16), 256, 0, rc.s>>>(
+                B.jkeys, B.jstart, B.jcount, B.jfirst, B.jgid, p.jt_gkey.as<unsigned long long>(), d_ngid, p.gid_koff,
+                p.jt_meta.as<ulonglong2>(), nslots);
             launch_check(rc.s, "k_pack_slots");
             VQ_CUDA(cudaGetLastError());
             VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
@@ -1344,6 +1369,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             }
             if (herr & 4) fail(VEXQ_EDEVICE, "join build: more long chains than the sort list holds");
             join_keys = (long long)nk;
+            p.gid_groups = join_keys;
             p.join_keys_seen = join_keys;
             p.join_rows_seen = bs.rows;
         }
@@ -1358,6 +1384,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         P.jstart = B.jstart;
         P.jrows = B.jrows;
         P.jslot = p.jt_meta.as<ulonglong2>();
+        P.jgid = p.jt_gid.as<int>();
         P.jmask = B.jmask;
         if (join_keys == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
             Groups g;
