@@ -1361,14 +1361,21 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
         std::string aiu = "(unsigned long long*)(" + ai + ")";
         switch (p.slots[s].kind) {
             case S_CNT:
-            case S_NN: os << in << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
-            case S_ISUM: os << in << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n"; break;
+            case S_NN:
+                // a block's count stays below 2^32: a 32-bit add on the counter's low word
+                if (p.cache_cnt32) os << in << "if (ag" << S << ") atomicAdd((unsigned*)(" << ai << "), (unsigned)ag" << S << ");\n";
+                else os << in << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n";
+                break;
+            case S_ISUM:
+                if (p.cache_fx32) os << in << "if (ah" << S << ") vq_add64_as32(" << ai << ", ag" << S << ");\n";
+                else os << in << "if (ah" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n";
+                break;
             case S_IMIN: os << in << "if (ah" << S << " && ag" << S << " < *(" << ai << ")) atomicMin(" << ai << ", ag" << S << ");\n"; break;
             case S_IMAX: os << in << "if (ah" << S << " && ag" << S << " > *(" << ai << ")) atomicMax(" << ai << ", ag" << S << ");\n"; break;
             case S_FMIN: os << in << "if (ah" << S << " && ag" << S << " < *" << aiu << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
             case S_FMAX: os << in << "if (ah" << S << " && ag" << S << " > *" << aiu << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
             case S_FSUM:
-                os << in << "if (ah" << S << ") { vq_fx_add_digits_s(" << L.fx << " + (long long)" << pos << " * 4 * " << C
+                os << in << "if (ah" << S << ") { " << (p.cache_fx32 ? "vq_fx_add_digits_s32(" : "vq_fx_add_digits_s(") << L.fx << " + (long long)" << pos << " * 4 * " << C
                    << " + (long long)slot, " << C << ", fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
                    << ") atomicOr(" << L.sp << " + " << pos << " * " << C << " + slot, fsp" << S << "); }\n";
                 break;
@@ -2142,9 +2149,9 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     loop.prologue(os);
     os << kernel_head("vq_build", block);
     // distinct keys counted per block, added to P.jnkeys once at the end
-    os << "    __shared__ unsigned long long vq_nkeys;\n";
+    os << "    __shared__ unsigned vq_nkeys;\n";
     os << "    unsigned long long vq_nrows = 0ull;\n";
-    os << "    if (threadIdx.x == 0) vq_nkeys = 0ull;\n    __syncthreads();\n";
+    os << "    if (threadIdx.x == 0) vq_nkeys = 0u;\n    __syncthreads();\n";
     loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
@@ -2166,7 +2173,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) {\n";
     os << "                    atomicAdd(P.jcount + js, 1);\n";
     os << "                    vq_nrows++;\n";
-    os << "                    if (fresh) { P.jfirst[js] = (int)r; atomicAdd(&vq_nkeys, 1ull); }\n";
+    os << "                    if (fresh) { P.jfirst[js] = (int)r; atomicAdd(&vq_nkeys, 1u); }\n";
     os << "                }\n";
     os << "            } else {\n";
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
@@ -2175,7 +2182,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "        }\n";
     loop.close(os);
     os << "    __syncthreads();\n";
-    os << "    if (threadIdx.x == 0 && vq_nkeys) atomicAdd(P.jnkeys, vq_nkeys);\n";
+    os << "    if (threadIdx.x == 0 && vq_nkeys) atomicAdd(P.jnkeys, (unsigned long long)vq_nkeys);\n";
     os << "    for (int o = 16; o > 0; o >>= 1) vq_nrows += __shfl_xor_sync(0xffffffffu, vq_nrows, o);\n";
     os << "    if ((threadIdx.x & 31) == 0 && vq_nrows) atomicAdd(P.jtotal, vq_nrows);\n";
     os << "}\n";
@@ -2405,19 +2412,22 @@ static std::string gen_rjoin_kernel(Plan& p, const std::vector<int>& key_nodes, 
             const int pos = p.slot_pos[s];
             const std::string li = "LI + " + std::to_string(pos) + " * " + CAP + " + lo";
             switch (p.slots[s].kind) {
-                case S_CNT: os << in << "  atomicAdd((unsigned long long*)(" << li << "), 1ull);\n"; break;
-                case S_NN: os << in << "  if (sok" << S << ") atomicAdd((unsigned long long*)(" << li << "), 1ull);\n"; break;
-                case S_ISUM: os << in << "  if (sok" << S << ") atomicAdd((unsigned long long*)(" << li << "), (unsigned long long)sv" << S << ");\n"; break;
+                // shared memory: 32-bit atomics (a partition's count stays below 2^32)
+                case S_CNT: os << in << "  atomicAdd((unsigned*)(" << li << "), 1u);\n"; break;
+                case S_NN: os << in << "  if (sok" << S << ") atomicAdd((unsigned*)(" << li << "), 1u);\n"; break;
+                case S_ISUM: os << in << "  if (sok" << S << ") vq_add64_as32((long long*)(" << li << "), (long long)sv" << S << ");\n"; break;
                 case S_IMIN: os << in << "  if (sok" << S << " && sv" << S << " < *(" << li << ")) atomicMin(" << li << ", sv" << S << ");\n"; break;
                 case S_IMAX: os << in << "  if (sok" << S << " && sv" << S << " > *(" << li << ")) atomicMax(" << li << ", sv" << S << ");\n"; break;
                 case S_FMIN:
-                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) atomicMin((unsigned long long*)(" << li << "), vq_fkey(sv" << S << "));\n";
+                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) { const unsigned long long q = vq_fkey(sv" << S
+                       << "); if (q < *(unsigned long long*)(" << li << ")) atomicMin((unsigned long long*)(" << li << "), q); }\n";
                     break;
                 case S_FMAX:
-                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) atomicMax((unsigned long long*)(" << li << "), vq_fkey(sv" << S << "));\n";
+                    os << in << "  if (sok" << S << " && !isnan(sv" << S << ")) { const unsigned long long q = vq_fkey(sv" << S
+                       << "); if (q > *(unsigned long long*)(" << li << ")) atomicMax((unsigned long long*)(" << li << "), q); }\n";
                     break;
                 case S_FSUM:
-                    os << in << "  if (sok" << S << ") vq_fx_add<true>(LX + ((long long)lo * " << p.nf << " + " << pos << ") * 4, sv" << S
+                    os << in << "  if (sok" << S << ") vq_fx_add<true, true>(LX + ((long long)lo * " << p.nf << " + " << pos << ") * 4, sv" << S
                        << ", P.fx_lsb[" << pos << "], LS + " << pos << " * " << CAP << " + lo, P.error);\n";
                     break;
             }
@@ -2500,11 +2510,13 @@ static void choose_tunables(Plan& p) {
     // measured on Zipf(1.1) keys: per-lane shared-memory atomics beat folding
     // the peers of a warp first (the fold serialises over distinct groups)
     p.warp_agg = false;
-    // dense path: the largest group of the last run accumulates in each
-    // thread's registers (measured on 4M Zipf(1.1) rows: one hot group 122 /
-    // 140 us at 1,000 / 65,536 groups, none 144 / 157, two 145 / 148 — more
-    // registers cost more occupancy than the atomics they save)
-    p.hot_n = (p.path == AggPath::Dense && !p.is_join) ? 1 : 0;
+    // dense path, shared-memory cache: 32-bit atomics (a 64-bit shared atomic
+    // add measured 6x slower than a 32-bit one, 50x with a hot address). 4M
+    // Zipf(1.1) rows, 1,000 / 65,536 groups: 60 / 75 us against 124 / 142 us
+    // with 64-bit adds; the hottest groups in registers (hot=N) then cost more
+    // than they save (67 / 82 us with one)
+    p.cache_cnt32 = p.cache_fx32 = true;
+    p.hot_n = 0;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -2515,6 +2527,9 @@ static void choose_tunables(Plan& p) {
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
         int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb="), ho = get("hot=");
+        int c32 = get("cnt32="), f32 = get("fx32=");
+        if (c32 >= 0) p.cache_cnt32 = c32 != 0;
+        if (f32 >= 0) p.cache_fx32 = f32 != 0;
         if (ho >= 0 && p.path == AggPath::Dense && !p.is_join) p.hot_n = std::min(ho, VQ_MAXHOT);
         if (as >= 0) p.async_stages = as;
         if (mb >= 0) p.min_blocks = mb;
@@ -2627,6 +2642,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
        << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
     if (hot_on(p)) ex << " hot_groups=" << p.hot_n;
+    if (p.path == AggPath::Dense && !join && !(p.cache_cnt32 && p.cache_fx32)) ex << " atomics64";
     if (p.join_gid) ex << " groups=build_key_numbers";
     if (p.path == AggPath::Regs && !join) {
         int nx = 0, nm = 0, na = 0;

@@ -162,6 +162,10 @@ struct Plan {
     // dense path: the kernel accumulates hot_n groups per thread in registers;
     // which groups is a launch value, the largest-count groups of the last run
     int hot_n = 0;
+    // dense path, shared-memory cache: counts added as 32-bit atomics on the
+    // counter's low word; fixed-point digits as 32-bit atomics with the carry
+    // (from the returned old value) added to the high word
+    bool cache_cnt32 = false, cache_fx32 = false;
     std::vector<unsigned long long> hot_keys;
     mutable std::mutex hot_mu;
     long long hash_rows_seen = 0;          //   and the rows that run scanned
