@@ -412,25 +412,55 @@ __global__ void k_sample(const unsigned long long* rank, long long n, int S, uns
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < S) out[j] = rank[(long long)j * n / S];
 }
-// One block sorts the S samples (a power of two, at most 4096) descending in
-// shared memory (bitonic network) and stores the q-th as the selection
-// threshold, so the host needs no copy of the samples.
+// One block finds the q-th largest of the S samples (S <= 4096, q < S) by radix
+// select, most significant byte first: each round counts, in shared memory,
+// the next byte of the samples that match the bytes chosen so far, and one
+// warp walks the 256 counts from the top to the byte holding the q-th largest.
+// The result is the selection threshold, so the host needs no copy of the
+// samples.
 __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* samp, int S, int q, unsigned long long* thr) {
-    extern __shared__ unsigned long long sv[];
-    for (int i = threadIdx.x; i < S; i += blockDim.x) sv[i] = samp[i];
-    __syncthreads();
-    for (int k = 2; k <= S; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < S; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = sv[i], b = sv[l];
-                    if ((i & k) == 0 ? a < b : a > b) { sv[i] = b; sv[l] = a; }
+    __shared__ unsigned hist[256];
+    __shared__ unsigned long long prefix;
+    __shared__ unsigned need;
+    unsigned long long v[4];
+    int nv = 0;
+    for (int i = threadIdx.x; i < S && nv < 4; i += blockDim.x) v[nv++] = samp[i];
+    if (threadIdx.x == 0) { prefix = 0ull; need = (unsigned)q; }
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
+        __syncthreads();
+        const unsigned long long hi_mask = shift == 56 ? 0ull : (~0ull << (shift + 8));
+        const unsigned long long pre = prefix;
+        const unsigned nd = need;  // both rewritten only after the next barrier
+        for (int k = 0; k < nv; k++)
+            if ((v[k] & hi_mask) == pre) atomicAdd(&hist[(v[k] >> shift) & 255u], 1u);
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            unsigned c[8], sum = 0u;
+#pragma unroll
+            for (int k = 0; k < 8; k++) { c[k] = hist[255 - (8 * lane + k)]; sum += c[k]; }
+            unsigned incl = sum;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const unsigned excl = incl - sum;
+            if (excl <= nd && nd < incl) {  // exactly one lane holds the q-th largest
+                unsigned acc = excl;
+                for (int k = 0; k < 8; k++) {
+                    if (nd < acc + c[k]) {
+                        prefix = pre | ((unsigned long long)(255 - (8 * lane + k)) << shift);
+                        need = nd - acc;
+                        break;
+                    }
+                    acc += c[k];
                 }
             }
-            __syncthreads();
         }
-    if (threadIdx.x == 0) *thr = q < S ? sv[q] : 0ull;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *thr = q < S ? prefix : 0ull;
 }
 __global__ void k_select(const unsigned long long* rank, long long n, const unsigned long long* thrp, unsigned long long* nsel,
                          long long* sel, long long cap) {
@@ -785,7 +815,7 @@ Groups fetch_groups(RunCtx& rc, const Compacted& c) {
 
 // Device top-k candidates for ORDER BY <aggregate> LIMIT k: every group's sort
 // rank (raw int64 bits in the ExternalSort order, NULLs first) is computed on
-// the device; the q-th largest of a 4096-point sample, sorted on the device,
+// the device; the q-th largest of a 4096-point sample, found on the device,
 // is a threshold that keeps about 4·LIMIT + 64 groups; the groups at or above
 // it (ties included) are gathered, and the host finishes the stable sort on
 // them. Two copies back: the count, then the gathered groups. Returns false
@@ -822,7 +852,7 @@ bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
     // threshold: expected (q+1)·n/S groups at or above the q-th largest sample
     // (c.n > 4·limit + 4096 keeps q below S)
     const int q = (int)std::ceil((4.0 * o.limit + 64.0) * S / (double)c.n) - 1;
-    k_threshold<<<1, 1024, S * 8, rc.s>>>(samp, S, q, thr);
+    k_threshold<<<1, 1024, 0, rc.s>>>(samp, S, q, thr);
     launch_check(rc.s, "k_threshold");
     VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
     k_select<<<gr, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
