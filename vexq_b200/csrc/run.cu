@@ -322,31 +322,69 @@ __global__ void k_part_starts(const int* off, const int* hist, int np, int grid,
     }
 }
 
-// Packs each slot's chain start and length into one 8-byte probe read.
-// The probe's view of the build table: key and chain of a slot in one 16-byte
-// word pair; a key with a single build row carries the row id itself (count
-// word -1), which saves the probe its read of the row list.
-// Each key also gets a group number (positions claimed once per block, so
-// numbers are dense in 0..keys-1) and gkey[number] = its key's code (key -
-// koff) for plans that group by the join key; a one-row chain's count word is
-// ~number (negative), so the probe finds both its row and its group in the slot.
+// Positions for m items a thread holds, claimed once per block: an exclusive
+// scan of the threads' counts (warp shuffles, then the warps in order) and one
+// atomic on the counter. Every thread of the block calls it.
+__device__ __forceinline__ unsigned long long vq_claim_block_n(unsigned m, unsigned long long* ctr) {
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned long long base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    unsigned incl = m;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned tot = 0;
+        for (int w = 0; w < nw; w++) {
+            const unsigned c = wsum[w];
+            wsum[w] = tot;
+            tot += c;
+        }
+        base = tot ? atomicAdd(ctr, (unsigned long long)tot) : 0ull;
+    }
+    __syncthreads();
+    const unsigned long long pos = base + wsum[warp] + (incl - m);
+    __syncthreads();  // wsum and base are rewritten by the next call
+    return pos;
+}
+
+// The probe's slots, four a thread at block-size stride (coalesced). For plans grouping by
+// the join key (want_gid) each key also gets a group number (dense in
+// 0..keys-1, claimed once per block) and gkey[number] = its key's code (key -
+// koff); a one-row chain's count word is then ~number (negative), else -1, so
+// the probe finds the row, and the group, in the slot.
 __global__ void k_pack_slots(const unsigned long long* keys, const int* start, const int* count, const int* first,
-                             int* gid, unsigned long long* gkey, unsigned long long* ngid, long long koff,
+                             int want_gid, int* gid, unsigned long long* gkey, unsigned long long* ngid, long long koff,
                              ulonglong2* slots, long long n) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < n; b0 += stride) {  // block-uniform trip count
-        const long long i = b0 + threadIdx.x;
-        const int c = i < n ? count[i] : 0;
-        const unsigned long long g = vq_claim_block(c > 0, ngid);
-        if (i >= n) continue;
-        const int a = c == 1 ? first[i] : start[i];  // start is computed only when some key repeats
-        const int b = c == 1 ? ~(int)g : c;
-        // the last slot holds the key equal to the empty sentinel (its key word is a used flag)
-        const unsigned long long key = i == n - 1 ? VQ_EMPTY_KEY : keys[i];
-        slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
-        if (c > 0) {
-            gid[i] = (int)g;
-            gkey[g] = (unsigned long long)((long long)key - koff);
+    const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    for (long long b0 = (long long)blockIdx.x * blockDim.x * 4; b0 < n; b0 += stride) {  // block-uniform trip count
+        const long long i0 = b0 + threadIdx.x;
+        int c[4];
+        unsigned m = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const long long i = i0 + (long long)k * blockDim.x;
+            c[k] = i < n ? count[i] : 0;
+            m += c[k] > 0;
+        }
+        unsigned long long g = want_gid ? vq_claim_block_n(m, ngid) : 0ull;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const long long i = i0 + (long long)k * blockDim.x;
+            if (i >= n) break;
+            const int a = c[k] == 1 ? first[i] : start[i];  // start is computed only when some key repeats
+            const int b = c[k] == 1 ? (want_gid ? ~(int)g : -1) : c[k];
+            slots[i] = make_ulonglong2(keys[i], (unsigned long long)(unsigned)a | ((unsigned long long)(unsigned)b << 32));
+            if (want_gid && c[k] > 0) {
+                // the last slot holds the key equal to the empty sentinel (its key word is a used flag)
+                const unsigned long long key = i == n - 1 ? VQ_EMPTY_KEY : keys[i];
+                gid[i] = (int)g;
+                gkey[g] = (unsigned long long)((long long)key - koff);
+                g++;
+            }
         }
     }
 }
@@ -1382,9 +1420,9 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
                 }
                 rc.launches += 5;
             }
-            k_pack_slots<<<(int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16), 256, 0, rc.s>>>(
-                B.jkeys, B.jstart, B.jcount, B.jfirst, B.jgid, p.jt_gkey.as<unsigned long long>(), d_ngid, p.gid_koff,
-                p.jt_meta.as<ulonglong2>(), nslots);
+            k_pack_slots<<<(int)std::min<long long>((nslots + 1023) / 1024, (long long)sm_count() * 16), 256, 0, rc.s>>>(
+                B.jkeys, B.jstart, B.jcount, B.jfirst, p.join_gid ? 1 : 0, B.jgid, p.jt_gkey.as<unsigned long long>(), d_ngid,
+                p.gid_koff, p.jt_meta.as<ulonglong2>(), nslots);
             launch_check(rc.s, "k_pack_slots");
             VQ_CUDA(cudaGetLastError());
             VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
