@@ -188,3 +188,90 @@ def test_device_top_k_matches_oracle(gpu_lib, order_col, desc, limit):
             assert_rows_match(g.rows(), r.rows(), ordered=True)
     finally:
         op.close()
+
+
+def fused_aggs():
+    return [P.count_star("n"), P.sum_(P.col(3), "sq"), P.avg(P.col(3), "aq"), P.count(P.col(3), "cq"),
+            P.sum_(P.col(2), "sv"), P.avg(P.col(2), "av"), P.sum_(P.col(2) * (1 - P.col(2) / 1e6), "se"),
+            P.min_(P.col(3), "mn"), P.max_(P.col(3), "mx")]
+
+
+def test_merge_inside_the_scan_resets_between_runs(gpu_lib, monkeypatch):
+    """Sums of finite bounded floats, integer sums, integer MIN/MAX and counts:
+    the scan merges its own block partials (global accumulators, the last
+    block writes the row and restores the identities; forced here for six
+    groups, which by default keep the merge kernel). Repeated runs, runs over
+    sub-ranges of row groups and a run that prunes every row group each match
+    the oracle, so nothing of one run leaks into the next."""
+    X = gpu_lib
+    monkeypatch.setenv("VEXQ_TUNE", "rfuse=2")
+    n, rg = 400_000, 8192
+    valid = np.random.default_rng(8).random(n) > 0.1
+    iv = np.random.default_rng(9).integers(-500, 500, n)
+    host = key_table(n, 7, ivals=iv, valid=valid, rg=rg)
+    plan = P.AggPlan(P.col(4) <= P.lit("1998-09-02"), [0, 1], fused_aggs())
+    op = X.GpuHashAggregate(X.GpuTable(host), plan)
+    try:
+        assert "merge=in_scan" in op.explain(), op.explain()
+        ref = R.agg(R.RefTable(host), plan, workers=0)
+        first = op.run().rows()
+        assert_rows_match(first, ref.rows(), ordered=True)
+        assert_float_vs_exact(first, ref)
+        for _ in range(3):
+            assert op.run().rows() == first  # the same value each run, bit for bit
+        nrg = (n + rg - 1) // rg
+        rt = R.RefTable(host)
+        for a, b in ((0, 1), (3, 17), (nrg - 2, nrg), (5, 5)):
+            g = op.run(a, b)
+            assert_rows_match(g.rows(), R.agg(rt, plan, workers=0, rg_start=a, rg_end=b).rows(), ordered=True)
+        assert op.run().rows() == first
+    finally:
+        op.close()
+    none = P.AggPlan(P.col(4) < P.lit("1990-01-01"), [0, 1], fused_aggs())  # zone maps prune every row group
+    g, ex = run(X, host, none)
+    assert "merge=in_scan" in ex and g.rows() == R.agg(R.RefTable(host), none, workers=0).rows()
+
+
+def test_merge_inside_the_scan_agrees_with_the_merge_kernel(gpu_lib, monkeypatch):
+    """The same plan compiled with the separate merge kernel: integer entries
+    equal bit for bit, float sums within the float tolerance (the in-scan
+    merge adds the block partials exactly, the kernel with TwoSum)."""
+    X = gpu_lib
+    host = key_table(600_000, 10)
+    plan = P.AggPlan(None, [0, 1], fused_aggs())
+    monkeypatch.setenv("VEXQ_TUNE", "rfuse=2")
+    g1, ex1 = run(X, host, plan)
+    monkeypatch.setenv("VEXQ_TUNE", "rfuse=0")
+    g2, ex2 = run(X, host, plan)
+    assert "merge=in_scan" in ex1 and "merge=kernel" in ex2, (ex1, ex2)
+    assert_rows_match(g1.rows(), g2.rows(), ordered=True)
+    for a, b in zip(g1.rows(), g2.rows()):
+        assert [v for v in a if not isinstance(v, float)] == [v for v in b if not isinstance(v, float)]
+    r = R.agg(R.RefTable(host), plan, workers=0)
+    assert_float_vs_exact(g1.rows(), r)
+    assert_float_vs_exact(g2.rows(), r)
+
+
+def test_float_min_max_keep_the_merge_kernel(gpu_lib):
+    X = gpu_lib
+    host = key_table(50_000, 11)
+    g, ex = run(X, host, P.AggPlan(None, [0], [P.min_(P.col(2), "mn"), P.sum_(P.col(2), "s")]))
+    assert "merge=kernel" in ex, ex
+    r = R.agg(R.RefTable(host), P.AggPlan(None, [0], [P.min_(P.col(2), "mn"), P.sum_(P.col(2), "s")]), workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+
+
+def test_merge_placement_by_accumulator_count(gpu_lib, monkeypatch):
+    """Default placement: a one-group sum and count merges inside the scan;
+    six groups of eight accumulators keep the merge kernel."""
+    X = gpu_lib
+    monkeypatch.delenv("VEXQ_TUNE", raising=False)
+    host = key_table(200_000, 12)
+    small = P.AggPlan(P.col(4) <= P.lit("1997-01-01"), [], [P.sum_(P.col(2) * P.col(3), "s"), P.count_star("n")])
+    g, ex = run(X, host, small)
+    assert "merge=in_scan" in ex, ex
+    r = R.agg(R.RefTable(host), small, workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_float_vs_exact(g.rows(), r)
+    g, ex = run(X, host, P.AggPlan(None, [0, 1], fused_aggs()))
+    assert "merge=kernel" in ex, ex

@@ -1081,6 +1081,51 @@ static void choose_regs_forms(Plan& p) {
     }
 }
 
+// Register path: the per-block partials are merged inside the scan kernel
+// (each block adds its partials into global accumulators, the last block to
+// arrive writes the merged row) when every float accumulator is a SUM of
+// finite, bounded values: those partials add exactly as fixed-point integers
+// (the window of the dense path's exact sums), so the merged sums do not
+// depend on the order in which blocks finish, and integer sums, MIN, MAX and
+// first-row keys are order-free as atomics. Float MIN/MAX keep the merge
+// kernel, whose fold in block order keeps the first of two equal extremes
+// (+0 against -0), and so do plans with many accumulators, where the merge
+// kernel measured faster. VEXQ_TUNE "rfuse=0" keeps the merge kernel for
+// measurement, "rfuse=2" folds any eligible plan into the scan.
+static void choose_regs_fused(Plan& p) {
+    p.rfused = false;
+    if (p.path != AggPath::Regs || p.is_join || !p.t || p.nf > 16) return;
+    if (p.t->nrows > (int64_t(1) << 31)) return;  // the window holds sums of 2^31 rows
+    int force = 1;
+    if (const char* e = std::getenv("VEXQ_TUNE")) {
+        const char* at = std::strstr(e, "rfuse=");
+        if (at) force = std::atoi(at + 6);
+    }
+    if (force == 0) return;
+    // atomics a block adds: up to three fixed-point digits a float sum, one
+    // a counter. 6M-row scans: one group of 2 entries (5 atomics) 37.4 us in
+    // the scan against 39.5 us with the merge kernel; six groups of 8 (108)
+    // 66.5 us against 60.3 us (every block arrives at once, so the atomics
+    // on the same few L2 lines serialise)
+    const int64_t atomics = p.domain * (3 * (int64_t)p.nf + p.ni + 1);
+    if (atomics > 16 && force != 2) return;
+    std::vector<int> lsb(std::max(p.nf, 1), 0);
+    for (size_t s = 0; s < p.slots.size(); s++) {
+        const Slot& sl = p.slots[s];
+        if (sl.kind == S_FMIN || sl.kind == S_FMAX) return;
+        if (sl.kind != S_FSUM) continue;
+        if (!p.rfma[s] && !p.rdx[s]) return;  // a sum that may meet NaN or inf
+        const INode& x = p.ir[sl.input];
+        if (!x.bounded || !std::isfinite(x.lo) || !std::isfinite(x.hi)) return;
+        const double m = std::max(std::fabs(x.lo), std::fabs(x.hi));
+        int e = 0;
+        if (m > 0) std::frexp(m, &e);  // |x| <= m < 2^e
+        lsb[p.slot_pos[s]] = e - 97;
+    }
+    p.fx_lsb = lsb;
+    p.rfused = true;
+}
+
 // The predicated update of an aggregate scan writes first-row keys only on a
 // lane's first row of each group, so they live in a per-thread array (local
 // memory, written at most once per group) instead of registers.
@@ -1274,6 +1319,50 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
         os << "    if ((threadIdx.x & 31) == 0) sh_i[fw][" << g * (ni + 1) + ni << "] = fo" << g << ";\n";
     }
     os << "    __syncthreads();\n";
+    // merge folded into the scan (runs that pass the accumulators): the
+    // block's combined partials go to the global accumulators as atomics; the
+    // last block to arrive (threadfence before the arrival count, so every
+    // earlier block's atomics are visible to it) reads each accumulator back
+    // with an exchange that also restores its identity for the next run
+    const bool fused = p.rfused && !fc.dyn_smem;
+    if (fused) {
+        const int NF = std::max(nf, 1), NI1 = ni + 1;
+        os << "    if (P.racc_i) {\n";
+        os << "        for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
+        os << "            const int s = t % " << NF << ";\n";
+        os << "            double v = sh_f[0][t];\n";
+        os << "            for (int w = 1; w < " << warps << "; w++) v = vq_fcomb(" << fc.kinds << "fkind(s), v, sh_f[w][t]);\n";
+        os << "            vq_fx_add<true>(P.racc_fx + (long long)t * 4, v, P.fx_lsb[s], P.racc_sp + t, P.error);\n";
+        os << "        }\n";
+        os << "        for (int t = threadIdx.x; t < " << G * NI1 << "; t += blockDim.x) {\n";
+        os << "            const int s = t % " << NI1 << ";\n";
+        os << "            long long v = sh_i[0][t];\n";
+        os << "            for (int w = 1; w < " << warps << "; w++) v = vq_icomb(" << fc.kinds << "ikind(s), v, sh_i[w][t]);\n";
+        os << "            vq_racc_add(P.racc_i + t, " << fc.kinds << "ikind(s), v);\n";
+        os << "        }\n";
+        os << "        __threadfence();\n";
+        os << "        __syncthreads();\n";
+        os << "        __shared__ int vq_rlast;\n";
+        os << "        if (threadIdx.x == 0) vq_rlast = atomicAdd(P.racc_done, 1u) == gridDim.x - 1u;\n";
+        os << "        __syncthreads();\n";
+        os << "        if (vq_rlast) {\n";
+        os << "            __threadfence();\n";
+        os << "            for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
+        os << "                vq_i64 c[4];\n";
+        os << "#pragma unroll\n";
+        os << "                for (int d = 0; d < 4; d++) c[d] = (vq_i64)atomicExch((unsigned long long*)(P.racc_fx + (long long)t * 4 + d), 0ull);\n";
+        os << "                P.rout_f[t] = vq_fx_result(c, P.fx_lsb[t % " << NF << "], atomicExch(P.racc_sp + t, 0u));\n";
+        os << "            }\n";
+        os << "            for (int t = threadIdx.x; t < " << G * NI1 << "; t += blockDim.x)\n";
+        os << "                P.rout_i[t] = (long long)atomicExch((unsigned long long*)(P.racc_i + t), (unsigned long long)vq_racc_identity("
+           << fc.kinds << "ikind(t % " << NI1 << ")));\n";
+        os << "            if (threadIdx.x == 0) {\n";
+        os << "                *P.rerr_out = atomicExch(P.error, 0);\n";
+        os << "                atomicExch(P.racc_done, 0u);\n";
+        os << "            }\n";
+        os << "        }\n";
+        os << "    } else {\n";
+    }
     // fixed-order combine over warps; kinds per bank entry
     os << "    for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
     os << "        const int s = t % " << std::max(nf, 1) << ";\n";
@@ -1285,6 +1374,7 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
     os << "        long long v = sh_i[0][t];\n";
     os << "        for (int w = 1; w < " << warps << "; w++) v = vq_icomb(" << fc.kinds << "ikind(s), v, sh_i[w][t]);\n";
     os << "        P.part_i[(long long)(" << fc.part_index << ") * " << G * (ni + 1) << " + t] = v;\n    }\n";
+    if (fused) os << "    }\n";
 }
 
 // Atomic path: group table in global memory.
@@ -2517,6 +2607,13 @@ static void choose_tunables(Plan& p) {
     // than they save (67 / 82 us with one)
     p.cache_cnt32 = p.cache_fx32 = true;
     p.hot_n = 0;
+    // register path with many accumulators: three 128-thread blocks an SM
+    // (~148 registers a thread), too few loads in flight to fill HBM; a
+    // two-chunk cp.async pipeline a warp keeps the next chunk's columns in
+    // flight without registers. 6M-row Q1 shape (6 groups x 8 accumulators):
+    // 56.7 us against 59.8 us; with 40 warps an SM (one group) it costs
+    // occupancy instead (Q6 shape: 43.9 us against 37.6 us)
+    p.async_stages = p.path == AggPath::Regs && !p.is_join && acc > 24 ? 2 : 0;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -2527,7 +2624,8 @@ static void choose_tunables(Plan& p) {
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
         int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb="), ho = get("hot=");
-        int c32 = get("cnt32="), f32 = get("fx32=");
+        int c32 = get("cnt32="), f32 = get("fx32="), gs = get("gsm=");
+        if (gs >= 0) p.grid_per_sm = gs;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;
         if (ho >= 0 && p.path == AggPath::Dense && !p.is_join) p.hot_n = std::min(ho, VQ_MAXHOT);
@@ -2579,6 +2677,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     }
     choose_tunables(p);
     choose_regs_forms(p);
+    choose_regs_fused(p);
     // numeric literals become launch-time values (first VQ_MAXLITS of them)
     p.lits.clear();
     for (auto& n : p.ir) {
@@ -2652,9 +2751,11 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
             na += slot_alias(p, s) >= 0;
         }
         ex << " exact_int_sums=" << nx << " fma_sums=" << nm << " shared_sums=" << na;
+        ex << " merge=" << (p.rfused ? "in_scan" : "kernel");
     }
-    p.explain = ex.str();
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
+    ex << " regs=" << p.k_main.regs << " blocks_per_sm=" << p.k_main.max_blocks_per_sm;
+    p.explain = ex.str();
     if (join) {
         p.k_build = jit_get(p.src_build, "vq_build", kBlock, p.bsmem);
         // radix-partitioned join (exec/parallel_join.go:72-109): the partition

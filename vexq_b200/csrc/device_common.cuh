@@ -332,6 +332,15 @@ __device__ __host__ inline double vq_fx_value(const vq_i64* c, int lsb) {
     return neg ? -r : r;
 }
 
+// The value of an exact float sum: NaN when a NaN or both infinities were
+// added, else the infinity that was added, else the fixed-point total.
+__device__ __forceinline__ double vq_fx_result(const vq_i64* c, int lsb, unsigned sp) {
+    if ((sp & 1u) || (sp & 6u) == 6u) return __longlong_as_double(0x7FF8000000000001LL);
+    if (sp & 2u) return __longlong_as_double(0x7FF0000000000000LL);
+    if (sp & 4u) return __longlong_as_double((long long)0xFFF0000000000000ULL);
+    return vq_fx_value(c, lsb);
+}
+
 #define VQ_NOSLOT 0xFFFFFFFFFFFFFFFFull
 
 // Open-addressing insert (linear probing, atomicCAS on the key). The key equal
@@ -420,6 +429,18 @@ __device__ __forceinline__ double vq_fminr(double a, double b) { return b < a ? 
 __device__ __forceinline__ double vq_fmaxr(double a, double b) { return b > a ? b : a; }
 __device__ __forceinline__ double vq_fcomb(int kind, double a, double b) {
     return kind == 1 ? vq_fminr(a, b) : kind == 2 ? vq_fmaxr(a, b) : a + b;
+}
+// Register path with the merge folded into the scan: one block partial into
+// its global accumulator (kind 0 wrapping sum, 1 min, 2 max). A partial equal
+// to the kind's identity changes nothing and takes no atomic.
+__device__ __forceinline__ vq_i64 vq_racc_identity(int kind) {
+    return kind == 1 ? (vq_i64)0x7FFFFFFFFFFFFFFFLL : kind == 2 ? (vq_i64)(-0x7FFFFFFFFFFFFFFFLL - 1) : (vq_i64)0;
+}
+__device__ __forceinline__ void vq_racc_add(vq_i64* a, int kind, vq_i64 v) {
+    if (v == vq_racc_identity(kind)) return;
+    if (kind == 1) atomicMin(reinterpret_cast<long long*>(a), (long long)v);
+    else if (kind == 2) atomicMax(reinterpret_cast<long long*>(a), (long long)v);
+    else atomicAdd(reinterpret_cast<unsigned long long*>(a), (unsigned long long)v);
 }
 __device__ __forceinline__ vq_i64 vq_icomb(int kind, vq_i64 a, vq_i64 b) {
     return kind == 1 ? (b < a ? b : a) : kind == 2 ? (b > a ? b : a) : (vq_i64)((vq_u64)a + (vq_u64)b);

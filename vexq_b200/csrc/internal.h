@@ -119,6 +119,7 @@ struct JitKernel {
     int block = 256;
     int smem = 0;        // dynamic shared memory bytes
     int max_blocks_per_sm = 0;
+    int regs = 0;        // registers a thread
 };
 JitKernel jit_get(const std::string& source, const std::string& entry, int block, int smem = 0);
 void jit_launch(const JitKernel& k, int grid, const void* params, size_t params_size, cudaStream_t s);

@@ -36,6 +36,7 @@ struct Driver {
     PFN_cuLaunchKernel_v7000_ptsz launch = nullptr;
     PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor_v6050 occ = nullptr;
     PFN_cuFuncSetAttribute_v9000 setattr = nullptr;
+    PFN_cuFuncGetAttribute_v2020 getattr = nullptr;
     bool ok = false;
 };
 
@@ -50,7 +51,7 @@ Driver& drv() {
         d.ok = get("cuModuleLoadData", (void**)&d.load) && get("cuModuleUnload", (void**)&d.unload) &&
                get("cuModuleGetFunction", (void**)&d.get) && get("cuLaunchKernel", (void**)&d.launch) &&
                get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&d.occ) &&
-               get("cuFuncSetAttribute", (void**)&d.setattr);
+               get("cuFuncSetAttribute", (void**)&d.setattr) && get("cuFuncGetAttribute", (void**)&d.getattr);
     });
     if (!d.ok) fail(VEXQ_EDEVICE, "CUDA driver entry points unavailable");
     return d;
@@ -211,6 +212,8 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     }
     int nb = 0;
     if (d.occ(&nb, f, block, (size_t)smem) == CUDA_SUCCESS) k.max_blocks_per_sm = nb;
+    int regs = 0;
+    if (d.getattr(&regs, CU_FUNC_ATTRIBUTE_NUM_REGS, f) == CUDA_SUCCESS) k.regs = regs;
     return k;
 }
 

@@ -63,6 +63,16 @@ struct VQParams {
     const int* qrows;
     unsigned long long* qpay[8];   // probe columns used above the join, per probe entry (raw 8-byte words)
     unsigned char* qpayv[8];       // their validity (nullable columns)
+    // ---- register path with the merge folded into the scan (racc_i set):
+    //      every block adds its partials into these accumulators and the
+    //      last block to arrive writes the merged row and resets them ----
+    long long* racc_fx;            // [G][NF][4] fixed-point digits of the float sums
+    unsigned* racc_sp;             // [G][NF] non-finite flags (bit0 NaN, bit1 +inf, bit2 -inf)
+    long long* racc_i;             // [G][NI + 1] integer accumulators, first-row key last
+    unsigned* racc_done;           // blocks that have added their partials
+    double* rout_f;                // [G][NF] merged float entries
+    long long* rout_i;             // [G][NI + 1] merged integer entries
+    int* rerr_out;                 // the error word handed out with the merged row
     // ---- numeric literals of the plan's expressions (int64, date, float64 bits):
     //      plans that differ only in constants share one compiled kernel ----
     long long lit[VQ_MAXLITS];

@@ -139,6 +139,7 @@ struct Plan {
     int tile = 128, smem = 0;  // main kernel: rows per loop unit, dynamic shared memory
     int async_stages = 0;      // >1: per-warp cp.async pipeline of that many 128-row chunks
     int min_blocks = 0;        // >0: __launch_bounds__ minimum resident blocks per SM
+    int grid_per_sm = 0;       // >0: register path grid of at most this many blocks per SM
     // register-path accumulator forms, per slot (aggregate scans only):
     //  rdx    integer-valued sum (COUNT, integer SUM, float SUM of an integer
     //         input) kept as a double, exact while |sum| <= 2^53
@@ -146,6 +147,12 @@ struct Plan {
     //  rfma   float SUM of a never-NaN/inf value, updated as fma(v, hit, acc)
     std::vector<char> rdx, rfma;
     std::vector<int> ralias;
+    // register path, merge folded into the scan: blocks add their partials
+    // into global accumulators (float sums as exact fixed-point digits) and
+    // the last block writes the merged row; racc holds those accumulators
+    // (kept at their identities between runs) and the arrival counter
+    bool rfused = false;
+    DevBuf racc;
     // value-range epochs of the tables the plan was compiled against
     uint64_t range_epoch = 0, brange_epoch = 0;
     int btile = 128, bsmem = 0;  // join build kernel

@@ -7,6 +7,7 @@
 // global aggregate over no rows emits one row (aggregate.go:961-982), and
 // ExternalSort's comparison on raw int64 bits with NULLs first
 // (exec/sort.go:130-163) followed by Limit (exec/limit.go:20-50).
+#include <climits>
 #include <cstdlib>
 #include <algorithm>
 #include <chrono>
@@ -147,13 +148,8 @@ __device__ __forceinline__ void finalize_write(long long i, unsigned long long p
     o_first[pos] = first[i];
     for (int s = 0; s < ni; s++) o_i[(long long)s * cap_out + pos] = acc_i[(long long)s * nslots + i];
     for (int f = 0; f < nf; f++) {
-        unsigned sp = special[(long long)f * nslots + i];
-        double v;
-        if ((sp & 1u) || (sp & 6u) == 6u) v = __longlong_as_double(0x7FF8000000000001LL);
-        else if (sp & 2u) v = __longlong_as_double(0x7FF0000000000000LL);
-        else if (sp & 4u) v = __longlong_as_double((long long)0xFFF0000000000000ULL);
-        else v = vq_fx_value(acc_fx + ((long long)f * nslots + i) * 4, fx_lsb[f]);
-        o_f[(long long)f * cap_out + pos] = v;
+        o_f[(long long)f * cap_out + pos] =
+            vq_fx_result(acc_fx + ((long long)f * nslots + i) * 4, fx_lsb[f], special[(long long)f * nslots + i]);
     }
 }
 
@@ -560,8 +556,9 @@ double vq_fkey_inv_host(uint64_t k) {
 // Grid of a scan kernel: every SM filled to its occupancy, never more blocks
 // than loop units (staged kernels: one tile per block per iteration; chunk
 // loops: one 128-row chunk per warp).
-int grid_for(const JitKernel& k, long long units, bool staged) {
+int grid_for(const JitKernel& k, long long units, bool staged, int cap_per_sm = 0) {
     int per_sm = std::max(1, k.max_blocks_per_sm);
+    if (cap_per_sm > 0) per_sm = std::min(per_sm, cap_per_sm);
     long long want = staged ? units : (units + (k.block / 32) - 1) / (k.block / 32);
     long long g = std::min<long long>((long long)sm_count() * per_sm, want);
     return (int)std::max<long long>(g, 1);
@@ -637,12 +634,15 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     int G = (int)p.domain, nf = p.nf, ni = p.ni;
     int nfb = std::max(nf, 1);
     const JitKernel& K = rc.k ? *rc.k : p.k_main;
-    int grid = rc.k ? rc.grid : grid_for(p.k_main, nchunks, p.staged);
-    size_t pf = (size_t)grid * G * nfb, pi = (size_t)grid * G * (ni + 1);
-    p.scratch_a.ensure(pf * 8);
-    p.scratch_b.ensure(pi * 8);
-    P.part_f = p.scratch_a.as<double>();
-    P.part_i = p.scratch_b.as<long long>();
+    int grid = rc.k ? rc.grid : grid_for(p.k_main, nchunks, p.staged, p.grid_per_sm);
+    const bool fused = p.rfused && !rc.k;  // the scan merges its own partials
+    if (!fused) {
+        size_t pf = (size_t)grid * G * nfb, pi = (size_t)grid * G * (ni + 1);
+        p.scratch_a.ensure(pf * 8);
+        p.scratch_b.ensure(pi * 8);
+        P.part_f = p.scratch_a.as<double>();
+        P.part_i = p.scratch_b.as<long long>();
+    }
     if (!p.d_kinds.p) {  // combiner kind per bank entry (0 sum, 1 min, 2 max), uploaded once
         std::vector<int> k(nfb + ni + 1, 0);
         for (size_t s = 0; s < p.slots.size(); s++) {
@@ -669,12 +669,41 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     ensure_events(p);
     if (!p.regs_err_clean) VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
     p.regs_err_clean = false;  // until the merge below has run
+    if (fused) {
+        // accumulators at their identities: fixed-point digits and flags 0,
+        // integer entries by combiner kind, arrival count 0; the last block
+        // of every run restores this state
+        const size_t b_fx = (size_t)G * nf * 32, b_i = (size_t)G * (ni + 1) * 8, b_sp = (size_t)G * nf * 4;
+        if (!p.racc.p) {
+            std::vector<unsigned char> img(b_fx + b_i + b_sp + 16, 0);
+            std::vector<long long> ident(ni + 1, 0);
+            ident[ni] = LLONG_MAX;  // first-row key: min
+            for (size_t s = 0; s < p.slots.size(); s++) {
+                if (p.slots[s].is_float()) continue;
+                const int kd = p.slots[s].kind;
+                ident[p.slot_pos[s]] = kd == S_IMIN ? LLONG_MAX : kd == S_IMAX ? LLONG_MIN : 0;
+            }
+            long long* ii = (long long*)(img.data() + b_fx);
+            for (int gi = 0; gi < G; gi++)
+                for (int u = 0; u <= ni; u++) ii[(size_t)gi * (ni + 1) + u] = ident[u];
+            p.racc.alloc(img.size());
+            VQ_CUDA(cudaMemcpy(p.racc.p, img.data(), img.size(), cudaMemcpyHostToDevice));
+        }
+        unsigned char* base = p.racc.as<unsigned char>();
+        P.racc_fx = (long long*)base;
+        P.racc_i = (long long*)(base + b_fx);
+        P.racc_sp = (unsigned*)(base + b_fx + b_i);
+        P.racc_done = (unsigned*)(base + b_fx + b_i + b_sp);
+        P.rout_f = out_f;
+        P.rout_i = out_i;
+        P.rerr_out = err_out;
+    }
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(K, grid, &P, sizeof P, rc.s);
     launch_check(rc.s, "p.k_main");
     // no event between the scan and its merge: an event record there stops the
     // merge's launch from overlapping the scan's drain (measured 5-6 us a run)
-    {
+    if (!fused) {
         const int tot = G * nf + G * (ni + 1);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((tot + 7) / 8);
@@ -688,17 +717,18 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         VQ_CUDA(cudaLaunchKernelEx(&cfg, k_merge_regs_dep, (const double*)P.part_f, (const long long*)P.part_i, grid, G, nf,
                                    ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
     }
-    launch_check(rc.s, "k_merge_regs_dep");
+    if (!fused) launch_check(rc.s, "k_merge_regs_dep");
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
     VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
     p.regs_err_clean = true;
-    if (*(const int*)((const char*)p.h_stage.p + nout_f + nout_i) & 8)
-        fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
-    const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge overlapping its drain
+    const int herr = *(const int*)((const char*)p.h_stage.p + nout_f + nout_i);
+    if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+    if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
+    const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge (overlapping its drain, or inside it)
     rc.scan_ms += span;
     rc.kernel_ms += span;
-    rc.launches += 2;
+    rc.launches += fused ? 1 : 2;
     const double* hf = (const double*)p.h_stage.p;
     const long long* hi = (const long long*)((const char*)p.h_stage.p + nout_f);
     g.ival.assign(ni, {});
