@@ -47,6 +47,9 @@ enum {
     VEXQ_EDEVICE    = -5,    /* CUDA runtime / driver error                  */
     VEXQ_ECANCELED  = -125,  /* cancelled through vexq_cancel                */
     VEXQ_ENOTSUP    = -95,   /* feature outside the supported subset         */
+    VEXQ_ECORRUPT   = -74,   /* a .vxq file fails a checksum or does not parse
+                                (storage.ErrChecksum / ErrCorruptFooter /
+                                ErrBadMagic, storage/errors.go:9-17)         */
     VEXQ_EJIT       = -201   /* kernel specialisation failed to compile      */
 };
 
@@ -111,6 +114,33 @@ int32_t vexq_table_destroy(vexq_table_t t);
 int32_t vexq_table_num_row_groups(vexq_table_t t, int32_t* out);
 /* Device bytes held by the table (columns, bitmaps, dictionaries). */
 int32_t vexq_table_device_bytes(vexq_table_t t, int64_t* out);
+/* ---- .vxq files ------------------------------------------------------------
+ * Replaces storage.Open + ColumnReader.NextBlock / Dictionary + TableScan's
+ * block decode (storage/reader.go:175-190, 295-408; storage/rowgroup.go:101-
+ * 195; exec/scan.go:199-409) for a table that is then scanned on the GPU:
+ * the file's footer CRC and every block and dictionary CRC of the selected
+ * columns are checked (CRC-32/IEEE, internal/encoding/crc.go), the columns
+ * decoded on the host cores and uploaded as vexq_table_upload uploads them,
+ * the file's row groups becoming the table's (every row group but the last
+ * must hold the same number of rows, else VEXQ_ENOTSUP). `columns` names the
+ * columns to load, in the table's order; NULL loads every column. Corrupt
+ * files fail with VEXQ_ECORRUPT and a message naming the row group, column
+ * and file offset. */
+int32_t vexq_table_load_vxq(const char* path, const char* const* columns, int32_t ncolumns,
+                            vexq_table_t* out);
+/* Host-only check of a whole file (no device): footer, every block and
+ * dictionary CRC, RLE and dictionary structure, dictionary codes in range.
+ * The block checks `vexq fsck` makes (runFsck, cmd/vexq/main.go:241-330). */
+typedef struct {
+    int64_t nrows;
+    int32_t ncols;
+    int32_t n_rg;
+    int32_t rg_rows;        /* rows of every row group but the last */
+    int32_t null_columns;   /* columns holding at least one NULL     */
+    int64_t bytes_checked;  /* column section bytes read and verified */
+} vexq_vxq_summary;
+int32_t vexq_vxq_verify(const char* path, vexq_vxq_summary* out);
+
 /* Zone map of (column, row group): storage.ZoneMap (storage/schema.go:26-35). */
 typedef struct {
     int64_t  null_count;

@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvexqcuda.so")
 
 # ---- constants (same values as the header) ----------------------------------
-OK, EINVAL, ENOMEM, EADMIT, ETIMEDOUT, EDEVICE, ECANCELED, ENOTSUP, EJIT = (
-    0, -22, -12, -11, -110, -5, -125, -95, -201)
+OK, EINVAL, ENOMEM, EADMIT, ETIMEDOUT, EDEVICE, ECANCELED, ENOTSUP, EJIT, ECORRUPT = (
+    0, -22, -12, -11, -110, -5, -125, -95, -201, -74)
 
 TYPE_INT64, TYPE_FLOAT64, TYPE_BOOL, TYPE_STRING, TYPE_DATE = 1, 2, 3, 4, 5
 TYPE_NAMES = {1: "INT64", 2: "FLOAT64", 3: "BOOL", 4: "STRING", 5: "DATE"}
@@ -39,6 +39,17 @@ class ColumnDesc(C.Structure):
         ("dict_str_off", C.c_void_p),
         ("dict_bytes", C.c_void_p),
         ("dict_entries", C.c_int64),
+    ]
+
+
+class VxqSummary(C.Structure):
+    _fields_ = [
+        ("nrows", C.c_int64),
+        ("ncols", C.c_int32),
+        ("n_rg", C.c_int32),
+        ("rg_rows", C.c_int32),
+        ("null_columns", C.c_int32),
+        ("bytes_checked", C.c_int64),
     ]
 
 
@@ -128,7 +139,7 @@ EXPORTS = [
     "vexq_init", "vexq_last_error", "vexq_abi_version",
     "vexq_table_upload", "vexq_table_destroy", "vexq_table_num_row_groups",
     "vexq_table_device_bytes", "vexq_table_zone_map", "vexq_table_dict_size",
-    "vexq_table_dict_entry",
+    "vexq_table_dict_entry", "vexq_table_load_vxq", "vexq_vxq_verify",
     "vexq_agg_plan_create", "vexq_join_plan_create", "vexq_plan_destroy",
     "vexq_plan_explain", "vexq_zone_prune", "vexq_plan_run", "vexq_plan_run_host",
     "vexq_result_num_rows", "vexq_result_num_cols", "vexq_result_next",
@@ -176,6 +187,8 @@ def load() -> C.CDLL:
         "vexq_table_num_row_groups": (i32, [vp, C.POINTER(i32)]),
         "vexq_table_device_bytes": (i32, [vp, C.POINTER(i64)]),
         "vexq_table_zone_map": (i32, [vp, i32, i32, C.POINTER(ZoneMap)]),
+        "vexq_table_load_vxq": (i32, [C.c_char_p, C.POINTER(C.c_char_p), i32, C.POINTER(vp)]),
+        "vexq_vxq_verify": (i32, [C.c_char_p, C.POINTER(VxqSummary)]),
         "vexq_table_dict_size": (i32, [vp, i32, C.POINTER(i32)]),
         "vexq_table_dict_entry": (i32, [vp, i32, i32, C.POINTER(C.c_char_p), C.POINTER(i32)]),
         "vexq_agg_plan_create": (i32, [vp, C.POINTER(AggPlanDesc), C.POINTER(vp)]),

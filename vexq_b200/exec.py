@@ -18,9 +18,10 @@ Every call goes to the CUDA library; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import struct
 from dataclasses import dataclass
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -59,6 +60,37 @@ class GpuTable:
         self.host = t
         self.h = C.c_void_p()
         abi.check(abi.load().vexq_table_upload(t.descs(), len(t.columns), t.nrows, t.rg_rows, C.byref(self.h)))
+
+    @classmethod
+    def from_vxq(cls, path: str, columns: Optional[Sequence[str]] = None) -> "GpuTable":
+        """Loads a .vxq file (all columns, or those named, in that order)
+        straight into HBM: storage.Open + TableScan's decode for the GPU."""
+        init()
+        self = cls.__new__(cls)
+        self.host = None
+        self.h = C.c_void_p()
+        names = None
+        if columns is not None:
+            names = (C.c_char_p * max(len(columns), 1))(*[c.encode() for c in columns])
+        abi.check(abi.load().vexq_table_load_vxq(os.fsencode(path), names, 0 if columns is None else len(columns),
+                                                 C.byref(self.h)))
+        return self
+
+    def num_row_groups(self) -> int:
+        v = C.c_int32()
+        abi.check(abi.load().vexq_table_num_row_groups(self.h, C.byref(v)))
+        return v.value
+
+    def dict_entries(self, col: int) -> List[str]:
+        """The global dictionary of a STRING column, in code order."""
+        n = C.c_int32()
+        abi.check(abi.load().vexq_table_dict_size(self.h, col, C.byref(n)))
+        out = []
+        for i in range(n.value):
+            p, ln = C.c_char_p(), C.c_int32()
+            abi.check(abi.load().vexq_table_dict_entry(self.h, col, i, C.byref(p), C.byref(ln)))
+            out.append(C.string_at(p, ln.value).decode() if ln.value else "")
+        return out
 
     def zone_map(self, col: int, rg: int) -> abi.ZoneMap:
         z = abi.ZoneMap()
