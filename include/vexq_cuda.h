@@ -245,6 +245,19 @@ int32_t vexq_agg_plan_create(vexq_table_t t, const vexq_agg_plan_desc* d, vexq_p
 int32_t vexq_join_plan_create(vexq_table_t build, vexq_table_t probe,
                               const vexq_join_plan_desc* d, vexq_plan_t* out);
 int32_t vexq_plan_destroy(vexq_plan_t p);
+/* HAVING over the merged aggregate: the Filter the planner puts above the
+ * aggregate (planner/build.go:59-75), evaluated with the WHERE expression
+ * rules (exec/filter.go:49-78) over the plan's output columns — group-by
+ * columns, then aggregates, in order — before ORDER BY / LIMIT. Node COLUMN
+ * indices are output column indices. Then only the first `visible` output
+ * columns are kept (-1: all), dropping the hidden aggregates the planner
+ * appends for a HAVING aggregate missing from the SELECT list
+ * (rewriteHavingAggs / buildHavingProjection, planner/build.go:512-637).
+ * predicate = -1 removes the HAVING. Plans with HAVING return every group
+ * to the host before the sort (no device top-k). */
+int32_t vexq_plan_set_having(vexq_plan_t p, const vexq_expr* nodes, int32_t nnodes,
+                             const int32_t* children, int32_t nchildren, int32_t predicate,
+                             int32_t visible);
 /* Short description of the chosen strategy (for logs and tests). */
 const char* vexq_plan_explain(vexq_plan_t p);
 

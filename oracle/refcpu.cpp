@@ -2173,6 +2173,90 @@ int32_t ref_filter_run(ref_table_t t, const vexq_expr* nodes, int32_t nnodes, co
     });
 }
 
+// HAVING (planner/build.go:59-75): the Filter above the aggregate runs over
+// the aggregate's output batches with the WHERE machinery, so the output
+// columns become a one-row-group table scanned and filtered like any other;
+// then buildHavingProjection keeps the first `visible` columns
+// (planner/build.go:617-637) and ExternalSort + Limit run on what is left.
+int32_t ref_result_having(ref_result_t r, const vexq_expr* nodes, int32_t nnodes, const int32_t* children,
+                          int32_t nchildren, int32_t predicate, int32_t visible, const vexq_order_desc* order) {
+    return guarded([&]() -> int32_t {
+        const int64_t n = r->rows;
+        Table t;
+        t.nrows = n;
+        t.rg_rows = (int)std::max<int64_t>(n, 1);
+        t.n_rg = n > 0 ? 1 : 0;
+        for (const OutCol& oc : r->cols) {
+            Column col;
+            col.name = oc.name;
+            col.type = oc.type;
+            col.nullable = true;
+            col.valid = oc.valid;
+            switch (oc.type) {
+                case VEXQ_TYPE_INT64: col.i64 = oc.bits; break;
+                case VEXQ_TYPE_FLOAT64:
+                    col.f64.resize(n);
+                    for (int64_t i = 0; i < n; i++) col.f64[i] = bitsToF(oc.bits[i]);
+                    break;
+                case VEXQ_TYPE_DATE:
+                    col.i32.resize(n);
+                    for (int64_t i = 0; i < n; i++) col.i32[i] = (int32_t)oc.bits[i];
+                    break;
+                case VEXQ_TYPE_BOOL:
+                    col.b8.resize(n);
+                    for (int64_t i = 0; i < n; i++) col.b8[i] = oc.bits[i] != 0;
+                    break;
+                case VEXQ_TYPE_STRING: {  // newStringVector: the batch's strings in first-occurrence order
+                    auto dict = std::make_shared<Dict>();
+                    col.codes.assign(n, 0);
+                    for (int64_t i = 0; i < n; i++)
+                        if (oc.valid[i]) col.codes[i] = dict->add(oc.strs[i]);
+                    if (t.n_rg) col.dicts.push_back(dict);
+                    break;
+                }
+                default: throw Error("unknown output column type");
+            }
+            t.cols.push_back(std::move(col));
+        }
+        computeZones(t);
+        std::vector<int64_t> keep;
+        if (predicate >= 0) {
+            Nodes N{nodes, nnodes, children, nchildren};
+            Schema sch = tableSchema(t);
+            XP pred = build(N, predicate, sch);
+            if (pred->type != VEXQ_TYPE_BOOL) throw Error("HAVING predicate must return BOOL");
+            Scan sc(&t);
+            Batch b;
+            for (int64_t s0 = 0; s0 < n; s0 += kBlockRows) {
+                const int m = (int)std::min<int64_t>(kBlockRows, n - s0);
+                sc.load(0, s0, m, b);
+                selectInto(b, eval(pred.get(), b));
+                for (uint16_t i : b.sel) keep.push_back(s0 + i);
+            }
+        } else {
+            for (int64_t i = 0; i < n; i++) keep.push_back(i);
+        }
+        for (auto& c : r->cols) {
+            OutCol k = c;
+            k.bits.resize(keep.size());
+            k.valid.resize(keep.size());
+            k.strs.resize(keep.size());
+            k.exact.resize(keep.size());
+            for (size_t j = 0; j < keep.size(); j++) {
+                k.bits[j] = c.bits[keep[j]];
+                k.valid[j] = c.valid[keep[j]];
+                k.strs[j] = c.strs[keep[j]];
+                k.exact[j] = c.exact[keep[j]];
+            }
+            c = std::move(k);
+        }
+        r->rows = (int64_t)keep.size();
+        if (visible >= 0 && visible < (int)r->cols.size()) r->cols.resize(visible);
+        if (order) applyOrder(r, *order);
+        return VEXQ_OK;
+    });
+}
+
 int64_t ref_result_rows(ref_result_t r) { return r ? r->rows : 0; }
 int32_t ref_result_cols(ref_result_t r) { return r ? (int32_t)r->cols.size() : 0; }
 int32_t ref_result_col_type(ref_result_t r, int32_t col) { return r->cols[col].type; }

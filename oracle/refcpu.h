@@ -58,6 +58,10 @@ int32_t ref_result_get(ref_result_t r, int64_t row, int32_t col, int64_t* bits,
 /* Exact sum (correctly rounded, Shewchuk) of the float aggregate inputs per
  * output row, for SUM/AVG columns; NaN for others. Serial results only. */
 int32_t ref_result_exact(ref_result_t r, int64_t row, int32_t col, double* out);
+/* HAVING over a result, then the column cut and ORDER BY / LIMIT. */
+int32_t ref_result_having(ref_result_t r, const vexq_expr* nodes, int32_t nnodes,
+                          const int32_t* children, int32_t nchildren, int32_t predicate,
+                          int32_t visible, const vexq_order_desc* order);
 void    ref_result_free(ref_result_t r);
 const char* ref_last_error(void);
 

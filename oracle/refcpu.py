@@ -56,6 +56,9 @@ def lib() -> C.CDLL:
         L.ref_result_exact.argtypes = [vp, i64, i32, C.POINTER(C.c_double)]
         L.ref_result_exact.restype = i32
         L.ref_result_free.argtypes = [vp]
+        L.ref_result_having.argtypes = [vp, C.POINTER(abi.Expr), i32, C.POINTER(i32), i32, i32, i32,
+                                        C.POINTER(abi.OrderDesc)]
+        L.ref_result_having.restype = i32
         L.ref_last_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -126,6 +129,34 @@ class RefResult:
 def agg(table: RefTable, plan, workers: int = 0, rg_start: int = 0, rg_end: int = -1) -> RefResult:
     h = C.c_void_p()
     _check(lib().ref_agg_run(table.h, C.byref(plan.desc), rg_start, rg_end, workers, C.byref(h)))
+    return RefResult(h)
+
+
+def _having(h, having, visible: int, order):
+    from vexq_b200.plan import predicate_arrays
+    keep, nodes, nn, ch, nc, root = predicate_arrays(having)
+    o = abi.OrderDesc(*order) if order is not None else abi.OrderDesc(-1, 0, -1)
+    try:
+        _check(lib().ref_result_having(h, nodes, nn, ch, nc, root, visible, C.byref(o)))
+    except Exception:
+        lib().ref_result_free(h)
+        raise
+
+
+def agg_having(table: RefTable, plan, having, visible: int = -1, order=None, workers: int = 0) -> RefResult:
+    """The aggregate of `plan` (which must carry no ORDER BY / LIMIT), then
+    HAVING, the column cut and `order` = (column, descending, limit)."""
+    h = C.c_void_p()
+    _check(lib().ref_agg_run(table.h, C.byref(plan.desc), 0, -1, workers, C.byref(h)))
+    _having(h, having, visible, order)
+    return RefResult(h)
+
+
+def join_having(build: RefTable, probe: RefTable, plan, having, visible: int = -1, order=None,
+                workers: int = 0) -> RefResult:
+    h = C.c_void_p()
+    _check(lib().ref_join_run(build.h, probe.h, C.byref(plan.desc), workers, C.byref(h)))
+    _having(h, having, visible, order)
     return RefResult(h)
 
 

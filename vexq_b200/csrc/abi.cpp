@@ -160,6 +160,16 @@ int32_t vexq_plan_destroy(vexq_plan_t p) {
 
 const char* vexq_plan_explain(vexq_plan_t p) { return p ? p->p->explain.c_str() : ""; }
 
+int32_t vexq_plan_set_having(vexq_plan_t p, const vexq_expr* nodes, int32_t nnodes, const int32_t* children,
+                             int32_t nchildren, int32_t predicate, int32_t visible) {
+    return guard([&]() -> int32_t {
+        if (!p) fail(VEXQ_EINVAL, "null plan");
+        std::lock_guard<std::mutex> lk(plan_mutex(p->p));
+        set_having(*p->p, nodes, nnodes, children, nchildren, predicate, visible);
+        return VEXQ_OK;
+    });
+}
+
 int32_t vexq_zone_prune(vexq_plan_t p, uint8_t* out_mask, int32_t n_rg) {
     return guard([&]() -> int32_t {
         if (!p || !out_mask) fail(VEXQ_EINVAL, "null argument");

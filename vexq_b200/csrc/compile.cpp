@@ -2976,6 +2976,51 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
 // Standalone filter (Filter.Next + BoolToSelVecInto, exec/filter.go:49-78):
 // each lane evaluates four rows; warp ballots assemble a 128-row selection
 // bitmap (bit = row passes: predicate true AND valid) per chunk.
+// HAVING (planner/build.go:59-75, 512-637): exec.Filter over the
+// aggregate's output batches, so the predicate is translated with the WHERE
+// rules (coercion, StringEqExpr, casts) against the output schema — group-by
+// columns, then aggregates — and evaluated per output row before ORDER BY /
+// LIMIT; then only the first `visible` columns are kept (the hidden
+// aggregates the planner appends for HAVING are projected away).
+void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int root, int visible) {
+    const int nout = (int)(p.keys.size() + p.outs.size());
+    p.having_ir.clear();
+    p.having_schema.reset();
+    p.having_root = -1;
+    p.having_visible = -1;
+    if (root < 0) return;
+    if (visible < -1 || visible > nout) fail(VEXQ_EINVAL, "HAVING keeps more columns than the aggregate outputs");
+    if (!nodes || nnodes <= 0) fail(VEXQ_EINVAL, "HAVING without expression nodes");
+    auto schema = std::make_unique<Table>();
+    schema->cols.resize(nout);
+    for (size_t k = 0; k < p.keys.size(); k++) {
+        const KeyCol& kc = p.keys[k];
+        Column& c = schema->cols[k];
+        const Table* src = kc.build ? p.bt : p.t;
+        c.name = kc.name.empty() ? src->cols[kc.col].name : kc.name;
+        c.type = kc.type;
+        c.nullable = true;
+        c.per_rg_dicts = false;
+        if (kc.type == VEXQ_TYPE_STRING) c.dict = src->cols[kc.col].dict;
+    }
+    for (size_t a = 0; a < p.outs.size(); a++) {
+        Column& c = schema->cols[p.keys.size() + a];
+        c.name = p.outs[a].name;
+        c.type = p.outs[a].out_type;
+        c.nullable = true;
+        c.per_rg_dicts = false;
+    }
+    Plan hp;
+    hp.t = schema.get();
+    Translator tr{hp, nodes, nnodes, children, nchildren, schema.get(), nullptr};
+    const int r = tr.tr(root);
+    if (hp.ir[r].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "HAVING is not a boolean expression");
+    p.having_ir = std::move(hp.ir);
+    p.having_root = r;
+    p.having_visible = visible;
+    p.having_schema = std::move(schema);
+}
+
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred) {
     std::unique_ptr<Plan> p(new Plan);
     p->t = t;

@@ -68,6 +68,7 @@ size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64_t* out_values, uint8_t* out_valid,
                         int32_t n_out) {
     if (p.is_join) fail(VEXQ_ENOTSUP, "the no-allocation run takes aggregate plans over one table, not joins");
+    if (p.having_root >= 0) fail(VEXQ_ENOTSUP, "the no-allocation run takes aggregates without HAVING");
     check_ranges(p);
     if (!p.keys.empty() || p.path != AggPath::Regs || p.domain != 1)
         fail(VEXQ_ENOTSUP, "the no-allocation run takes aggregates without GROUP BY");

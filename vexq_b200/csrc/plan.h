@@ -153,6 +153,15 @@ struct Plan {
     // (kept at their identities between runs) and the arrival counter
     bool rfused = false;
     DevBuf racc;
+    // HAVING over the merged output (exec.Filter above the aggregate,
+    // planner/build.go:59-75): predicate IR over the output columns (group-by
+    // columns, then aggregates) typed by a host-only schema table, and the
+    // number of leading output columns kept (buildHavingProjection,
+    // planner/build.go:617-637); -1: none
+    std::vector<INode> having_ir;
+    int having_root = -1;
+    int having_visible = -1;
+    std::unique_ptr<Table> having_schema;
     // value-range epochs of the tables the plan was compiled against
     uint64_t range_epoch = 0, brange_epoch = 0;
     int btile = 128, bsmem = 0;  // join build kernel
@@ -215,6 +224,7 @@ struct OutColumn {
 Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d);
 Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d);
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred);
+void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int root, int visible);
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
 // Copies the plan's launch-time constants (literals, float-sum windows, cache size) into P.
 void set_plan_constants(const Plan& p, VQParams& P);

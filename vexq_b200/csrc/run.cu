@@ -894,7 +894,8 @@ bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
     const vexq_order_desc& o = p.order;
     int ngb = (int)p.keys.size();
     const long long kCap = 65536;
-    if (o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096) return false;
+    // HAVING filters groups before the sort: every group comes back
+    if (p.having_root >= 0 || o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096) return false;
     const AggOut& a = p.outs[o.sort_col - ngb];
     int vslot = a.value_slot;
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
@@ -956,6 +957,153 @@ bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
 
 // Decodes group keys, computes aggregate outputs, orders groups, and applies
 // ORDER BY / LIMIT.
+// HAVING evaluation over one output row: the IR semantics of the scan
+// kernels' expression code (validity and value per node: comparisons and
+// arithmetic propagate NULL; AND/OR combine values and validity bitwise;
+// NOT flips valid bits; float x/0 is NaN and integer x/0 is 0; IN tests the
+// value set; CASE takes the first true branch), over the output columns.
+struct HVal {
+    bool ok = false, b = false;
+    int64_t i = 0;
+    double d = 0;
+};
+
+static HVal having_eval(const std::vector<INode>& ir, int idx, const std::vector<OutColumn>& cols, size_t row) {
+    const INode& n = ir[idx];
+    HVal v;
+    auto E = [&](int k) { return having_eval(ir, n.ch[k], cols, row); };
+    switch (n.k) {
+        case NK::Col: {
+            const OutColumn& c = cols[n.col];
+            v.ok = c.valid[row] != 0;
+            const int64_t raw = c.v[row];
+            switch (n.type) {
+                case VEXQ_TYPE_FLOAT64: std::memcpy(&v.d, &raw, 8); break;
+                case VEXQ_TYPE_DATE: v.i = (int32_t)raw; break;
+                case VEXQ_TYPE_BOOL: v.b = v.ok && raw != 0; break;
+                case VEXQ_TYPE_STRING: v.i = (uint32_t)raw; break;
+                default: v.i = raw; break;
+            }
+            return v;
+        }
+        case NK::Lit:
+            v.ok = true;
+            if (n.type == VEXQ_TYPE_FLOAT64) v.d = n.lf;
+            else if (n.type == VEXQ_TYPE_DATE) v.i = n.ld;
+            else if (n.type == VEXQ_TYPE_BOOL) v.b = n.lb;
+            else if (n.type == VEXQ_TYPE_INT64) v.i = n.li;
+            return v;
+        case NK::Cmp: {
+            const HVal a = E(0), b = E(1);
+            v.ok = a.ok && b.ok;
+            const bool fl = ir[n.ch[0]].type == VEXQ_TYPE_FLOAT64;
+            bool c = false;
+            switch (n.op) {
+                case VEXQ_OP_EQ: c = fl ? a.d == b.d : a.i == b.i; break;
+                case VEXQ_OP_NE: c = fl ? a.d != b.d : a.i != b.i; break;
+                case VEXQ_OP_LT: c = fl ? a.d < b.d : a.i < b.i; break;
+                case VEXQ_OP_LE: c = fl ? a.d <= b.d : a.i <= b.i; break;
+                case VEXQ_OP_GT: c = fl ? a.d > b.d : a.i > b.i; break;
+                case VEXQ_OP_GE: c = fl ? a.d >= b.d : a.i >= b.i; break;
+            }
+            v.b = v.ok && c;
+            return v;
+        }
+        case NK::Arith: {
+            const HVal a = E(0), b = E(1);
+            v.ok = a.ok && b.ok;
+            if (!v.ok) return v;
+            if (n.type == VEXQ_TYPE_FLOAT64) {
+                switch (n.op) {
+                    case VEXQ_OP_ADD: v.d = a.d + b.d; break;
+                    case VEXQ_OP_SUB: v.d = a.d - b.d; break;
+                    case VEXQ_OP_MUL: v.d = a.d * b.d; break;
+                    case VEXQ_OP_DIV: {  // applyArithFloat64: x/0 → math.NaN()
+                        if (b.d == 0.0) { const int64_t nan = 0x7FF8000000000001LL; std::memcpy(&v.d, &nan, 8); }
+                        else v.d = a.d / b.d;
+                        break;
+                    }
+                }
+            } else {
+                const uint64_t x = (uint64_t)a.i, y = (uint64_t)b.i;
+                switch (n.op) {
+                    case VEXQ_OP_ADD: v.i = (int64_t)(x + y); break;
+                    case VEXQ_OP_SUB: v.i = (int64_t)(x - y); break;
+                    case VEXQ_OP_MUL: v.i = (int64_t)(x * y); break;
+                    case VEXQ_OP_DIV: v.i = b.i == 0 ? 0 : b.i == -1 ? (int64_t)(0ull - x) : a.i / b.i; break;
+                }
+            }
+            return v;
+        }
+        case NK::Cast: {
+            const HVal a = E(0);
+            v.ok = a.ok;
+            v.d = (double)a.i;
+            return v;
+        }
+        case NK::And:
+        case NK::Or: {
+            const bool isand = n.k == NK::And;
+            for (size_t k = 0; k < n.ch.size(); k++) {
+                const HVal a = E((int)k);
+                if (k == 0) { v.b = a.b; v.ok = a.ok; }
+                else if (isand) { v.b = v.b && a.b; v.ok = v.ok && a.ok; }
+                else { v.b = v.b || a.b; v.ok = v.ok || a.ok; }
+            }
+            return v;
+        }
+        case NK::Not: {
+            const HVal a = E(0);
+            v.ok = a.ok;
+            v.b = a.b != a.ok;
+            return v;
+        }
+        case NK::IsNull:
+        case NK::IsNotNull: {
+            const HVal a = E(0);
+            v.ok = true;
+            v.b = n.k == NK::IsNull ? !a.ok : a.ok;
+            return v;
+        }
+        case NK::InInt:
+        case NK::InFloat: {
+            const HVal a = E(0);
+            v.ok = a.ok;
+            bool in = false;
+            if (n.k == NK::InInt) { for (auto x : n.seti) in = in || a.i == x; }
+            else { for (auto x : n.setf) in = in || a.d == x; }
+            v.b = a.ok && in;
+            return v;
+        }
+        case NK::InFalse:
+            v.ok = E(0).ok;
+            return v;
+        case NK::InCodes: {
+            const HVal a = E(0);
+            v.ok = a.ok;
+            v.b = a.ok && (uint64_t)a.i < n.codes.size() && n.codes[(size_t)a.i];
+            return v;
+        }
+        case NK::StrEq: {
+            if (n.streq_code < 0) { v.ok = v.b = n.negate; return v; }  // literal in no dictionary
+            const HVal a = E(0);
+            v.ok = a.ok;
+            v.b = a.ok && ((a.i == n.streq_code) != n.negate);
+            return v;
+        }
+        case NK::Case: {
+            const int nw = (int)(n.ch.size() - (n.has_else ? 1 : 0)) / 2;
+            for (int w = 0; w < nw; w++) {
+                const HVal c = E(2 * w);
+                if (c.ok && c.b) return E(2 * w + 1);
+            }
+            if (n.has_else) return E((int)n.ch.size() - 1);
+            return v;
+        }
+    }
+    return v;
+}
+
 vexq_result_s* build_result(Plan& p, Groups& g) {
     auto* r = new vexq_result_s;
     size_t n = g.n();
@@ -1033,6 +1181,25 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
             }
         }
         r->cols.push_back(std::move(oc));
+    }
+    // HAVING: keep the rows whose predicate is true and valid, then drop the
+    // hidden columns
+    if (p.having_root >= 0) {
+        std::vector<size_t> keep;
+        for (size_t j = 0; j < rows; j++) {
+            const HVal h = having_eval(p.having_ir, p.having_root, r->cols, j);
+            if (h.ok && h.b) keep.push_back(j);
+        }
+        if (keep.size() != rows) {
+            for (auto& c : r->cols) {
+                for (size_t j = 0; j < keep.size(); j++) { c.v[j] = c.v[keep[j]]; c.valid[j] = c.valid[keep[j]]; }
+                c.v.resize(keep.size());
+                c.valid.resize(keep.size());
+            }
+            rows = keep.size();
+            r->nrows = (int64_t)rows;
+        }
+        if (p.having_visible >= 0 && p.having_visible < (int)r->cols.size()) r->cols.resize(p.having_visible);
     }
     // ORDER BY (stable, raw int64 bits, NULLs first) + LIMIT
     const vexq_order_desc& o = p.order;

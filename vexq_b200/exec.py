@@ -233,6 +233,14 @@ class _PlanOp:
             pass
 
 
+def _set_having(h, plan):
+    hv = getattr(plan, "having", None)
+    if hv is None:
+        return
+    _, nodes, nn, ch, nc, root, visible = hv
+    abi.check(abi.load().vexq_plan_set_having(h, nodes, nn, ch, nc, root, visible))
+
+
 class GpuHashAggregate(_PlanOp):
     """Filter → (Project) → HashAggregate over one table; also stands in for
     ParallelHashAggregate (numWorkers/morselSize have no GPU meaning)."""
@@ -241,6 +249,7 @@ class GpuHashAggregate(_PlanOp):
         self.table, self.plan = table, plan
         self.h = C.c_void_p()
         abi.check(abi.load().vexq_agg_plan_create(table.h, C.byref(plan.desc), C.byref(self.h)))
+        _set_having(self.h, plan)
 
     def zone_prune(self) -> List[int]:
         n = self.table.host.n_rg
@@ -254,6 +263,7 @@ class GpuParallelHashJoinAggregate(_PlanOp):
         self.build, self.probe, self.plan = build, probe, plan
         self.h = C.c_void_p()
         abi.check(abi.load().vexq_join_plan_create(build.h, probe.h, C.byref(plan.desc), C.byref(self.h)))
+        _set_having(self.h, plan)
 
 
 class GpuFilter:

@@ -215,9 +215,11 @@ class AggPlan:
     """Filter → (Project) → HashAggregate over one table."""
 
     def __init__(self, predicate: Optional[E], group_by: Sequence[int], aggs: Sequence[Agg],
-                 order_col: int = -1, descending: bool = False, limit: int = -1):
+                 order_col: int = -1, descending: bool = False, limit: int = -1,
+                 having: Optional[E] = None, visible: int = -1):
         self.predicate, self.group_by, self.aggs = predicate, list(group_by), list(aggs)
         self.order = (order_col, descending, limit)
+        self.having = having_arrays(having, visible)
         a = _Arena()
         pred = a.add(predicate)
         aggarr = _aggs(a, self.aggs)
@@ -235,8 +237,9 @@ class JoinPlan:
     def __init__(self, build_key: int, probe_key: int, build_predicate: Optional[E],
                  probe_predicate: Optional[E], residual: Optional[E], group_by: Sequence[int],
                  aggs: Sequence[Agg], order_col: int = -1, descending: bool = False,
-                 limit: int = -1, radix_bits: int = -1):
+                 limit: int = -1, radix_bits: int = -1, having: Optional[E] = None, visible: int = -1):
         self.group_by, self.aggs = list(group_by), list(aggs)
+        self.having = having_arrays(having, visible)
         a = _Arena()
         bp, pp, rp = a.add(build_predicate), a.add(probe_predicate), a.add(residual)
         aggarr = _aggs(a, self.aggs)
@@ -247,6 +250,18 @@ class JoinPlan:
         self.desc = abi.JoinPlanDesc(nodes, nn, ch, nc, build_key, probe_key, bp, pp, rp, gb,
                                      len(self.group_by), aggarr, len(self.aggs),
                                      abi.OrderDesc(order_col, int(descending), limit), radix_bits)
+
+
+def having_arrays(having: Optional[E], visible: int = -1):
+    """HAVING (vexq_plan_set_having): a predicate over the output columns
+    (group-by columns, then aggregates) and how many leading output columns
+    to keep; None when there is no HAVING."""
+    if having is None:
+        return None
+    a = _Arena()
+    root = a.add(having)
+    nodes, nn, ch, nc = a.arrays()
+    return (a, nodes, nn, ch, nc, root, visible)
 
 
 def predicate_arrays(pred: E):
