@@ -143,3 +143,57 @@ def test_empty_and_one_row_files(gpu_lib, tmp_path, n):
             op.close()
     finally:
         t.close()
+
+
+def test_row_groups_not_a_multiple_of_eight_rows(gpu_lib, tmp_path):
+    """Row groups of 100 rows: blocks start mid-byte in the table's bitmaps,
+    so the device writes their validity bit by bit."""
+    X = gpu_lib
+    host = mixed_table(100 * 7 + 41, 100, 14)
+    p = tmp_path / "odd.vxq"
+    VW.write_vxq(str(p), host)
+    lt, ut = X.GpuTable.from_vxq(str(p)), X.GpuTable(host)
+    try:
+        for c in range(len(host.columns)):
+            for r in range(lt.num_row_groups()):
+                assert _zone_tuple(lt.zone_map(c, r)) == _zone_tuple(ut.zone_map(c, r)), (c, r)
+        plan = P.AggPlan(None, [3], [P.count(P.col(0), "ci"), P.count(P.col(2), "cd"), P.sum_(P.col(0), "s"),
+                                     P.count_star("n")])
+        a, b = X.GpuHashAggregate(lt, plan), X.GpuHashAggregate(ut, plan)
+        try:
+            assert _bits(a.run().rows()) == _bits(b.run().rows())
+        finally:
+            a.close()
+            b.close()
+    finally:
+        lt.close()
+        ut.close()
+
+
+def test_device_checks_find_corrupt_blocks(gpu_lib, tmp_path):
+    """The device CRC check fails a flipped byte; a re-sealed block with a
+    code past its row group's dictionary fails the device's code check."""
+    X = gpu_lib
+    host = mixed_table(5000, 2048, 15)
+    p = tmp_path / "bad.vxq"
+    meta = VW.write_vxq(str(p), host)
+    good = open(p, "rb").read()
+    sec = meta[1].cols[5]  # int64 column "k", row group 1: second block
+    at = sec.offset + (VW.BITMAP_BYTES + 1024 * 8 + 4) + VW.BITMAP_BYTES + 77
+    open(p, "wb").write(good[:at] + bytes([good[at] ^ 0x04]) + good[at + 1:])
+    with pytest.raises(abi.VexqError) as e:
+        X.GpuTable.from_vxq(str(p))
+    assert e.value.status == abi.ECORRUPT and "checksum mismatch" in str(e.value) and "col=k" in str(e.value)
+    sec = meta[1].cols[3]  # STRING codes, row group 1 (first block: 1,024 rows)
+    valid = host.columns[3].valid_mask(host.nrows)[2048:2048 + 1024]
+    row = int(np.flatnonzero(valid)[0])
+    b = bytearray(good)
+    blk = bytearray(b[sec.offset:sec.offset + VW.BITMAP_BYTES + 1024 * 4])
+    blk[VW.BITMAP_BYTES + 4 * row:VW.BITMAP_BYTES + 4 * row + 4] = struct.pack("<I", 1000)
+    b[sec.offset:sec.offset + VW.BITMAP_BYTES + 1024 * 4 + 4] = VW.with_crc(bytes(blk))
+    open(p, "wb").write(bytes(b))
+    with pytest.raises(abi.VexqError) as e:
+        X.GpuTable.from_vxq(str(p))
+    assert e.value.status == abi.ECORRUPT and "dictionary code out of range" in str(e.value), str(e.value)
+    open(p, "wb").write(good)
+    X.GpuTable.from_vxq(str(p)).close()

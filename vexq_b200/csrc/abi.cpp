@@ -9,7 +9,8 @@
 #include "plan.h"
 
 namespace vq {
-Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows);
+Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows,
+                    const int8_t* has_null = nullptr);
 void destroy_table(Table* t);
 const std::string& last_error();
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end);

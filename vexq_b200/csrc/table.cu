@@ -260,8 +260,8 @@ static std::mutex g_dictdev_mu;
 void fill_column(Table& t, int ci, const vexq_column_desc& d, cudaStream_t s, DevBuf& err) {
     Column& c = t.cols[ci];
     int w = type_width(c.type);
-    if (t.nrows > 0) VQ_CUDA(cudaMemcpyAsync(c.values.p, d.values, (size_t)w * t.nrows, cudaMemcpyHostToDevice, s));
-    if (c.nullable && t.nrows > 0) VQ_CUDA(cudaMemcpyAsync(c.validity.p, d.validity, (size_t)(t.nrows + 7) / 8, cudaMemcpyHostToDevice, s));
+    if (t.nrows > 0) VQ_CUDA(cudaMemcpyAsync(c.values.p, d.values, (size_t)w * t.nrows, cudaMemcpyDefault, s));
+    if (c.nullable && t.nrows > 0) VQ_CUDA(cudaMemcpyAsync(c.validity.p, d.validity, (size_t)(t.nrows + 7) / 8, cudaMemcpyDefault, s));
     if (c.type == VEXQ_TYPE_STRING && c.per_rg_dicts && t.nrows > 0) {
         DictDev* dd;
         {
@@ -354,7 +354,12 @@ void compute_zones(Table& t, cudaStream_t s) {
     t.zones_ready = true;
 }
 
-Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows) {
+// has_null (optional, one flag per column) says which columns hold a NULL
+// when the caller already knows; the values and bitmaps may then be device
+// pointers (the copies infer their direction), as the .vxq loader hands over
+// columns it decoded on the device. STRING columns with a table-wide
+// dictionary are checked on the host and must be host buffers.
+Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows, const int8_t* has_null) {
     if (ncols < 0 || ncols > VQ_MAXCOLS) fail(VEXQ_EINVAL, "column count out of range (max 32)");
     if (nrows < 0 || nrows >= (int64_t(1) << 40)) fail(VEXQ_EINVAL, "row count out of range");
     if (ncols > 0 && !cols) fail(VEXQ_EINVAL, "null column array");
@@ -378,7 +383,7 @@ Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, 
         int w = type_width(c.type);
         if (!w) fail(VEXQ_EINVAL, "column " + c.name + ": unknown type " + std::to_string(d.type));
         if (nrows > 0 && !d.values) fail(VEXQ_EINVAL, "column " + c.name + ": null values");
-        c.nullable = any_null(d.validity, nrows);
+        c.nullable = has_null ? (has_null[ci] != 0 && d.validity != nullptr) : any_null(d.validity, nrows);
         c.values.alloc((size_t)w * prow);
         VQ_CUDA(cudaMemsetAsync(c.values.p, 0, c.values.n, s));
         if (c.nullable) {

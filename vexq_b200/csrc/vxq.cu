@@ -36,7 +36,7 @@
 #include "plan.h"
 
 namespace vq {
-Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows);
+Table* upload_table(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows, const int8_t* has_null);
 }  // namespace vq
 
 using namespace vq;
@@ -262,7 +262,9 @@ bool all_valid(const uint8_t* bm, int rows) {
 // column at the row group's first row (ColumnReader.NextBlock,
 // storage/rowgroup.go:101-171; DecodeRLEBool, storage/codec.go:292-336;
 // UnmarshalDictionary, storage/codec.go:233-251).
-void decode_section(const VxqFile& f, int fi, int rg, int64_t row0, HostCol& hc) {
+// host_blocks = false checks the section's bounds and, for STRING, parses the
+// dictionary, leaving the blocks to the device.
+void decode_section(const VxqFile& f, int fi, int rg, int64_t row0, HostCol& hc, bool host_blocks = true) {
     const Field& fd = f.fields[fi];
     const ColMeta& m = f.rgs[rg].cols[fi];
     const uint32_t rows = f.rgs[rg].rows;
@@ -303,6 +305,12 @@ void decode_section(const VxqFile& f, int fi, int rg, int64_t row0, HostCol& hc)
     const int64_t end = m.off + m.len - (int64_t)m.dict_len;
     int64_t pos = m.off;
     const int w = value_width(fd.type);
+    if (!host_blocks) {  // fixed-size blocks: the section must hold all of them
+        const int64_t full = rows / kBlockRows, tail = rows % kBlockRows;
+        const int64_t need = full * (kBitmapBytes + (int64_t)kBlockRows * w + 4) + (tail ? kBitmapBytes + tail * w + 4 : 0);
+        if (need > end - m.off) corrupt("read block " + where(m.off) + ": unexpected EOF");
+        return;
+    }
     for (uint32_t done = 0; done < rows;) {
         const int n = (int)std::min<uint32_t>(kBlockRows, rows - done);
         const int64_t r = row0 + done;
@@ -379,6 +387,8 @@ void parallel_for(size_t n, F&& fn) {
 
 struct Loaded {
     std::vector<std::unique_ptr<HostCol>> cols;
+    std::vector<int> sel;        // file column of each loaded column
+    std::vector<int64_t> row0;   // first table row of each row group
     int64_t nrows = 0;
     int32_t rg_rows = VEXQ_ROW_GROUP_ROWS;
     int64_t bytes_checked = 0;
@@ -386,7 +396,9 @@ struct Loaded {
 
 // Selected columns decoded from the file. The table's row groups are the
 // file's: every row group but the last must hold the same number of rows.
-void load(const VxqFile& f, const char* const* names, int32_t nnames, Loaded& L) {
+// device = true leaves the fixed-width blocks to k_vxq_blocks (their columns
+// get no host arrays); BOOL sections and dictionaries are decoded here.
+void load(const VxqFile& f, const char* const* names, int32_t nnames, Loaded& L, bool device = false) {
     std::vector<int> sel;
     if (names) {
         if (nnames < 0) fail(VEXQ_EINVAL, "negative column count");
@@ -425,16 +437,20 @@ void load(const VxqFile& f, const char* const* names, int32_t nnames, Loaded& L)
         hc->type = f.fields[c].type;
         hc->name = f.fields[c].name;
         const int w = hc->type == VEXQ_TYPE_BOOL ? 1 : value_width(hc->type);
-        hc->values.assign((size_t)std::max<int64_t>(L.nrows, 1) * w, 0);
-        hc->validity.assign((size_t)(L.nrows + 7) / 8 + 1, 0);
+        if (!device || hc->type == VEXQ_TYPE_BOOL) {
+            hc->values.assign((size_t)std::max<int64_t>(L.nrows, 1) * w, 0);
+            hc->validity.assign((size_t)(L.nrows + 7) / 8 + 1, 0);
+        }
         if (hc->type == VEXQ_TYPE_STRING) hc->rg_dict.resize(nrg);
         L.cols.push_back(std::move(hc));
     }
     const size_t ntask = sel.size() * nrg;
     parallel_for(ntask, [&](size_t task) {
         const size_t k = task / std::max<size_t>(nrg, 1), r = task % std::max<size_t>(nrg, 1);
-        decode_section(f, sel[k], (int)r, row0[r], *L.cols[k]);
+        decode_section(f, sel[k], (int)r, row0[r], *L.cols[k], !device || L.cols[k]->type == VEXQ_TYPE_BOOL);
     });
+    L.sel = sel;
+    L.row0 = row0;
     for (size_t k = 0; k < sel.size(); k++)
         for (size_t r = 0; r < nrg; r++) L.bytes_checked += f.rgs[r].cols[sel[k]].len;
     // STRING dictionaries flattened into the upload's per-row-group form
@@ -452,6 +468,224 @@ void load(const VxqFile& f, const char* const* names, int32_t nnames, Loaded& L)
         if (hc->bytes.empty()) hc->bytes.push_back(0);
         hc->rg_dict.clear();
     }
+}
+
+// ---- device decode -----------------------------------------------------------------
+// The file's data region is copied to HBM once; one warp then checks and
+// scatters each fixed-width block: the CRC-32 of [bitmap][values] (each lane
+// folds a contiguous segment with a byte table in shared memory, and the
+// segments are joined by the CRC's linearity: crc(A‖B) = crc(A)·x^(8|B|) ⊕
+// crc(B) over GF(2) modulo the polynomial, with the 0xFFFFFFFF start value
+// entering as 0xFFFFFFFF·x^(8|M|)), the values into the column at the block's
+// first row, the validity bits, and for STRING codes the dictionary bound.
+
+struct VxqBlock {
+    long long src;       // file offset of the block
+    long long dst_row;   // table row of its first row
+    int rows;
+    int col;             // loaded-column slot
+    unsigned dict_n;     // STRING: entries of the row group's dictionary; ~0u otherwise
+    int pad;
+};
+struct VxqDevCol {
+    unsigned char* values;
+    unsigned* validity;  // zeroed, 4-byte words
+    int width;
+    int pad;
+};
+struct VxqPow {
+    unsigned x[24];      // x^(8·2^k) mod P, reflected
+};
+
+// a·b modulo the CRC polynomial, both in the reflected order (bit 31 = x^0).
+__host__ __device__ inline unsigned vq_gf_mul(unsigned a, unsigned b) {
+    unsigned p = 0;
+    for (int i = 0; i < 32; i++) {
+        if (a & (0x80000000u >> i)) p ^= b;
+        b = (b & 1u) ? (b >> 1) ^ 0xEDB88320u : b >> 1;
+    }
+    return p;
+}
+// x^(8n) modulo the polynomial.
+__device__ inline unsigned vq_x8n(unsigned n, const VxqPow& pw) {
+    unsigned r = 0x80000000u;
+    for (int k = 0; n; k++, n >>= 1)
+        if (n & 1u) r = vq_gf_mul(r, pw.x[k]);
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_vxq_blocks(const unsigned char* __restrict__ raw, const VxqBlock* __restrict__ blk,
+                                                    long long nblk, const VxqDevCol* __restrict__ cols, VxqPow pw,
+                                                    unsigned long long* bad, int* has_null) {
+    __shared__ unsigned tab[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        unsigned c = (unsigned)i;
+        for (int b = 0; b < 8; b++) c = (c & 1u) ? (c >> 1) ^ 0xEDB88320u : c >> 1;
+        tab[i] = c;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long b = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += nw) {
+        const VxqBlock d = blk[b];
+        const VxqDevCol c = cols[d.col];
+        const int w = c.width;
+        const int len = kBitmapBytes + d.rows * w;
+        const unsigned char* p = raw + d.src;
+        const int seg = ((len + 31) / 32 + 3) & ~3;
+        const int a = min(lane * seg, len), e = min(a + seg, len);
+        unsigned r = 0;
+        for (int i = a; i < e; i++) r = (r >> 8) ^ tab[(r ^ __ldg(p + i)) & 0xFFu];
+        unsigned part = vq_gf_mul(r, vq_x8n((unsigned)(len - e), pw));
+        if (lane == 0) part ^= vq_gf_mul(0xFFFFFFFFu, vq_x8n((unsigned)len, pw));
+        for (int o = 16; o > 0; o >>= 1) part ^= __shfl_xor_sync(0xffffffffu, part, o);
+        const unsigned stored = (unsigned)p[len] | ((unsigned)p[len + 1] << 8) | ((unsigned)p[len + 2] << 16) |
+                                ((unsigned)p[len + 3] << 24);
+        if ((part ^ 0xFFFFFFFFu) != stored) {
+            if (lane == 0) atomicMin(bad, (unsigned long long)b);
+            continue;
+        }
+        // values
+        const unsigned char* src = p + kBitmapBytes;
+        unsigned char* dst = c.values + d.dst_row * w;
+        const int nb = d.rows * w;
+        if ((((unsigned long long)src) & 3ull) == 0)
+            for (int i = lane; i < nb / 4; i += 32) reinterpret_cast<unsigned*>(dst)[i] = __ldg(reinterpret_cast<const unsigned*>(src) + i);
+        else
+            for (int i = lane; i < nb; i += 32) dst[i] = __ldg(src + i);
+        // validity: whole bytes the block owns as plain stores, the rest as
+        // bit ORs into zeroed words (a neighbour may share the byte)
+        bool null_seen = false;
+        unsigned char* vb = reinterpret_cast<unsigned char*>(c.validity);
+        const int own = (d.dst_row & 7) == 0 ? d.rows / 8 : 0;
+        for (int i = lane; i < own; i += 32) {
+            const unsigned char v = p[i];
+            vb[(d.dst_row >> 3) + i] = v;
+            null_seen |= v != 0xFFu;
+        }
+        for (int i = own * 8 + lane; i < d.rows; i += 32) {
+            const bool v = (p[i >> 3] >> (i & 7)) & 1;
+            null_seen |= !v;
+            if (v) {
+                const long long row = d.dst_row + i;
+                atomicOr(c.validity + (row >> 5), 1u << (row & 31));
+            }
+        }
+        if (__any_sync(0xffffffffu, null_seen) && lane == 0) atomicOr(has_null + d.col, 1);
+        // dictionary codes of valid rows within the row group's dictionary
+        if (d.dict_n != ~0u) {
+            bool out = false;
+            for (int i = lane; i < d.rows; i += 32) {
+                if (!((p[i >> 3] >> (i & 7)) & 1)) continue;
+                const unsigned char* q = src + (size_t)i * 4;
+                const unsigned code = (unsigned)q[0] | ((unsigned)q[1] << 8) | ((unsigned)q[2] << 16) | ((unsigned)q[3] << 24);
+                out |= code >= d.dict_n;
+            }
+            if (__any_sync(0xffffffffu, out) && lane == 0) atomicMin(bad + 1, (unsigned long long)b);
+        }
+    }
+}
+
+// The table from a mapped file: BOOL columns and dictionaries decoded on the
+// host, every fixed-width block checked and scattered on the device.
+Table* load_device(const VxqFile& f, const char* const* names, int32_t nnames) {
+    Loaded L;
+    load(f, names, nnames, L, true);
+    const size_t nrg = f.rgs.size(), ncol = L.cols.size();
+    // the data region: everything before the footer (the device copy holds
+    // only this, so every block must lie inside it)
+    const int64_t flen = rd<int64_t>(f.base + f.size - kTrailer + 4);
+    const int64_t data_end = (int64_t)f.size - kTrailer - flen;
+    std::vector<VxqBlock> blocks;
+    std::vector<int> dev_slot(ncol, -1);
+    std::vector<int> slot_col;
+    for (size_t k = 0; k < ncol; k++) {
+        const HostCol& hc = *L.cols[k];
+        if (hc.type == VEXQ_TYPE_BOOL) continue;
+        dev_slot[k] = (int)slot_col.size();
+        slot_col.push_back((int)k);
+        const int w = value_width(hc.type);
+        for (size_t r = 0; r < nrg; r++) {
+            const ColMeta& m = f.rgs[r].cols[L.sel[k]];
+            const unsigned dict_n = hc.type == VEXQ_TYPE_STRING ? hc.rg_first[r + 1] - hc.rg_first[r] : ~0u;
+            int64_t pos = m.off;
+            for (uint32_t done = 0; done < f.rgs[r].rows;) {
+                const int n = (int)std::min<uint32_t>(kBlockRows, f.rgs[r].rows - done);
+                if (pos < 0 || pos + kBitmapBytes + (int64_t)n * w + 4 > data_end)
+                    corrupt("read block rg=" + std::to_string(r) + " col=" + hc.name + " off=" + std::to_string(pos) +
+                            ": outside the data region");
+                blocks.push_back(VxqBlock{pos, L.row0[r] + done, n, dev_slot[k], dict_n, 0});
+                pos += kBitmapBytes + (int64_t)n * w + 4;
+                done += (uint32_t)n;
+            }
+        }
+    }
+    // device columns: values and zeroed validity words
+    std::vector<DevBuf> vals(slot_col.size()), valid(slot_col.size());
+    std::vector<VxqDevCol> dc(slot_col.size());
+    const int64_t nrows = L.nrows;
+    for (size_t j = 0; j < slot_col.size(); j++) {
+        const int w = value_width(L.cols[slot_col[j]]->type);
+        vals[j].alloc((size_t)std::max<int64_t>(nrows, 1) * w);
+        valid[j].alloc(((size_t)(nrows + 31) / 32 + 1) * 4);
+        VQ_CUDA(cudaMemset(valid[j].p, 0, valid[j].n));
+        dc[j] = VxqDevCol{vals[j].as<unsigned char>(), valid[j].as<unsigned>(), w, 0};
+    }
+    std::vector<int> has_null(slot_col.size() + 1, 0);
+    if (!blocks.empty()) {
+        DevBuf raw(std::max<size_t>((size_t)data_end, 4));
+        VQ_CUDA(cudaMemcpy(raw.p, f.base, (size_t)data_end, cudaMemcpyHostToDevice));
+        DevBuf d_blk(blocks.size() * sizeof(VxqBlock)), d_col(std::max<size_t>(dc.size(), 1) * sizeof(VxqDevCol));
+        DevBuf d_flags(16 + has_null.size() * 4);
+        VQ_CUDA(cudaMemcpy(d_blk.p, blocks.data(), d_blk.n, cudaMemcpyHostToDevice));
+        VQ_CUDA(cudaMemcpy(d_col.p, dc.data(), dc.size() * sizeof(VxqDevCol), cudaMemcpyHostToDevice));
+        VQ_CUDA(cudaMemset(d_flags.p, 0xFF, 16));
+        VQ_CUDA(cudaMemset((char*)d_flags.p + 16, 0, has_null.size() * 4));
+        VxqPow pw;
+        pw.x[0] = 0x00800000u;  // x^8
+        for (int k = 1; k < 24; k++) pw.x[k] = vq_gf_mul(pw.x[k - 1], pw.x[k - 1]);
+        const long long nb = (long long)blocks.size();
+        const int grid = (int)std::min<long long>((nb + 7) / 8, (long long)sm_count() * 8);
+        k_vxq_blocks<<<grid, 256>>>(raw.as<unsigned char>(), d_blk.as<VxqBlock>(), nb, d_col.as<VxqDevCol>(), pw,
+                                    d_flags.as<unsigned long long>(), (int*)((char*)d_flags.p + 16));
+        VQ_CUDA(cudaGetLastError());
+        unsigned long long bad[2];
+        VQ_CUDA(cudaMemcpy(bad, d_flags.p, 16, cudaMemcpyDeviceToHost));
+        VQ_CUDA(cudaMemcpy(has_null.data(), (char*)d_flags.p + 16, has_null.size() * 4, cudaMemcpyDeviceToHost));
+        auto where = [&](unsigned long long i) {
+            const VxqBlock& b = blocks[(size_t)i];
+            const int k = slot_col[(size_t)b.col];
+            int rg = 0;
+            while (rg + 1 < (int)nrg && L.row0[rg + 1] <= b.dst_row) rg++;
+            return "rg=" + std::to_string(rg) + " col=" + L.cols[k]->name + " off=" + std::to_string(b.src);
+        };
+        if (bad[0] != ~0ull) corrupt("crc block " + where(bad[0]) + ": checksum mismatch");
+        if (bad[1] != ~0ull) corrupt("crc block " + where(bad[1]) + ": dictionary code out of range");
+    }
+    std::vector<vexq_column_desc> d(ncol);
+    std::vector<int8_t> nulls(ncol, 0);
+    for (size_t k = 0; k < ncol; k++) {
+        HostCol& hc = *L.cols[k];
+        d[k] = vexq_column_desc{};
+        d[k].name = hc.name.c_str();
+        d[k].type = hc.type;
+        if (dev_slot[k] >= 0) {
+            const int j = dev_slot[k];
+            nulls[k] = has_null[(size_t)j] ? 1 : 0;
+            d[k].values = vals[(size_t)j].p;
+            d[k].validity = nulls[k] ? (const uint8_t*)valid[(size_t)j].p : nullptr;
+        } else {
+            nulls[k] = hc.any_null ? 1 : 0;
+            d[k].values = hc.values.data();
+            d[k].validity = nulls[k] ? hc.validity.data() : nullptr;
+        }
+        if (hc.type == VEXQ_TYPE_STRING) {
+            d[k].dict_rg_first = hc.rg_first.data();
+            d[k].dict_str_off = hc.str_off.data();
+            d[k].dict_bytes = hc.bytes.data();
+        }
+    }
+    return upload_table(d.data(), (int32_t)d.size(), L.nrows, L.rg_rows, nulls.data());
 }
 
 }  // namespace
@@ -490,23 +724,7 @@ int32_t vexq_table_load_vxq(const char* path, const char* const* columns, int32_
         set_error("");
         if (!out) fail(VEXQ_EINVAL, "null output handle");
         VxqFile f(path);
-        Loaded L;
-        load(f, columns, ncolumns, L);
-        std::vector<vexq_column_desc> d(L.cols.size());
-        for (size_t k = 0; k < L.cols.size(); k++) {
-            HostCol& hc = *L.cols[k];
-            d[k] = vexq_column_desc{};
-            d[k].name = hc.name.c_str();
-            d[k].type = hc.type;
-            d[k].values = hc.values.data();
-            d[k].validity = hc.any_null ? hc.validity.data() : nullptr;
-            if (hc.type == VEXQ_TYPE_STRING) {
-                d[k].dict_rg_first = hc.rg_first.data();
-                d[k].dict_str_off = hc.str_off.data();
-                d[k].dict_bytes = hc.bytes.data();
-            }
-        }
-        Table* t = upload_table(d.data(), (int32_t)d.size(), L.nrows, L.rg_rows);
+        Table* t = load_device(f, columns, ncolumns);
         *out = new vexq_table_s{t};
         return VEXQ_OK;
     } catch (const Status& s) {
