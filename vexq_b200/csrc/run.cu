@@ -666,6 +666,19 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     int* err_out = (int*)((char*)p.scratch_c.p + nout_f + nout_i);
     P.error = err_out + 2;
     p.h_stage.ensure(nout_f + nout_i + 16);
+    // the merge writes the merged row and the handed-out error word straight
+    // into the pinned staging buffer when the device can address it, so no
+    // copy follows the merge (the kernels' own error word stays on the device)
+    void* mapped = nullptr;
+    if (cudaHostGetDevicePointer(&mapped, p.h_stage.p, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        mapped = nullptr;
+    }
+    if (mapped) {
+        out_f = (double*)mapped;
+        out_i = (long long*)((char*)mapped + nout_f);
+        err_out = (int*)((char*)mapped + nout_f + nout_i);
+    }
     ensure_events(p);
     if (!p.regs_err_clean) VQ_CUDA(cudaMemsetAsync(P.error, 0, 4, rc.s));
     p.regs_err_clean = false;  // until the merge below has run
@@ -719,7 +732,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     }
     if (!fused) launch_check(rc.s, "k_merge_regs_dep");
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
-    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
+    if (!mapped) VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
     p.regs_err_clean = true;
     const int herr = *(const int*)((const char*)p.h_stage.p + nout_f + nout_i);
