@@ -29,7 +29,6 @@
 #include <cerrno>
 #include <cstring>
 #include <memory>
-#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -587,49 +586,6 @@ __global__ void __launch_bounds__(256) k_vxq_blocks(const unsigned char* __restr
     }
 }
 
-// Copies [0, n) of the mapped file to device memory at dst. Host threads
-// each own a pinned staging buffer and a stream: a thread copies its next
-// 4 MB of the file into its buffer (page-cache reads, in parallel) while the
-// copy engine moves the buffers filled before. The staging buffers are kept
-// for the next load.
-void copy_file_to_device(const uint8_t* src, size_t n, void* dst) {
-    constexpr size_t kChunk = 4u << 20;
-    constexpr int kThreads = 8;
-    static std::mutex mu;
-    static PinnedBuf* stage = new PinnedBuf[kThreads];  // never freed: outlives the runtime's teardown at exit
-    static cudaStream_t streams[kThreads] = {};
-    std::lock_guard<std::mutex> lk(mu);
-    const size_t nchunks = (n + kChunk - 1) / kChunk;
-    const int threads = (int)std::min<size_t>(kThreads, std::max<size_t>(nchunks, 1));
-    int dev = 0;
-    VQ_CUDA(cudaGetDevice(&dev));
-    for (int t = 0; t < threads; t++) {
-        stage[t].ensure(kChunk);
-        if (!streams[t]) VQ_CUDA(cudaStreamCreateWithFlags(&streams[t], cudaStreamNonBlocking));
-    }
-    std::vector<std::string> errs(threads);
-    auto work = [&](int t) {
-        try {
-            cudaSetDevice(dev);
-            for (size_t c = (size_t)t; c < nchunks; c += (size_t)threads) {
-                const size_t off = c * kChunk, m = std::min(kChunk, n - off);
-                VQ_CUDA(cudaStreamSynchronize(streams[t]));  // the buffer's previous copy is done
-                std::memcpy(stage[t].p, src + off, m);
-                VQ_CUDA(cudaMemcpyAsync((char*)dst + off, stage[t].p, m, cudaMemcpyHostToDevice, streams[t]));
-            }
-            VQ_CUDA(cudaStreamSynchronize(streams[t]));
-        } catch (const std::exception& e) {
-            errs[t] = e.what();
-        }
-    };
-    std::vector<std::thread> th;
-    for (int t = 1; t < threads; t++) th.emplace_back(work, t);
-    work(0);
-    for (auto& x : th) x.join();
-    for (auto& e : errs)
-        if (!e.empty()) fail(VEXQ_EDEVICE, "copying the file to the device: " + e);
-}
-
 // The table from a mapped file: BOOL columns and dictionaries decoded on the
 // host, every fixed-width block checked and scattered on the device.
 Table* load_device(const VxqFile& f, const char* const* names, int32_t nnames) {
@@ -678,7 +634,7 @@ Table* load_device(const VxqFile& f, const char* const* names, int32_t nnames) {
     std::vector<int> has_null(slot_col.size() + 1, 0);
     if (!blocks.empty()) {
         DevBuf raw(std::max<size_t>((size_t)data_end, 4));
-        copy_file_to_device(f.base, (size_t)data_end, raw.p);
+        VQ_CUDA(cudaMemcpy(raw.p, f.base, (size_t)data_end, cudaMemcpyHostToDevice));
         DevBuf d_blk(blocks.size() * sizeof(VxqBlock)), d_col(std::max<size_t>(dc.size(), 1) * sizeof(VxqDevCol));
         DevBuf d_flags(16 + has_null.size() * 4);
         VQ_CUDA(cudaMemcpy(d_blk.p, blocks.data(), d_blk.n, cudaMemcpyHostToDevice));
