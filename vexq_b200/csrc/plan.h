@@ -172,6 +172,8 @@ struct Plan {
     DevBuf d_bseg;
     DevBuf d_kinds;                        // register-path combiner kinds
     PinnedBuf h_stage;                     // pinned staging for small results
+    void* h_stage_mapped = nullptr;        // its device address (null: not addressable, copy back)
+    void* h_stage_mapped_for = nullptr;    // the staging allocation that address belongs to
     bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
     ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
     long long hash_groups_seen = -1;       // hash path: groups the last run found (sizes the next table)

@@ -669,11 +669,15 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     // the merge writes the merged row and the handed-out error word straight
     // into the pinned staging buffer when the device can address it, so no
     // copy follows the merge (the kernels' own error word stays on the device)
-    void* mapped = nullptr;
-    if (cudaHostGetDevicePointer(&mapped, p.h_stage.p, 0) != cudaSuccess) {
-        (void)cudaGetLastError();
-        mapped = nullptr;
+    if (p.h_stage_mapped_for != p.h_stage.p) {  // looked up once per staging allocation
+        p.h_stage_mapped = nullptr;
+        if (cudaHostGetDevicePointer(&p.h_stage_mapped, p.h_stage.p, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            p.h_stage_mapped = nullptr;
+        }
+        p.h_stage_mapped_for = p.h_stage.p;
     }
+    void* mapped = p.h_stage_mapped;
     if (mapped) {
         out_f = (double*)mapped;
         out_i = (long long*)((char*)mapped + nout_f);
