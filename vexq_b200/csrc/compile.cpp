@@ -486,6 +486,13 @@ void analyze(Plan& p) {
                 n.nullable = C(0).nullable || n.present_idx >= 0 || n.streq_code < 0;
                 n.finite = true;
                 break;
+            case NK::StrRank:
+                n.nullable = C(0).nullable;
+                n.bounded = true;
+                n.lo = 0;
+                n.hi = n.rank.empty() ? 0.0 : (double)(n.rank.size() - 1);
+                n.finite = true;
+                break;
             default: {
                 bool any = false;
                 for (int c : n.ch) any = any || p.ir[c].nullable;
@@ -716,6 +723,11 @@ struct Gen {
                 }
                 break;
             }
+            case NK::StrRank:  // a NULL row reads rank 0; its slot update is skipped by ok
+                os << ind << "const bool " << ok << " = " << OK(0) << ";\n";
+                os << ind << "const long long " << x << " = " << ok << " ? (long long)__ldg(P.sets[" << n.set_idx << "] + "
+                   << X(0) << ") : 0LL;\n";
+                break;
             case NK::Case: {
                 std::string t = ctype(n.type);
                 int nw = (int)(n.ch.size() - (n.has_else ? 1 : 0)) / 2;
@@ -793,8 +805,34 @@ void plan_aggs(Plan& p, const std::vector<std::pair<int, int>>& aggs_ir, const v
                 break;
             case VEXQ_AGG_MIN:
             case VEXQ_AGG_MAX:
-                if (x.type == VEXQ_TYPE_STRING)
-                    fail(VEXQ_ENOTSUP, "MIN/MAX over a STRING column is not supported on the GPU path");
+                if (x.type == VEXQ_TYPE_STRING) {
+                    // MIN/MAX over strings (HashAggregate.strAccs, exec/aggregate.go:98-110;
+                    // merged in mergePartialAgg, exec/parallel.go:283-297): Go compares
+                    // strings byte by byte, so the dictionary is ranked in that order,
+                    // the slot takes MIN/MAX of the rank, and the rank maps back to the code
+                    if (x.k != NK::Col) fail(VEXQ_ENOTSUP, "MIN/MAX over a STRING expression that is not a column");
+                    const Table* tt = x.tab ? x.tab : (x.build ? p.bt : p.t);
+                    const GlobalDict& dict = tt->cols[x.col].dict;
+                    std::vector<uint32_t> order(dict.keys.size());
+                    std::iota(order.begin(), order.end(), 0u);
+                    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return dict.keys[a] < dict.keys[b]; });
+                    INode r;
+                    r.k = NK::StrRank;
+                    r.type = VEXQ_TYPE_INT64;
+                    r.col = x.col;
+                    r.build = x.build;
+                    r.tab = x.tab;
+                    r.ch = {in};
+                    r.rank.assign(order.size(), 0);
+                    for (size_t k = 0; k < order.size(); k++) r.rank[order[k]] = (uint32_t)k;
+                    p.ir.push_back(std::move(r));
+                    const int rn = (int)p.ir.size() - 1;
+                    o.value_slot = add_slot(p, seen, kind == VEXQ_AGG_MIN ? S_IMIN : S_IMAX, rn);
+                    o.out_type = VEXQ_TYPE_STRING;
+                    o.rank_code = order;
+                    o.rank_dict = &dict;
+                    break;
+                }
                 if (x.type == VEXQ_TYPE_FLOAT64)
                     o.value_slot = add_slot(p, seen, kind == VEXQ_AGG_MIN ? S_FMIN : S_FMAX, in);
                 else
@@ -2651,8 +2689,14 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     p.range_epoch = p.t ? p.t->range_epoch : 0;
     p.brange_epoch = p.bt ? p.bt->range_epoch : 0;
     analyze(p);
-    // large IN/LIKE code sets go to device bitsets
+    // large IN/LIKE code sets go to device bitsets; string rank tables beside them
     for (auto& n : p.ir) {
+        if (n.k == NK::StrRank) {
+            if ((int)p.sets.size() >= VQ_MAXSETS) fail(VEXQ_ENOTSUP, "too many large IN/LIKE sets and string MIN/MAX columns");
+            n.set_idx = (int)p.sets.size();
+            p.sets.push_back(n.rank.empty() ? std::vector<uint32_t>(1, 0u) : n.rank);
+            continue;
+        }
         if (n.k == NK::InCodes && n.codes.size() > 64) {
             if ((int)p.sets.size() >= VQ_MAXSETS) fail(VEXQ_ENOTSUP, "too many large IN/LIKE sets");
             std::vector<uint32_t> bits((n.codes.size() + 31) / 32, 0);
@@ -3009,6 +3053,7 @@ void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* chil
         c.type = p.outs[a].out_type;
         c.nullable = true;
         c.per_rg_dicts = false;
+        if (p.outs[a].rank_dict) c.dict = *p.outs[a].rank_dict;
     }
     Plan hp;
     hp.t = schema.get();

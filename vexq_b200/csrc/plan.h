@@ -8,7 +8,8 @@ namespace vq {
 
 enum class NK {
     Col, Lit, Cmp, Arith, Cast, And, Or, Not, IsNull, IsNotNull,
-    InInt, InFloat, InCodes, InFalse, StrEq, Case
+    InInt, InFloat, InCodes, InFalse, StrEq, Case,
+    StrRank  // a STRING column's code → its place in the dictionary's byte order (MIN/MAX)
 };
 
 struct INode {
@@ -41,6 +42,7 @@ struct INode {
     bool is_literal_raw = false;  // literal before coercion (SQL level)
     int lit_kind = 0;
     int lit_slot = -1;            // numeric literal passed at launch: index into VQParams::lit
+    std::vector<uint32_t> rank;   // StrRank: rank of each global code (device table at set_idx)
 };
 
 // Accumulator slot kinds.
@@ -58,6 +60,10 @@ struct AggOut {
     int nn_slot;      // slot giving the non-null count (CNT when the input is never NULL)
     int out_type;     // result vector type
     std::string name;
+    // MIN/MAX over a STRING column: the slot holds the rank of the string in
+    // the dictionary's byte order; rank_code maps it back to the code
+    std::vector<uint32_t> rank_code;
+    const GlobalDict* rank_dict = nullptr;
 };
 
 struct KeyCol {

@@ -1172,6 +1172,7 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
         oc.type = a.out_type;
         oc.v.assign(rows, 0);
         oc.valid.assign(rows, 0);
+        if (a.rank_dict) oc.dict = a.rank_dict;  // string MIN/MAX: codes of this dictionary
         if (emptyGlobal) {
             if (a.kind == VEXQ_AGG_COUNT) oc.valid[0] = 1;
             r->cols.push_back(std::move(oc));
@@ -1192,6 +1193,10 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
                 std::memcpy(&oc.v[j], &v, 8);
             } else {
                 int64_t v = slot_int(p, g, a.value_slot, i);
+                if (a.rank_dict) {  // the winning rank back to its code
+                    if (v < 0 || (size_t)v >= a.rank_code.size()) fail(VEXQ_EDEVICE, "string MIN/MAX rank out of range");
+                    v = a.rank_code[(size_t)v];
+                }
                 if (a.out_type == VEXQ_TYPE_DATE) v = (int64_t)(int32_t)v;
                 if (a.out_type == VEXQ_TYPE_BOOL) v = v != 0;
                 oc.v[j] = v;
