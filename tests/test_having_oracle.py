@@ -49,3 +49,16 @@ def test_oracle_having_then_order_and_limit():
     res = R.agg_having(rt, P.AggPlan(None, [0], [P.count_star("cnt"), P.sum_(P.col(1), "s")]),
                        P.col(2) >= 10, -1, order=(2, 1, 2))
     assert res.rows() == [(2, 2, 200), (1, 5, 50)]
+
+
+def test_oracle_string_min_max_is_byte_order():
+    """Go compares strings byte by byte (exec/aggregate.go:98-110): "é"
+    (0xC3 0xA9) sorts after "z", "B" before "a", and "" first."""
+    from vexq_b200.table import string_column
+    words = ["z", "é", "", "a", "B", "ab"]
+    idx = np.arange(len(words))
+    t = HostTable([int_column("g", np.zeros(len(words), np.int64)), string_column("s", idx, words, len(words), 65536)],
+                  len(words), 65536)
+    res = R.agg(R.RefTable(t), P.AggPlan(None, [0], [P.min_(P.col(1), "mn"), P.max_(P.col(1), "mx")]), workers=0)
+    assert res.rows() == [(0, "", "é")]
+    assert sorted(w.encode() for w in words)[1] == b"B"
