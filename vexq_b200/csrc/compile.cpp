@@ -2328,7 +2328,8 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     collect_cols(p, p.resid, cols);
     for (int k : key_nodes) collect_cols(p, k, cols);
     for (auto& s : p.slots) collect_cols(p, s.input, cols);
-    ScanLoop loop(p, p.t, cols, block, "probe");
+    // the cp.async ring (register path only, where registers limit occupancy)
+    ScanLoop loop(p, p.t, cols, block, "probe", p.path == AggPath::Regs);
     p.tile = loop.tile_rows();
     p.smem = loop.smem();
     loop.prologue(os);
@@ -2336,9 +2337,10 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     loop.open(os);
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
-    os << "            const long long r = r0 + k;\n";
+    os << "            const long long r = r0 + " << (loop.strided() ? "(k << 5)" : "k") << ";\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
     Gen g(p, os);
+    if (loop.strided()) g.kidx = "(k << 5)";
     if (p.pred >= 0) {
         g.emit(p.pred);
         os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
@@ -2357,6 +2359,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     // above-join expressions: a fresh memo scope per match for build-side reads
     Gen g2(p, os);
     g2.done = g.done;
+    g2.kidx = g.kidx;
     g2.ind = "                ";
     if (p.resid >= 0) {
         g2.emit(p.resid);
@@ -2780,7 +2783,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     ex << (join ? "join+agg" : "agg") << " path=" << (p.path == AggPath::Regs ? "regs" : p.path == AggPath::Dense ? "dense" : "hash")
        << " groups_domain=" << p.domain << " slots=" << p.slots.size() << " nf=" << p.nf << " ni=" << p.ni
        << " block=" << p.block
-       << (p.staged ? " staged=tma" : (p.async_stages > 1 && p.path == AggPath::Regs && !join) ? " async=" + std::to_string(p.async_stages)
+       << (p.staged ? " staged=tma" : (p.async_stages > 1 && p.path == AggPath::Regs) ? " async=" + std::to_string(p.async_stages)
            : p.pipeline ? " pipeline=1" : " pipeline=0")
        << (p.min_blocks > 0 ? " minb=" + std::to_string(p.min_blocks) : std::string())
        << " tile=" << p.tile << " smem=" << p.smem << " smem_groups=" << p.smem_groups << " warp_agg=" << p.warp_agg;
