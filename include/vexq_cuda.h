@@ -406,6 +406,17 @@ int32_t vexq_server_stop(vexq_server_t s);
 /* Host-set cancellation flag polled between launches of a running plan. */
 int32_t vexq_cancel(vexq_plan_t p);
 
+/* Fault injection on the host, for tests of the error paths (the reference's
+ * counterpart is the failing-operator tests of exec/parallel_join.go:430-476:
+ * the first error wins and the query returns it). After `after` more device
+ * allocations succeed, the next one fails as cudaMalloc does when memory is
+ * exhausted, and the call that made it returns VEXQ_ENOMEM; the injection then
+ * switches itself off. -1 switches it off at once. No device fault is made. */
+int32_t vexq_debug_fail_alloc(int32_t after);
+/* Bytes of device memory the library holds right now (tables, plan buffers,
+ * batch workspaces), all devices together: a leak check for the tests. */
+int32_t vexq_debug_live_device_bytes(int64_t* out);
+
 /* ---- global aggregate without allocation --------------------------------
  * No counterpart in the reference: its operators work on the Go heap.
  * Runs an aggregate plan without GROUP BY (one result row) through the same

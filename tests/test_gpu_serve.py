@@ -141,3 +141,26 @@ def test_admission_by_footprint(tables):
     finally:
         for op in ops:
             op.close()
+
+
+def test_two_workers_same_handles_repeated(tables):
+    """The same few plan handles submitted many times to two batching
+    workers: batches of one worker read a plan while the other worker's
+    batch (or join) uses the same handle, and batch workspaces grow between
+    launches. Every result must equal the plan's single run."""
+    X, li, o, i = tables
+    ops = make_queries(X, li, o, i, 7, seed=13)
+    try:
+        ref = alone(ops)
+        rng = np.random.default_rng(14)
+        for rep in range(3):
+            order = [int(k) for k in rng.integers(0, len(ops), 60)]
+            seq = [ops[k] for k in order]
+            rows, _, (launches, queries, max_batch, max_running) = serve(
+                X, seq, max_inflight=16, workers=2, gap_s=0.0005 * rep)
+            assert queries == len(seq)
+            for k, r in zip(order, rows):
+                assert_rows_match(r, ref[k], ordered=True, rtol=SERVE_RTOL)
+    finally:
+        for op in ops:
+            op.close()

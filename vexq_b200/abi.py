@@ -148,7 +148,7 @@ EXPORTS = [
     "vexq_batch_run",
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
-    "vexq_cancel",
+    "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes",
     "vexq_plan_run_global_noalloc",
     "vexq_batch_create",
     "vexq_batch_exec",
@@ -219,6 +219,8 @@ def load() -> C.CDLL:
         "vexq_server_latency": (i32, [vp, i64, C.POINTER(C.c_double)]),
         "vexq_server_stop": (i32, [vp]),
         "vexq_cancel": (i32, [vp]),
+        "vexq_debug_fail_alloc": (i32, [i32]),
+        "vexq_debug_live_device_bytes": (i32, [C.POINTER(i64)]),
         "vexq_plan_run_global_noalloc": (i32, [vp, i32, i32, vp, C.POINTER(i64), C.POINTER(C.c_uint8), i32]),
         "vexq_batch_create": (i32, [C.POINTER(vp), i32, C.c_uint32, C.POINTER(vp)]),
         "vexq_batch_exec": (i32, [vp, C.POINTER(vp)]),

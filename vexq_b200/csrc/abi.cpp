@@ -339,4 +339,16 @@ int32_t vexq_cancel(vexq_plan_t p) {
     return VEXQ_OK;
 }
 
+int32_t vexq_debug_fail_alloc(int32_t after) {
+    if (after < -1) return VEXQ_EINVAL;
+    vq::g_fail_alloc_after.store(after);
+    return VEXQ_OK;
+}
+
+int32_t vexq_debug_live_device_bytes(int64_t* out) {
+    if (!out) return VEXQ_EINVAL;
+    *out = (int64_t)vq::g_live_device_bytes.load();
+    return VEXQ_OK;
+}
+
 }  // extern "C"

@@ -288,7 +288,7 @@ struct Batch {
         put(a_params, params.data(), params.size() * sizeof(VQParams));
         put(a_tdesc, td.data(), td.size() * sizeof(VQTableDesc));
         put(a_mdesc, md.data(), md.size() * sizeof(VQMergeDesc));
-        VQ_CUDA(cudaMemcpy(dev.p, blob.data(), upload, cudaMemcpyHostToDevice));
+        h2d(dev.p, blob.data(), upload, s);
         std::ostringstream ex;
         ex << "batch plans=" << items.size() << " regs_plans=" << ck[0].items.size() << " regs_bodies=" << ck[0].nbodies
            << " regs_units=" << ck[0].nunits << " table_plans=" << ck[1].items.size() << " table_bodies=" << ck[1].nbodies

@@ -2821,7 +2821,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         p.d_sets.alloc(tot * 4);
         size_t off = 0;
         for (auto& s : p.sets) {
-            VQ_CUDA(cudaMemcpy(p.d_sets.as<uint32_t>() + off, s.data(), s.size() * 4, cudaMemcpyHostToDevice));
+            h2d_now(p.d_sets.as<uint32_t>() + off, s.data(), s.size() * 4);
             off += s.size();
         }
     }
@@ -2833,7 +2833,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
             for (int rg = 0; rg < tt->n_rg; rg++) pres[i * tt->n_rg + rg] = c.rg_present[rg][pl[i].second];
         }
         dst.alloc(pres.size());
-        VQ_CUDA(cudaMemcpy(dst.p, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+        h2d_now(dst.p, pres.data(), pres.size());
     };
     upload_presence(p.t, p.presence, p.d_present);
     if (p.bt) upload_presence(p.bt, p.bpresence, p.d_bpresent);
@@ -3132,7 +3132,7 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
         p->d_sets.alloc(tot * 4);
         size_t off = 0;
         for (auto& st : p->sets) {
-            VQ_CUDA(cudaMemcpy(p->d_sets.as<uint32_t>() + off, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+            h2d_now(p->d_sets.as<uint32_t>() + off, st.data(), st.size() * 4);
             off += st.size();
         }
     }
@@ -3142,7 +3142,7 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
             for (int rg = 0; rg < t->n_rg; rg++)
                 pres[i * t->n_rg + rg] = t->cols[p->presence[i].first].rg_present[rg][p->presence[i].second];
         p->d_present.alloc(pres.size());
-        VQ_CUDA(cudaMemcpy(p->d_present.p, pres.data(), pres.size(), cudaMemcpyHostToDevice));
+        h2d_now(p->d_present.p, pres.data(), pres.size());
     }
     p->explain = "filter";
     return p.release();

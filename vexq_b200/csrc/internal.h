@@ -34,6 +34,11 @@ void set_error(const std::string& msg);
     } while (0)
 
 // ---- device memory ------------------------------------------------------------------
+// allocations left before an injected failure (-1: none; vexq_debug_fail_alloc)
+extern std::atomic<int> g_fail_alloc_after;
+// bytes held by live DevBufs (vexq_debug_live_device_bytes)
+extern std::atomic<long long> g_live_device_bytes;
+
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
@@ -52,6 +57,23 @@ struct DevBuf {
     void release();
     template <class T> T* as() const { return (T*)p; }
 };
+
+// Host → device copy ordered on stream s: kernels launched on s afterwards see
+// the bytes. (A plain cudaMemcpy from pageable memory may return before its
+// DMA has landed, and the legacy stream it runs on does not order work on
+// non-blocking streams, so a kernel launched next on such a stream could read
+// the old contents.) The host buffer may be reused once this returns: pageable
+// sources are staged before the call returns.
+inline void h2d(void* dst, const void* src, size_t n, cudaStream_t s) {
+    if (n) VQ_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s));
+}
+// A one-time upload that has completed on the device when this returns (for
+// buffers read later from any stream).
+inline void h2d_now(void* dst, const void* src, size_t n) {
+    if (!n) return;
+    VQ_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, cudaStreamLegacy));
+    VQ_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+}
 
 struct PinnedBuf {
     void* p = nullptr;

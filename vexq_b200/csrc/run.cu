@@ -652,7 +652,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         }
         k[nfb + ni] = 1;  // first-occurrence key: min
         p.d_kinds.alloc(k.size() * 4);
-        VQ_CUDA(cudaMemcpy(p.d_kinds.p, k.data(), k.size() * 4, cudaMemcpyHostToDevice));
+        h2d(p.d_kinds.p, k.data(), k.size() * 4, rc.s);
     }
     const int* d_kinds = p.d_kinds.as<int>();
     size_t nout_f = (size_t)G * nfb * 8, nout_i = (size_t)G * (ni + 1) * 8;
@@ -704,7 +704,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
             for (int gi = 0; gi < G; gi++)
                 for (int u = 0; u <= ni; u++) ii[(size_t)gi * (ni + 1) + u] = ident[u];
             p.racc.alloc(img.size());
-            VQ_CUDA(cudaMemcpy(p.racc.p, img.data(), img.size(), cudaMemcpyHostToDevice));
+            h2d(p.racc.p, img.data(), img.size(), rc.s);
         }
         unsigned char* base = p.racc.as<unsigned char>();
         P.racc_fx = (long long*)base;
@@ -1461,7 +1461,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             set_columns(B, bt, false);
             if (bs.seg != p.bseg_cache || !p.d_bseg.p) {
                 p.d_bseg.ensure(std::max<size_t>(bs.seg.size(), 3) * 8);
-                if (!bs.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice));
+                h2d(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, rc.s);
                 p.bseg_cache = bs.seg;
             }
             B.seg = p.d_bseg.as<long long>();
@@ -1539,7 +1539,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         set_columns(B, bt, false);
         if (bs.seg != p.bseg_cache || !p.d_bseg.p) {  // uploaded once per distinct pruning
             p.d_bseg.ensure(std::max<size_t>(bs.seg.size(), 3) * 8);
-            if (!bs.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, cudaMemcpyHostToDevice));
+            h2d(p.d_bseg.p, bs.seg.data(), bs.seg.size() * 8, rc.s);
             p.bseg_cache = bs.seg;
         }
         B.seg = p.d_bseg.as<long long>();
@@ -1698,7 +1698,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     set_columns(P, t, false);
     if (ss.seg != p.seg_cache || !p.d_seg.p) {  // segment list uploaded once per distinct pruning
         p.d_seg.ensure(std::max<size_t>(ss.seg.size(), 3) * 8);
-        if (!ss.seg.empty()) VQ_CUDA(cudaMemcpy(p.d_seg.p, ss.seg.data(), ss.seg.size() * 8, cudaMemcpyHostToDevice));
+        h2d(p.d_seg.p, ss.seg.data(), ss.seg.size() * 8, rc.s);
         p.seg_cache = ss.seg;
     }
     P.seg = p.d_seg.as<long long>();

@@ -20,9 +20,20 @@ void set_error(const std::string& m) { t_err = m; }
 const std::string& last_error() { return t_err; }
 [[noreturn]] void fail(int32_t code, const std::string& msg) { throw Status(code, msg); }
 
+// allocations left before an injected failure (-1: no injection)
+std::atomic<int> g_fail_alloc_after{-1};
+std::atomic<long long> g_live_device_bytes{0};
+
 void DevBuf::alloc(size_t bytes) {
     n = bytes;
     if (bytes == 0) { p = nullptr; return; }
+    int left = g_fail_alloc_after.load();
+    while (left >= 0 && !g_fail_alloc_after.compare_exchange_weak(left, left - 1)) {}
+    if (left == 0) {
+        p = nullptr;
+        n = 0;
+        fail(VEXQ_ENOMEM, "cudaMalloc(" + std::to_string(bytes) + "): out of memory (injected)");
+    }
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -30,9 +41,13 @@ void DevBuf::alloc(size_t bytes) {
         cudaGetLastError();
         fail(VEXQ_ENOMEM, "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
     }
+    g_live_device_bytes += (long long)bytes;
 }
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) {
+        cudaFree(p);
+        g_live_device_bytes -= (long long)n;
+    }
     p = nullptr;
     n = 0;
 }
