@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--impl", default="vexq", choices=["vexq", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="default line without the join and batch objects")
     ap.add_argument("--profile", nargs="?", const="lineitem", default=None,
                     choices=["lineitem", "groupby", "join", "radix", "batch", "filter"],
                     help="profiling driver, no timing: a short fixed launch sequence of one workload for ncu "
@@ -151,34 +152,42 @@ def serve_workload(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_workload(args):
-    """256 independent GROUP BYs: rows log-uniform over 10K-4M, key
+def batch_plans(nplans):
+    """The batching workload's plans: rows log-uniform over 10K-4M, key
     cardinality log-uniform over 2-65,536 with Zipf(1.1) frequencies as
     dictionary codes, float64 values U(0,1e5) at 2 decimals, mixed
-    SUM/COUNT/MIN/MAX/AVG. One step = all plans; the batched arm (one
-    persistent launch per path class, graph replay, autotuned) is the line's
-    value, the same plans one by one through vexq_plan_run are beside it.
-    Device time: CUDA events, kernels only (before the copy back)."""
+    SUM/COUNT/MIN/MAX/AVG. Returns (host tables, plans)."""
     import math
 
     import numpy as np
 
-    from vexq_b200 import build, datagen as D, exec as X, plan as P
-    build.build()
-    X.init(0)
+    from vexq_b200 import datagen as D, plan as P
     rng = np.random.default_rng(2024)
     mixes = [lambda v: [P.sum_(v, "sum"), P.count_star("count")],
              lambda v: [P.min_(v, "min"), P.max_(v, "max"), P.count_star("count")],
              lambda v: [P.avg(v, "avg"), P.sum_(v, "sum")],
              lambda v: [P.sum_(v, "sum"), P.count_star("count"), P.min_(v, "min"), P.max_(v, "max"), P.avg(v, "avg")]]
-    tabs, ops = [], []
-    for i in range(args.plans):
+    hosts, plans = [], []
+    for i in range(nplans):
         rows = int(math.exp(rng.uniform(math.log(1e4), math.log(4e6))))
         card = int(round(math.exp(rng.uniform(math.log(2), math.log(65536)))))
         mix = int(rng.integers(4))
-        g = X.GpuTable(D.zipf_groups(rows, card, seed=i))
-        tabs.append(g)
-        ops.append(X.GpuHashAggregate(g, P.AggPlan(None, [0], mixes[mix](P.col(1)))))
+        hosts.append(D.zipf_groups(rows, card, seed=i))
+        plans.append(P.AggPlan(None, [0], mixes[mix](P.col(1))))
+    return hosts, plans
+
+
+def batch_leg(nplans, steps, warmup, peak, cpu=True):
+    """One step = every plan of the batching workload. The batched arm (one
+    persistent launch per path class, graph replay, autotuned) against the
+    same plans one by one through vexq_plan_run; device time is the kernels
+    alone (CUDA events inside the library, before the copy back). The CPU
+    figure is one pass of the C++ restatement of ParallelHashAggregate over
+    every plan on all host threads."""
+    from vexq_b200 import exec as X
+    hosts, plans = batch_plans(nplans)
+    tabs = [X.GpuTable(h) for h in hosts]
+    ops = [X.GpuHashAggregate(t, p) for t, p in zip(tabs, plans)]
 
     def plain():
         ms, nbytes = 0.0, 0
@@ -189,18 +198,18 @@ def batch_workload(args):
             r.close()
         return ms, nbytes
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         plain()
     pms = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         ms, nbytes = plain()
         pms.append(ms)
     b = X.GpuBatch(ops, autotune=True)
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         for r in b.exec():
             r.close()
     bms, walls = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         res = b.exec()
         walls.append(time.perf_counter() - t0)
@@ -209,17 +218,108 @@ def batch_workload(args):
         bms.append(b.stats()[1])
     explain = b.explain()
     b.close()
+    for op in ops:
+        op.close()
     p_ms, b_ms = statistics.median(pms), statistics.median(bms)
-    line = {"metric": "GB/s scanned", "value": round(nbytes / b_ms / 1e6, 3), "unit": "GB/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(b_ms, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+    out = {"workload": f"{nplans} GROUP BYs, 10K-4M rows, 2-65,536 groups, Zipf(1.1)",
+           "bytes_per_step": nbytes, "rows_per_step": sum(h.nrows for h in hosts),
+           "batched": {"value": round(nbytes / b_ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(b_ms, 4),
+                       "frac_of_peak": round(nbytes / b_ms / 1e6 / peak, 4),
+                       "wall_ms_per_step": round(statistics.median(walls) * 1e3, 3)},
+           "plain_one_by_one": {"value": round(nbytes / p_ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(p_ms, 4)},
+           "batched_over_plain": round(p_ms / b_ms, 3), "tuning": explain}
+    if cpu:
+        from oracle import refcpu as R
+        workers = os.cpu_count() or 1
+        rts = [R.RefTable(h) for h in hosts]
+        t0 = time.perf_counter()
+        for rt, pl in zip(rts, plans):
+            R.agg_raw(rt, pl, workers=workers)
+        cdt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(nbytes / cdt / 1e9, 3), "unit": "GB/s", "ms_per_step": round(cdt * 1e3, 1),
+                               "cores": workers, "cpu": cpu_model(), "kind": "port",
+                               "sample": "one pass over every plan (C++ restatement of ParallelHashAggregate)"}
+    return out
+
+
+def batch_workload(args):
+    """256 independent GROUP BYs (batch_leg) as their own JSON line."""
+    from vexq_b200 import build, exec as X
+    build.build()
+    X.init(0)
+    peaks, _ = measured_peaks()
+    leg = batch_leg(args.plans, args.steps, args.warmup, float(peaks.get("hbm_gbs", 6650.0)), cpu=not args.no_cpu)
+    line = {"metric": "GB/s scanned", "value": leg["batched"]["value"], "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["batched"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Zipf(1.1) dictionary codes, 2-decimal values)",
-            "config": {"workload": f"{args.plans} GROUP BYs, 10K-4M rows, 2-65,536 groups, Zipf(1.1)",
-                       "bytes_per_step": nbytes, "batch": explain},
-            "plain_one_by_one": {"value": round(nbytes / p_ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(p_ms, 4)},
-            "batched_over_plain": round(p_ms / b_ms, 3),
-            "batched_wall_ms_per_step": round(statistics.median(walls) * 1e3, 3)}
+            "config": {"workload": leg["workload"], "bytes_per_step": leg["bytes_per_step"], "batch": leg["tuning"]},
+            **{k: leg[k] for k in ("batched", "plain_one_by_one", "batched_over_plain") if k in leg},
+            "cpu_baseline": leg.get("cpu_baseline")}
     print(json.dumps(line), flush=True)
+
+
+def join_leg(steps, warmup, peak, cpu=True):
+    """The join workload on the plain drop-in: orders (1.5M rows, unique
+    int64 keys) as the build side, items (6M rows, foreign keys uniform over
+    the build keys) as the probe side, Q3 shape (GROUP BY key, SUM, top 10)
+    and Q12 shape (mode IN list, date range, CASE counts by mode). Per query:
+    device ms (CUDA events on the plan's stream around `steps` runs, host work
+    between launches included) and the result's kernel ms; algorithmic bytes
+    are the referenced columns of both sides. The CPU figure is the C++
+    restatement of ParallelHashJoinAggregate on all host threads."""
+    import torch
+
+    from vexq_b200 import datagen as D, exec as X, workloads as W
+    ho, hp = D.orders(1_500_000, seed=5), D.items(6_000_000, 1_500_000, seed=6)
+    go, gp = X.GpuTable(ho), X.GpuTable(hp)
+    stream = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": "orders 1.5M (build) x items 6M (probe), int64 keys"}
+    rts = None
+    if cpu:
+        from oracle import refcpu as R
+        rts = (R.RefTable(ho), R.RefTable(hp))
+    for name, mk in (("q3", W.q3_plan), ("q12", W.q12_plan)):
+        op = X.GpuParallelHashJoinAggregate(go, gp, mk())
+        op.set_stream(stream.cuda_stream)
+        for _ in range(max(warmup, 3)):
+            op.run().close()
+        torch.cuda.synchronize()
+        kms, nbytes, launches = 0.0, 0, 0
+        e0.record(stream)
+        for _ in range(steps):
+            r = op.run()
+            kms += r.kernel_ms
+            nbytes = r.bytes_scanned
+            launches += r.launches
+            r.close()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        kms /= steps
+        q = {"device_ms": round(ms, 4), "kernel_ms": round(kms, 4), "bytes": nbytes,
+             "gbs": round(nbytes / ms / 1e6, 1), "kernel_gbs": round(nbytes / kms / 1e6, 1),
+             "frac_of_peak": round(nbytes / kms / 1e6 / peak, 4), "launches_per_query": launches / steps,
+             "plan": op.explain()}
+        op.close()
+        if rts is not None:
+            from oracle import refcpu as R
+            workers = os.cpu_count() or 1
+            R.join_raw(rts[0], rts[1], mk(), workers=workers)
+            reps, t0 = 0, time.perf_counter()
+            while reps < 2 or (time.perf_counter() - t0 < 4.0 and reps < 10):
+                R.join_raw(rts[0], rts[1], mk(), workers=workers)
+                reps += 1
+            cdt = (time.perf_counter() - t0) / reps
+            q["cpu_port_ms"] = round(cdt * 1e3, 2)
+            q["cpu_port_gbs"] = round(nbytes / cdt / 1e9, 3)
+        out[name] = q
+    if rts is not None:
+        out["cpu_cores"] = os.cpu_count() or 1
+    go.close()
+    gp.close()
+    return out
 
 
 def profile_driver(kind="lineitem"):
@@ -278,6 +378,53 @@ def profile_driver(kind="lineitem"):
             f = X.GpuFilter(gt, pred)
             for _ in range(3):
                 f.bitmap()
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def parity_report(gpu_rows, ref, names):
+    """Float cells of one query against the oracle's serial fold (the
+    reference's row-order result) and its exact sum. A cell whose distance to
+    the serial fold exceeds 1e-12 relative passes only when the GPU value is
+    within 1e-13 of the exact sum and the serial fold's own error explains
+    the gap; such cells are listed by name."""
+    import math
+    ref_rows = ref.rows()
+    worst = {"gpu_vs_serial": 0.0, "gpu_vs_exact": 0.0, "serial_vs_exact": 0.0}
+    via_exact, ok = [], len(gpu_rows) == len(ref_rows)
+    for i, (g, r) in enumerate(zip(gpu_rows, ref_rows)):
+        for j, (a, b) in enumerate(zip(g, r)):
+            if not isinstance(a, float) or not isinstance(b, float) or math.isnan(a) or math.isnan(b):
+                ok = ok and (a == b or (isinstance(a, float) and isinstance(b, float)))
+                continue
+            ex = ref.exact[j][i]
+            sc = max(abs(b), 1e-300)
+            d = abs(a - b) / sc
+            worst["gpu_vs_serial"] = max(worst["gpu_vs_serial"], d)
+            if not math.isnan(ex):
+                se = max(abs(ex), 1e-300)
+                eg, er = abs(a - ex) / se, abs(b - ex) / se
+                worst["gpu_vs_exact"] = max(worst["gpu_vs_exact"], eg)
+                worst["serial_vs_exact"] = max(worst["serial_vs_exact"], er)
+                if d > 1e-12:
+                    passed = eg <= 1e-13 and abs(a - b) / se <= er + 1e-13
+                    ok = ok and passed
+                    via_exact.append({"row": i, "col": names[j], "gpu_vs_serial": d, "gpu_vs_exact": eg,
+                                      "serial_vs_exact": er})
+            elif d > 1e-12:
+                ok = False
+    return {"rows": len(gpu_rows), "pass": ok, **{k: float(f"{v:.3g}") for k, v in worst.items()},
+            "cells_passing_via_exact_arbiter": via_exact}
 
 
 def measured_peaks():
@@ -504,7 +651,7 @@ def main():
                "d2h_bytes_per_step": d2h, "ms_per_step": round(dt * 1e3, 3)}
 
     # ---- CPU baseline: the oracle's ParallelHashAggregate on host cores ----
-    cpu = None
+    cpu = parity = None
     if rank == 0 and not args.no_cpu:
         from oracle import refcpu as R
         tbl = R.RefTable(host)
@@ -516,9 +663,19 @@ def main():
             cpu_reference_step(tbl, plans, workers)
             reps += 1
         cdt = (time.perf_counter() - t0) / reps
-        cpu = {"value": round(step_bytes / cdt / 1e9, 3), "unit": "GB/s", "cores": workers, "kind": "port",
+        cpu = {"value": round(step_bytes / cdt / 1e9, 3), "unit": "GB/s", "cores": workers, "cpu": cpu_model(),
+               "kind": "port",
                "sample": f"{reps} full steps ({NROWS} rows, Q1+Q6) of the C++ restatement of "
                          "ParallelHashAggregate, one row group per morsel"}
+        # the same oracle as the checker: the serial fold and exact sums of
+        # both queries against one GPU run of each
+        parity = {}
+        for name, op, pl in (("q1", q1, plans[0]), ("q6", q6, plans[1])):
+            r = op.run()
+            rows = r.rows()
+            names = r.names
+            r.close()
+            parity[name] = parity_report(rows, R.agg(tbl, pl, workers=0), names)
 
     peaks, src = measured_peaks()
     peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -541,7 +698,11 @@ def main():
             "rows_per_s": round(2 * NROWS * world / (ms_step / 1e3), 1),
             "kernel_only_gbs": round(step_bytes / ((q1_scan + q6_scan) / 1e3) / 1e9, 1),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "parity": parity,
         }
+        if world == 1 and not args.no_extra:
+            line["join"] = join_leg(max(5, args.steps // 2), args.warmup, peak, cpu=not args.no_cpu)
+            line["batch"] = batch_leg(args.plans, max(3, args.steps // 4), args.warmup, peak, cpu=not args.no_cpu)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

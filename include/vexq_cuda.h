@@ -341,6 +341,52 @@ int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
 int32_t vexq_selvec_from_bits(const uint8_t* bits, int64_t nrows, int64_t block,
                               uint16_t* out_sel, int32_t* out_len);
 
+/* ---- Filter as a streaming operator: exec.Filter over exec.TableScan ----
+ * Replaces exec.NewFilter(TableScan, predicate) and its Next
+ * (exec/filter.go:40-78, exec/scan.go:199-236). Open evaluates the predicate
+ * once over the row groups [rg_start, rg_end) (rg_end < 0: to the end) that
+ * the zone maps keep, and builds every 1024-row block's selection vector on
+ * the device. Next hands out one block per call, in row order, as the scan's
+ * batch with its SelVec installed: the table's columns for the block's rows
+ * (from a pinned host copy of the HBM columns, made on first use), `length`
+ * = len(SelVec) kept rows among `physical` rows. Blocks where no row
+ * survives are skipped, as Filter.Next skips them; length 0 is EOF. A batch
+ * never spans two row groups. The views and the SelVec stay valid until the
+ * next call on this filter (exec/filter.go:10-28's ownership contract).
+ * STRING vectors carry codes of the column's table-wide dictionary, which the
+ * view's dictionary fields hold. Re-filling the table invalidates open
+ * filters. */
+typedef struct vexq_filter_s* vexq_filter_t;
+typedef struct {
+    int32_t                 ncols;
+    int32_t                 length;    /* len(SelVec); 0 at EOF              */
+    int32_t                 physical;  /* rows in the vectors (<= 1024)      */
+    int32_t                 rg;        /* row group of the block             */
+    int64_t                 row0;      /* table row of the vectors' first row */
+    const uint16_t*         sel;       /* ascending indices into [0, physical) */
+    const vexq_vector_view* cols;      /* every column of the table          */
+} vexq_filter_batch;
+int32_t vexq_filter_open(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
+                         const int32_t* children, int32_t nchildren, int32_t predicate,
+                         int32_t rg_start, int32_t rg_end, vexq_filter_t* out);
+int32_t vexq_filter_next(vexq_filter_t f, vexq_filter_batch* out);
+/* Rows kept, blocks scanned, and the device milliseconds of open. */
+int32_t vexq_filter_stats(vexq_filter_t f, int64_t* selected, int64_t* blocks, double* kernel_ms);
+int32_t vexq_filter_close(vexq_filter_t f);
+
+/* ---- Project over a filtered scan: exec.Project -------------------------
+ * Replaces exec.NewProject(Filter(TableScan), exprs) (exec/project.go:64-128):
+ * each of the nexprs expressions (roots into nodes; names may be NULL) is
+ * evaluated on the device for the rows the predicate keeps (predicate < 0:
+ * every row of the kept row groups), and the kept rows are written compacted
+ * in row order, as Project.materialize writes them under a SelVec. The result
+ * has no SelVec (rows are materialised) and is read with vexq_result_next in
+ * 1024-row batches. A STRING expression must be a column reference. */
+int32_t vexq_project_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
+                         const int32_t* children, int32_t nchildren, int32_t predicate,
+                         const int32_t* roots, const char* const* names, int32_t nexprs,
+                         int32_t rg_start, int32_t rg_end, vexq_result_t* out);
+
 /* ---- batching: many aggregates in one persistent launch ----------------
  * No reference counterpart: the Go engine runs one operator tree per query.
  * A batch holds n prepared plans (each over its own table). Aggregate plans
@@ -420,8 +466,12 @@ int32_t vexq_debug_live_device_bytes(int64_t* out);
 /* ---- global aggregate without allocation --------------------------------
  * No counterpart in the reference: its operators work on the Go heap.
  * Runs an aggregate plan without GROUP BY (one result row) through the same
- * kernels as vexq_plan_run but allocates no device, pinned or managed
- * memory: the per-block partials, row ranges, merge outputs and error flag
+ * scan kernel as vexq_plan_run but allocates no device, pinned or managed
+ * memory. The per-block partials are always merged by the separate merge
+ * kernel (a fixed-order TwoSum merge); where vexq_plan_run folds the merge
+ * into the scan (float sums merged exactly in fixed point), float SUM/AVG
+ * may differ from its result by rounding in the last bits. Otherwise the
+ * results are equal. Memory: the per-block partials, row ranges, merge outputs and error flag
  * live in one static device array of VEXQ_NOALLOC_SCRATCH_BYTES per device,
  * and the row is written to caller memory. Meant for callers that must not
  * allocate: a serving loop with other queries in flight (cudaMalloc and

@@ -13,7 +13,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("VEXQ_REFERENCE_ROOT", "/root/reference")
+# the vexq checkout: VEXQ_REFERENCE_ROOT, else a directory named "reference"
+# beside this repository (absent on machines that only run the prebuilt files)
+REF_ROOT = os.environ.get("VEXQ_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 REF_FILTER_SRC = os.path.join(REF_ROOT, "bench", "simd_filter", "cpp", "filter_kernel.cpp")
 ORACLE_SO = os.path.join(HERE, "_build", "librefcpu.so")
 REF_FILTER_SO = os.path.join(HERE, "_ref", "libreffilter.so")

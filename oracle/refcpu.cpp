@@ -2173,6 +2173,62 @@ int32_t ref_filter_run(ref_table_t t, const vexq_expr* nodes, int32_t nnodes, co
     });
 }
 
+// TableScan (zone-map skip, exec/scan.go:212-215) → Filter (filter.go:49-78,
+// BoolToSelVecInto) → Project (project.go:64-128): each expression evaluated
+// over the batch's physical rows and materialised through the SelVec
+// (Project.materialize), batches concatenated in row order. The zone check
+// uses the predicate tree, as planner.Physical hands TableScan its zonePred.
+int32_t ref_project_run(ref_table_t t, const vexq_expr* nodes, int32_t nnodes, const int32_t* children,
+                        int32_t nchildren, int32_t predicate, const int32_t* roots, int32_t nroots, int32_t rg_start,
+                        int32_t rg_end, ref_result_t* out) {
+    return guarded([&]() -> int32_t {
+        Nodes N{nodes, nnodes, children, nchildren};
+        const Table& tb = t->t;
+        Schema s = tableSchema(tb);
+        XP pred;
+        if (predicate >= 0) {
+            pred = build(N, predicate, s);
+            if (pred->type != VEXQ_TYPE_BOOL) throw Error("filter predicate must return BOOL");
+        }
+        std::vector<XP> ex;
+        for (int j = 0; j < nroots; j++) ex.push_back(build(N, roots[j], s));
+        auto* r = new ref_result_s;
+        std::unique_ptr<ref_result_s> keep(r);
+        r->cols.resize(nroots);
+        for (int j = 0; j < nroots; j++) r->cols[j].type = ex[j]->type;
+        const int rge = rg_end < 0 ? tb.n_rg : std::min(rg_end, tb.n_rg);
+        Scan sc(&tb);
+        Batch b;
+        Vec m;
+        for (int rg = std::max(0, rg_start); rg < rge; rg++) {
+            if (predicate >= 0 && !zoneEval(N, predicate, tb, rg)) continue;
+            for (int64_t s0 = tb.rgStart(rg); s0 < tb.rgEnd(rg); s0 += kBlockRows) {
+                const int n = (int)std::min<int64_t>(kBlockRows, tb.rgEnd(rg) - s0);
+                sc.load(rg, s0, n, b);
+                if (pred) {
+                    selectInto(b, eval(pred.get(), b));
+                    if (b.sel.empty()) continue;
+                }
+                for (int j = 0; j < nroots; j++) {
+                    const Vec* v = eval(ex[j].get(), b);
+                    const Vec* src = v;
+                    if (b.has_sel) { materialize(*v, b.sel, m); src = &m; }
+                    OutCol& oc = r->cols[j];
+                    for (int i = 0; i < src->n; i++) {
+                        oc.bits.push_back(src->valid[i] ? extractInt64(*src, i) : 0);
+                        oc.valid.push_back(src->valid[i]);
+                        oc.strs.push_back(src->type == VEXQ_TYPE_STRING && src->valid[i] ? src->str(i) : std::string());
+                        oc.exact.push_back(std::nan(""));
+                    }
+                }
+                r->rows += b.rows();
+            }
+        }
+        *out = keep.release();
+        return VEXQ_OK;
+    });
+}
+
 // HAVING (planner/build.go:59-75): the Filter above the aggregate runs over
 // the aggregate's output batches with the WHERE machinery, so the output
 // columns become a one-row-group table scanned and filtered like any other;

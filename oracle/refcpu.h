@@ -58,6 +58,12 @@ int32_t ref_result_get(ref_result_t r, int64_t row, int32_t col, int64_t* bits,
 /* Exact sum (correctly rounded, Shewchuk) of the float aggregate inputs per
  * output row, for SUM/AVG columns; NaN for others. Serial results only. */
 int32_t ref_result_exact(ref_result_t r, int64_t row, int32_t col, double* out);
+/* Filter (predicate < 0: none) → Project of nroots expressions over row
+ * groups [rg_start, rg_end) with zone-map pruning; rows in row order. */
+int32_t ref_project_run(ref_table_t t, const vexq_expr* nodes, int32_t nnodes,
+                        const int32_t* children, int32_t nchildren, int32_t predicate,
+                        const int32_t* roots, int32_t nroots, int32_t rg_start, int32_t rg_end,
+                        ref_result_t* out);
 /* HAVING over a result, then the column cut and ORDER BY / LIMIT. */
 int32_t ref_result_having(ref_result_t r, const vexq_expr* nodes, int32_t nnodes,
                           const int32_t* children, int32_t nchildren, int32_t predicate,

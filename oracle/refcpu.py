@@ -42,6 +42,9 @@ def lib() -> C.CDLL:
         L.ref_filter_run.argtypes = [vp, C.POINTER(abi.Expr), i32, C.POINTER(i32), i32, i32,
                                      C.POINTER(C.c_uint8), C.POINTER(i64)]
         L.ref_filter_run.restype = i32
+        L.ref_project_run.argtypes = [vp, C.POINTER(abi.Expr), i32, C.POINTER(i32), i32, i32, C.POINTER(i32), i32,
+                                      i32, i32, C.POINTER(vp)]
+        L.ref_project_run.restype = i32
         L.ref_result_rows.argtypes = [vp]
         L.ref_result_rows.restype = i64
         L.ref_result_cols.argtypes = [vp]
@@ -198,6 +201,16 @@ def filter_bits(table: RefTable, pred):
     cnt = C.c_int64()
     _check(lib().ref_filter_run(table.h, nodes, nn, ch, nc, root, out, C.byref(cnt)))
     return bytes(out)[:nbytes], cnt.value
+
+
+def project(table: RefTable, exprs, predicate=None, rg_start: int = 0, rg_end: int = -1) -> RefResult:
+    """Filter → Project over the table (ref_project_run): rows in row order."""
+    from vexq_b200.plan import project_arrays
+    keep, nodes, nn, ch, nc, root, roots = project_arrays(predicate, exprs)
+    r = (C.c_int32 * max(len(roots), 1))(*roots)
+    h = C.c_void_p()
+    _check(lib().ref_project_run(table.h, nodes, nn, ch, nc, root, r, len(roots), rg_start, rg_end, C.byref(h)))
+    return RefResult(h)
 
 
 # ---- the reference's own AVX2 filter kernel (oracle/_ref) -------------------

@@ -149,3 +149,41 @@ def test_batch_run_and_empty(mixed):
     abi.check(L.vexq_batch_run(plans, 3, outs))
     check_against_single([X.Result(C.c_void_p(outs[k])) for k in range(3)], single, ops[:3])
     abi.check(L.vexq_batch_run(plans, 0, outs))
+
+
+def test_c3_batch_as_configured(gpu_lib):
+    """The batching workload as configured: 256 GROUP BYs, rows log-uniform
+    over 10K-4M, 2-65,536 Zipf(1.1) groups, mixed SUM/COUNT/MIN/MAX/AVG, one
+    autotuned batch. Every result against the oracle's serial fold: keys,
+    counts, MIN and MAX exact; group-table float sums equal to the exact sum
+    bit for bit; register-path float cells within 1e-12 of the serial fold
+    and 1e-13 of the exact sum."""
+    import bench
+    from tests.helpers import assert_float_vs_exact
+    X = gpu_lib
+    hosts, plans = bench.batch_plans(256)
+    assert sum(h.nrows for h in hosts) > 100_000_000
+    tabs = [X.GpuTable(h) for h in hosts]
+    ops = [X.GpuHashAggregate(t, p) for t, p in zip(tabs, plans)]
+    try:
+        b = X.GpuBatch(ops, autotune=True)
+        res = b.exec()
+        regs = table = 0
+        for k, (h, pl, r) in enumerate(zip(hosts, plans, res)):
+            rows = r.rows()
+            ref = R.agg(R.RefTable(h), pl, workers=0)
+            if "path=regs" in ops[k].explain():
+                assert_float_vs_exact(rows, ref, ordered=True)
+                regs += 1
+            else:
+                assert_rows_match(rows, ref.rows(), ordered=True)
+                assert_sums_exact(r, ref)
+                table += 1
+            r.close()
+        assert regs > 0 and table > 0
+        b.close()
+    finally:
+        for op in ops:
+            op.close()
+        for t in tabs:
+            t.close()

@@ -129,9 +129,23 @@ def test_q3_join_all_groups_small(gpu_lib, join_small):
 
 
 def test_q3_join_top10_full(gpu_lib, join_full):
+    """The join workload at full size (1.5M build x 6M probe rows) against the
+    oracle's serial fold: keys exact, revenue within 1e-12, and every revenue
+    equal to the exact sum bit for bit (the group table sums in fixed point)."""
     o, i = join_full
-    g, r = run_join(gpu_lib, o, i, W.q3_plan(), workers=8)
-    assert_rows_match(g.rows(), r.rows(), ordered=True, rtol=1e-9)
+    g, r = run_join(gpu_lib, o, i, W.q3_plan(), workers=0)
+    assert g.nrows == 10
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_sums_exact(g, r)
+
+
+def test_q12_join_full(gpu_lib, join_full):
+    """The Q12-shape join at full size against the serial oracle: the CASE
+    counts are integer sums, compared bit for bit."""
+    o, i = join_full
+    g, r = run_join(gpu_lib, o, i, W.q12_plan(), workers=0)
+    assert g.nrows == 2
+    assert_rows_match(g.rows(), r.rows(), ordered=True, rtol=0.0)
 
 
 def test_q12_join_case_counts(gpu_lib, join_small):

@@ -20,7 +20,11 @@ from vexq_b200.table import HostTable, date_column, float_column, int_column
 
 pytestmark = pytest.mark.gpu
 
-FLOAT_RTOL = 1e-12  # both paths run the same kernels; equality is expected
+# The scan kernel is the same. The merge may differ: where vexq_plan_run merges
+# float sums exactly inside the scan, this entry point merges the per-block
+# partials with the fixed-order TwoSum merge, so float cells agree to
+# rounding; every other cell is compared exactly.
+FLOAT_RTOL = 1e-12
 
 
 def noalloc(op, n_out, rg_start=0, rg_end=-1, stream=None):

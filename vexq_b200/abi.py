@@ -1,8 +1,8 @@
 """ctypes mirror of include/vexq_cuda.h and the loader for libvexqcuda.so.
 
-The structures here are the C ABI a Go cgo shim binds;
-Python uses them for tests and the benchmark. Loading fails loudly when the
-shared library has not been built: there is no CPU fallback behind this API.
+The structures here are the C ABI a Go cgo shim binds; Python uses them for
+tests and the benchmark. Loading fails loudly when the shared library has not
+been built: there is no CPU fallback behind this API.
 """
 from __future__ import annotations
 
@@ -131,6 +131,11 @@ class BatchView(C.Structure):
     _fields_ = [("ncols", C.c_int32), ("length", C.c_int32), ("cols", C.POINTER(VectorView))]
 
 
+class FilterBatch(C.Structure):
+    _fields_ = [("ncols", C.c_int32), ("length", C.c_int32), ("physical", C.c_int32), ("rg", C.c_int32),
+                ("row0", C.c_int64), ("sel", C.POINTER(C.c_uint16)), ("cols", C.POINTER(VectorView))]
+
+
 # Every symbol include/vexq_cuda.h declares (checked by the CPU test suite).
 BATCH_AUTOTUNE = 1  # VEXQ_BATCH_AUTOTUNE
 SERVE_NO_BATCH = 1  # VEXQ_SERVE_NO_BATCH
@@ -145,6 +150,7 @@ EXPORTS = [
     "vexq_result_num_rows", "vexq_result_num_cols", "vexq_result_next",
     "vexq_result_free", "vexq_result_stats", "vexq_result_scan_ms", "vexq_result_info", "vexq_plan_set_stream",
     "vexq_filter_run", "vexq_selvec_from_bits",
+    "vexq_filter_open", "vexq_filter_next", "vexq_filter_stats", "vexq_filter_close", "vexq_project_run",
     "vexq_batch_run",
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
@@ -210,6 +216,12 @@ def load() -> C.CDLL:
         "vexq_filter_run": (i32, [vp, C.POINTER(Expr), i32, C.POINTER(i32), i32, i32, i64, i64,
                                   C.POINTER(C.c_uint8), C.POINTER(i64)]),
         "vexq_selvec_from_bits": (i32, [C.POINTER(C.c_uint8), i64, i64, C.POINTER(C.c_uint16), C.POINTER(i32)]),
+        "vexq_filter_open": (i32, [vp, C.POINTER(Expr), i32, C.POINTER(i32), i32, i32, i32, i32, C.POINTER(vp)]),
+        "vexq_filter_next": (i32, [vp, C.POINTER(FilterBatch)]),
+        "vexq_filter_stats": (i32, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_double)]),
+        "vexq_filter_close": (i32, [vp]),
+        "vexq_project_run": (i32, [vp, C.POINTER(Expr), i32, C.POINTER(i32), i32, i32, C.POINTER(i32),
+                                   C.POINTER(C.c_char_p), i32, i32, i32, C.POINTER(vp)]),
         "vexq_batch_run": (i32, [C.POINTER(vp), i32, C.POINTER(vp)]),
         "vexq_server_start": (i32, [i64, i32, i32, C.c_uint32, C.POINTER(vp)]),
         "vexq_server_stats": (i32, [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]),

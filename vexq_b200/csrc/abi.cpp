@@ -86,6 +86,7 @@ int32_t vexq_table_upload(const vexq_column_desc* cols, int32_t ncols, int64_t n
 int32_t vexq_table_destroy(vexq_table_t t) {
     return guard([&]() -> int32_t {
         if (!t) return VEXQ_OK;
+        drop_host_mirror(t->t);
         destroy_table(t->t);
         delete t;
         return VEXQ_OK;

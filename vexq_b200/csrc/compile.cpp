@@ -3069,6 +3069,8 @@ void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* chil
     p.having_schema = std::move(schema);
 }
 
+static void upload_scan_tables(Plan& p);
+
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred) {
     std::unique_ptr<Plan> p(new Plan);
     p->t = t;
@@ -3126,25 +3128,164 @@ Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t
     os << "}\n";
     p->src_main = os.str();
     p->k_main = jit_get(p->src_main, "vq_filter", kBlock, p->smem);
-    if (!p->sets.empty()) {
+    upload_scan_tables(*p);
+    p->explain = "filter";
+    return p.release();
+}
+
+// Large IN sets and StringEqExpr presence rows of a one-table scan plan, to
+// the device once.
+static void upload_scan_tables(Plan& p) {
+    const Table* t = p.t;
+    if (!p.sets.empty()) {
         size_t tot = 0;
-        for (auto& st : p->sets) tot += st.size();
-        p->d_sets.alloc(tot * 4);
+        for (auto& st : p.sets) tot += st.size();
+        p.d_sets.alloc(tot * 4);
         size_t off = 0;
-        for (auto& st : p->sets) {
-            h2d_now(p->d_sets.as<uint32_t>() + off, st.data(), st.size() * 4);
+        for (auto& st : p.sets) {
+            h2d_now(p.d_sets.as<uint32_t>() + off, st.data(), st.size() * 4);
             off += st.size();
         }
     }
-    if (!p->presence.empty()) {
-        std::vector<uint8_t> pres(p->presence.size() * (size_t)t->n_rg, 0);
-        for (size_t i = 0; i < p->presence.size(); i++)
+    if (!p.presence.empty()) {
+        std::vector<uint8_t> pres(p.presence.size() * (size_t)t->n_rg, 0);
+        for (size_t i = 0; i < p.presence.size(); i++)
             for (int rg = 0; rg < t->n_rg; rg++)
-                pres[i * t->n_rg + rg] = t->cols[p->presence[i].first].rg_present[rg][p->presence[i].second];
-        p->d_present.alloc(pres.size());
-        h2d_now(p->d_present.p, pres.data(), pres.size());
+                pres[i * t->n_rg + rg] = t->cols[p.presence[i].first].rg_present[rg][p.presence[i].second];
+        p.d_present.alloc(pres.size());
+        h2d_now(p.d_present.p, pres.data(), pres.size());
     }
-    p->explain = "filter";
+}
+
+// Filter → Project over one table (exec/filter.go:49-78, exec/project.go:64-128).
+// Two generated kernels over the same chunk loop:
+//   vq_pmark   the predicate's selection bitmap (bit r = row r kept; every
+//              row of the scanned ranges when there is no predicate), words
+//              assembled with warp shuffles, one atomicOr a word;
+//   vq_pwrite  (projections only) for every kept row, its place in row order
+//              (the chunk's offset from an exclusive scan of per-128-row-chunk
+//              counts, plus the kept rows before it in its chunk) and the
+//              projected values: raw 8-byte images into P.qpay[j % 8] and
+//              validity bytes into P.qpayv[j % 8] for expressions j of the
+//              group P.mode (eight expressions a launch).
+Plan* compile_select(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred,
+                     const int32_t* roots, int nroots) {
+    if (nroots < 0 || nroots > 64) fail(VEXQ_EINVAL, "project: between 0 and 64 expressions");
+    if (nroots > 0 && !roots) fail(VEXQ_EINVAL, "project: null expression roots");
+    if (pred >= 0 && (!nodes || pred >= nnodes)) fail(VEXQ_EINVAL, "predicate index out of range");
+    std::unique_ptr<Plan> p(new Plan);
+    p->t = t;
+    p->range_epoch = t->range_epoch;
+    Translator tr{*p, nodes, nnodes, children, nchildren, t, nullptr};
+    if (pred >= 0) {
+        p->pred = tr.tr(pred);
+        if (p->ir[p->pred].type != VEXQ_TYPE_BOOL) fail(VEXQ_EINVAL, "exec: filter predicate must return BOOL");
+    }
+    for (int j = 0; j < nroots; j++) {
+        if (roots[j] < 0 || roots[j] >= nnodes) fail(VEXQ_EINVAL, "project: expression index out of range");
+        const int r = tr.tr(roots[j]);
+        const INode& n = p->ir[r];
+        if (n.type == VEXQ_TYPE_STRING && n.k != NK::Col)
+            fail(VEXQ_ENOTSUP, "project: a STRING expression must be a column reference");
+        p->key_nodes.push_back(r);
+    }
+    analyze(*p);
+    for (auto& n : p->ir) {
+        if (n.k == NK::InCodes && n.codes.size() > 64) {
+            if ((int)p->sets.size() >= VQ_MAXSETS) fail(VEXQ_ENOTSUP, "too many large IN/LIKE sets");
+            std::vector<uint32_t> bits((n.codes.size() + 31) / 32, 0);
+            for (size_t c = 0; c < n.codes.size(); c++) if (n.codes[c]) bits[c >> 5] |= 1u << (c & 31);
+            n.set_idx = (int)p->sets.size();
+            p->sets.push_back(std::move(bits));
+        }
+    }
+    if (pred >= 0) {
+        copy_zone_tree(*p, nodes, nnodes, children, nchildren);
+        keep_zone_strings(*p, nodes, nnodes);
+        p->zn_pred = pred;
+    }
+    p->staged = false;
+    p->pipeline = false;
+    std::set<int> pcols, wcols;
+    if (p->pred >= 0) collect_cols(*p, p->pred, pcols);
+    for (int r : p->key_nodes) collect_cols(*p, r, wcols);
+    // the mark kernel
+    {
+        std::ostringstream os;
+        ScanLoop loop(*p, t, pcols, kBlock, "pmark");
+        p->tile = loop.tile_rows();
+        p->smem = loop.smem();
+        os << prelude_source() << "\n";
+        loop.prologue(os);
+        os << kernel_head("vq_pmark", kBlock);
+        loop.open(os);
+        os << "        unsigned nib = 0u;\n";
+        os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+        os << "            const long long r = r0 + k;\n";
+        os << "            if (r < s0 || r >= s1) continue;\n";
+        if (p->pred >= 0) {
+            Gen g(*p, os);
+            g.emit(p->pred);
+            os << "            if (x" << p->pred << " && ok" << p->pred << ") nib |= 1u << k;\n";
+        } else {
+            os << "            nib |= 1u << k;\n";
+        }
+        os << "        }\n";
+        os << "        const unsigned long long spread = ((unsigned long long)nib) << (4 * (lane & 7));\n";
+        os << "        unsigned word = (unsigned)spread;\n";
+        os << "        for (int o = 1; o < 8; o <<= 1) word |= __shfl_xor_sync(0xffffffffu, word, o);\n";
+        os << "        if ((lane & 7) == 0 && word) atomicOr(reinterpret_cast<unsigned*>(P.acc_i) + (r0 - lane * 4) / 32 + (lane >> 3), word);\n";
+        loop.close(os);
+        os << "}\n";
+        p->src_main = os.str();
+        p->k_main = jit_get(p->src_main, "vq_pmark", kBlock, p->smem);
+    }
+    // the write kernel
+    if (nroots > 0) {
+        std::ostringstream os;
+        ScanLoop loop(*p, t, wcols, kBlock, "pwrite");
+        os << prelude_source() << "\n";
+        loop.prologue(os);
+        os << kernel_head("vq_pwrite", kBlock);
+        loop.open(os);
+        os << "        const unsigned* vq_w = reinterpret_cast<const unsigned*>(P.acc_i);\n";
+        os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+        os << "            const long long r = r0 + k;\n";
+        os << "            if (r < s0 || r >= s1) continue;\n";
+        os << "            const unsigned wv = vq_w[r >> 5];\n";
+        os << "            if (!((wv >> (r & 31)) & 1u)) continue;\n";
+        os << "            const long long cw = (r >> 7) << 2;\n";
+        os << "            int below = __popc(wv & ((1u << (r & 31)) - 1u));\n";
+        os << "            for (long long w = cw; w < (r >> 5); w++) below += __popc(vq_w[w]);\n";
+        os << "            const long long pos = P.first[r >> 7] + below;\n";
+        Gen g(*p, os);
+        for (int j = 0; j < nroots; j++) {
+            const int r = p->key_nodes[j];
+            const INode& n = p->ir[r];
+            os << "            if (P.mode == " << j / 8 << ") {\n";
+            g.ind = "                ";
+            std::fill(g.done.begin(), g.done.end(), 0);
+            g.emit(r);
+            std::string X = "x" + std::to_string(r), OK = "ok" + std::to_string(r), bits;
+            switch (n.type) {
+                case VEXQ_TYPE_FLOAT64: bits = "(unsigned long long)__double_as_longlong(" + X + ")"; break;
+                case VEXQ_TYPE_INT64: bits = "(unsigned long long)" + X; break;
+                case VEXQ_TYPE_DATE: bits = "(unsigned long long)(long long)" + X; break;
+                case VEXQ_TYPE_STRING: bits = "(unsigned long long)" + X; break;
+                default: bits = "(" + X + " ? 1ull : 0ull)"; break;
+            }
+            os << "                P.qpay[" << j % 8 << "][pos] = " << OK << " ? " << bits << " : 0ull;\n";
+            os << "                P.qpayv[" << j % 8 << "][pos] = " << OK << " ? 1 : 0;\n";
+            os << "            }\n";
+        }
+        os << "        }\n";
+        loop.close(os);
+        os << "}\n";
+        p->src_build = os.str();
+        p->k_build = jit_get(p->src_build, "vq_pwrite", kBlock, 0);
+    }
+    upload_scan_tables(*p);
+    p->explain = nroots ? "project" : "filter";
     return p.release();
 }
 
@@ -3240,25 +3381,13 @@ void set_plan_constants(const Plan& p, VQParams& P) {
 
 ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& mask, int rg_start, int rg_end, int unit) {
     ScanSegs s;
-    const long long U = unit;
-    long long chunks = 0;
-    int rg = rg_start;
-    while (rg < rg_end) {
-        if (!mask[rg]) { rg++; continue; }
-        int e = rg;
-        while (e < rg_end && mask[e]) e++;
-        long long a = t.rg_start(rg), b = t.rg_end(e - 1);
-        if (b > a) {
-            s.seg.push_back(a);
-            s.seg.push_back(b);
-            s.seg.push_back(chunks);
-            long long base = a & ~(U - 1);
-            chunks += (b - base + U - 1) / U;
-            s.rows += b - a;
-        }
-        rg = e;
-    }
-    s.nchunks = chunks;
+    s.nchunks = walk_segments(t, [&](int rg) { return mask[rg] != 0; }, rg_start, rg_end, unit,
+                              [&](long long a, long long b, long long c0) {
+                                  s.seg.push_back(a);
+                                  s.seg.push_back(b);
+                                  s.seg.push_back(c0);
+                                  s.rows += b - a;
+                              });
     return s;
 }
 

@@ -95,30 +95,20 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
     const int rgs = std::max(0, rg_start);
     long long seg[3 * kMaxSegments];
     int nseg = 0;
-    long long chunks = 0;
-    const long long U = p.tile;
-    for (int rg = rgs; rg < rge;) {
-        if (!zone_eval(p, p.zn_pred, t, rg)) { rg++; continue; }
-        int e = rg + 1;
-        while (e < rge && zone_eval(p, p.zn_pred, t, e)) e++;
-        long long a = t.rg_start(rg), b = t.rg_end(e - 1);
-        if (b > a) {
+    const long long chunks = walk_segments(
+        t, [&](int rg) { return zone_eval(p, p.zn_pred, t, rg); }, rgs, rge, p.tile,
+        [&](long long a, long long b, long long c0) {
             if (nseg == kMaxSegments)
                 fail(VEXQ_EINVAL, "more than 512 row ranges remain after zone-map pruning; the no-allocation run keeps at most 512");
             seg[3 * nseg] = a;
             seg[3 * nseg + 1] = b;
-            seg[3 * nseg + 2] = chunks;
-            chunks += (b - (a & ~(U - 1)) + U - 1) / U;
+            seg[3 * nseg + 2] = c0;
             nseg++;
-        }
-        rg = e;
-    }
+        });
 
     // grid as the plain path sizes it, shrunk while the partials do not fit
     const JitKernel& k = p.k_main;
-    const int per_sm = std::max(1, k.max_blocks_per_sm);
-    const long long want = p.staged ? chunks : (chunks + k.block / 32 - 1) / (k.block / 32);
-    int grid = (int)std::max<long long>(1, std::min<long long>((long long)sm_count() * per_sm, want));
+    int grid = grid_for(k, chunks, p.staged, p.grid_per_sm);
     const size_t fixed = round256(merged + 16) + round256((size_t)(nfb + ni + 1) * 4) + round256((size_t)std::max(nseg, 1) * 24);
     const size_t per_block = (size_t)nfb * 8 + (size_t)(ni + 1) * 8;
     auto need = [&](int g) { return fixed + round256((size_t)g * nfb * 8) + round256((size_t)g * (ni + 1) * 8); };
@@ -180,9 +170,7 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
         VQ_CUDA(cudaGetLastError());
         VQ_CUDA(cudaMemcpyAsync(stage, d_out, merged + 4, cudaMemcpyDeviceToHost, s));
         VQ_CUDA(cudaStreamSynchronize(s));
-        const int herr = *(const int*)(stage + merged);
-        if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
-        if (herr) fail(VEXQ_EDEVICE, "the scan kernel reported error flags " + std::to_string(herr));
+        check_regs_flags(*(const int*)(stage + merged));
         cnt = hi[p.slot_pos[0]];
     }
 

@@ -232,6 +232,11 @@ struct OutColumn {
 Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d);
 Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d);
 Plan* compile_filter(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred);
+// Filter (pred >= 0, else every row) → Project (nroots expressions, 0: none)
+// over one table: k_main = vq_pmark (selection bitmap), k_build = vq_pwrite
+// (kept rows' projected values in row order); key_nodes = the expressions' IR.
+Plan* compile_select(Table* t, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int pred,
+                     const int32_t* roots, int nroots);
 void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int root, int visible);
 bool zone_eval(const Plan& p, int root, const Table& t, int rg);
 // Copies the plan's launch-time constants (literals, float-sum windows, cache size) into P.
@@ -315,7 +320,41 @@ struct VQMergeDesc {           // one register-path plan's partials
     int e0;                    // first global merge entry of this plan
 };
 ScanSegs make_segments(const Table& t, const std::vector<uint8_t>& rg_mask, int rg_start, int rg_end, int unit);
+// The row ranges a scan covers: each maximal run of kept row groups in
+// [rg_start, rg_end) becomes one (start row, end row, first chunk) triple,
+// handed to emit(a, b, chunk0); a range of rows [a, b) takes the chunks of
+// `unit` rows from a rounded down to a multiple of unit. Returns the chunks.
+// The one place the chunk arithmetic the kernels' segment lookup relies on is
+// written (make_segments and the no-allocation run both use it).
+template <class Keep, class Emit>
+long long walk_segments(const Table& t, Keep&& keep, int rg_start, int rg_end, int unit, Emit&& emit) {
+    const long long U = unit;
+    long long chunks = 0;
+    int rg = rg_start;
+    while (rg < rg_end) {
+        if (!keep(rg)) { rg++; continue; }
+        int e = rg + 1;
+        while (e < rg_end && keep(e)) e++;
+        const long long a = t.rg_start(rg), b = t.rg_end(e - 1);
+        if (b > a) {
+            emit(a, b, chunks);
+            chunks += (b - (a & ~(U - 1)) + U - 1) / U;
+        }
+        rg = e;
+    }
+    return chunks;
+}
+// Grid of a scan kernel: every SM filled to its occupancy (at most cap_per_sm
+// blocks an SM when > 0), never more blocks than loop units.
+int grid_for(const JitKernel& k, long long units, bool staged, int cap_per_sm = 0);
+// Status of a register-path scan from its error word: bit 8 a staged copy
+// timed out, bit 2 a float sum left its exact window; any other bit is a
+// device error. Returns normally when the word is 0.
+void check_regs_flags(int herr);
 bool parse_date(const char* s, int64_t* days);
+// Frees the pinned host copy of a table's columns the filter operator reads
+// (select.cu); called when the table is destroyed.
+void drop_host_mirror(const Table* t);
 
 }  // namespace vq
 

@@ -556,12 +556,18 @@ double vq_fkey_inv_host(uint64_t k) {
 // Grid of a scan kernel: every SM filled to its occupancy, never more blocks
 // than loop units (staged kernels: one tile per block per iteration; chunk
 // loops: one 128-row chunk per warp).
-int grid_for(const JitKernel& k, long long units, bool staged, int cap_per_sm = 0) {
+int grid_for(const JitKernel& k, long long units, bool staged, int cap_per_sm) {
     int per_sm = std::max(1, k.max_blocks_per_sm);
     if (cap_per_sm > 0) per_sm = std::min(per_sm, cap_per_sm);
     long long want = staged ? units : (units + (k.block / 32) - 1) / (k.block / 32);
     long long g = std::min<long long>((long long)sm_count() * per_sm, want);
     return (int)std::max<long long>(g, 1);
+}
+
+void check_regs_flags(int herr) {
+    if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+    if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
+    if (herr) fail(VEXQ_EDEVICE, "the scan kernel reported error flags " + std::to_string(herr));
 }
 
 void set_columns(VQParams& P, const Table& t, bool build_side) {
@@ -739,9 +745,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     if (!mapped) VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
     p.regs_err_clean = true;
-    const int herr = *(const int*)((const char*)p.h_stage.p + nout_f + nout_i);
-    if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
-    if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
+    check_regs_flags(*(const int*)((const char*)p.h_stage.p + nout_f + nout_i));
     const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge (overlapping its drain, or inside it)
     rc.scan_ms += span;
     rc.kernel_ms += span;

@@ -1,13 +1,16 @@
 """Python mirror of vexq's operator contract over libvexqcuda's C ABI.
 
-The Go engine would bind the same entry points through cgo;
-this module gives tests and the benchmark the reference's shapes:
+The Go engine would bind the same entry points through cgo; this module gives
+tests and the benchmark the reference's shapes:
 
   GpuTable                     ≈ the uploaded columns a TableScan would read
   GpuHashAggregate             ≈ exec.NewHashAggregate / NewParallelHashAggregate
                                  (exec/aggregate.go:131, exec/parallel.go:78)
   GpuParallelHashJoinAggregate ≈ exec.NewParallelHashJoinAggregate (exec/parallel_join.go:718)
-  GpuFilter                    ≈ exec.NewFilter + BoolToSelVecInto (exec/filter.go:40-78)
+  GpuFilter                    ≈ exec.NewFilter over a TableScan + BoolToSelVecInto
+                                 (exec/filter.go:40-78): next() → the scan's batch with
+                                 its SelVec; bitmap() for a whole-table selection
+  GpuProject                   ≈ exec.NewProject over that filter (exec/project.go:64-128)
   GpuBatch                     many prepared plans in one persistent launch per path class
                                under a captured CUDA graph (no reference counterpart)
 
@@ -26,7 +29,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import abi
-from .plan import AggPlan, JoinPlan, predicate_arrays
+from .plan import AggPlan, JoinPlan, predicate_arrays, project_arrays
 from .table import HostTable
 
 _initialised = False
@@ -266,12 +269,79 @@ class GpuParallelHashJoinAggregate(_PlanOp):
         _set_having(self.h, plan)
 
 
-class GpuFilter:
-    """Filter over a table: a selection bitmap, handed out as per-block SelVecs."""
+@dataclass
+class SelBatch:
+    """The batch Filter.Next returns: the scan's vectors (physical rows) with
+    the selection vector installed; length = len(sel)."""
+    vectors: List[Vector]
+    physical: int
+    sel: List[int]
+    rg: int
+    row0: int
 
-    def __init__(self, table: GpuTable, predicate):
+    @property
+    def length(self) -> int:
+        return len(self.sel)
+
+
+def _view_values(v, n: int):
+    width = {abi.TYPE_INT64: 8, abi.TYPE_FLOAT64: 8, abi.TYPE_DATE: 4, abi.TYPE_STRING: 4, abi.TYPE_BOOL: 1}[v.type]
+    vals = _decode(v.type, C.string_at(v.values, n * width), n) if n else []
+    bm = C.string_at(v.validity, (n + 7) // 8) if n else b""
+    if v.type == abi.TYPE_STRING:
+        off = np.frombuffer(C.string_at(v.dict_str_off, (v.dict_len + 1) * 4), dtype=np.uint32) if v.dict_len else []
+        data = C.string_at(v.dict_bytes, int(off[-1])) if v.dict_len else b""
+        strs = [data[off[i]:off[i + 1]].decode() for i in range(v.dict_len)]
+        vals = [strs[x] if x < len(strs) else "" for x in vals]
+    return [vals[i] if (bm[i >> 3] >> (i & 7)) & 1 else None for i in range(n)]
+
+
+class GpuFilter:
+    """exec.Filter over a table's scan. next() streams 1024-row blocks with
+    device-built SelVecs (vexq_filter_open/next); bitmap() returns a
+    whole-range selection bitmap (vexq_filter_run)."""
+
+    def __init__(self, table: GpuTable, predicate, rg_start: int = 0, rg_end: int = -1):
         self.table, self.predicate = table, predicate
+        self.rg_start, self.rg_end = rg_start, rg_end
         self._arena, self.nodes, self.nn, self.ch, self.nc, self.root = predicate_arrays(predicate)
+        self.h = C.c_void_p()
+
+    def open(self) -> None:
+        if not self.h:
+            abi.check(abi.load().vexq_filter_open(self.table.h, self.nodes, self.nn, self.ch, self.nc, self.root,
+                                                  self.rg_start, self.rg_end, C.byref(self.h)))
+
+    def next(self) -> Optional[SelBatch]:
+        """Filter.Next: the next block with at least one kept row, None at EOF."""
+        self.open()
+        fb = abi.FilterBatch()
+        abi.check(abi.load().vexq_filter_next(self.h, C.byref(fb)))
+        if fb.length == 0:
+            return None
+        vecs = []
+        for c in range(fb.ncols):
+            v = fb.cols[c]
+            vecs.append(Vector(v.name.decode() if v.name else "", v.type, _view_values(v, fb.physical)))
+        return SelBatch(vecs, fb.physical, list(fb.sel[:fb.length]), fb.rg, fb.row0)
+
+    def stats(self):
+        """(rows kept, blocks scanned, device ms of open)"""
+        self.open()
+        s, b, ms = C.c_int64(), C.c_int64(), C.c_double()
+        abi.check(abi.load().vexq_filter_stats(self.h, C.byref(s), C.byref(b), C.byref(ms)))
+        return s.value, b.value, ms.value
+
+    def close(self):
+        if self.h:
+            abi.load().vexq_filter_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def bitmap(self, row_start: int = 0, row_end: int = -1):
         n = (self.table.host.nrows if row_end < 0 else row_end) - row_start
@@ -288,6 +358,27 @@ class GpuFilter:
         n = C.c_int32()
         abi.check(abi.load().vexq_selvec_from_bits(buf, nrows, block, sel, C.byref(n)))
         return list(sel[:n.value])
+
+
+class GpuProject:
+    """exec.Project over Filter(TableScan): the named expressions of the kept
+    rows, materialised on the device in row order (no SelVec on the output)."""
+
+    def __init__(self, table: GpuTable, exprs, names=None, predicate=None, rg_start: int = 0, rg_end: int = -1):
+        self.table = table
+        self._arena, self.nodes, self.nn, self.ch, self.nc, self.root, roots = project_arrays(predicate, exprs)
+        self.roots = (C.c_int32 * len(roots))(*roots)
+        names = names or [f"col{i}" for i in range(len(roots))]
+        self._names = [n.encode() for n in names]
+        self.names = (C.c_char_p * len(roots))(*self._names)
+        self.n = len(roots)
+        self.rg_start, self.rg_end = rg_start, rg_end
+
+    def run(self) -> Result:
+        h = C.c_void_p()
+        abi.check(abi.load().vexq_project_run(self.table.h, self.nodes, self.nn, self.ch, self.nc, self.root,
+                                              self.roots, self.names, self.n, self.rg_start, self.rg_end, C.byref(h)))
+        return Result(h)
 
 
 class GpuBatch:

@@ -270,3 +270,13 @@ def predicate_arrays(pred: E):
     root = a.add(pred)
     nodes, nn, ch, nc = a.arrays()
     return a, nodes, nn, ch, nc, root
+
+
+def project_arrays(pred: Optional[E], exprs: Sequence[E]):
+    """Node arrays for Filter → Project (vexq_project_run): one arena holding
+    the predicate (root -1 when there is none) and every projected expression."""
+    a = _Arena()
+    root = a.add(pred) if pred is not None else -1
+    roots = [a.add(e) for e in exprs]
+    nodes, nn, ch, nc = a.arrays()
+    return a, nodes, nn, ch, nc, root, roots
