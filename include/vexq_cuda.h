@@ -192,7 +192,11 @@ typedef struct {
 /* AggKind values of exec/aggregate.go:15-21 (COUNT DISTINCT is not offered:
  * the reference's planner runs it serially, planner/parallel.go:224-228). */
 enum { VEXQ_AGG_COUNT = 0, VEXQ_AGG_SUM = 1, VEXQ_AGG_AVG = 2,
-       VEXQ_AGG_MIN = 3, VEXQ_AGG_MAX = 4 };
+       VEXQ_AGG_MIN = 3, VEXQ_AGG_MAX = 4,
+       /* COUNT(DISTINCT col): the number of distinct non-NULL values per group
+        * (exec/aggregate.go:117-124, 474-493, 810-823); never NULL. Strings
+        * compare by value, every other type by its raw 64-bit image. */
+       VEXQ_AGG_COUNT_DISTINCT = 5 };
 
 typedef struct {
     int32_t     kind;       /* VEXQ_AGG_*                                      */

@@ -23,6 +23,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 namespace {
@@ -988,6 +989,10 @@ struct Group {
     std::vector<GroupByVal> sample;
     std::vector<std::string> strs;
     std::vector<ExactSum> exact;  // serial only, per agg (SUM/AVG float)
+    // COUNT(DISTINCT) sets (aggregate.go:117-124): raw int64 images, or the
+    // resolved strings of STRING inputs
+    std::vector<std::unordered_set<int64_t>> dints;
+    std::vector<std::unordered_set<std::string>> dstrs;
 };
 
 struct HashAgg {
@@ -1034,7 +1039,24 @@ struct HashAgg {
         }
         if (hasStrAgg) g.strs.assign(aggs.size(), std::string());
         if (trackExact) g.exact.assign(aggs.size(), ExactSum());
+        if (hasDistinct()) {
+            g.dints.resize(aggs.size());
+            g.dstrs.resize(aggs.size());
+        }
         return g;
+    }
+
+    bool hasDistinct() const {
+        for (auto& a : aggs) if (a.kind == VEXQ_AGG_COUNT_DISTINCT) return true;
+        return false;
+    }
+
+    // COUNT(DISTINCT) fold of one row (aggregate.go:474-493): NULLs are not
+    // in the set; strings by their value, other types by extractInt64
+    static void foldDistinct(Group& g, size_t j, const Vec* v, int r) {
+        if (v->isNull(r)) return;
+        if (v->type == VEXQ_TYPE_STRING) g.dstrs[j].insert(v->str(r));
+        else g.dints[j].insert(extractInt64(*v, r));
     }
 
     static void minMaxString(std::vector<std::string>& strs, size_t j, const std::string& s, bool seen, bool less) {
@@ -1051,6 +1073,9 @@ struct HashAgg {
             switch (a.kind) {
                 case VEXQ_AGG_COUNT:
                     if (a.star || !v->isNull(r)) { g.accs[j]++; g.nonNull[j]++; }
+                    break;
+                case VEXQ_AGG_COUNT_DISTINCT:
+                    foldDistinct(g, j, v, r);
                     break;
                 case VEXQ_AGG_SUM:
                     if (v->isNull(r)) break;
@@ -1225,6 +1250,7 @@ struct HashAgg {
                     const Vec* vv = v;
                     switch (aa.kind) {
                         case VEXQ_AGG_COUNT: if (!vv->isNull(r)) { g.accs[j]++; g.nonNull[j]++; } break;
+                        case VEXQ_AGG_COUNT_DISTINCT: foldDistinct(g, j, vv, r); break;
                         case VEXQ_AGG_SUM:
                             if (!vv->isNull(r)) { g.accs[j] = (int64_t)((uint64_t)g.accs[j] + (uint64_t)extractInt64(*vv, r)); g.nonNull[j]++; }
                             break;
@@ -1260,9 +1286,9 @@ struct HashAgg {
             }
             return;
         }
-        if (!ikDecided) {  // canUseIntKey (agg_intkey.go:104-116)
+        if (!ikDecided) {  // canUseIntKey (agg_intkey.go:104-116); COUNT(DISTINCT) turns it off (aggregate.go:396-399)
             ikDecided = true;
-            bool ok = groupBy.size() <= 8;
+            bool ok = groupBy.size() <= 8 && !hasDistinct();
             for (int c : groupBy) if (b.cols[c]->type != VEXQ_TYPE_STRING || !b.cols[c]->dict) ok = false;
             if (ok) { ikEnabled = true; initIntKey((int)groupBy.size()); }
         }
@@ -1408,13 +1434,14 @@ ref_result_s* buildOutput(HashAgg& h, const std::vector<int>& gbOutTypes) {
         c.strs.assign(rows, "");
         c.exact.assign(rows, NAN);
         switch (a.kind) {
-            case VEXQ_AGG_COUNT: c.type = VEXQ_TYPE_INT64; break;
+            case VEXQ_AGG_COUNT:
+            case VEXQ_AGG_COUNT_DISTINCT: c.type = VEXQ_TYPE_INT64; break;
             case VEXQ_AGG_SUM: c.type = a.accum == VEXQ_TYPE_FLOAT64 ? VEXQ_TYPE_FLOAT64 : VEXQ_TYPE_INT64; break;
             case VEXQ_AGG_AVG: c.type = VEXQ_TYPE_FLOAT64; break;
             default: c.type = a.outType; break;
         }
         if (emptyGlobal) {
-            if (a.kind == VEXQ_AGG_COUNT) c.valid[0] = 1;  // COUNT → 0, others NULL
+            if (a.kind == VEXQ_AGG_COUNT || a.kind == VEXQ_AGG_COUNT_DISTINCT) c.valid[0] = 1;  // COUNT → 0, others NULL
             res->cols.push_back(std::move(c));
             continue;
         }
@@ -1423,6 +1450,10 @@ ref_result_s* buildOutput(HashAgg& h, const std::vector<int>& gbOutTypes) {
             int64_t nn = g.nonNull[j];
             switch (a.kind) {
                 case VEXQ_AGG_COUNT: c.valid[i] = 1; c.bits[i] = g.accs[j]; break;
+                case VEXQ_AGG_COUNT_DISTINCT:  // the set's size, never NULL (aggregate.go:810-823)
+                    c.valid[i] = 1;
+                    c.bits[i] = g.dints.empty() ? 0 : (int64_t)(g.dints[j].size() + g.dstrs[j].size());
+                    break;
                 case VEXQ_AGG_SUM:
                     if (nn == 0) break;
                     c.valid[i] = 1;
@@ -1513,7 +1544,7 @@ AggPlan resolveAggs(const Nodes& N, const vexq_agg_desc* aggs, int naggs, const 
         AggSpec a;
         a.kind = aggs[j].kind;
         a.name = aggs[j].out_name ? aggs[j].out_name : "";
-        if (a.kind < VEXQ_AGG_COUNT || a.kind > VEXQ_AGG_MAX) throw Error("unknown aggregate kind");
+        if (a.kind < VEXQ_AGG_COUNT || a.kind > VEXQ_AGG_COUNT_DISTINCT) throw Error("unknown aggregate kind");
         a.star = aggs[j].input < 0;
         if (a.star && a.kind != VEXQ_AGG_COUNT) throw Error("aggregate column not found");
         XP in;
@@ -1525,9 +1556,11 @@ AggPlan resolveAggs(const Nodes& N, const vexq_agg_desc* aggs, int naggs, const 
             a.srcType = VEXQ_TYPE_INT64;
             p.plain.push_back(true);
         }
-        a.accum = a.kind == VEXQ_AGG_COUNT ? VEXQ_TYPE_INT64 : accumTypeFor(a.kind, a.srcType);
+        a.accum = a.kind == VEXQ_AGG_COUNT || a.kind == VEXQ_AGG_COUNT_DISTINCT ? VEXQ_TYPE_INT64
+                                                                                : accumTypeFor(a.kind, a.srcType);
         switch (a.kind) {
-            case VEXQ_AGG_COUNT: a.outType = VEXQ_TYPE_INT64; break;
+            case VEXQ_AGG_COUNT:
+            case VEXQ_AGG_COUNT_DISTINCT: a.outType = VEXQ_TYPE_INT64; break;
             case VEXQ_AGG_AVG: a.outType = VEXQ_TYPE_FLOAT64; break;
             default: a.outType = a.srcType; break;
         }
@@ -1668,6 +1701,10 @@ ref_result_s* runAgg(const Table& t, const vexq_agg_plan_desc* d, int rgs, int r
     collectCols(N, d->predicate, need);
     for (int i = 0; i < d->ngroup_by; i++) if (d->group_by[i] >= 0 && d->group_by[i] < (int)need.size()) need[d->group_by[i]] = 1;
     for (int j = 0; j < d->naggs; j++) collectCols(N, d->aggs[j].input, need);
+    // COUNT(DISTINCT) runs serially: partial distinct counts cannot be summed
+    // (planner/parallel.go:218-228)
+    for (int j = 0; j < d->naggs; j++)
+        if (d->aggs[j].kind == VEXQ_AGG_COUNT_DISTINCT) workers = 0;
     if (workers <= 0) {  // planner.Physical: one pipeline, strict row order
         AggPipeline p = makeAggPipeline(N, d, s, true);
         Scan sc(&t, need);

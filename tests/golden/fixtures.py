@@ -15,7 +15,8 @@ TYPES = {"INT64": abi.TYPE_INT64, "FLOAT64": abi.TYPE_FLOAT64, "DATE": abi.TYPE_
          "STRING": abi.TYPE_STRING, "BOOL": abi.TYPE_BOOL}
 OPS = {"EQ": abi.OP_EQ, "NE": abi.OP_NE, "LT": abi.OP_LT, "LE": abi.OP_LE, "GT": abi.OP_GT,
        "GE": abi.OP_GE, "ADD": abi.OP_ADD, "SUB": abi.OP_SUB, "MUL": abi.OP_MUL, "DIV": abi.OP_DIV}
-AGGS = {"COUNT": P.count, "SUM": P.sum_, "AVG": P.avg, "MIN": P.min_, "MAX": P.max_}
+AGGS = {"COUNT": P.count, "SUM": P.sum_, "AVG": P.avg, "MIN": P.min_, "MAX": P.max_,
+        "COUNT_DISTINCT": P.count_distinct}
 
 
 def load_cases():

@@ -139,6 +139,56 @@ case("join_sentinel_and_extreme_keys", "exec/join_table_test.go:159-187",
      JOIN_GB, [[0, 0, 1], [1, 1, 1], [2, 2, 1], [3, 3, 1], [4, 4, 1]], ordered=True, kind="join")
 
 
+# COUNT(DISTINCT) (exec/aggregate.go:117-124, 474-493, 810-823).
+# exec/distinct_test.go:19-41 writeDistinctTestFile + :158-171 TestCountDistinct.
+DISTINCT_T = {"rg_rows": 65536, "nrows": 10, "columns": [
+    col("id", "INT64", [1, 2, 2, 3, 3, 3, 4, 4, 4, 4]),
+    col("val", "INT64", [10, 20, 20, 30, 30, 30, 40, 40, 40, 40])]}
+case("count_distinct_id", "exec/distinct_test.go:158-165", {"t": DISTINCT_T},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 0], "d"]]}, [[4]])
+case("count_distinct_val", "exec/distinct_test.go:167-171", {"t": DISTINCT_T},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 1], "d"]]}, [[4]])
+# exec/distinct_test.go:204-236 writeMultiRowGroupFile + :279-305: the same
+# strings under different local codes in two row groups.
+MULTI_RG = {"rg_rows": 4, "nrows": 8, "columns": [
+    strcol("category", [["alpha", "beta", "gamma"], ["gamma", "beta", "alpha"]], [0, 1, 0, 2, 0, 1, 1, 2]),
+    col("amount", "INT64", [10, 20, 30, 40, 50, 60, 70, 80])]}
+case("count_distinct_multi_rg_strings", "exec/distinct_test.go:279-286", {"t": MULTI_RG},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 0], "d"]]}, [[3]])
+case("count_distinct_multi_rg_ints", "exec/distinct_test.go:288-292", {"t": MULTI_RG},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 1], "d"]]}, [[8]])
+# exec/distinct_test.go:238-270 writeNullableFile + :306-335: NULLs stay out
+# of the sets.
+NULLABLE_T = {"rg_rows": 65536, "nrows": 8, "columns": [
+    strcol("grp", [["a", "b"]], [0, 0, 0, 0, 1, 1, 1, 1]),
+    col("val", "INT64", [1, 2, 0, 1, 0, 0, 0, 3], [1, 1, 0, 1, 0, 0, 0, 1])]}
+case("count_distinct_nulls_excluded", "exec/distinct_test.go:306-314", {"t": NULLABLE_T},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 1], "d"]]}, [[3]])
+case("count_distinct_all_null_group", "exec/distinct_test.go:316-335", {"t": NULLABLE_T},
+     {"predicate": None, "group_by": [0], "aggs": [["COUNT_DISTINCT", ["col", 1], "d"]]}, [["a", 2], ["b", 1]])
+# exec/distinct_test.go:337-372: every value NULL → 0, not NULL.
+case("count_distinct_all_null", "exec/distinct_test.go:337-372",
+     {"t": {"rg_rows": 65536, "nrows": 4, "columns": [col("id", "INT64", [0, 0, 0, 0], [0, 0, 0, 0])]}},
+     {"predicate": None, "group_by": [], "aggs": [["COUNT_DISTINCT", ["col", 0], "d"]]}, [[0]])
+# exec/aggregate_rows_test.go:292-299 count_distinct_disables_int_key over the
+# SelVec batches above: 5 distinct prices, 1 qty, 1 flag.
+case("selvec_count_distinct", "exec/aggregate_rows_test.go:292-299", {"t": SELVEC_TABLE},
+     {"predicate": SEL_A, "group_by": [0],
+      "aggs": [["COUNT_DISTINCT", ["col", 2], "d_price"], ["COUNT_DISTINCT", ["col", 3], "d_qty"],
+               ["COUNT_DISTINCT", ["col", 0], "d_flag"]]},
+     [["A", 5, 1, 1]])
+# exec/agg_string_fallback_test.go:252-298 TestStringMinMaxWithCountDistinct:
+# string MIN/MAX, COUNT(DISTINCT) and COUNT over one string column.
+case("string_min_max_with_count_distinct", "exec/agg_string_fallback_test.go:252-298",
+     {"t": {"rg_rows": 65536, "nrows": 5, "columns": [
+         strcol("grp", [["east", "west"]], [0, 0, 0, 0, 1]),
+         strcol("mode", [["MAIL", "AIR", "SHIP"]], [0, 1, 0, 0, 2], [1, 1, 1, 0, 1])]}},
+     {"predicate": None, "group_by": [0],
+      "aggs": [["MIN", ["col", 1], "lo"], ["MAX", ["col", 1], "hi"], ["COUNT_DISTINCT", ["col", 1], "ndistinct"],
+               ["COUNT", ["col", 1], "n"]]},
+     [["east", "AIR", "MAIL", 2, 3], ["west", "SHIP", "SHIP", 1, 1]])
+
+
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(out, "w") as f:

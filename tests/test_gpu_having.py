@@ -36,6 +36,19 @@ def test_reference_cases(gpu_lib):
         assert {r[0]: r for r in rows} == want, (name, rows)
 
 
+def test_reference_cases_on_device(gpu_lib, monkeypatch):
+    """The reference's six HAVING cases with the groups in a device group
+    table (the register path turned off for the fixture's few groups), so the
+    predicate runs on the device (vq_having) before the groups come back."""
+    X = gpu_lib
+    monkeypatch.setenv("VEXQ_TUNE", "regs_groups=0")
+    gt = X.GpuTable(grouped_table())
+    for name, (aggs, having, visible, want) in CASES.items():
+        rows, explain = gpu_rows(X, gt, P.AggPlan(None, [0], aggs, having=having, visible=visible))
+        assert "path=dense" in explain and "having=device" in explain, (name, explain)
+        assert {r[0]: r for r in rows} == want, (name, rows)
+
+
 def test_having_over_float_avg_string_keys_and_nulls(gpu_lib):
     X = gpu_lib
     n = 200_000
@@ -83,7 +96,7 @@ def test_having_before_order_and_limit_on_many_groups(gpu_lib):
     having = P.col(2) >= 14
     plan = P.AggPlan(None, [0], aggs, order_col=1, descending=True, limit=10, having=having)
     rows, ex = gpu_rows(X, X.GpuTable(host), plan)
-    assert "path=hash" in ex, ex
+    assert "path=hash" in ex and "having=device" in ex, ex
     ref = R.agg_having(R.RefTable(host), P.AggPlan(None, [0], aggs), having, -1, order=(1, 1, 10))
     assert len(rows) == 10 and all(r[2] >= 14 for r in rows)
     assert_rows_match(rows, ref.rows(), ordered=True)

@@ -23,7 +23,7 @@ E_COLUMN, E_LITERAL, E_BINARY, E_AND, E_OR, E_NOT, E_NEG, E_IS_NULL, \
     E_IS_NOT_NULL, E_BETWEEN, E_IN, E_LIKE, E_CASE = range(1, 14)
 OP_EQ, OP_NE, OP_LT, OP_LE, OP_GT, OP_GE, OP_ADD, OP_SUB, OP_MUL, OP_DIV = range(1, 11)
 LIT_INT, LIT_FLOAT, LIT_STRING, LIT_BOOL = 1, 2, 3, 4
-AGG_COUNT, AGG_SUM, AGG_AVG, AGG_MIN, AGG_MAX = 0, 1, 2, 3, 4
+AGG_COUNT, AGG_SUM, AGG_AVG, AGG_MIN, AGG_MAX, AGG_COUNT_DISTINCT = 0, 1, 2, 3, 4, 5
 
 BLOCK_ROWS = 1024
 ROW_GROUP_ROWS = 65536

@@ -51,6 +51,8 @@ int64_t plan_footprint(const Plan& p) {
     int64_t per = 16 + 8 * p.ni + 36 * p.nf;
     int64_t f = slots * per;
     if (p.is_join) f += (int64_t)p.bt->nrows * 2 * 24;
+    // COUNT(DISTINCT) sets: 20 bytes a slot, twice the table's rows
+    if (p.ndist > 0 && p.t) f += (int64_t)p.ndist * 2 * std::max<int64_t>(p.t->nrows, 512) * 20;
     return f;
 }
 

@@ -453,7 +453,7 @@ void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
         Item it;
         Plan* p = handles[i]->p;
         it.p = p;
-        if (p->is_join) {  // joins run on their own after the graph
+        if (p->is_join || p->ndist > 0) {  // joins and COUNT(DISTINCT) run on their own after the graph
             b->items.push_back(std::move(it));
             continue;
         }

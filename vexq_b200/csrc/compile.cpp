@@ -776,7 +776,7 @@ void plan_aggs(Plan& p, const std::vector<std::pair<int, int>>& aggs_ir, const v
         AggOut o;
         o.kind = kind;
         o.name = aggs[j].out_name ? aggs[j].out_name : "";
-        if (kind < VEXQ_AGG_COUNT || kind > VEXQ_AGG_MAX) fail(VEXQ_EINVAL, "unknown aggregate kind");
+        if (kind < VEXQ_AGG_COUNT || kind > VEXQ_AGG_COUNT_DISTINCT) fail(VEXQ_EINVAL, "unknown aggregate kind");
         if (in < 0) {
             if (kind != VEXQ_AGG_COUNT) fail(VEXQ_EINVAL, "aggregate column not found in schema");
             o.value_slot = 0;
@@ -786,6 +786,26 @@ void plan_aggs(Plan& p, const std::vector<std::pair<int, int>>& aggs_ir, const v
             continue;
         }
         const INode& x = p.ir[in];
+        if (kind == VEXQ_AGG_COUNT_DISTINCT) {
+            // COUNT(DISTINCT x) (exec/aggregate.go:474-493, 810-823): a count of
+            // the rows whose (group, x) pair is new to the plan's distinct set
+            // number d; output like COUNT (never NULL). One set per distinct
+            // input expression.
+            const std::string key = "D|" + sig(p, in);
+            auto it = seen.find(key);
+            if (it == seen.end()) {
+                if (p.ndist >= VQ_MAXDIST) fail(VEXQ_ENOTSUP, "more than 4 COUNT(DISTINCT) aggregates in one plan");
+                Slot sl{S_NN, in};
+                sl.dset = p.ndist++;
+                p.slots.push_back(sl);
+                it = seen.emplace(key, (int)p.slots.size() - 1).first;
+            }
+            o.kind = VEXQ_AGG_COUNT;
+            o.value_slot = o.nn_slot = it->second;
+            o.out_type = VEXQ_TYPE_INT64;
+            p.outs.push_back(o);
+            continue;
+        }
         int nn = x.nullable ? add_slot(p, seen, S_NN, in) : 0;
         o.nn_slot = nn;
         switch (kind) {
@@ -1026,12 +1046,30 @@ std::string order_expr(const Plan& p, const std::string& pos) {
     return "((anynull ? 0ll : (1ll << 56)) | " + pos + ")";
 }
 
-void emit_slot_values(std::ostringstream& os, const Plan& p, const std::string& ind) {
+// live: the expression that says the row is in the scan and passes the
+// predicate, where the loop runs rows that do not (atomic paths).
+void emit_slot_values(std::ostringstream& os, const Plan& p, const std::string& ind, const std::string& live = "true") {
     for (size_t s = 1; s < p.slots.size(); s++) {
         const Slot& sl = p.slots[s];
         const INode& x = p.ir[sl.input];
         std::string X = "x" + std::to_string(sl.input), OK = "ok" + std::to_string(sl.input);
         std::string S = std::to_string(s);
+        if (sl.dset >= 0) {
+            // COUNT(DISTINCT): strings by global code (one code a string),
+            // other types by extractInt64's image (raw float bits, dates
+            // sign-extended, bools 0/1)
+            std::string img;
+            switch (x.type) {
+                case VEXQ_TYPE_FLOAT64: img = "(unsigned long long)__double_as_longlong(" + X + ")"; break;
+                case VEXQ_TYPE_BOOL: img = "(" + X + " ? 1ull : 0ull)"; break;
+                case VEXQ_TYPE_DATE: img = "(unsigned long long)(long long)" + X; break;
+                default: img = "(unsigned long long)" + X; break;
+            }
+            const std::string d = std::to_string(sl.dset);
+            os << ind << "const bool sok" << S << " = " << OK << " && (" << live << ") && vq_dset_insert(P.dkeys[" << d
+               << "], P.dstate[" << d << "], P.dmask, key, " << img << ", P.error);\n";
+            continue;
+        }
         os << ind << "const bool sok" << S << " = " << OK << ";\n";
         if (sl.is_float() || sl.kind == S_FSUM) {
             os << ind << "const double sv" << S << " = (double)" << (x.type == VEXQ_TYPE_BOOL ? "(" + X + " ? 1 : 0)" : X) << ";\n";
@@ -2122,7 +2160,7 @@ static void emit_agg_rows(std::ostringstream& os, Plan& p, const std::vector<int
     for (int k : key_nodes) g.emit(k);
     for (auto& s : p.slots) if (s.input >= 0) g.emit(s.input);
     emit_key(os, p, key_nodes, "            ");
-    emit_slot_values(os, p, "            ");
+    emit_slot_values(os, p, "            ", warp_sync ? "live" : "true");
     std::string order = order_expr(p, "r");
     if (p.path == AggPath::Regs) {
         if (p.regs_pred) emit_regs_update_pred(os, p, "            ", order);
@@ -2918,6 +2956,9 @@ Plan* compile_agg(Table* t, const vexq_agg_plan_desc* d) {
     plan_keys(*p);
     resolve_intkey(*p);
     plan_aggs(*p, aggs, d->aggs);
+    // COUNT(DISTINCT) turns the integer-key path off (exec/aggregate.go:396-399):
+    // groups keep plain first-row order
+    if (p->ndist > 0) p->intkey_order = false;
     copy_zone_tree(*p, d->nodes, d->nnodes, d->children, d->nchildren);
     keep_zone_strings(*p, d->nodes, d->nnodes);
     p->zn_pred = d->predicate;
@@ -3010,6 +3051,7 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
     plan_keys(*p);
     resolve_intkey(*p);
     plan_aggs(*p, aggs, d->aggs);
+    if (p->ndist > 0) fail(VEXQ_ENOTSUP, "COUNT(DISTINCT) over a join is not supported on the GPU path");
     copy_zone_tree(*p, d->nodes, d->nnodes, d->children, d->nchildren);
     keep_zone_strings(*p, d->nodes, d->nnodes);
     p->zn_pred = d->probe_predicate;
@@ -3029,6 +3071,8 @@ Plan* compile_join(Table* bt, Table* pt, const vexq_join_plan_desc* d) {
 // columns, then aggregates — and evaluated per output row before ORDER BY /
 // LIMIT; then only the first `visible` columns are kept (the hidden
 // aggregates the planner appends for HAVING are projected away).
+void gen_having_kernel(Plan& p);
+
 void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* children, int nchildren, int root, int visible) {
     const int nout = (int)(p.keys.size() + p.outs.size());
     p.having_ir.clear();
@@ -3067,6 +3111,123 @@ void set_having(Plan& p, const vexq_expr* nodes, int nnodes, const int32_t* chil
     p.having_root = r;
     p.having_visible = visible;
     p.having_schema = std::move(schema);
+    gen_having_kernel(p);
+    const size_t at = p.explain.find(" having=");
+    if (at != std::string::npos) p.explain.resize(at);
+    p.explain += p.k_having.fn || !p.src_having.empty() ? " having=device" : " having=host";
+}
+
+// HAVING on the device, for plans whose groups live in a group table (dense,
+// hash and join tables): vq_having runs one thread per compacted group, decodes
+// the output columns the predicate reads exactly as the host result builder
+// does (key columns from the packed key, COUNT, SUM, AVG = sum / non-null
+// count, MIN/MAX, NULL when no input was non-null), evaluates the predicate
+// with the scan kernels' expression code, and compacts the groups it keeps
+// (one atomic a warp). Parameters, in the fields of VQParams:
+//   in   P.keys / P.first / P.acc_i [NI][P.cap] / P.part_f [NF][P.cap], n = P.nchunks
+//   out  P.pkeys / P.part_i / P.racc_i [NI][P.jmask] / P.rout_f [NF][P.jmask], count *P.jtotal
+// Plans whose HAVING reads a string MIN/MAX output or a large IN set keep the
+// host evaluation (k_having stays empty).
+void gen_having_kernel(Plan& p) {
+    p.k_having = JitKernel();
+    p.src_having.clear();
+    if (p.having_root < 0 || p.path == AggPath::Regs) return;
+    const int nk = (int)p.keys.size();
+    std::vector<INode> ir = p.having_ir;
+    for (auto& n : ir) {
+        n.lit_slot = -1;  // literals inline: the kernel is per plan
+        if (n.k == NK::InCodes && n.codes.size() > 64) return;
+        if (n.k == NK::StrRank || n.present_idx >= 0) return;
+        if (n.k == NK::Col && n.col >= nk && p.outs[n.col - nk].rank_dict) return;
+    }
+    Plan hp;
+    hp.ir = ir;
+    std::ostringstream os;
+    os << prelude_source() << "\n";
+    os << kernel_head("vq_having", 256);
+    os << "    const int lane = threadIdx.x & 31;\n";
+    os << "    const long long vq_n = P.nchunks;\n";
+    os << "    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < vq_n; b0 += (long long)gridDim.x * blockDim.x) {\n";
+    os << "        const long long j = b0 + threadIdx.x;\n";
+    os << "        bool keep = false;\n";
+    os << "        if (j < vq_n) {\n";
+    os << "            const unsigned long long vq_key = P.keys[j];\n";
+    const std::string in = "            ";
+    Gen g(hp, os);
+    g.ind = in;
+    auto ival = [&](int slot) { return "P.acc_i[(long long)" + std::to_string(p.slot_pos[slot]) + " * P.cap + j]"; };
+    auto fval = [&](int slot) {
+        if (p.slots[slot].kind == S_FSUM) return "P.part_f[(long long)" + std::to_string(p.slot_pos[slot]) + " * P.cap + j]";
+        return "vq_fkey_inv((unsigned long long)" + ival(slot) + ")";
+    };
+    for (size_t i = 0; i < ir.size(); i++) {
+        const INode& n = ir[i];
+        if (n.k != NK::Col) continue;
+        const std::string x = "x" + std::to_string(i), ok = "ok" + std::to_string(i), ct = ctype(n.type);
+        if (n.col < nk) {
+            const KeyCol& k = p.keys[n.col];
+            os << in << "long long kc" << i << "; bool kn" << i << " = false;\n";
+            if (p.path != AggPath::Hash) {
+                long long stride = 1;
+                for (int kj = 0; kj < n.col; kj++) stride *= p.keys[kj].domain > 0 ? p.keys[kj].domain : 1;
+                os << in << "kc" << i << " = (long long)((vq_key / " << stride << "ull) % " << k.domain << "ull);\n";
+                if (k.nullable) os << in << "kn" << i << " = kc" << i << " == " << k.domain - 1 << "LL;\n";
+            } else {
+                const std::string m = k.bits >= 64 ? "0xFFFFFFFFFFFFFFFFull" : std::to_string((1ull << k.bits) - 1) + "ull";
+                os << in << "{ const unsigned long long raw = (vq_key >> " << k.shift << ") & " << m << ";\n";
+                if (k.domain > 0) {
+                    os << in << "  kc" << i << " = (long long)raw;";
+                    if (k.nullable) os << " kn" << i << " = kc" << i << " == " << k.domain - 1 << "LL;";
+                    os << " }\n";
+                } else if (k.type == VEXQ_TYPE_DATE) {
+                    os << in << "  kn" << i << " = ((raw >> 32) & 1ull) != 0ull; kc" << i << " = (long long)(int)(unsigned)raw; }\n";
+                } else {
+                    os << in << "  kc" << i << " = (long long)raw; }\n";
+                }
+            }
+            os << in << "const bool " << ok << " = !kn" << i << ";\n";
+            std::string v = "kc" + std::to_string(i);
+            if (k.domain > 0 && (k.type == VEXQ_TYPE_DATE || k.type == VEXQ_TYPE_INT64)) v = "(" + v + " + " + ilit(k.vmin) + ")";
+            if (n.type == VEXQ_TYPE_BOOL) os << in << "const bool " << x << " = " << ok << " && " << v << " != 0LL;\n";
+            else os << in << "const " << ct << " " << x << " = (" << ct << ")" << v << ";\n";
+        } else {
+            const AggOut& a = p.outs[n.col - nk];
+            const Slot& sl = p.slots[a.value_slot];
+            os << in << "const long long nn" << i << " = " << ival(a.nn_slot) << ";\n";
+            if (a.kind == VEXQ_AGG_COUNT) {
+                os << in << "const bool " << ok << " = true;\n";
+                os << in << "const long long " << x << " = " << ival(a.value_slot) << ";\n";
+                continue;
+            }
+            os << in << "const bool " << ok << " = nn" << i << " != 0LL;\n";
+            if (a.kind == VEXQ_AGG_AVG)
+                os << in << "const double " << x << " = " << ok << " ? " << fval(a.value_slot) << " / (double)nn" << i << " : 0.0;\n";
+            else if (sl.is_float())
+                os << in << "const double " << x << " = " << ok << " ? " << fval(a.value_slot) << " : 0.0;\n";
+            else if (n.type == VEXQ_TYPE_BOOL)
+                os << in << "const bool " << x << " = " << ok << " && " << ival(a.value_slot) << " != 0LL;\n";
+            else
+                os << in << "const " << ct << " " << x << " = " << ok << " ? (" << ct << ")" << ival(a.value_slot) << " : (" << ct << ")0;\n";
+        }
+        g.done[i] = 1;
+    }
+    g.emit(p.having_root);
+    os << in << "keep = x" << p.having_root << " && ok" << p.having_root << ";\n";
+    os << "        }\n";
+    os << "        const unsigned bal = __ballot_sync(0xffffffffu, keep);\n";
+    os << "        unsigned long long base = 0ull;\n";
+    os << "        if (lane == 0 && bal) base = atomicAdd(P.jtotal, (unsigned long long)__popc(bal));\n";
+    os << "        base = __shfl_sync(0xffffffffu, base, 0);\n";
+    os << "        if (keep) {\n";
+    os << "            const long long pos = (long long)(base + __popc(bal & ((1u << lane) - 1u)));\n";
+    os << "            P.pkeys[pos] = P.keys[j];\n";
+    os << "            P.part_i[pos] = P.first[j];\n";
+    os << "            for (int s = 0; s < " << p.ni << "; s++) P.racc_i[(long long)s * (long long)P.jmask + pos] = P.acc_i[(long long)s * (long long)P.cap + j];\n";
+    os << "            for (int f = 0; f < " << p.nf << "; f++) P.rout_f[(long long)f * (long long)P.jmask + pos] = P.part_f[(long long)f * (long long)P.cap + j];\n";
+    os << "        }\n";
+    os << "    }\n}\n";
+    p.src_having = os.str();
+    p.k_having = jit_get(p.src_having, "vq_having", 256, 0);
 }
 
 static void upload_scan_tables(Plan& p);

@@ -341,6 +341,47 @@ __device__ __forceinline__ double vq_fx_result(const vq_i64* c, int lsb, unsigne
     return vq_fx_value(c, lsb);
 }
 
+// COUNT(DISTINCT) set insert: open addressing over (group key k0, value
+// image k1) pairs. A slot's state goes 0 → 1 (claimed, being written) → 2
+// (published); a thread that finds a slot being written waits for it. Returns
+// true for the one insert that adds a pair, so summing the results per group
+// counts its distinct values whatever order rows arrive in. Both waits are
+// bounded: error bit 16 when the probe limit is reached (the table is sized
+// for twice the rows scanned, so only a broken size reaches it), bit 32 when
+// a claimed slot is not published in time.
+__device__ __forceinline__ bool vq_dset_insert(unsigned long long* keys, unsigned* state, unsigned long long mask,
+                                               unsigned long long k0, unsigned long long k1, int* error) {
+    const unsigned long long h = vq_hash(k0 * 0x9E3779B97F4A7C15ull ^ vq_hash(k1 + 0x632BE59BD9B4E019ull));
+    const int limit = mask < 4095ull ? (int)mask + 1 : 4096;
+    for (int probe = 0; probe < limit; probe++) {
+        const unsigned long long i = (h + (unsigned long long)probe) & mask;
+        unsigned s = *(volatile unsigned*)(state + i);
+        if (s == 0u) {
+            s = atomicCAS(state + i, 0u, 1u);
+            if (s == 0u) {
+                keys[2 * i] = k0;
+                keys[2 * i + 1] = k1;
+                __threadfence();
+                atomicExch(state + i, 2u);
+                return true;
+            }
+        }
+        for (int spin = 0; s == 1u; spin++) {
+            if (spin > (1 << 22)) {
+                atomicOr(error, 32);
+                return false;
+            }
+            s = *(volatile unsigned*)(state + i);
+        }
+        __threadfence();
+        const unsigned long long a = *(volatile unsigned long long*)(keys + 2 * i);
+        const unsigned long long b = *(volatile unsigned long long*)(keys + 2 * i + 1);
+        if (a == k0 && b == k1) return false;
+    }
+    atomicOr(error, 16);
+    return false;
+}
+
 #define VQ_NOSLOT 0xFFFFFFFFFFFFFFFFull
 
 // Open-addressing insert (linear probing, atomicCAS on the key). The key equal

@@ -10,6 +10,7 @@
 #define VQ_MAXHOT 4     // dense path: hottest groups accumulated in registers
 #define VQ_RADIX_CAP 4096      // radix join: build entries of one partition held in shared memory
 #define VQ_RADIX_MAX_BITS 12   // radix join: at most 4,096 partitions
+#define VQ_MAXDIST 4    // COUNT(DISTINCT) aggregates of one plan
 
 struct VQParams {
     // ---- scanned table (aggregate: the table; join: probe or build side) ----
@@ -73,6 +74,12 @@ struct VQParams {
     double* rout_f;                // [G][NF] merged float entries
     long long* rout_i;             // [G][NI + 1] merged integer entries
     int* rerr_out;                 // the error word handed out with the merged row
+    // ---- COUNT(DISTINCT) sets, one per distinct aggregate: [cap][2] (group
+    //      key, value image) and a state word per slot (0 empty, 1 being
+    //      written, 2 published); cap = dmask + 1 ----
+    unsigned long long* dkeys[VQ_MAXDIST];
+    unsigned* dstate[VQ_MAXDIST];
+    unsigned long long dmask;
     // ---- numeric literals of the plan's expressions (int64, date, float64 bits):
     //      plans that differ only in constants share one compiled kernel ----
     long long lit[VQ_MAXLITS];

@@ -69,6 +69,7 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
                         int32_t n_out) {
     if (p.is_join) fail(VEXQ_ENOTSUP, "the no-allocation run takes aggregate plans over one table, not joins");
     if (p.having_root >= 0) fail(VEXQ_ENOTSUP, "the no-allocation run takes aggregates without HAVING");
+    if (p.ndist > 0) fail(VEXQ_ENOTSUP, "the no-allocation run takes no COUNT(DISTINCT): its sets need device memory");
     for (const AggOut& a : p.outs)
         if (a.rank_dict) fail(VEXQ_ENOTSUP, "the no-allocation run takes no MIN/MAX over strings");
     check_ranges(p);

@@ -51,6 +51,9 @@ enum SlotKind { S_CNT = 0, S_NN, S_ISUM, S_IMIN, S_IMAX, S_FSUM, S_FMIN, S_FMAX 
 struct Slot {
     SlotKind kind;
     int input = -1;  // IR node (value), -1 for CNT
+    // COUNT(DISTINCT): an S_NN slot whose row condition is "the (group,
+    // value) pair entered distinct set `dset` for the first time"
+    int dset = -1;
     bool is_float() const { return kind == S_FSUM || kind == S_FMIN || kind == S_FMAX; }
 };
 
@@ -111,6 +114,8 @@ struct Plan {
     int zn_pred = -1, zn_bpred = -1;
     std::vector<KeyCol> keys;
     bool intkey_order = false;     // reference int-key path ordering rules apply
+    int ndist = 0;                 // COUNT(DISTINCT) aggregates (device sets)
+    DevBuf dist_keys[VQ_MAXDIST], dist_state[VQ_MAXDIST];
     int intkey_width = 32;
     std::vector<Slot> slots;
     std::vector<AggOut> outs;
@@ -168,6 +173,9 @@ struct Plan {
     int having_root = -1;
     int having_visible = -1;
     std::unique_ptr<Table> having_schema;
+    // HAVING on the device over the compacted group table (empty: host)
+    std::string src_having;
+    JitKernel k_having;
     // value-range epochs of the tables the plan was compiled against
     uint64_t range_epoch = 0, brange_epoch = 0;
     int btile = 128, bsmem = 0;  // join build kernel
@@ -259,6 +267,7 @@ struct Groups {
     std::vector<int64_t> first;
     std::vector<std::vector<int64_t>> ival;   // per int-bank slot
     std::vector<std::vector<double>> fval;    // per float-bank slot
+    bool having_done = false;                 // HAVING already applied on the device
     size_t n() const { return key.size(); }
 };
 std::vector<long long> init_values(const Plan& p);

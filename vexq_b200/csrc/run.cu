@@ -564,7 +564,31 @@ int grid_for(const JitKernel& k, long long units, bool staged, int cap_per_sm) {
     return (int)std::max<long long>(g, 1);
 }
 
+// COUNT(DISTINCT) sets of a plan for a scan over at most `rows` rows: twice
+// that many slots (a power of two, at least 1,024), their states cleared on
+// stream s before every launch (a hash-table rerun starts from empty sets).
+void bind_distinct(Plan& p, VQParams& P, long long rows, cudaStream_t s) {
+    if (p.ndist == 0) return;
+    unsigned long long cap = 1024;
+    while ((long long)cap < 2 * std::max<long long>(rows, 1)) cap <<= 1;
+    for (int d = 0; d < p.ndist; d++) {
+        p.dist_keys[d].ensure(cap * 16);
+        p.dist_state[d].ensure(cap * 4);
+        VQ_CUDA(cudaMemsetAsync(p.dist_state[d].p, 0, cap * 4, s));
+        P.dkeys[d] = p.dist_keys[d].as<unsigned long long>();
+        P.dstate[d] = p.dist_state[d].as<unsigned>();
+    }
+    P.dmask = cap - 1;
+}
+
+// Error bits of a COUNT(DISTINCT) set insert (vq_dset_insert).
+static void check_distinct_flags(int herr) {
+    if (herr & 16) fail(VEXQ_EDEVICE, "COUNT(DISTINCT) set reached its probe limit");
+    if (herr & 32) fail(VEXQ_ETIMEDOUT, "COUNT(DISTINCT) set: a slot being written was not published within the wait limit");
+}
+
 void check_regs_flags(int herr) {
+    check_distinct_flags(herr);
     if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
     if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
     if (herr) fail(VEXQ_EDEVICE, "the scan kernel reported error flags " + std::to_string(herr));
@@ -721,6 +745,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         P.rout_i = out_i;
         P.rerr_out = err_out;
     }
+    bind_distinct(p, P, nchunks * 128, rc.s);
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(K, grid, &P, sizeof P, rc.s);
     launch_check(rc.s, "p.k_main");
@@ -774,6 +799,7 @@ struct Compacted {
     long long* first = nullptr;
     long long* ival = nullptr;
     double* fval = nullptr;
+    bool having_done = false;  // only the groups HAVING keeps
 };
 
 Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows) {
@@ -846,6 +872,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
         k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
         launch_check(rc.s, "k_init_table");
+        bind_distinct(p, P, nchunks * 128, rc.s);
         VQ_CUDA(cudaGetLastError());
         const JitKernel& K = rc.k ? *rc.k : p.k_main;
         int grid = rc.k ? rc.grid : grid_for(p.k_main, nchunks, p.staged);
@@ -868,6 +895,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         rc.launches += 3;
         unsigned long long nn = *(unsigned long long*)p.h_stage.p;
         int herr = *(int*)((char*)p.h_stage.p + 8);
+        check_distinct_flags(herr);
         if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
         if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
         if (herr & 1) {  // probe limit: grow the table and rerun
@@ -902,6 +930,51 @@ Groups fetch_groups(RunCtx& rc, const Compacted& c) {
     return g;
 }
 
+// HAVING over the compacted groups on the device (vq_having): the groups it
+// keeps, compacted again into scratch_f.
+Compacted having_device(RunCtx& rc, const Compacted& c) {
+    Plan& p = rc.p;
+    Compacted o;
+    o.having_done = true;
+    o.cap_out = std::max<long long>(c.n, 1);
+    p.scratch_f.ensure(64 + (size_t)o.cap_out * (16 + 8 * (size_t)(p.ni + p.nf)));
+    char* b = (char*)p.scratch_f.p;
+    unsigned long long* cnt = (unsigned long long*)b;
+    o.key = (unsigned long long*)(b + 64);
+    o.first = (long long*)(o.key + o.cap_out);
+    o.ival = o.first + o.cap_out;
+    o.fval = (double*)(o.ival + (size_t)p.ni * o.cap_out);
+    VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
+    VQ_CUDA(cudaMemsetAsync(cnt, 0, 8, rc.s));
+    if (c.n > 0) {
+        VQParams P;
+        std::memset(&P, 0, sizeof P);
+        P.keys = c.key;
+        P.first = c.first;
+        P.acc_i = c.ival;
+        P.part_f = c.fval;
+        P.cap = (unsigned long long)c.cap_out;
+        P.nchunks = c.n;
+        P.pkeys = o.key;
+        P.part_i = o.first;
+        P.racc_i = o.ival;
+        P.rout_f = o.fval;
+        P.jmask = (unsigned long long)o.cap_out;
+        P.jtotal = cnt;
+        const int grid = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
+        jit_launch(p.k_having, grid, &P, sizeof P, rc.s);
+        launch_check(rc.s, "vq_having");
+        rc.launches++;
+    }
+    VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
+    p.h_stage.ensure(16);
+    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, cnt, 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    rc.kernel_ms += elapsed(p.ev[2], p.ev[3]);
+    o.n = (long long)std::min<unsigned long long>(*(const unsigned long long*)p.h_stage.p, (unsigned long long)o.cap_out);
+    return o;
+}
+
 // Device top-k candidates for ORDER BY <aggregate> LIMIT k: every group's sort
 // rank (raw int64 bits in the ExternalSort order, NULLs first) is computed on
 // the device; the q-th largest of a 4096-point sample, found on the device,
@@ -915,8 +988,10 @@ bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
     const vexq_order_desc& o = p.order;
     int ngb = (int)p.keys.size();
     const long long kCap = 65536;
-    // HAVING filters groups before the sort: every group comes back
-    if (p.having_root >= 0 || o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096) return false;
+    // HAVING filters groups before the sort: every group comes back, unless
+    // the device already kept only the groups HAVING passes
+    if ((p.having_root >= 0 && !c.having_done) || o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096)
+        return false;
     const AggOut& a = p.outs[o.sort_col - ngb];
     int vslot = a.value_slot;
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
@@ -959,6 +1034,7 @@ bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
     // an unlucky sample (fewer than LIMIT selected) or too many ties at the
     // threshold: the caller fetches every group
     if (ns < o.limit || ns > kCap) return false;
+    g.having_done = c.having_done;
     std::vector<long long> h((size_t)ns * w);
     VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
@@ -1210,7 +1286,7 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
     }
     // HAVING: keep the rows whose predicate is true and valid, then drop the
     // hidden columns
-    if (p.having_root >= 0) {
+    if (p.having_root >= 0 && !g.having_done) {
         std::vector<size_t> keep;
         for (size_t j = 0; j < rows; j++) {
             const HVal h = having_eval(p.having_ir, p.having_root, r->cols, j);
@@ -1225,8 +1301,8 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
             rows = keep.size();
             r->nrows = (int64_t)rows;
         }
-        if (p.having_visible >= 0 && p.having_visible < (int)r->cols.size()) r->cols.resize(p.having_visible);
     }
+    if (p.having_root >= 0 && p.having_visible >= 0 && p.having_visible < (int)r->cols.size()) r->cols.resize(p.having_visible);
     // ORDER BY (stable, raw int64 bits, NULLs first) + LIMIT
     const vexq_order_desc& o = p.order;
     if (o.sort_col >= 0) {
@@ -1296,7 +1372,11 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
         g = run_regs(rc, P, nchunks);
     } else {
         Compacted c = run_atomic(rc, P, nchunks, estimate, rows);
-        if (!topk_groups(rc, c, g)) g = fetch_groups(rc, c);
+        if (p.k_having.fn) c = having_device(rc, c);
+        if (!topk_groups(rc, c, g)) {
+            g = fetch_groups(rc, c);
+            g.having_done = c.having_done;
+        }
     }
     note_hot_groups(p, g);
     vexq_result_s* r = build_result(p, g);

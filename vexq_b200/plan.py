@@ -154,6 +154,11 @@ def count(x, name="count") -> Agg:
     return Agg(abi.AGG_COUNT, _wrap(x), name)
 
 
+def count_distinct(x, name="count_distinct") -> Agg:
+    """COUNT(DISTINCT x): distinct non-NULL values per group, never NULL."""
+    return Agg(abi.AGG_COUNT_DISTINCT, _wrap(x), name)
+
+
 def sum_(x, name="sum") -> Agg:
     return Agg(abi.AGG_SUM, _wrap(x), name)
 
