@@ -406,9 +406,13 @@ int32_t vexq_project_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
  * may differ in the last bits (a different row partition), both within their
  * stated tolerance. Repeated execs give identical bits.
  * flags: VEXQ_BATCH_AUTOTUNE times graph replays over the shared-memory
- * group-cache size (the shared-versus-global table cutover) and the unit
- * size, and keeps the fastest. */
+ * group-cache size (the shared-versus-global table cutover), the unit size
+ * and each class's block shape, and keeps the fastest; the choice is stored
+ * in batch_tuning.json beside the kernel cache, keyed by the batch's shape,
+ * and a later batch of that shape takes it without timing.
+ * VEXQ_BATCH_RETUNE times again and replaces the stored choice. */
 #define VEXQ_BATCH_AUTOTUNE 1u
+#define VEXQ_BATCH_RETUNE 2u
 typedef struct vexq_batch_s* vexq_batch_t;
 int32_t vexq_batch_create(vexq_plan_t* plans, int32_t n, uint32_t flags, vexq_batch_t* out);
 /* One result per plan, in plan order (each freed with vexq_result_free). */

@@ -129,14 +129,29 @@ def test_batch_group_tables_exact(mixed):
 
 
 def test_batch_autotune(mixed):
+    """Autotuning over cache size, unit size and block shapes; a second batch
+    of the same shape takes the stored choice without timing, a retune times
+    again; every tuning gives the single runs' results."""
+    import ctypes as C
     X, _, ops, _ = mixed
     single = single_rows(ops)
-    b = X.GpuBatch(ops, autotune=True)
-    try:
-        assert "autotuned" in b.explain()
-        check_against_single(b.exec(), single, ops)
-    finally:
-        b.close()
+    L = abi.load()
+    arr = (C.c_void_p * len(ops))(*[op.h for op in ops])
+
+    def batch(flags):
+        h = C.c_void_p()
+        abi.check(L.vexq_batch_create(arr, len(ops), flags, C.byref(h)))
+        return h
+
+    for flags, want in ((abi.BATCH_RETUNE, "candidates"), (abi.BATCH_AUTOTUNE, "autotuned(cached")):
+        h = batch(flags)
+        try:
+            assert want in L.vexq_batch_explain(h).decode(), L.vexq_batch_explain(h)
+            outs = (C.c_void_p * len(ops))()
+            abi.check(L.vexq_batch_exec(h, outs))
+            check_against_single([X.Result(C.c_void_p(outs[k])) for k in range(len(ops))], single, ops)
+        finally:
+            L.vexq_batch_destroy(h)
 
 
 def test_batch_run_and_empty(mixed):

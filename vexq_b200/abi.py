@@ -138,6 +138,7 @@ class FilterBatch(C.Structure):
 
 # Every symbol include/vexq_cuda.h declares (checked by the CPU test suite).
 BATCH_AUTOTUNE = 1  # VEXQ_BATCH_AUTOTUNE
+BATCH_RETUNE = 2    # VEXQ_BATCH_RETUNE
 SERVE_NO_BATCH = 1  # VEXQ_SERVE_NO_BATCH
 
 EXPORTS = [

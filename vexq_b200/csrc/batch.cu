@@ -9,12 +9,16 @@
 // streams), the partial merge and the table finalize are captured once in a
 // CUDA graph and replayed by each execution, followed by one copy of every
 // output back to pinned host memory. The autotuner picks the shared-memory group
-// cache size (the shared-versus-global table cutover) and the unit size by
-// timing graph replays. Join plans are not batched: they run after the graph,
-// one after another, as vexq_plan_run would run them.
+// cache size (the shared-versus-global table cutover), the unit size and the
+// block shape of each class by timing graph replays, and keeps its choice in a
+// JSON file keyed by the batch's shape. Join plans are not batched: they run
+// after the graph, one after another, as vexq_plan_run would run them.
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <fstream>
 #include <numeric>
 #include <sstream>
 #include <thread>
@@ -396,6 +400,39 @@ struct Batch {
         return finish_timing();
     }
 
+    // Source of class c for its current block size (bodies are generated
+    // per block size and cached per plan).
+    void gen_class(int c) {
+        ck[c].k_src.clear();
+        ck[c].smem_extra = 0;
+        ck[c].nbodies = 0;
+        std::vector<Plan*> ps;
+        for (int i : ck[c].items) ps.push_back(items[i].p);
+        if (ps.empty()) return;
+        std::vector<int> body_of;
+        int smem = 0, nb = 0;
+        ck[c].k_src = gen_batch_source(ps, ck[c].block, body_of, smem, nb);
+        ck[c].smem_extra = smem;
+        ck[c].nbodies = nb;
+        for (size_t j = 0; j < ps.size(); j++) items[ck[c].items[j]].body = body_of[j];
+    }
+
+    // The batch's shape for the tuning cache: per class, the plans, distinct
+    // bodies and chunks (log2), and the group-table slots (log2).
+    std::string shape_key() const {
+        std::ostringstream k;
+        for (int c = 0; c < 2; c++) {
+            long long chunks = 0, slots = 0;
+            for (int i : ck[c].items) {
+                chunks += items[i].nchunks;
+                slots += items[i].nslots;
+            }
+            auto lg = [](long long v) { int l = 0; while (v > 1) { v >>= 1; l++; } return l; };
+            k << (c ? "|t" : "r") << ck[c].items.size() << "b" << ck[c].nbodies << "c" << lg(chunks) << "s" << lg(slots);
+        }
+        return k.str();
+    }
+
     // grid of each class at the current shared-memory size
     void size_grids() {
         for (int c = 0; c < 2; c++) {
@@ -406,31 +443,138 @@ struct Batch {
         }
     }
 
-    // Times graph replays over cache sizes (0 = every group in the global
-    // table) and unit sizes, then keeps the fastest.
-    void autotune() {
-        struct Cand { int cache_kb, unit_div; };
-        std::vector<Cand> cands;
-        std::vector<int> caches = ck[1].items.empty() ? std::vector<int>{cache_kb} : std::vector<int>{0, 48, 96, 160};
-        for (int c : caches)
-            for (int u : {2, 4, 8}) cands.push_back({c, u});
-        Cand best = {cache_kb, unit_div};
-        float best_ms = 1e30f;
-        for (const Cand& c : cands) {
-            cache_kb = c.cache_kb;
-            unit_div = c.unit_div;
-            size_grids();
-            layout();
-            replay();  // warm-up, graph capture
-            float t = 1e30f;
-            for (int r = 0; r < 3; r++) t = std::min(t, replay());
-            if (t < best_ms) { best_ms = t; best = c; }
+    struct Tuning {
+        int cache_kb, unit_div, block_regs, block_table;
+    };
+    Tuning tuning() const { return {cache_kb, unit_div, ck[0].block, ck[1].block}; }
+    void apply(const Tuning& t) {
+        cache_kb = t.cache_kb;
+        unit_div = t.unit_div;
+        for (int c = 0; c < 2; c++) {
+            const int b = c ? t.block_table : t.block_regs;
+            if (b != ck[c].block) {
+                ck[c].block = b;
+                gen_class(c);
+            }
         }
-        cache_kb = best.cache_kb;
-        unit_div = best.unit_div;
         size_grids();
+        for (int c = 0; c < 2; c++)
+            if (!ck[c].items.empty() && ck[c].k.fn && ck[c].k.max_blocks_per_sm < 1)
+                fail(VEXQ_ENOTSUP, "batch class kernel does not fit an SM at block " + std::to_string(ck[c].block));
         layout();
-        explain += " autotuned(" + std::to_string(cands.size()) + " candidates, best " + std::to_string(best_ms) + " ms)";
+    }
+    float time_replays() {
+        replay();  // warm-up, graph capture
+        float t = 1e30f;
+        for (int r = 0; r < 3; r++) t = std::min(t, replay());
+        return t;
+    }
+
+    // Times graph replays over cache sizes (0 = every group in the global
+    // table) and unit sizes, then over block shapes at the best of those,
+    // and keeps the fastest. The choice is kept in a JSON file beside the
+    // kernel cache, keyed by the batch's shape, so a batch of the same shape
+    // takes it without timing (flags & VEXQ_BATCH_RETUNE times again).
+    void autotune(bool retune) {
+        const std::string key = shape_key();
+        Tuning t;
+        if (!retune && tuning_cache_get(key, t)) {
+            apply(t);
+            explain += " autotuned(cached " + key + ")";
+            return;
+        }
+        std::vector<Tuning> cands;
+        std::vector<int> caches = ck[1].items.empty() ? std::vector<int>{cache_kb} : std::vector<int>{0, 48, 96, 160};
+        const Tuning base = tuning();
+        for (int c : caches)
+            for (int u : {2, 4, 8}) cands.push_back({c, u, base.block_regs, base.block_table});
+        Tuning best = base;
+        float best_ms = 1e30f;
+        int tried = 0;
+        for (const Tuning& c : cands) {
+            apply(c);
+            const float ms = time_replays();
+            tried++;
+            if (ms < best_ms) { best_ms = ms; best = c; }
+        }
+        // block shapes at the best cache and unit sizes
+        std::vector<Tuning> shapes;
+        for (int br : {128, 256})
+            for (int bt : {128, 256, 512}) {
+                if (ck[0].items.empty() && br != base.block_regs) continue;
+                if (ck[1].items.empty() && bt != base.block_table) continue;
+                if (br == best.block_regs && bt == best.block_table) continue;
+                shapes.push_back({best.cache_kb, best.unit_div, br, bt});
+            }
+        for (const Tuning& c : shapes) {
+            float ms;
+            try {
+                apply(c);
+                ms = time_replays();
+            } catch (const Status&) {
+                continue;  // a shape the kernels cannot launch (registers or shared memory)
+            }
+            tried++;
+            if (ms < best_ms) { best_ms = ms; best = c; }
+        }
+        apply(best);
+        tuning_cache_put(key, best, best_ms);
+        explain += " autotuned(" + std::to_string(tried) + " candidates, best " + std::to_string(best_ms) + " ms, block " +
+                   std::to_string(best.block_regs) + "/" + std::to_string(best.block_table) + ")";
+    }
+
+    // ---- the tuning cache: <kernel cache dir>/batch_tuning.json, one entry a
+    // line: "key": {"cache_kb": C, "unit_div": U, "block_regs": R, "block_table": T, "ms": M}
+    static std::mutex& tuning_mu() {
+        static std::mutex m;
+        return m;
+    }
+    static std::string tuning_path() { return jit_cache_dir() + "/batch_tuning.json"; }
+    static bool tuning_cache_get(const std::string& key, Tuning& t) {
+        std::lock_guard<std::mutex> lk(tuning_mu());
+        std::ifstream f(tuning_path());
+        std::string line;
+        const std::string want = "\"" + key + "\":";
+        while (std::getline(f, line)) {
+            if (line.find(want) == std::string::npos) continue;
+            auto num = [&](const char* name, int& v) {
+                const size_t at = line.find(std::string("\"") + name + "\":");
+                if (at == std::string::npos) return false;
+                v = std::atoi(line.c_str() + at + std::strlen(name) + 3);
+                return true;
+            };
+            return num("cache_kb", t.cache_kb) && num("unit_div", t.unit_div) && num("block_regs", t.block_regs) &&
+                   num("block_table", t.block_table) && t.unit_div > 0 &&
+                   (t.block_regs == 128 || t.block_regs == 256) &&
+                   (t.block_table == 128 || t.block_table == 256 || t.block_table == 512);
+        }
+        return false;
+    }
+    static void tuning_cache_put(const std::string& key, const Tuning& t, float ms) {
+        std::lock_guard<std::mutex> lk(tuning_mu());
+        std::vector<std::string> keep;
+        {
+            std::ifstream f(tuning_path());
+            std::string line;
+            const std::string want = "\"" + key + "\":";
+            while (std::getline(f, line))
+                if (line.size() > 2 && line[0] == ' ' && line.find(want) == std::string::npos) {
+                    if (line.back() == ',') line.pop_back();
+                    keep.push_back(line);
+                }
+        }
+        std::ostringstream e;
+        e << "  \"" << key << "\": {\"cache_kb\": " << t.cache_kb << ", \"unit_div\": " << t.unit_div
+          << ", \"block_regs\": " << t.block_regs << ", \"block_table\": " << t.block_table << ", \"ms\": " << ms << "}";
+        keep.push_back(e.str());
+        const std::string tmp = tuning_path() + ".tmp" + std::to_string(getpid());
+        {
+            std::ofstream f(tmp);
+            f << "{\n";
+            for (size_t i = 0; i < keep.size(); i++) f << keep[i] << (i + 1 < keep.size() ? ",\n" : "\n");
+            f << "}\n";
+        }
+        std::rename(tmp.c_str(), tuning_path().c_str());
     }
 };
 
@@ -490,19 +634,9 @@ void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
     b->ck[0].block = kBlockRegs;
     b->ck[1].block = kBlockTable;
     for (int c = 0; c < 2; c++) {
-        std::vector<Plan*> ps;
         for (size_t i = 0; i < b->items.size(); i++)
-            if (b->items[i].cls == c) {
-                b->ck[c].items.push_back((int)i);
-                ps.push_back(b->items[i].p);
-            }
-        if (ps.empty()) continue;
-        std::vector<int> body_of;
-        int smem = 0, nb = 0;
-        b->ck[c].k_src = gen_batch_source(ps, b->ck[c].block, body_of, smem, nb);
-        b->ck[c].smem_extra = smem;
-        b->ck[c].nbodies = nb;
-        for (size_t j = 0; j < ps.size(); j++) b->items[b->ck[c].items[j]].body = body_of[j];
+            if (b->items[i].cls == c) b->ck[c].items.push_back((int)i);
+        b->gen_class(c);
     }
     b->size_grids();
     b->layout();
@@ -519,7 +653,7 @@ Batch* new_batch() {
 Batch* create_batch(vexq_plan_s* const* handles, int n, uint32_t flags) {
     std::unique_ptr<Batch> b(new_batch());
     build_batch(b.get(), handles, n);
-    if (flags & VEXQ_BATCH_AUTOTUNE) b->autotune();
+    if (flags & (VEXQ_BATCH_AUTOTUNE | VEXQ_BATCH_RETUNE)) b->autotune((flags & VEXQ_BATCH_RETUNE) != 0);
     return b.release();
 }
 

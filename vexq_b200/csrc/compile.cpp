@@ -2703,7 +2703,8 @@ static void choose_tunables(Plan& p) {
         int b = get("block="), pl = get("pipeline="), st = get("staged="), sb = get("stage_kb="), rp = get("regs_pred=");
         if (rp >= 0) p.regs_pred = rp != 0;
         int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb="), ho = get("hot=");
-        int c32 = get("cnt32="), f32 = get("fx32="), gs = get("gsm=");
+        int c32 = get("cnt32="), f32 = get("fx32="), gs = get("gsm="), cs = get("cs=");
+        if (cs >= 0) p.stream_loads = cs != 0;
         if (gs >= 0) p.grid_per_sm = gs;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;
@@ -2777,6 +2778,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         p.lits.push_back(v);
     }
     std::ostringstream src;
+    if (p.stream_loads) src << "#define VQ_STREAM_LOADS 1\n";
     src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
     std::string body = join ? gen_probe_kernel(p, key_nodes, p.block) : gen_agg_kernel(p, key_nodes, p.block);
     p.src_main = src.str() + body;

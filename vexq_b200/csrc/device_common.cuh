@@ -29,26 +29,34 @@ __device__ __forceinline__ unsigned vq_bits4(const unsigned char* bm, vq_i64 r0)
 
 // 128-bit vectorised loads of four consecutive rows (r0 % 4 == 0) through the
 // read-only path; columns are 256-byte aligned and padded past the last row.
+// A kernel generated with VQ_STREAM_LOADS reads its columns as streaming
+// (ld.global.cs: evict first), so a table the kernel keeps probing stays in L2
+// while the columns pass through it once.
+#ifdef VQ_STREAM_LOADS
+#define VQ_LDC(p) __ldcs(p)
+#else
+#define VQ_LDC(p) __ldg(p)
+#endif
 __device__ __forceinline__ void vq_ld4_i64(const void* p, vq_i64 r0, vq_i64* v) {
     const longlong2* q = reinterpret_cast<const longlong2*>(static_cast<const vq_i64*>(p) + r0);
-    longlong2 a = __ldg(q), b = __ldg(q + 1);
+    longlong2 a = VQ_LDC(q), b = VQ_LDC(q + 1);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 __device__ __forceinline__ void vq_ld4_f64(const void* p, vq_i64 r0, double* v) {
     const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + r0);
-    double2 a = __ldg(q), b = __ldg(q + 1);
+    double2 a = VQ_LDC(q), b = VQ_LDC(q + 1);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 __device__ __forceinline__ void vq_ld4_i32(const void* p, vq_i64 r0, int* v) {
-    int4 a = __ldg(reinterpret_cast<const int4*>(static_cast<const int*>(p) + r0));
+    int4 a = VQ_LDC(reinterpret_cast<const int4*>(static_cast<const int*>(p) + r0));
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
 }
 __device__ __forceinline__ void vq_ld4_u32(const void* p, vq_i64 r0, unsigned* v) {
-    uint4 a = __ldg(reinterpret_cast<const uint4*>(static_cast<const unsigned*>(p) + r0));
+    uint4 a = VQ_LDC(reinterpret_cast<const uint4*>(static_cast<const unsigned*>(p) + r0));
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
 }
 __device__ __forceinline__ void vq_ld4_u8(const void* p, vq_i64 r0, unsigned* v) {
-    unsigned w = __ldg(reinterpret_cast<const unsigned*>(static_cast<const unsigned char*>(p) + r0));
+    unsigned w = VQ_LDC(reinterpret_cast<const unsigned*>(static_cast<const unsigned char*>(p) + r0));
     v[0] = w & 0xFF; v[1] = (w >> 8) & 0xFF; v[2] = (w >> 16) & 0xFF; v[3] = w >> 24;
 }
 
