@@ -460,6 +460,30 @@ int32_t vexq_server_stop(vexq_server_t s);
 /* Host-set cancellation flag polled between launches of a running plan. */
 int32_t vexq_cancel(vexq_plan_t p);
 
+/* ---- shards: partials merged in shard order ------------------------------
+ * Replaces ParallelHashAggregate's per-worker partial aggregates and
+ * mergePartialAgg (exec/parallel.go:124-210, 237-314) with shards of row
+ * groups: each shard (one per GPU, each GPU holding the whole table, or a
+ * row-group range on one GPU) runs the plan over [rg_start, rg_end) and gets a
+ * partial — every group unfinished: key, first-row order key, accumulators.
+ * Partials travel as bytes (serialize / deserialize, e.g. over
+ * torch.distributed) and vexq_partial_merge folds them in array order — counts
+ * and integer sums add, MIN/MAX keep the extreme (the earlier partial's on a
+ * tie), float sums add with a compensation term — then applies HAVING, ORDER BY
+ * and LIMIT once and returns the result. A join's probe side is sharded; its
+ * build side is the whole build table on every shard. COUNT(DISTINCT) returns
+ * VEXQ_ENOTSUP (planner/parallel.go:218-228). */
+typedef struct vexq_partial_s* vexq_partial_t;
+int32_t vexq_plan_run_partial(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_partial_t* out);
+/* Groups in the partial and device milliseconds of its run. */
+int32_t vexq_partial_info(vexq_partial_t part, int64_t* groups, double* kernel_ms);
+/* Bytes of the partial, valid until the next call on it or its free. */
+int32_t vexq_partial_serialize(vexq_partial_t part, const void** data, int64_t* len);
+/* A partial from bytes made by a plan of the same shape (VEXQ_EINVAL otherwise). */
+int32_t vexq_partial_deserialize(vexq_plan_t p, const void* data, int64_t len, vexq_partial_t* out);
+int32_t vexq_partial_merge(vexq_plan_t p, const vexq_partial_t* parts, int32_t n, vexq_result_t* out);
+int32_t vexq_partial_free(vexq_partial_t part);
+
 /* Fault injection on the host, for tests of the error paths (the reference's
  * counterpart is the failing-operator tests of exec/parallel_join.go:430-476:
  * the first error wins and the query returns it). After `after` more device

@@ -156,6 +156,8 @@ EXPORTS = [
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
     "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes",
+    "vexq_plan_run_partial", "vexq_partial_info", "vexq_partial_serialize", "vexq_partial_deserialize",
+    "vexq_partial_merge", "vexq_partial_free",
     "vexq_plan_run_global_noalloc",
     "vexq_batch_create",
     "vexq_batch_exec",
@@ -233,6 +235,12 @@ def load() -> C.CDLL:
         "vexq_server_stop": (i32, [vp]),
         "vexq_cancel": (i32, [vp]),
         "vexq_debug_fail_alloc": (i32, [i32]),
+        "vexq_plan_run_partial": (i32, [vp, i32, i32, C.POINTER(vp)]),
+        "vexq_partial_info": (i32, [vp, C.POINTER(i64), C.POINTER(C.c_double)]),
+        "vexq_partial_serialize": (i32, [vp, C.POINTER(vp), C.POINTER(i64)]),
+        "vexq_partial_deserialize": (i32, [vp, vp, i64, C.POINTER(vp)]),
+        "vexq_partial_merge": (i32, [vp, C.POINTER(vp), i32, C.POINTER(vp)]),
+        "vexq_partial_free": (i32, [vp]),
         "vexq_debug_live_device_bytes": (i32, [C.POINTER(i64)]),
         "vexq_plan_run_global_noalloc": (i32, [vp, i32, i32, vp, C.POINTER(i64), C.POINTER(C.c_uint8), i32]),
         "vexq_batch_create": (i32, [C.POINTER(vp), i32, C.c_uint32, C.POINTER(vp)]),

@@ -115,6 +115,7 @@ struct Plan {
     std::vector<KeyCol> keys;
     bool intkey_order = false;     // reference int-key path ordering rules apply
     int ndist = 0;                 // COUNT(DISTINCT) aggregates (device sets)
+    struct Groups* partial_out = nullptr;  // set: a run hands its groups here unfinished (a shard's partial)
     DevBuf dist_keys[VQ_MAXDIST], dist_state[VQ_MAXDIST];
     int intkey_width = 32;
     std::vector<Slot> slots;

@@ -1372,11 +1372,23 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
         g = run_regs(rc, P, nchunks);
     } else {
         Compacted c = run_atomic(rc, P, nchunks, estimate, rows);
-        if (p.k_having.fn) c = having_device(rc, c);
-        if (!topk_groups(rc, c, g)) {
-            g = fetch_groups(rc, c);
-            g.having_done = c.having_done;
+        if (p.partial_out) {
+            g = fetch_groups(rc, c);  // a shard's partial: every group, no HAVING, no LIMIT
+        } else {
+            if (p.k_having.fn) c = having_device(rc, c);
+            if (!topk_groups(rc, c, g)) {
+                g = fetch_groups(rc, c);
+                g.having_done = c.having_done;
+            }
         }
+    }
+    if (p.partial_out) {
+        *p.partial_out = std::move(g);
+        auto* r = new vexq_result_s;
+        r->kernel_ms = rc.kernel_ms;
+        r->scan_ms = rc.scan_ms;
+        r->launches = rc.launches;
+        return r;
     }
     note_hot_groups(p, g);
     vexq_result_s* r = build_result(p, g);
@@ -1825,7 +1837,12 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         Groups g;
         g.ival.assign(p.ni, {});
         g.fval.assign(p.nf, {});
-        r = build_result(p, g);
+        if (p.partial_out) {
+            *p.partial_out = g;
+            r = new vexq_result_s;
+        } else {
+            r = build_result(p, g);
+        }
         r->kernel_ms = rc.kernel_ms;
         r->launches = rc.launches;
     } else {

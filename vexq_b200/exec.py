@@ -211,6 +211,37 @@ class _PlanOp:
     def explain(self) -> str:
         return abi.load().vexq_plan_explain(self.h).decode()
 
+    # shards ----------------------------------------------------------------------
+    def run_partial(self, rg_start: int, rg_end: int) -> bytes:
+        """This shard's groups, unfinished, as bytes (vexq_plan_run_partial)."""
+        L = abi.load()
+        part = C.c_void_p()
+        abi.check(L.vexq_plan_run_partial(self.h, rg_start, rg_end, C.byref(part)))
+        try:
+            ptr, ln = C.c_void_p(), C.c_int64()
+            abi.check(L.vexq_partial_serialize(part, C.byref(ptr), C.byref(ln)))
+            return C.string_at(ptr, ln.value)
+        finally:
+            L.vexq_partial_free(part)
+
+    def merge_partials(self, parts) -> Result:
+        """The finished result of shard partials, folded in list order."""
+        L = abi.load()
+        hs = []
+        try:
+            for b in parts:
+                h = C.c_void_p()
+                buf = C.create_string_buffer(b, len(b))
+                abi.check(L.vexq_partial_deserialize(self.h, buf, len(b), C.byref(h)))
+                hs.append(h)
+            arr = (C.c_void_p * max(len(hs), 1))(*[h.value for h in hs])
+            out = C.c_void_p()
+            abi.check(L.vexq_partial_merge(self.h, arr, len(hs), C.byref(out)))
+            return Result(out)
+        finally:
+            for h in hs:
+                L.vexq_partial_free(h)
+
     def set_stream(self, stream_ptr: int) -> None:
         """Runs on a caller-owned cudaStream_t (0 restores the plan's own)."""
         abi.check(abi.load().vexq_plan_set_stream(self.h, C.c_void_p(stream_ptr or None)))
