@@ -1450,6 +1450,31 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
     os << "        long long v = sh_i[0][t];\n";
     os << "        for (int w = 1; w < " << warps << "; w++) v = vq_icomb(" << fc.kinds << "ikind(s), v, sh_i[w][t]);\n";
     os << "        P.part_i[(long long)(" << fc.part_index << ") * " << G * (ni + 1) << " + t] = v;\n    }\n";
+    if (!fc.dyn_smem) {
+        // merge by the last block to arrive (runs that pass P.mdone): the
+        // partials are written above; a threadfence before the arrival count
+        // makes them visible to the last block, whose warps each merge output
+        // entries in block order, exactly as the merge kernel does
+        const int tot = G * nf + G * (ni + 1), nfb = std::max(nf, 1);
+        os << "    if (P.mdone) {\n";
+        os << "        __threadfence();\n";
+        os << "        __syncthreads();\n";
+        os << "        __shared__ int vq_mlast;\n";
+        os << "        if (threadIdx.x == 0) vq_mlast = atomicAdd(P.mdone, 1u) == gridDim.x - 1u;\n";
+        os << "        __syncthreads();\n";
+        os << "        if (vq_mlast) {\n";
+        os << "            __threadfence();\n";
+        os << "            for (int e = threadIdx.x >> 5; e < " << tot << "; e += blockDim.x >> 5)\n";
+        os << "                merge_entry(e, P.part_f, P.part_i, (int)gridDim.x, " << G << ", " << nf << ", " << ni
+           << ", P.mkinds, P.mkinds + " << nfb << ", P.mout_f, P.mout_i);\n";
+        os << "            __syncthreads();\n";
+        os << "            if (threadIdx.x == 0) {\n";
+        os << "                *P.merr_out = atomicExch(P.error, 0);\n";
+        os << "                atomicExch(P.mdone, 0u);\n";
+        os << "            }\n";
+        os << "        }\n";
+        os << "    }\n";
+    }
     if (fused) os << "    }\n";
 }
 
@@ -2713,7 +2738,9 @@ static void choose_tunables(Plan& p) {
         if (mb >= 0) p.min_blocks = mb;
         if (ck >= 0) cache_kb = ck;
         if (wa >= 0) p.warp_agg = wa != 0;
-        if (b == 64 || b == 128 || b == 256 || b == 512) p.block = b;
+        if (b == 64 || b == 128 || b == 256 || b == 384 || b == 512) p.block = b;
+        const int ml = get("mlast=");
+        if (ml >= 0) p.merge_last = ml != 0;
         if (pl >= 0) p.pipeline = pl != 0;
         if (st >= 0) p.staged = st != 0;
         if (sb > 0) p.stage_budget = sb * 1024;

@@ -495,6 +495,69 @@ __device__ __forceinline__ vq_i64 vq_icomb(int kind, vq_i64 a, vq_i64 b) {
     return kind == 1 ? (b < a ? b : a) : kind == 2 ? (b > a ? b : a) : (vq_i64)((vq_u64)a + (vq_u64)b);
 }
 
+// Compensated addition (Knuth's TwoSum): hi + lo carries the running sum, lo
+// the rounding error of each step.
+__device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
+    double s = hi + x;
+    double bb = s - hi;
+    lo += (hi - (s - bb)) + (x - bb);
+    hi = s;
+}
+
+// One merged output entry of the register path, computed by one warp: lane l
+// folds partials l, l+32, l+64, ... in that order (a compensated TwoSum pair
+// for float sums, min/max/wrapping sum otherwise), then a fixed shuffle tree
+// combines the lanes, so the result does not depend on scheduling. Loads are
+// issued eight at a time ahead of their folds.
+static __device__ __noinline__ void merge_entry(int e, const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
+                            const int* fkind, const int* ikind, double* out_f, long long* out_i) {
+    const int lane = threadIdx.x & 31;
+    const int totf = G * nf, toti = G * (ni + 1);
+    if (e < totf) {
+        const int kind = fkind[e % nf];
+        double hi = kind == 1 ? 1.7976931348623157e308 : kind == 2 ? -1.7976931348623157e308 : 0.0, lo = 0.0;
+        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
+            double x[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_f[(long long)(b0 + 32 * j) * totf + e] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (b0 + 32 * j >= nblocks) break;
+                if (kind == 0) vq_two_sum(hi, lo, x[j]);
+                else hi = vq_fcomb(kind, hi, x[j]);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double h2 = __shfl_down_sync(0xffffffffu, hi, o), l2 = __shfl_down_sync(0xffffffffu, lo, o);
+            if (kind == 0) {
+                double h = hi, l = lo + l2;
+                vq_two_sum(h, l, h2);
+                hi = h;
+                lo = l;
+            } else {
+                hi = vq_fcomb(kind, hi, h2);
+            }
+        }
+        if (lane == 0) out_f[e] = kind == 0 ? hi + lo : hi;
+    } else if (e < totf + toti) {
+        const int u = e - totf;
+        const int kind = ikind[u % (ni + 1)];
+        long long v = kind == 1 ? 0x7FFFFFFFFFFFFFFFLL : kind == 2 ? (-0x7FFFFFFFFFFFFFFFLL - 1) : 0LL;
+        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
+            long long x[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_i[(long long)(b0 + 32 * j) * toti + u] : 0LL;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (b0 + 32 * j >= nblocks) break;
+                v = vq_icomb(kind, v, x[j]);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) v = vq_icomb(kind, v, (long long)__shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) out_i[u] = v;
+    }
+}
+
 // ---- bulk asynchronous copies (TMA, untiled) into a shared-memory ring ----
 // One thread issues cp.async.bulk copies of a tile's column slices into a
 // stage and arms the stage's mbarrier with the byte count; consumers wait on

@@ -74,6 +74,14 @@ struct VQParams {
     double* rout_f;                // [G][NF] merged float entries
     long long* rout_i;             // [G][NI + 1] merged integer entries
     int* rerr_out;                 // the error word handed out with the merged row
+    // ---- register path, partials merged by the last block (mdone set): every
+    //      block writes its partial row, the last to arrive merges all of them
+    //      in block order (the merge kernel's fold) and resets mdone ----
+    const int* mkinds;             // combiner kind per bank entry: float bank, then int bank
+    double* mout_f;                // [G][NF] merged float entries
+    long long* mout_i;             // [G][NI + 1] merged integer entries
+    int* merr_out;                 // the error word handed out with the merged row
+    unsigned* mdone;               // blocks that have written their partials
     // ---- COUNT(DISTINCT) sets, one per distinct aggregate: [cap][2] (group
     //      key, value image) and a state word per slot (0 empty, 1 being
     //      written, 2 published); cap = dmask + 1 ----

@@ -152,6 +152,8 @@ struct Plan {
     int async_stages = 0;      // >1: per-warp cp.async pipeline of that many 128-row chunks
     int min_blocks = 0;        // >0: __launch_bounds__ minimum resident blocks per SM
     int grid_per_sm = 0;       // >0: register path grid of at most this many blocks per SM
+    bool merge_last = false;   // register path: the last block merges the partials (no merge launch)
+    DevBuf mdone;              //   its arrival counter (0 between runs)
     bool stream_loads = false; // columns read evict-first (ld.global.cs): tables the kernel probes stay in L2
     // register-path accumulator forms, per slot (aggregate scans only):
     //  rdx    integer-valued sum (COUNT, integer SUM, float SUM of an integer

@@ -25,69 +25,6 @@ void refill_table(Table& t, const vexq_column_desc* cols, int32_t ncols, cudaStr
 
 // ---- static kernels ----------------------------------------------------------------
 
-// Compensated addition (Knuth's TwoSum): hi + lo carries the running sum, lo
-// the rounding error of each step.
-__device__ __forceinline__ void vq_two_sum(double& hi, double& lo, double x) {
-    double s = hi + x;
-    double bb = s - hi;
-    lo += (hi - (s - bb)) + (x - bb);
-    hi = s;
-}
-
-// One merged output entry of the register path, computed by one warp: lane l
-// folds partials l, l+32, l+64, ... in that order (a compensated TwoSum pair
-// for float sums, min/max/wrapping sum otherwise), then a fixed shuffle tree
-// combines the lanes, so the result does not depend on scheduling. Loads are
-// issued eight at a time ahead of their folds.
-__device__ void merge_entry(int e, const double* part_f, const long long* part_i, int nblocks, int G, int nf, int ni,
-                            const int* fkind, const int* ikind, double* out_f, long long* out_i) {
-    const int lane = threadIdx.x & 31;
-    const int totf = G * nf, toti = G * (ni + 1);
-    if (e < totf) {
-        const int kind = fkind[e % nf];
-        double hi = kind == 1 ? 1.7976931348623157e308 : kind == 2 ? -1.7976931348623157e308 : 0.0, lo = 0.0;
-        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
-            double x[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_f[(long long)(b0 + 32 * j) * totf + e] : 0.0;
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                if (b0 + 32 * j >= nblocks) break;
-                if (kind == 0) vq_two_sum(hi, lo, x[j]);
-                else hi = vq_fcomb(kind, hi, x[j]);
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double h2 = __shfl_down_sync(0xffffffffu, hi, o), l2 = __shfl_down_sync(0xffffffffu, lo, o);
-            if (kind == 0) {
-                double h = hi, l = lo + l2;
-                vq_two_sum(h, l, h2);
-                hi = h;
-                lo = l;
-            } else {
-                hi = vq_fcomb(kind, hi, h2);
-            }
-        }
-        if (lane == 0) out_f[e] = kind == 0 ? hi + lo : hi;
-    } else if (e < totf + toti) {
-        const int u = e - totf;
-        const int kind = ikind[u % (ni + 1)];
-        long long v = kind == 1 ? 0x7FFFFFFFFFFFFFFFLL : kind == 2 ? (-0x7FFFFFFFFFFFFFFFLL - 1) : 0LL;
-        for (int b0 = lane; b0 < nblocks; b0 += 32 * 8) {
-            long long x[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) x[j] = b0 + 32 * j < nblocks ? part_i[(long long)(b0 + 32 * j) * toti + u] : 0LL;
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                if (b0 + 32 * j >= nblocks) break;
-                v = vq_icomb(kind, v, x[j]);
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) v = vq_icomb(kind, v, (long long)__shfl_down_sync(0xffffffffu, v, o));
-        if (lane == 0) out_i[u] = v;
-    }
-}
-
 // Entry of the calling warp: eight warps (256 threads) a block.
 __device__ __forceinline__ int merge_warp() { return (int)blockIdx.x * 8 + ((int)threadIdx.x >> 5); }
 
@@ -745,13 +682,26 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         P.rout_i = out_i;
         P.rerr_out = err_out;
     }
+    // the last block merges the partials inside the scan: no merge launch
+    const bool last = !fused && p.merge_last;
+    if (last) {
+        if (!p.mdone.p) {
+            p.mdone.alloc(16);
+            VQ_CUDA(cudaMemsetAsync(p.mdone.p, 0, 16, rc.s));
+        }
+        P.mkinds = d_kinds;
+        P.mout_f = out_f;
+        P.mout_i = out_i;
+        P.merr_out = err_out;
+        P.mdone = p.mdone.as<unsigned>();
+    }
     bind_distinct(p, P, nchunks * 128, rc.s);
     VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
     jit_launch(K, grid, &P, sizeof P, rc.s);
     launch_check(rc.s, "p.k_main");
     // no event between the scan and its merge: an event record there stops the
     // merge's launch from overlapping the scan's drain (measured 5-6 us a run)
-    if (!fused) {
+    if (!fused && !last) {
         const int tot = G * nf + G * (ni + 1);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((tot + 7) / 8);
@@ -765,7 +715,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         VQ_CUDA(cudaLaunchKernelEx(&cfg, k_merge_regs_dep, (const double*)P.part_f, (const long long*)P.part_i, grid, G, nf,
                                    ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
     }
-    if (!fused) launch_check(rc.s, "k_merge_regs_dep");
+    if (!fused && !last) launch_check(rc.s, "k_merge_regs_dep");
     VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
     if (!mapped) VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
@@ -774,7 +724,7 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
     const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge (overlapping its drain, or inside it)
     rc.scan_ms += span;
     rc.kernel_ms += span;
-    rc.launches += fused ? 1 : 2;
+    rc.launches += fused || last ? 1 : 2;
     const double* hf = (const double*)p.h_stage.p;
     const long long* hi = (const long long*)((const char*)p.h_stage.p + nout_f);
     g.ival.assign(ni, {});
