@@ -192,7 +192,8 @@ def test_c3_batch_as_configured(gpu_lib):
                 regs += 1
             else:
                 assert_rows_match(rows, ref.rows(), ordered=True)
-                assert_sums_exact(r, ref)
+                if any(k in (abi.AGG_SUM, abi.AGG_AVG) for k in (a.kind for a in pl.aggs)):
+                    assert_sums_exact(r, ref)
                 table += 1
             r.close()
         assert regs > 0 and table > 0

@@ -88,6 +88,7 @@ def test_injected_allocation_failure(tables, kind):
     """A device allocation fails at each point of a plan's first run in turn:
     the run returns VEXQ_ENOMEM, the same plan's next run is correct, and
     destroying the plan gives every byte back."""
+    import gc
     X, li, o, i = tables
     L = abi.load()
 
@@ -99,10 +100,11 @@ def test_injected_allocation_failure(tables, kind):
     warm = make()
     ref = warm.run().rows()  # kernels compiled and loaded once
     warm.close()
-    base = _free_bytes()  # the tables
     failed = 0
     try:
         for after in range(0, 40):
+            gc.collect()
+            base = _free_bytes()  # everything but the plan made next
             op = make()
             abi.check(L.vexq_debug_fail_alloc(after))
             st = _run_status(op)
@@ -116,6 +118,7 @@ def test_injected_allocation_failure(tables, kind):
             # the plan that failed stays usable: its next run allocates again
             assert_rows_match(op.run().rows(), ref, ordered=True, rtol=0.0)
             op.close()
+            gc.collect()
             assert _free_bytes() == base, f"device memory not returned after a failure at allocation {after}"
         assert failed >= 1
         op = make()

@@ -3193,6 +3193,7 @@ void gen_having_kernel(Plan& p) {
         const INode& n = ir[i];
         if (n.k != NK::Col) continue;
         const std::string x = "x" + std::to_string(i), ok = "ok" + std::to_string(i), ct = ctype(n.type);
+        g.done[i] = 1;  // the output column is computed here, not read from a scanned column
         if (n.col < nk) {
             const KeyCol& k = p.keys[n.col];
             os << in << "long long kc" << i << "; bool kn" << i << " = false;\n";
@@ -3238,7 +3239,6 @@ void gen_having_kernel(Plan& p) {
             else
                 os << in << "const " << ct << " " << x << " = " << ok << " ? (" << ct << ")" << ival(a.value_slot) << " : (" << ct << ")0;\n";
         }
-        g.done[i] = 1;
     }
     g.emit(p.having_root);
     os << in << "keep = x" << p.having_root << " && ok" << p.having_root << ";\n";
