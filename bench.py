@@ -63,7 +63,7 @@ def serve_workload(args):
     the Q6-shape range SUM and the Q3-shape join with randomised date
     cutoffs, prepared once (64 plans); queries submitted to the serving loop.
     Arms: plain (one query per launch, one worker) and batched (continuous
-    batching, one worker), closed loop (all queued at once: throughput) and
+    batching, two workers), closed loop (all queued at once: throughput) and
     open loop (Poisson arrivals at 70% of the plain arm's closed-loop rate:
     p50/p99 latency, submit to result ready)."""
     import ctypes as C
@@ -136,11 +136,11 @@ def serve_workload(args):
 
     n = args.queries
     closed_plain = arm(np.zeros(n), 1, abi.SERVE_NO_BATCH)
-    closed_batched = arm(np.zeros(n), 1, 0)
+    closed_batched = arm(np.zeros(n), 2, 0)
     qps = 0.7 * closed_plain["qps"]
     arrivals = np.cumsum(rng.exponential(1.0 / qps, n))
     poisson_plain = arm(arrivals, 1, abi.SERVE_NO_BATCH)
-    poisson_batched = arm(arrivals, 1, 0)
+    poisson_batched = arm(arrivals, 2, 0)
     line = {"metric": "queries/s", "value": closed_batched["qps"], "unit": "queries/s", "n_gpus": 1,
             "steps": n, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded lineitem / orders / items generators)",
