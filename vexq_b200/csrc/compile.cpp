@@ -2339,11 +2339,16 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     p.bsmem = loop.smem();
     loop.prologue(os);
     os << kernel_head("vq_build", block);
-    // distinct keys counted per block, added to P.jnkeys once at the end
+    // distinct keys counted per lane and block, added to P.jnkeys once at the end
     os << "    __shared__ unsigned vq_nkeys;\n";
     os << "    unsigned long long vq_nrows = 0ull;\n";
+    os << "    unsigned vq_nk = 0u;  // mode 2: fresh keys of this lane\n";
     os << "    if (threadIdx.x == 0) vq_nkeys = 0u;\n    __syncthreads();\n";
     loop.open(os);
+    // mode 2 (keys unique in the last build): insert straight into the probe's
+    // 16-byte slots; a lane's fresh slots wait in registers for their group
+    // numbers, claimed once per warp and chunk
+    os << "        long long vq_fs[4]; int vq_fr[4]; unsigned long long vq_fk[4]; int vq_nf = 0;\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -2356,7 +2361,30 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     std::string K = std::to_string(key_node);
     os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
     os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
-    os << "            if (P.mode == 0) {\n";
+    os << "            if (P.mode == 2) {\n";
+    os << "                ulonglong2* sl = const_cast<ulonglong2*>(P.jslot);\n";
+    os << "                long long at = -1;\n";
+    os << "                if (jk == VQ_EMPTY_KEY) {\n";
+    os << "                    const unsigned long long old = atomicCAS(&sl[P.jmask + 1].x, 0ull, 1ull);\n";
+    os << "                    if (old == 0ull) at = (long long)P.jmask + 1; else atomicOr(P.error, 16);\n";
+    os << "                } else {\n";
+    os << "                    unsigned long long i = vq_hash(jk) & P.jmask;\n";
+    os << "                    const unsigned long long lim = P.jmask < (unsigned long long)VQ_MAX_PROBES ? P.jmask + 1 : (unsigned long long)VQ_MAX_PROBES;\n";
+    os << "                    unsigned long long n = 0;\n";
+    os << "                    for (; n < lim; n++) {\n";
+    os << "                        const unsigned long long old = atomicCAS(&sl[i].x, VQ_EMPTY_KEY, jk);\n";
+    os << "                        if (old == VQ_EMPTY_KEY) { at = (long long)i; break; }\n";
+    os << "                        if (old == jk) { atomicOr(P.error, 16); break; }  // a repeated key: the general build runs\n";
+    os << "                        i = (i + 1) & P.jmask;\n";
+    os << "                    }\n";
+    os << "                    if (n == lim) atomicOr(P.error, 1);\n";
+    os << "                }\n";
+    os << "                if (at >= 0) {\n";
+    os << "                    vq_nrows++;\n";
+    os << "                    if (P.jgid) { vq_fs[vq_nf] = at; vq_fr[vq_nf] = (int)r; vq_fk[vq_nf] = at == (long long)P.jmask + 1 ? VQ_EMPTY_KEY : jk; vq_nf++; }\n";
+    os << "                    else { sl[at].y = (unsigned long long)(unsigned)r | 0xFFFFFFFF00000000ull; vq_nk++; }\n";
+    os << "                }\n";
+    os << "            } else if (P.mode == 0) {\n";
     // pass 0 also keeps each slot's first row: a key with one build row needs
     // no row list, and a build whose keys never repeat skips pass 1
     os << "                bool fresh;\n";
@@ -2364,14 +2392,32 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) {\n";
     os << "                    atomicAdd(P.jcount + js, 1);\n";
     os << "                    vq_nrows++;\n";
-    os << "                    if (fresh) { P.jfirst[js] = (int)r; atomicAdd(&vq_nkeys, 1u); }\n";
+    os << "                    if (fresh) { P.jfirst[js] = (int)r; vq_nk++; }\n";
     os << "                }\n";
     os << "            } else {\n";
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
+    // mode 2 with group numbers (GROUP BY the join key): one claim per warp
+    os << "        if (P.mode == 2 && P.jgid) {\n";
+    os << "            int inc = vq_nf;\n";
+    os << "            for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
+    os << "            const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
+    os << "            unsigned long long base = 0ull;\n";
+    os << "            if (lane == 31 && tot) base = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
+    os << "            base = __shfl_sync(0xffffffffu, base, 31) + (unsigned long long)(inc - vq_nf);\n";
+    os << "            ulonglong2* sl = const_cast<ulonglong2*>(P.jslot);\n";
+    os << "            for (int j = 0; j < vq_nf; j++) {\n";
+    os << "                const unsigned long long g = base + (unsigned long long)j;\n";
+    os << "                sl[vq_fs[j]].y = (unsigned long long)(unsigned)vq_fr[j] | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
+    os << "                P.jgkey[g] = (unsigned long long)((long long)vq_fk[j] - P.jgoff);\n";
+    os << "            }\n";
+    os << "        }\n";
     loop.close(os);
+    // distinct keys a lane inserted, counted in registers (a shared counter
+    // taking one atomic per fresh key serialised the warps)
+    os << "    if (vq_nk) atomicAdd(&vq_nkeys, vq_nk);\n";
     os << "    __syncthreads();\n";
     os << "    if (threadIdx.x == 0 && vq_nkeys) atomicAdd(P.jnkeys, (unsigned long long)vq_nkeys);\n";
     os << "    for (int o = 16; o > 0; o >>= 1) vq_nrows += __shfl_xor_sync(0xffffffffu, vq_nrows, o);\n";
@@ -2718,6 +2764,10 @@ static void choose_tunables(Plan& p) {
     // 56.7 us against 59.8 us; with 40 warps an SM (one group) it costs
     // occupancy instead (Q6 shape: 43.9 us against 37.6 us)
     p.async_stages = p.path == AggPath::Regs && !p.is_join && acc > 24 ? 2 : 0;
+    // with the ring, one 384-thread block an SM (the same twelve warps as three
+    // 128-thread blocks) writes a third of the partials the merge reads:
+    // 6M-row Q1 shape 63.2 us against 65.1 us (scan + merge span)
+    if (p.async_stages > 1) p.block = 384;
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -2730,6 +2780,8 @@ static void choose_tunables(Plan& p) {
         int ck = get("cache_kb="), wa = get("warp_agg="), as = get("async="), mb = get("minb="), ho = get("hot=");
         int c32 = get("cnt32="), f32 = get("fx32="), gs = get("gsm="), cs = get("cs=");
         if (cs >= 0) p.stream_loads = cs != 0;
+        const int kt = get("keep=");
+        if (kt >= 0) p.keep_tables = kt != 0;
         if (gs >= 0) p.grid_per_sm = gs;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;
@@ -2806,6 +2858,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
     }
     std::ostringstream src;
     if (p.stream_loads) src << "#define VQ_STREAM_LOADS 1\n";
+    if (p.keep_tables) src << "#define VQ_KEEP_TABLES 1\n";
     src << prelude_source() << "\n" << gen_kind_tables(p) << "\n";
     std::string body = join ? gen_probe_kernel(p, key_nodes, p.block) : gen_agg_kernel(p, key_nodes, p.block);
     p.src_main = src.str() + body;

@@ -439,18 +439,33 @@ __device__ __forceinline__ vq_u64 vq_insert_fresh(vq_u64* keys, vq_u64 mask, vq_
     return VQ_NOSLOT;
 }
 
+// A kernel generated with VQ_KEEP_TABLES reads the join's slot table with an
+// L2 evict-last policy, so the table stays in L2 while the probe columns
+// stream past it.
+__device__ __forceinline__ ulonglong2 vq_ld_slot(const ulonglong2* p) {
+#ifdef VQ_KEEP_TABLES
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    ulonglong2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(p), "l"(pol));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 // Probe of the packed build table (key + chain in one 16-byte slot). Returns
 // whether the key is present and its chain word.
 __device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain, vq_u64& at) {
     if (key == VQ_EMPTY_KEY) {
-        const ulonglong2 s = __ldg(slots + mask + 1);
+        const ulonglong2 s = vq_ld_slot(slots + mask + 1);
         chain = s.y;
         at = mask + 1;
         return s.x != 0ull;
     }
     vq_u64 i = vq_hash(key) & mask;
     for (vq_u64 n = 0; n <= mask; n++) {
-        const ulonglong2 s = __ldg(slots + i);
+        const ulonglong2 s = vq_ld_slot(slots + i);
         if (s.x == key) { chain = s.y; at = i; return true; }
         if (s.x == VQ_EMPTY_KEY) return false;
         i = (i + 1) & mask;

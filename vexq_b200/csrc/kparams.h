@@ -52,6 +52,8 @@ struct VQParams {
     unsigned long long* jtotal;    // build rows inserted (pass 0)
     const ulonglong2* jslot;
     unsigned long long* jnkeys;
+    unsigned long long* jgkey;     // join build, mode 2 with group numbers: each number's key code
+    long long jgoff;               //   the key's code offset
     // ---- radix-partitioned join ----
     unsigned long long* pkeys;     // partition pass: keys written per partition
     int* prows;                    //                 their row ids

@@ -155,6 +155,7 @@ struct Plan {
     bool merge_last = false;   // register path: the last block merges the partials (no merge launch)
     DevBuf mdone;              //   its arrival counter (0 between runs)
     bool stream_loads = false; // columns read evict-first (ld.global.cs): tables the kernel probes stay in L2
+    bool keep_tables = false;  // join slot table read with an L2 evict-last policy
     // register-path accumulator forms, per slot (aggregate scans only):
     //  rdx    integer-valued sum (COUNT, integer SUM, float SUM of an integer
     //         input) kept as a double, exact while |sum| <= 2^53
@@ -213,6 +214,7 @@ struct Plan {
     long long gid_groups = 0;              // group numbers the last build handed out
     long long join_keys_seen = -1;         // join build: distinct keys the last build inserted
     long long join_rows_seen = 0;          //   from this many build rows
+    bool join_fast_failed = false;         // a one-pass (unique-key) build met a repeated key
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)

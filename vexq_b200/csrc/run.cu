@@ -1596,6 +1596,9 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         B.present = p.d_bpresent.as<unsigned char>();
         B.sets[0] = nullptr;
         for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
+        // keys unique in the last build (the primary-key side of a join): one
+        // pass straight into the probe's 16-byte slots
+        bool fast_unique = p.join_keys_seen > 0 && p.join_keys_seen == p.join_rows_seen && !p.join_fast_failed;
         for (;;) {
         long long nslots = jcap + 1;
         p.jt_keys.ensure(nslots * 8);
@@ -1621,6 +1624,50 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         unsigned long long* d_ngid = (unsigned long long*)(p.jt_scalar.as<char>() + 32);
         int* bsums = (int*)(p.jt_scalar.as<char>() + 64);
         B.jmask = (unsigned long long)(jcap - 1);
+        if (fast_unique) {
+            // one CAS a row on the slot's key word, then the chain word (the
+            // build row; with GROUP BY the join key, the key's group number,
+            // claimed once per warp and chunk); no per-slot counts, chain
+            // pass or packing pass. A repeated key (bit 16) or a full table
+            // (bit 0) sends this build to the general path below.
+            ensure_events(p);
+            VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 40, rc.s));
+            static_assert(VQ_EMPTY_KEY == ~0ull, "the empty-key fill is a byte memset");
+            VQ_CUDA(cudaMemsetAsync(p.jt_meta.p, 0xFF, (size_t)jcap * 16, rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_meta.as<char>() + (size_t)jcap * 16, 0, 16, rc.s));
+            VQParams F = B;
+            F.mode = 2;
+            F.jslot = p.jt_meta.as<ulonglong2>();
+            F.jgid = p.join_gid ? B.jgid : nullptr;
+            F.jgkey = p.jt_gkey.as<unsigned long long>();
+            F.jgoff = p.gid_koff;
+            if (bs.nchunks > 0) {
+                jit_launch(p.k_build, grid_for(p.k_build, bs.nchunks, p.staged), &F, sizeof F, rc.s);
+                launch_check(rc.s, "p.k_build (unique keys)");
+            }
+            int herr = 0;
+            unsigned long long nk = 0, ntot = 0;
+            VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&ntot, B.jtotal, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+            VQ_CUDA(cudaStreamSynchronize(rc.s));
+            rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
+            rc.launches += 1;
+            if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+            if (!(herr & (1 | 16)) && nk == ntot) {
+                join_keys = (long long)nk;
+                p.gid_groups = join_keys;
+                p.join_keys_seen = join_keys;
+                p.join_rows_seen = bs.rows;
+                break;
+            }
+            fast_unique = false;
+            p.join_fast_failed = (herr & 16) != 0;  // keys repeat now: the general build from here on
+            if (herr & 1) jcap = jsafe;
+            continue;
+        }
         {
             ensure_events(p);
             VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
