@@ -190,6 +190,7 @@ struct Plan {
     std::vector<long long> bseg_cache;     // join build side: last uploaded segment list
     DevBuf d_bseg;
     DevBuf d_kinds;                        // register-path combiner kinds
+    DevBuf d_tinit;                        // group tables: identities of the int bank, float-sum windows
     PinnedBuf h_stage;                     // pinned staging for small results
     void* h_stage_mapped = nullptr;        // its device address (null: not addressable, copy back)
     void* h_stage_mapped_for = nullptr;    // the staging allocation that address belongs to

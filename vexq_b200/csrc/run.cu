@@ -63,12 +63,29 @@ __global__ void __launch_bounds__(256) k_merge_batch(const VQMergeDesc* d, int n
 }
 
 // Atomic path: per-slot initial values (counts 0, MIN/MAX identities).
+// Every slot at its identities in one pass (keys empty, first-row keys max,
+// integer accumulators at their kind's identity, fixed-point digits and
+// special flags 0), and the run's counters and error word cleared.
 __global__ void k_init_table(unsigned long long* keys, long long* first, long long* acc_i, int ni, const long long* init_i,
-                             long long nslots, int hash) {
+                             long long* acc_fx, unsigned* special, int nf, long long nslots, int hash,
+                             unsigned long long* ngroups, int* error, unsigned long long* n_out) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *ngroups = 0ull;
+        *error = 0;
+        *n_out = 0ull;
+    }
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         if (hash) keys[i] = (i == nslots - 1) ? 0ull : VQ_EMPTY_KEY;
         first[i] = 0x7FFFFFFFFFFFFFFFLL;
         for (int s = 0; s < ni; s++) acc_i[(long long)s * nslots + i] = init_i[s];
+        for (int f = 0; f < nf; f++) {
+            long long* d = acc_fx + ((long long)f * nslots + i) * 4;  // 8-byte aligned only (odd slot counts)
+            d[0] = 0;
+            d[1] = 0;
+            d[2] = 0;
+            d[3] = 0;
+            special[(long long)f * nslots + i] = 0u;
+        }
     }
 }
 
@@ -812,15 +829,22 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         c.first = (long long*)(ob + 16 + cap_out * 8);
         c.ival = (long long*)(ob + 16 + cap_out * 16);
         c.fval = (double*)(ob + 16 + cap_out * 16 + (size_t)ni * cap_out * 8);
-        int* d_lsb = (int*)(ob + 16 + cap_out * 16 + (size_t)ni * cap_out * 8 + (size_t)nf * cap_out * 8);
+        (void)d_init;
+        // the plan's constant identities and float-sum windows, uploaded once
+        const size_t tinit = iv.size() * 8 + (size_t)std::max(nf, 1) * 4;
+        if (p.d_tinit.n < tinit) {
+            std::vector<char> img(tinit, 0);
+            std::memcpy(img.data(), iv.data(), iv.size() * 8);
+            if (nf) std::memcpy(img.data() + iv.size() * 8, p.fx_lsb.data(), (size_t)nf * 4);
+            p.d_tinit.ensure(tinit);
+            h2d(p.d_tinit.p, img.data(), tinit, rc.s);
+        }
+        const long long* d_iv = p.d_tinit.as<long long>();
+        const int* d_lsb = (const int*)(p.d_tinit.as<char>() + iv.size() * 8);
         VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
-        VQ_CUDA(cudaMemcpyAsync(d_init, iv.data(), iv.size() * 8, cudaMemcpyHostToDevice, rc.s));
-        if (nf) VQ_CUDA(cudaMemcpyAsync(d_lsb, p.fx_lsb.data(), nf * 4, cudaMemcpyHostToDevice, rc.s));
-        VQ_CUDA(cudaMemsetAsync(P.ngroups, 0, 16, rc.s));
-        VQ_CUDA(cudaMemsetAsync(n_out, 0, 8, rc.s));
-        if (b_fx) VQ_CUDA(cudaMemsetAsync(P.acc_fx, 0, b_fx + b_sp, rc.s));
         int ig = (int)std::min<long long>((nslots + 255) / 256, (long long)sm_count() * 16);
-        k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_init, nslots, hash);
+        k_init_table<<<ig, 256, 0, rc.s>>>(P.keys, P.first, P.acc_i, ni, d_iv, P.acc_fx, P.special, nf, nslots, hash, P.ngroups,
+                                          P.error, n_out);
         launch_check(rc.s, "k_init_table");
         bind_distinct(p, P, nchunks * 128, rc.s);
         VQ_CUDA(cudaGetLastError());
