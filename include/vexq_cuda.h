@@ -457,6 +457,19 @@ int32_t vexq_server_wait(vexq_server_t s, int64_t ticket, int64_t timeout_ms, ve
 int32_t vexq_server_latency(vexq_server_t s, int64_t ticket, double* ms);
 int32_t vexq_server_stop(vexq_server_t s);
 
+/* ---- per-plan tuning ------------------------------------------------------
+ * Times the plan's own runs over its launch-time choices and keeps the
+ * fastest: a join's build table (0 = the global table, else radix
+ * partitioning at 6, 8, 10 or 12 bits — the reference fixes the bits from the
+ * build size, RadixBitsFor, exec/parallel_join.go:72-81); a dense group
+ * table's shared-memory group cache (0, 48, 96 or 160 KB). Other paths have
+ * nothing to choose (*out_choice = -1). The choice is stored in
+ * plan_tuning.json beside the kernel cache, keyed by the plan's shape and
+ * sizes; a later plan of that shape takes it without timing unless flags has
+ * VEXQ_PLAN_RETUNE. *out_ms: the best time measured (0 when stored). */
+#define VEXQ_PLAN_RETUNE 1u
+int32_t vexq_plan_autotune(vexq_plan_t p, uint32_t flags, int32_t* out_choice, double* out_ms);
+
 /* Host-set cancellation flag polled between launches of a running plan. */
 int32_t vexq_cancel(vexq_plan_t p);
 

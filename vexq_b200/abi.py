@@ -139,6 +139,7 @@ class FilterBatch(C.Structure):
 # Every symbol include/vexq_cuda.h declares (checked by the CPU test suite).
 BATCH_AUTOTUNE = 1  # VEXQ_BATCH_AUTOTUNE
 BATCH_RETUNE = 2    # VEXQ_BATCH_RETUNE
+PLAN_RETUNE = 1     # VEXQ_PLAN_RETUNE
 SERVE_NO_BATCH = 1  # VEXQ_SERVE_NO_BATCH
 
 EXPORTS = [
@@ -155,7 +156,7 @@ EXPORTS = [
     "vexq_batch_run",
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
-    "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes",
+    "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes", "vexq_plan_autotune",
     "vexq_plan_run_partial", "vexq_partial_info", "vexq_partial_serialize", "vexq_partial_deserialize",
     "vexq_partial_merge", "vexq_partial_free",
     "vexq_plan_run_global_noalloc",
@@ -235,6 +236,7 @@ def load() -> C.CDLL:
         "vexq_server_stop": (i32, [vp]),
         "vexq_cancel": (i32, [vp]),
         "vexq_debug_fail_alloc": (i32, [i32]),
+        "vexq_plan_autotune": (i32, [vp, C.c_uint32, C.POINTER(i32), C.POINTER(C.c_double)]),
         "vexq_plan_run_partial": (i32, [vp, i32, i32, C.POINTER(vp)]),
         "vexq_partial_info": (i32, [vp, C.POINTER(i64), C.POINTER(C.c_double)]),
         "vexq_partial_serialize": (i32, [vp, C.POINTER(vp), C.POINTER(i64)]),

@@ -23,7 +23,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 SOURCES = ["table.cu", "run.cu", "compile.cpp", "jit.cpp", "abi.cpp", "serve.cpp", "noalloc.cu", "batch.cu", "vxq.cu",
-           "select.cu", "shard.cpp"]
+           "select.cu", "shard.cpp", "tune.cpp"]
 HEADERS = ["internal.h", "plan.h", "kparams.h", "device_common.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fno-strict-aliasing",

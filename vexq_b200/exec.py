@@ -242,6 +242,13 @@ class _PlanOp:
             for h in hs:
                 L.vexq_partial_free(h)
 
+    def autotune(self, retune: bool = False):
+        """(choice, best ms): radix bits for a join (0 = global table), the
+        shared-memory group cache in KB for a dense aggregate, -1 otherwise."""
+        ch, ms = C.c_int32(), C.c_double()
+        abi.check(abi.load().vexq_plan_autotune(self.h, abi.PLAN_RETUNE if retune else 0, C.byref(ch), C.byref(ms)))
+        return ch.value, ms.value
+
     def set_stream(self, stream_ptr: int) -> None:
         """Runs on a caller-owned cudaStream_t (0 restores the plan's own)."""
         abi.check(abi.load().vexq_plan_set_stream(self.h, C.c_void_p(stream_ptr or None)))
