@@ -358,8 +358,9 @@ int32_t vexq_selvec_from_bits(const uint8_t* bits, int64_t nrows, int64_t block,
  * never spans two row groups. The views and the SelVec stay valid until the
  * next call on this filter (exec/filter.go:10-28's ownership contract).
  * STRING vectors carry codes of the column's table-wide dictionary, which the
- * view's dictionary fields hold. Re-filling the table invalidates open
- * filters. */
+ * view's dictionary fields hold. The table must outlive the filter;
+ * re-filling it invalidates open filters. Results (vexq_result_t) own the
+ * strings they show and stay readable after their plan and tables are gone. */
 typedef struct vexq_filter_s* vexq_filter_t;
 typedef struct {
     int32_t                 ncols;

@@ -216,6 +216,7 @@ struct Plan {
     long long join_keys_seen = -1;         // join build: distinct keys the last build inserted
     long long join_rows_seen = 0;          //   from this many build rows
     bool join_fast_failed = false;         // a one-pass (unique-key) build met a repeated key
+    bool join_unique_seen = false;         // the last build inserted every key once
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
@@ -279,6 +280,9 @@ struct Groups {
 };
 std::vector<long long> init_values(const Plan& p);
 vexq_result_s* build_result(Plan& p, Groups& g);
+// Gives the result's STRING columns dictionaries of their own (the strings
+// they use, codes renumbered), so the result outlives the tables it read.
+void own_dictionaries(vexq_result_s* r);
 // Dense path: the groups with the largest counts of a finished run become the
 // groups the next run accumulates in registers.
 void note_hot_groups(Plan& p, const Groups& g);
@@ -388,6 +392,9 @@ struct vexq_result_s {
     std::vector<std::vector<uint8_t>> bbuf;
     std::vector<std::vector<uint32_t>> doff;
     std::vector<std::string> dbytes;
+    // the strings of the result's STRING columns, copied out of the tables'
+    // dictionaries: a result stays readable after its plan and tables are gone
+    std::vector<std::unique_ptr<vq::GlobalDict>> owned_dicts;
 };
 
 // Opaque handles of the C ABI.

@@ -1309,7 +1309,29 @@ vexq_result_s* build_result(Plan& p, Groups& g) {
         for (auto& c : r->cols) { c.v.resize(o.limit); c.valid.resize(o.limit); }
         r->nrows = o.limit;
     }
+    own_dictionaries(r);
     return r;
+}
+
+void own_dictionaries(vexq_result_s* r) {
+    for (OutColumn& oc : r->cols) {
+        if (!oc.dict) continue;
+        auto d = std::make_unique<GlobalDict>();
+        std::unordered_map<int64_t, uint32_t> local;
+        for (size_t j = 0; j < oc.v.size(); j++) {
+            if (!oc.valid[j]) continue;
+            const int64_t g = oc.v[j];
+            if (g < 0 || (size_t)g >= oc.dict->keys.size()) fail(VEXQ_EDEVICE, "result string code outside its dictionary");
+            auto it = local.find(g);
+            if (it == local.end()) {
+                it = local.emplace(g, (uint32_t)d->keys.size()).first;
+                d->keys.push_back(oc.dict->keys[(size_t)g]);
+            }
+            oc.v[j] = it->second;
+        }
+        oc.dict = d.get();
+        r->owned_dicts.push_back(std::move(d));
+    }
 }
 
 long long estimate_groups(const Plan& p, long long rows, long long join_keys) {
@@ -1622,7 +1644,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
         // keys unique in the last build (the primary-key side of a join): one
         // pass straight into the probe's 16-byte slots
-        bool fast_unique = p.join_keys_seen > 0 && p.join_keys_seen == p.join_rows_seen && !p.join_fast_failed;
+        bool fast_unique = p.join_unique_seen && !p.join_fast_failed;
         for (;;) {
         long long nslots = jcap + 1;
         p.jt_keys.ensure(nslots * 8);
@@ -1681,6 +1703,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             rc.launches += 1;
             if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
             if (!(herr & (1 | 16)) && nk == ntot) {
+                p.join_unique_seen = true;
                 join_keys = (long long)nk;
                 p.gid_groups = join_keys;
                 p.join_keys_seen = join_keys;
@@ -1715,6 +1738,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
             VQ_CUDA(cudaMemcpyAsync(&ntot, B.jtotal, 8, cudaMemcpyDeviceToHost, rc.s));
             VQ_CUDA(cudaStreamSynchronize(rc.s));
             const bool unique = nk == ntot && !(herr & 1);
+            p.join_unique_seen = unique && nk > 0;
             if (!unique && !(herr & 1)) {
                 int nb = (int)((nslots + 4095) / 4096);
                 k_scan_blocks<<<nb, 1024, 0, rc.s>>>(B.jcount, B.jstart, nslots, bsums);

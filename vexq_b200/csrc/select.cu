@@ -519,6 +519,7 @@ int32_t vexq_project_run(vexq_table_t table, const vexq_expr* nodes, int32_t nno
         VQ_CUDA(cudaEventRecord(e.b, s));
         VQ_CUDA(cudaStreamSynchronize(s));
         r->nrows = total;
+        own_dictionaries(r.get());
         r->kernel_ms = ev_ms(e.a, e.b);
         r->scan_ms = r->kernel_ms;
         r->launches = launches;
