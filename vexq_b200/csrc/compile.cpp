@@ -2445,20 +2445,38 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     os << kernel_head("vq_agg", block);
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     loop.open(os);
+    const std::string rk = std::string("r0 + ") + (loop.strided() ? "(k << 5)" : "k");
+    std::string K = std::to_string(p.probe_key);
+    // first pass over the lane's four rows: the filter, the key and the load
+    // of the key's home slot, so four table loads are in flight at once
+    os << "        unsigned long long vq_h[4]; ulonglong2 vq_s[4]; bool vq_on[4];\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
-    os << "            const long long r = r0 + " << (loop.strided() ? "(k << 5)" : "k") << ";\n";
+    os << "            const long long r = " << rk << ";\n";
+    os << "            vq_on[k] = false;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
+    {
+        Gen g0(p, os);
+        if (loop.strided()) g0.kidx = "(k << 5)";
+        if (p.pred >= 0) {
+            g0.emit(p.pred);
+            os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
+        }
+        g0.emit(p.probe_key);
+        os << "            if (!ok" << K << ") continue;\n";
+        os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
+        os << "            vq_h[k] = jk == VQ_EMPTY_KEY ? P.jmask + 1 : (vq_hash(jk) & P.jmask);\n";
+        os << "            vq_s[k] = vq_ld_slot(P.jslot + vq_h[k]);\n";
+        os << "            vq_on[k] = true;\n";
+    }
+    os << "        }\n";
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = " << rk << ";\n";
+    os << "            if (!vq_on[k]) continue;\n";
     Gen g(p, os);
     if (loop.strided()) g.kidx = "(k << 5)";
-    if (p.pred >= 0) {
-        g.emit(p.pred);
-        os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
-    }
     g.emit(p.probe_key);
-    std::string K = std::to_string(p.probe_key);
-    os << "            if (!ok" << K << ") continue;\n";
     os << "            unsigned long long jc, jat;\n";
-    os << "            if (!vq_find_slot(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", jc, jat)) continue;\n";
+    os << "            if (!vq_find_slot_from(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", vq_h[k], vq_s[k], jc, jat)) continue;\n";
     // a single-row chain carries its build row in the slot (count word ~group number, negative)
     os << "            const int ja = (int)(unsigned)jc, jn = (int)(jc >> 32);\n";
     if (p.join_gid) os << "            const unsigned long long vq_gid = jn < 0 ? (unsigned long long)(unsigned)~jn : (unsigned long long)(unsigned)P.jgid[jat];\n";
@@ -2764,10 +2782,10 @@ static void choose_tunables(Plan& p) {
     // 56.7 us against 59.8 us; with 40 warps an SM (one group) it costs
     // occupancy instead (Q6 shape: 43.9 us against 37.6 us)
     p.async_stages = p.path == AggPath::Regs && !p.is_join && acc > 24 ? 2 : 0;
-    // with the ring, one 384-thread block an SM (the same twelve warps as three
-    // 128-thread blocks) writes a third of the partials the merge reads:
-    // 6M-row Q1 shape 63.2 us against 65.1 us (scan + merge span)
-    if (p.async_stages > 1) p.block = 384;
+    // measured: with the ring, one 384-thread block an SM (the same twelve
+    // warps as three 128-thread blocks, a third of the partials) gave 63.2-63.7
+    // against 64.2-65.1 us in one process and 67 against 63 us in the bench
+    // loop; it stays a tunable (block=384)
     int cache_kb = 96;
     if (const char* e = std::getenv("VEXQ_TUNE")) {
         std::string s(e);
@@ -2782,6 +2800,8 @@ static void choose_tunables(Plan& p) {
         if (cs >= 0) p.stream_loads = cs != 0;
         const int kt = get("keep=");
         if (kt >= 0) p.keep_tables = kt != 0;
+        const int fb = get("fastbuild=");
+        if (fb >= 0) p.fast_build = fb != 0;
         if (gs >= 0) p.grid_per_sm = gs;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;

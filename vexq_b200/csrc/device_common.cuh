@@ -473,6 +473,26 @@ __device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mas
     return false;
 }
 
+// The same probe continued from its first slot, loaded ahead (the probe
+// kernel issues the first loads of a lane's four rows together): i0 is the
+// key's home slot (mask + 1 for the sentinel key) and s its contents.
+__device__ __forceinline__ bool vq_find_slot_from(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64 i0, ulonglong2 s,
+                                                  vq_u64& chain, vq_u64& at) {
+    if (key == VQ_EMPTY_KEY) {
+        chain = s.y;
+        at = mask + 1;
+        return s.x != 0ull;
+    }
+    vq_u64 i = i0;
+    for (vq_u64 n = 0; n <= mask; n++) {
+        if (s.x == key) { chain = s.y; at = i; return true; }
+        if (s.x == VQ_EMPTY_KEY) return false;
+        i = (i + 1) & mask;
+        s = vq_ld_slot(slots + i);
+    }
+    return false;
+}
+
 // Read-only lookup in a table no kernel is writing any more.
 __device__ __forceinline__ vq_u64 vq_find(const vq_u64* keys, vq_u64 mask, vq_u64 cap, vq_u64 key) {
     if (key == VQ_EMPTY_KEY) return __ldg(keys + cap) ? cap : VQ_NOSLOT;

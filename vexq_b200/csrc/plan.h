@@ -156,6 +156,10 @@ struct Plan {
     DevBuf mdone;              //   its arrival counter (0 between runs)
     bool stream_loads = false; // columns read evict-first (ld.global.cs): tables the kernel probes stay in L2
     bool keep_tables = false;  // join slot table read with an L2 evict-last policy
+    // join build straight into the probe's 16-byte slots when the last build's
+    // keys were unique (measured slower than count + pack at 1.5M keys: the
+    // slot table is twice the key table the CAS walks), so off by default
+    bool fast_build = false;
     // register-path accumulator forms, per slot (aggregate scans only):
     //  rdx    integer-valued sum (COUNT, integer SUM, float SUM of an integer
     //         input) kept as a double, exact while |sum| <= 2^53

@@ -1644,7 +1644,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         for (size_t i = 0, off = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + off; off += p.sets[i].size(); }
         // keys unique in the last build (the primary-key side of a join): one
         // pass straight into the probe's 16-byte slots
-        bool fast_unique = p.join_unique_seen && !p.join_fast_failed;
+        bool fast_unique = p.fast_build && p.join_unique_seen && !p.join_fast_failed;
         for (;;) {
         long long nslots = jcap + 1;
         p.jt_keys.ensure(nslots * 8);
