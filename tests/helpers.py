@@ -39,6 +39,20 @@ def assert_rows_match(gpu_rows, ref_rows, ordered=True, rtol=FLOAT_RTOL, exact_f
             assert close(a, b, tol), f"row {i} col {j}: gpu={a!r} ref={b!r}\n gpu={g}\n ref={r}"
 
 
+def assert_sorted_rows_match(gpu_rows, ref_rows, order_col, descending=True, rtol=FLOAT_RTOL):
+    """ORDER BY a float aggregate: the sort-column values agree position by
+    position (within rtol) and the rows agree as a set. Rows whose sort values
+    tie within the tolerance may come in either order: the GPU sums are exact,
+    so two groups with the same exact sum tie there, while the reference's
+    row-order fold can leave them an ulp apart."""
+    assert len(gpu_rows) == len(ref_rows), (len(gpu_rows), len(ref_rows))
+    vals = [r[order_col] for r in gpu_rows]
+    assert all((a >= b) if descending else (a <= b) for a, b in zip(vals, vals[1:])), "GPU rows out of order"
+    for i, (g, r) in enumerate(zip(gpu_rows, ref_rows)):
+        assert close(g[order_col], r[order_col], rtol), f"row {i}: gpu={g} ref={r}"
+    assert_rows_match(gpu_rows, ref_rows, ordered=False, rtol=rtol)
+
+
 def assert_float_vs_exact(gpu_rows, ref, ordered=True, rtol=FLOAT_RTOL, exact_tol=1e-13):
     """Float64 SUM/AVG parity with the exact-summation oracle as arbiter.
 

@@ -9,7 +9,7 @@ import pytest
 
 from oracle import refcpu as R
 from tests.golden.fixtures import load_cases, make_plan, make_table, normalize
-from tests.helpers import assert_float_vs_exact, assert_rows_match, close
+from tests.helpers import assert_float_vs_exact, assert_rows_match, assert_sorted_rows_match, close
 from vexq_b200 import abi, datagen as D, workloads as W
 from vexq_b200 import plan as P
 from vexq_b200.table import HostTable, date_column, float_column, int_column, string_column
@@ -122,9 +122,10 @@ def test_q3_join_top10_small(gpu_lib, join_small):
 
 def test_q3_join_all_groups_small(gpu_lib, join_small):
     o, i = join_small
-    g, r = run_join(gpu_lib, o, i, W.q3_plan(limit=-1))
+    plan = W.q3_plan(limit=-1)
+    g, r = run_join(gpu_lib, o, i, plan)
     assert g.nrows > 10000
-    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_sorted_rows_match(g.rows(), r.rows(), plan.order_col, plan.descending)
     assert_sums_exact(g, r)
 
 
