@@ -1,10 +1,10 @@
-"""GPU tests of repeated join runs with the one-pass build turned on
-(VEXQ_TUNE=fastbuild=1): a join plan whose last build inserted every key once
-builds its next table in one pass straight into the probe's slots (group
-numbers claimed per warp when the GROUP BY is the join key); a first run
-takes the general build. Both must give the same rows, and the reference's
-join known answers (duplicate keys, NULL keys, the sentinel and extreme int64
-keys) must hold on every run."""
+"""GPU tests of repeated join runs with the one-pass hash build turned on
+(VEXQ_TUNE=fastbuild=1, the direct-mapped build off): a join plan whose
+last build inserted every key once builds its next table in one pass
+straight into the probe's slots (group numbers claimed per warp when the
+GROUP BY is the join key); a first run takes the general build. Both must
+give the same rows, and the reference's join known answers (duplicate keys,
+NULL keys, the sentinel and extreme int64 keys) must hold on every run."""
 from __future__ import annotations
 
 import pytest
@@ -21,7 +21,7 @@ JOIN_CASES = [c for c in load_cases() if c["kind"] == "join"]
 
 @pytest.mark.parametrize("case", JOIN_CASES, ids=[c["name"] for c in JOIN_CASES])
 def test_known_answers_every_run(gpu_lib, case, monkeypatch):
-    monkeypatch.setenv("VEXQ_TUNE", "fastbuild=1")
+    monkeypatch.setenv("VEXQ_TUNE", "fastbuild=1,dmap=0")
     X = gpu_lib
     b, p = X.GpuTable(make_table(case["tables"]["build"])), X.GpuTable(make_table(case["tables"]["probe"]))
     op = X.GpuParallelHashJoinAggregate(b, p, make_plan(case))
@@ -35,7 +35,7 @@ def test_known_answers_every_run(gpu_lib, case, monkeypatch):
 
 @pytest.mark.parametrize("q", ["q3", "q3_all", "q12"])
 def test_repeated_runs_agree(gpu_lib, q, monkeypatch):
-    monkeypatch.setenv("VEXQ_TUNE", "fastbuild=1")
+    monkeypatch.setenv("VEXQ_TUNE", "fastbuild=1,dmap=0")
     X = gpu_lib
     o, i = D.orders(300_000, seed=21), D.items(1_200_000, 300_000, seed=22)
     plan = {"q3": W.q3_plan(), "q3_all": W.q3_plan(limit=-1), "q12": W.q12_plan()}[q]

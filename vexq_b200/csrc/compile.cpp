@@ -2361,7 +2361,17 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     std::string K = std::to_string(key_node);
     os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
     os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
-    os << "            if (P.mode == 2) {\n";
+    // mode 3 (keys unique and inside the dense range [dmin, dmin + drange)):
+    // one CAS a row on the key's own word of the direct-mapped table
+    os << "            if (P.mode == 3) {\n";
+    os << "                const unsigned long long di = jk - (unsigned long long)P.dmin;\n";
+    os << "                if (di >= P.drange) { atomicOr(P.error, 32); continue; }  // outside the range: the general build runs\n";
+    os << "                const unsigned long long old = atomicCAS(P.dmap + di, 0ull, (unsigned long long)(unsigned)r | 0xFFFFFFFF00000000ull);\n";
+    os << "                if (old != 0ull) { atomicOr(P.error, 16); continue; }  // a repeated key: the general build runs\n";
+    os << "                vq_nrows++;\n";
+    os << "                if (P.jgid) { vq_fs[vq_nf] = (long long)di; vq_fr[vq_nf] = (int)r; vq_fk[vq_nf] = jk; vq_nf++; }\n";
+    os << "                else vq_nk++;\n";
+    os << "            } else if (P.mode == 2) {\n";
     os << "                ulonglong2* sl = const_cast<ulonglong2*>(P.jslot);\n";
     os << "                long long at = -1;\n";
     os << "                if (jk == VQ_EMPTY_KEY) {\n";
@@ -2399,8 +2409,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
-    // mode 2 with group numbers (GROUP BY the join key): one claim per warp
-    os << "        if (P.mode == 2 && P.jgid) {\n";
+    // modes 2 and 3 with group numbers (GROUP BY the join key): one claim per warp
+    os << "        if ((P.mode == 2 || P.mode == 3) && P.jgid) {\n";
     os << "            int inc = vq_nf;\n";
     os << "            for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
     os << "            const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
@@ -2410,7 +2420,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            ulonglong2* sl = const_cast<ulonglong2*>(P.jslot);\n";
     os << "            for (int j = 0; j < vq_nf; j++) {\n";
     os << "                const unsigned long long g = base + (unsigned long long)j;\n";
-    os << "                sl[vq_fs[j]].y = (unsigned long long)(unsigned)vq_fr[j] | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
+    os << "                const unsigned long long w = (unsigned long long)(unsigned)vq_fr[j] | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
+    os << "                if (P.mode == 3) P.dmap[vq_fs[j]] = w; else sl[vq_fs[j]].y = w;\n";
     os << "                P.jgkey[g] = (unsigned long long)((long long)vq_fk[j] - P.jgoff);\n";
     os << "            }\n";
     os << "        }\n";
@@ -2443,6 +2454,14 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     p.smem = loop.smem();
     loop.prologue(os);
     os << kernel_head("vq_agg", block);
+    // a build the host did not wait for: its failure or emptiness is raised
+    // in this kernel's error word, which comes back with the results
+    os << "    if (P.berr && blockIdx.x == 0 && threadIdx.x == 0) {\n";
+    os << "        const int be = *P.berr;\n";
+    os << "        if (be & 8) atomicOr(P.error, 8);\n";
+    os << "        if (be & ~8) atomicOr(P.error, 64);\n";
+    os << "        else if (*P.bnk == 0ull) atomicOr(P.error, 128);\n";
+    os << "    }\n";
     if (p.path == AggPath::Regs) emit_regs_decl(os, p);
     loop.open(os);
     const std::string rk = std::string("r0 + ") + (loop.strided() ? "(k << 5)" : "k");
@@ -2464,8 +2483,14 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
         g0.emit(p.probe_key);
         os << "            if (!ok" << K << ") continue;\n";
         os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
-        os << "            vq_h[k] = jk == VQ_EMPTY_KEY ? P.jmask + 1 : (vq_hash(jk) & P.jmask);\n";
-        os << "            vq_s[k] = vq_ld_slot(P.jslot + vq_h[k]);\n";
+        // direct-mapped table: the key's own word (0: no build row)
+        os << "            if (P.dmap) {\n";
+        os << "                const unsigned long long di = jk - (unsigned long long)P.dmin;\n";
+        os << "                vq_s[k].y = di < P.drange ? vq_ld_dword(P.dmap + di) : 0ull;\n";
+        os << "            } else {\n";
+        os << "                vq_h[k] = jk == VQ_EMPTY_KEY ? P.jmask + 1 : (vq_hash(jk) & P.jmask);\n";
+        os << "                vq_s[k] = vq_ld_slot(P.jslot + vq_h[k]);\n";
+        os << "            }\n";
         os << "            vq_on[k] = true;\n";
     }
     os << "        }\n";
@@ -2475,11 +2500,17 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     Gen g(p, os);
     if (loop.strided()) g.kidx = "(k << 5)";
     g.emit(p.probe_key);
-    os << "            unsigned long long jc, jat;\n";
-    os << "            if (!vq_find_slot_from(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", vq_h[k], vq_s[k], jc, jat)) continue;\n";
+    os << "            unsigned long long jc, jat = 0ull;\n";
+    os << "            if (P.dmap) { jc = vq_s[k].y; if (jc == 0ull) continue; }\n";
+    os << "            else if (!vq_find_slot_from(P.jslot, P.jmask, (unsigned long long)(long long)x" << K << ", vq_h[k], vq_s[k], jc, jat)) continue;\n";
     // a single-row chain carries its build row in the slot (count word ~group number, negative)
     os << "            const int ja = (int)(unsigned)jc, jn = (int)(jc >> 32);\n";
-    if (p.join_gid) os << "            const unsigned long long vq_gid = jn < 0 ? (unsigned long long)(unsigned)~jn : (unsigned long long)(unsigned)P.jgid[jat];\n";
+    if (p.join_gid) {
+        os << "            const unsigned long long vq_gid = jn < 0 ? (unsigned long long)(unsigned)~jn : (unsigned long long)(unsigned)P.jgid[jat];\n";
+        // the group table is sized by the last build's key count when the host
+        // did not wait for this one: a number beyond it is raised, not written
+        os << "            if (vq_gid >= P.cap) { atomicOr(P.error, 256); continue; }\n";
+    }
     os << "            const int jb = jn < 0 ? 0 : ja, je = jn < 0 ? 1 : ja + jn;\n";
     os << "            for (int ji = jb; ji < je; ji++) {\n";
     os << "                const long long brow = jn < 0 ? (long long)ja : (long long)P.jrows[ji];\n";
@@ -2780,8 +2811,10 @@ static void choose_tunables(Plan& p) {
     // two-chunk cp.async pipeline a warp keeps the next chunk's columns in
     // flight without registers. 6M-row Q1 shape (6 groups x 8 accumulators):
     // 56.7 us against 59.8 us; with 40 warps an SM (one group) it costs
-    // occupancy instead (Q6 shape: 43.9 us against 37.6 us)
-    p.async_stages = p.path == AggPath::Regs && !p.is_join && acc > 24 ? 2 : 0;
+    // occupancy instead (Q6 shape: 43.9 us against 37.6 us). Join probes on
+    // the register path likewise (Q12 shape, 1.5M x 6M rows: 0.269 against
+    // 0.283 ms a query)
+    p.async_stages = p.path == AggPath::Regs && acc > 24 ? 2 : 0;
     // measured: with the ring, one 384-thread block an SM (the same twelve
     // warps as three 128-thread blocks, a third of the partials) gave 63.2-63.7
     // against 64.2-65.1 us in one process and 67 against 63 us in the bench
@@ -2802,6 +2835,10 @@ static void choose_tunables(Plan& p) {
         if (kt >= 0) p.keep_tables = kt != 0;
         const int fb = get("fastbuild=");
         if (fb >= 0) p.fast_build = fb != 0;
+        const int dm = get("dmap=");
+        if (dm >= 0) p.dmap_on = dm != 0;
+        const int sp = get("spec=");
+        if (sp >= 0) p.spec_on = sp != 0;
         if (gs >= 0) p.grid_per_sm = gs;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;

@@ -454,6 +454,18 @@ __device__ __forceinline__ ulonglong2 vq_ld_slot(const ulonglong2* p) {
 #endif
 }
 
+// The same for one word of the direct-mapped build table.
+__device__ __forceinline__ unsigned long long vq_ld_dword(const unsigned long long* p) {
+#ifdef VQ_KEEP_TABLES
+    unsigned long long pol, v;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 // Probe of the packed build table (key + chain in one 16-byte slot). Returns
 // whether the key is present and its chain word.
 __device__ __forceinline__ bool vq_find_slot(const ulonglong2* slots, vq_u64 mask, vq_u64 key, vq_u64& chain, vq_u64& at) {

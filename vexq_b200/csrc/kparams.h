@@ -54,6 +54,17 @@ struct VQParams {
     unsigned long long* jnkeys;
     unsigned long long* jgkey;     // join build, mode 2 with group numbers: each number's key code
     long long jgoff;               //   the key's code offset
+    // direct-mapped build table (mode 3; keys unique and inside a dense range):
+    // [drange] chain words indexed by key - dmin, 0 where no build row has
+    // the key; a word is the one build row and ~group number, as in .y of jslot
+    unsigned long long* dmap;
+    long long dmin;
+    unsigned long long drange;
+    // probe after a direct-mapped build that the host did not wait for: the
+    // build's error word and key count, checked by the probe's first thread
+    // (error bit 64: the build failed, 128: it inserted no key)
+    const int* berr;
+    const unsigned long long* bnk;
     // ---- radix-partitioned join ----
     unsigned long long* pkeys;     // partition pass: keys written per partition
     int* prows;                    //                 their row ids
@@ -103,7 +114,7 @@ struct VQParams {
     // ---- 4-byte scalars ----
     int nseg;
     int n_rg;
-    int mode;                  // join build: 0 = insert/count, 1 = fill
+    int mode;                  // join build: 0 = insert/count, 1 = fill, 2 = unique keys into jslot, 3 = unique keys into dmap
     int cache_n;               // dense path: groups held in the block's shared-memory cache
     int nparts;                // radix join: partitions (a power of two)
     int pbits;                 // radix join: partition = top pbits bits of the key hash

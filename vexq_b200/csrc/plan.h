@@ -221,6 +221,14 @@ struct Plan {
     long long join_rows_seen = 0;          //   from this many build rows
     bool join_fast_failed = false;         // a one-pass (unique-key) build met a repeated key
     bool join_unique_seen = false;         // the last build inserted every key once
+    // direct-mapped build table: a word per value of the build key column's
+    // range [imin, imax] (keys unique and the range at most a few times the
+    // build rows); a build that meets a repeated key takes the hash table
+    bool dmap_on = true;                   // allowed (VEXQ_TUNE dmap=0 turns it off)
+    bool dmap_failed = false;              // a direct-mapped build met a repeated key
+    bool dmap_used = false;                // the last build was direct-mapped
+    bool spec_on = true;                   // a repeated direct-mapped build goes without a host wait (VEXQ_TUNE spec=0: off)
+    DevBuf jt_dmap;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)

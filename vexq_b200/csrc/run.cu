@@ -396,9 +396,12 @@ __device__ __forceinline__ unsigned long long vq_rank(long long bits, bool isnul
     u = desc ? u : ~u;
     return u == 0xFFFFFFFFFFFFFFFFull ? u - 1 : u;
 }
-__global__ void k_sample(const unsigned long long* rank, long long n, int S, unsigned long long* out) {
+// The top-k kernels read the group count from the device (*np, written by
+// the finalize or HAVING compaction), so they follow it without a copy back.
+__global__ void k_sample(const unsigned long long* rank, const unsigned long long* np, long long nmax, int S, unsigned long long* out) {
+    const long long n = (long long)min(*np, (unsigned long long)nmax);
     int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < S) out[j] = rank[(long long)j * n / S];
+    if (j < S) out[j] = n > 0 ? rank[(long long)j * n / S] : 0ull;
 }
 // One block finds the q-th largest of the S samples (S <= 4096, q < S) by radix
 // select, most significant byte first: each round counts, in shared memory,
@@ -406,7 +409,17 @@ __global__ void k_sample(const unsigned long long* rank, long long n, int S, uns
 // warp walks the 256 counts from the top to the byte holding the q-th largest.
 // The result is the selection threshold, so the host needs no copy of the
 // samples.
-__global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* samp, int S, int q, unsigned long long* thr) {
+__global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* samp, int S, const unsigned long long* np, long long nmax,
+                                                    int limit, unsigned long long* thr) {
+    const long long n = (long long)min(*np, (unsigned long long)nmax);
+    // few groups (at most 4·LIMIT + 4096): every group is a candidate
+    if (n <= 4LL * limit + 4096) {
+        if (threadIdx.x == 0) *thr = 0ull;
+        return;
+    }
+    // expected (q+1)·n/S groups at or above the q-th largest sample: about
+    // 4·LIMIT + 64 (n above 4·LIMIT + 4096 keeps q below S)
+    const int q = (int)ceil((4.0 * limit + 64.0) * S / (double)n) - 1;
     __shared__ unsigned hist[256];
     __shared__ unsigned long long prefix;
     __shared__ unsigned need;
@@ -450,8 +463,9 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
     }
     if (threadIdx.x == 0) *thr = q < S ? prefix : 0ull;
 }
-__global__ void k_select(const unsigned long long* rank, long long n, const unsigned long long* thrp, unsigned long long* nsel,
-                         long long* sel, long long cap) {
+__global__ void k_select(const unsigned long long* rank, const unsigned long long* np, long long nmax, const unsigned long long* thrp,
+                         unsigned long long* nsel, long long* sel, long long cap) {
+    const long long n = (long long)min(*np, (unsigned long long)nmax);
     const unsigned long long thr = *thrp;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (rank[i] >= thr) {
@@ -462,8 +476,9 @@ __global__ void k_select(const unsigned long long* rank, long long n, const unsi
 }
 // Rank of one aggregate output per compacted group: its sort key's raw bits
 // (NULL flag) mapped by vq_rank so that a larger rank sorts first.
-__global__ void k_sortrank(const long long* o_i, const double* o_f, long long cap_out, long long n, int kind, int vbank,
-                           int vpos, int nnpos, int fmin_key, int desc, unsigned long long* rank) {
+__global__ void k_sortrank(const long long* o_i, const double* o_f, long long cap_out, const unsigned long long* np, int kind,
+                           int vbank, int vpos, int nnpos, int fmin_key, int desc, unsigned long long* rank) {
+    const long long n = (long long)min(*np, (unsigned long long)cap_out);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         long long nn = o_i[(long long)nnpos * cap_out + i];
         bool isnull = kind != VEXQ_AGG_COUNT && nn == 0;
@@ -535,6 +550,18 @@ void bind_distinct(Plan& p, VQParams& P, long long rows, cudaStream_t s) {
     P.dmask = cap - 1;
 }
 
+// A join probe that followed a direct-mapped build the host did not wait for
+// raises the build's outcome in its own error word (64: the build met a
+// repeated or out-of-range key, 128: it inserted no key, 256: it numbered more
+// keys than the group table sized from the last build holds). The run is then
+// repeated with the host waiting for the build.
+struct SpecRetry {
+    int bits;
+};
+static void check_spec_flags(int herr) {
+    if (herr & (64 | 128 | 256)) throw SpecRetry{herr & (64 | 128 | 256)};
+}
+
 // Error bits of a COUNT(DISTINCT) set insert (vq_dset_insert).
 static void check_distinct_flags(int herr) {
     if (herr & 16) fail(VEXQ_EDEVICE, "COUNT(DISTINCT) set reached its probe limit");
@@ -542,6 +569,7 @@ static void check_distinct_flags(int herr) {
 }
 
 void check_regs_flags(int herr) {
+    check_spec_flags(herr);
     check_distinct_flags(herr);
     if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
     if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
@@ -760,16 +788,23 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
 // Atomic path: group table, main kernel (retried with a larger table when a
 // probe limit is hit), finalize + compaction on the device.
 struct Compacted {
-    long long n = 0;
+    long long n = 0;           // groups (-1: not copied back yet; the device holds it in *n_dev)
     long long cap_out = 0;
     unsigned long long* key = nullptr;
     long long* first = nullptr;
     long long* ival = nullptr;
     double* fval = nullptr;
+    const unsigned long long* n_dev = nullptr;  // the group count on the device
+    const int* err_dev = nullptr;  // deferred run: the kernels' error word, read with the results
+    bool hash = false;             // deferred run on a hash table: its group count sizes the next run
+    long long rows = 0;
     bool having_done = false;  // only the groups HAVING keeps
 };
 
-Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows) {
+// A deferred run (defer set) launches the table kernels and returns without
+// waiting: the caller's top-k launches follow on the stream, and one copy back
+// after them brings the group count and the error word with the results.
+Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estimate, long long rows, bool defer = false) {
     Plan& p = rc.p;
     // a join grouping by its key on the global table: one slot per build key
     // number, no key inserts; the keys come from the build's number→key array
@@ -860,6 +895,15 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         launch_check(rc.s, "k_finalize");
         VQ_CUDA(cudaGetLastError());
         VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
+        c.n_dev = n_out;
+        if (defer) {
+            c.n = -1;
+            c.err_dev = P.error;
+            c.hash = hash;
+            c.rows = rows;
+            rc.launches += 3;
+            return c;
+        }
         p.h_stage.ensure(32);
         VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, n_out, 8, cudaMemcpyDeviceToHost, rc.s));
         VQ_CUDA(cudaMemcpyAsync((char*)p.h_stage.p + 8, P.error, 4, cudaMemcpyDeviceToHost, rc.s));
@@ -869,6 +913,7 @@ Compacted run_atomic(RunCtx& rc, VQParams& P, long long nchunks, long long estim
         rc.launches += 3;
         unsigned long long nn = *(unsigned long long*)p.h_stage.p;
         int herr = *(int*)((char*)p.h_stage.p + 8);
+        check_spec_flags(herr);
         check_distinct_flags(herr);
         if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
         if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
@@ -946,84 +991,124 @@ Compacted having_device(RunCtx& rc, const Compacted& c) {
     VQ_CUDA(cudaStreamSynchronize(rc.s));
     rc.kernel_ms += elapsed(p.ev[2], p.ev[3]);
     o.n = (long long)std::min<unsigned long long>(*(const unsigned long long*)p.h_stage.p, (unsigned long long)o.cap_out);
+    o.n_dev = cnt;
     return o;
 }
 
 // Device top-k candidates for ORDER BY <aggregate> LIMIT k: every group's sort
 // rank (raw int64 bits in the ExternalSort order, NULLs first) is computed on
 // the device; the q-th largest of a 4096-point sample, found on the device,
-// is a threshold that keeps about 4·LIMIT + 64 groups; the groups at or above
-// it (ties included) are gathered, and the host finishes the stable sort on
-// them. Two copies back: the count, then the gathered groups. Returns false
-// (the caller fetches every group) when the plan has no such ORDER BY, the
-// groups are few, or the sample was unlucky.
-bool topk_groups(RunCtx& rc, const Compacted& c, Groups& g) {
-    Plan& p = rc.p;
+// is a threshold that keeps about 4·LIMIT + 64 groups (every group when there
+// are at most 4·LIMIT + 4096); the groups at or above it (ties included) are
+// gathered, and the host finishes the stable sort on them. The kernels read
+// the group count on the device, so they follow a deferred table run without
+// a copy back; one copy brings the count, the error word, the selected count
+// and the first gathered rows. Returns 1 with g filled; 0 when the caller
+// fetches every group instead (the plan has no such ORDER BY, the groups are
+// few and already counted, or the sample was unlucky; c.n is set); -1 when a
+// deferred run hit its table's probe limit and must run again.
+bool topk_applies(const Plan& p, bool having_done) {
     const vexq_order_desc& o = p.order;
-    int ngb = (int)p.keys.size();
-    const long long kCap = 65536;
     // HAVING filters groups before the sort: every group comes back, unless
     // the device already kept only the groups HAVING passes
-    if ((p.having_root >= 0 && !c.having_done) || o.sort_col < ngb || o.limit < 0 || o.limit > 4096 || c.n <= 4 * o.limit + 4096)
-        return false;
-    const AggOut& a = p.outs[o.sort_col - ngb];
+    return !((p.having_root >= 0 && !having_done) || o.sort_col < (int)p.keys.size() || o.limit < 0 || o.limit > 4096);
+}
+
+int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
+    Plan& p = rc.p;
+    const vexq_order_desc& o = p.order;
+    const long long kCap = 65536;
+    if (!topk_applies(p, c.having_done)) return 0;
+    if (c.n >= 0 && c.n <= 4 * o.limit + 4096) return 0;
+    const AggOut& a = p.outs[o.sort_col - (int)p.keys.size()];
     int vslot = a.value_slot;
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
     int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
     if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
     const int S = 4096;
     const long long w = 2 + p.ni + p.nf;
+    const long long nmax = c.n >= 0 ? c.n : c.cap_out;
     // rank | samples | threshold, count | selected indices | gathered rows
-    size_t need = (size_t)c.n * 8 + S * 8 + 16 + kCap * 8 + (size_t)kCap * w * 8 + 64;
+    size_t need = (size_t)nmax * 8 + S * 8 + 16 + kCap * 8 + (size_t)kCap * w * 8 + 64;
     p.scratch_d.ensure(need);
     unsigned long long* rank = p.scratch_d.as<unsigned long long>();
-    unsigned long long* samp = rank + c.n;
+    unsigned long long* samp = rank + nmax;
     unsigned long long* thr = samp + S;
     unsigned long long* nsel = thr + 1;
     long long* dsel = (long long*)(nsel + 1);
     long long* dout = dsel + kCap;
-    int gr = (int)std::min<long long>((c.n + 255) / 256, (long long)sm_count() * 8);
-    k_sortrank<<<gr, 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n, a.kind, vbank, p.slot_pos[vslot], p.slot_pos[a.nn_slot],
-                                     fmin_key, o.descending, rank);
+    int gr = (int)std::min<long long>((nmax + 255) / 256, (long long)sm_count() * 8);
+    k_sortrank<<<std::max(gr, 1), 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n_dev, a.kind, vbank, p.slot_pos[vslot],
+                                                  p.slot_pos[a.nn_slot], fmin_key, o.descending, rank);
     launch_check(rc.s, "k_sortrank");
-    k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n, S, samp);
+    k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n_dev, nmax, S, samp);
     launch_check(rc.s, "k_sample");
-    // threshold: expected (q+1)·n/S groups at or above the q-th largest sample
-    // (c.n > 4·limit + 4096 keeps q below S)
-    const int q = (int)std::ceil((4.0 * o.limit + 64.0) * S / (double)c.n) - 1;
-    k_threshold<<<1, 1024, 0, rc.s>>>(samp, S, q, thr);
+    k_threshold<<<1, 1024, 0, rc.s>>>(samp, S, c.n_dev, nmax, (int)o.limit, thr);
     launch_check(rc.s, "k_threshold");
     VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
-    k_select<<<gr, 256, 0, rc.s>>>(rank, c.n, thr, nsel, dsel, kCap);
+    k_select<<<std::max(gr, 1), 256, 0, rc.s>>>(rank, c.n_dev, nmax, thr, nsel, dsel, kCap);
     launch_check(rc.s, "k_select");
     k_gather<<<(int)((kCap + 127) / 128), 128, 0, rc.s>>>(dsel, nsel, kCap, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni,
                                                           p.nf, dout);
     launch_check(rc.s, "k_gather");
     VQ_CUDA(cudaGetLastError());
-    p.h_stage.ensure(16);
-    VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
-    VQ_CUDA(cudaStreamSynchronize(rc.s));
     rc.launches += 5;
-    const long long ns = (long long)*(const unsigned long long*)p.h_stage.p;
-    // an unlucky sample (fewer than LIMIT selected) or too many ties at the
-    // threshold: the caller fetches every group
-    if (ns < o.limit || ns > kCap) return false;
-    g.having_done = c.having_done;
-    std::vector<long long> h((size_t)ns * w);
-    VQ_CUDA(cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+    // one copy back: group count, error word, selected count, and the first
+    // R gathered rows (twice the expected candidates)
+    const long long R = std::min<long long>(kCap, 2 * (4LL * o.limit + 64));
+    p.h_stage.ensure(32 + (size_t)R * w * 8);
+    char* hs = (char*)p.h_stage.p;
+    std::memset(hs, 0, 32);
+    VQ_CUDA(cudaMemcpyAsync(hs, c.n_dev, 8, cudaMemcpyDeviceToHost, rc.s));
+    if (c.err_dev) VQ_CUDA(cudaMemcpyAsync(hs + 8, c.err_dev, 4, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(hs + 16, nsel, 8, cudaMemcpyDeviceToHost, rc.s));
+    VQ_CUDA(cudaMemcpyAsync(hs + 32, dout, (size_t)R * w * 8, cudaMemcpyDeviceToHost, rc.s));
+    if (c.n < 0) VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
+    if (c.n < 0) {  // a deferred table run: its time, count and error word
+        rc.scan_ms += elapsed(p.ev[1], p.ev[2]);
+        rc.kernel_ms += elapsed(p.ev[0], p.ev[3]);
+        c.n = (long long)std::min<unsigned long long>(*(const unsigned long long*)hs, (unsigned long long)c.cap_out);
+        const int herr = *(const int*)(hs + 8);
+        check_spec_flags(herr);
+        check_distinct_flags(herr);
+        if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+        if (herr & 2) fail(VEXQ_ENOTSUP, "float sum exceeded its exact accumulation window");
+        if (herr & 1) {
+            if (!c.hash) fail(VEXQ_EDEVICE, "dense group table reported a probe failure");
+            return -1;
+        }
+        if (c.hash) {
+            p.hash_groups_seen = c.n;
+            p.hash_rows_seen = c.rows;
+        }
+    }
+    const long long ns = (long long)*(const unsigned long long*)(hs + 16);
+    // few groups: all of them were selected; otherwise an unlucky sample (fewer
+    // than LIMIT selected) or too many ties at the threshold: the caller
+    // fetches every group
+    if (c.n > 4 * o.limit + 4096 && (ns < o.limit || ns > kCap)) return 0;
+    if (ns > kCap) return 0;
+    g.having_done = c.having_done;
+    std::vector<long long> rest;
+    if (ns > R) {
+        rest.resize((size_t)(ns - R) * w);
+        VQ_CUDA(cudaMemcpyAsync(rest.data(), dout + R * w, rest.size() * 8, cudaMemcpyDeviceToHost, rc.s));
+        VQ_CUDA(cudaStreamSynchronize(rc.s));
+    }
     g.key.resize(ns);
     g.first.resize(ns);
     g.ival.assign(p.ni, std::vector<int64_t>(ns));
     g.fval.assign(p.nf, std::vector<double>(ns));
+    const long long* head = (const long long*)(hs + 32);
     for (long long j = 0; j < ns; j++) {
-        const long long* r = h.data() + j * w;
+        const long long* r = j < R ? head + j * w : rest.data() + (j - R) * w;
         g.key[j] = (uint64_t)r[0];
         g.first[j] = r[1];
         for (int s = 0; s < p.ni; s++) g.ival[s][j] = r[2 + s];
         for (int f = 0; f < p.nf; f++) std::memcpy(&g.fval[f][j], &r[2 + p.ni + f], 8);
     }
-    return true;
+    return 1;
 }
 
 // Decodes group keys, computes aggregate outputs, orders groups, and applies
@@ -1367,12 +1452,20 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
     if (p.path == AggPath::Regs) {
         g = run_regs(rc, P, nchunks);
     } else {
-        Compacted c = run_atomic(rc, P, nchunks, estimate, rows);
+        // ORDER BY an aggregate with a LIMIT and no HAVING: the top-k kernels
+        // follow the table run without waiting for its count
+        const bool defer = !p.partial_out && p.having_root < 0 && p.ndist == 0 && topk_applies(p, false);
+        Compacted c = run_atomic(rc, P, nchunks, estimate, rows, defer);
         if (p.partial_out) {
             g = fetch_groups(rc, c);  // a shard's partial: every group, no HAVING, no LIMIT
         } else {
             if (p.k_having.fn) c = having_device(rc, c);
-            if (!topk_groups(rc, c, g)) {
+            int st = topk_groups(rc, c, g);
+            if (st < 0) {  // the deferred run's hash table was too small: the sizing loop runs it again
+                c = run_atomic(rc, P, nchunks, estimate, rows);
+                st = topk_groups(rc, c, g);
+            }
+            if (st == 0) {
                 g = fetch_groups(rc, c);
                 g.having_done = c.having_done;
             }
@@ -1465,6 +1558,18 @@ cudaStream_t plan_stream(Plan& p) {
     return p.stream;
 }
 
+// Sets " name=value" in the plan's explain string (appended the first time).
+static void explain_tag(Plan& p, const std::string& name, const std::string& value) {
+    const std::string k = " " + name + "=";
+    const size_t at = p.explain.find(k);
+    if (at != std::string::npos) {
+        const size_t end = p.explain.find(' ', at + 1);
+        if (p.explain.compare(at + k.size(), (end == std::string::npos ? p.explain.size() : end) - at - k.size(), value) == 0) return;
+        p.explain.erase(at, end == std::string::npos ? std::string::npos : end - at);
+    }
+    p.explain += k + value;
+}
+
 // One radix partition pass over a side (Q: its columns, row ranges, filter
 // inputs): histogram, partition-major scan, starts, then — unless a
 // partition exceeds the shared-memory capacity and *maxpart is asked for —
@@ -1533,6 +1638,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     long long join_keys = 0;
     int64_t bytes = 0, rows_scanned = 0;
     bool use_radix = false;
+    bool spec = false;  // the probe follows a direct-mapped build without the host waiting
     int pbits = 0;
     if (p.is_join) {
         Table& bt = *p.bt;
@@ -1645,7 +1751,82 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         // keys unique in the last build (the primary-key side of a join): one
         // pass straight into the probe's 16-byte slots
         bool fast_unique = p.fast_build && p.join_unique_seen && !p.join_fast_failed;
+        // a build key column whose value range is at most a few times its rows
+        // (dense primary keys): a word per key value, indexed by key - imin,
+        // one CAS a build row and one load a probe row, no hashing or packing
+        const Column& bkc = bt.cols[p.build_key];
+        bool direct = false;
+        long long dmin = 0;
+        unsigned long long drange = 0;
+        if (p.dmap_on && !p.dmap_failed && bkc.has_range && bkc.imax >= bkc.imin) {
+            const __int128 r = (__int128)bkc.imax - (__int128)bkc.imin + 1;
+            if (r <= ((__int128)1 << 31) && r <= 4 * (__int128)std::max<int64_t>(bt.nrows, 1) + 65536) {
+                direct = true;
+                dmin = bkc.imin;
+                drange = (unsigned long long)r;
+            }
+        }
+        // the last build was direct-mapped over the same rows: this one is
+        // launched and the probe follows without the host waiting for it (the
+        // group table sized from the last build's key count); the probe
+        // raises a failed, empty or larger build in its error word
+        spec = direct && p.dmap_used && p.join_rows_seen == bs.rows && p.join_keys_seen > 0 && p.spec_on;
+        p.dmap_used = false;
         for (;;) {
+        if (direct) {
+            p.jt_scalar.ensure(64);
+            p.jt_gid.ensure(8);  // a non-null flag: group numbers are handed out
+            p.jt_gkey.ensure((size_t)std::max<long long>(bs.rows, 1) * 8);
+            p.jt_dmap.ensure((size_t)drange * 8);
+            B.jnkeys = p.jt_scalar.as<unsigned long long>();
+            B.error = (int*)(p.jt_scalar.as<char>() + 8);
+            B.jtotal = (unsigned long long*)(p.jt_scalar.as<char>() + 24);
+            ensure_events(p);
+            VQ_CUDA(cudaEventRecord(p.ev[4], rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_scalar.p, 0, 40, rc.s));
+            VQ_CUDA(cudaMemsetAsync(p.jt_dmap.p, 0, (size_t)drange * 8, rc.s));
+            VQParams F = B;
+            F.mode = 3;
+            F.dmap = p.jt_dmap.as<unsigned long long>();
+            F.dmin = dmin;
+            F.drange = drange;
+            F.jgid = p.join_gid ? p.jt_gid.as<int>() : nullptr;
+            F.jgkey = p.jt_gkey.as<unsigned long long>();
+            F.jgoff = p.gid_koff;
+            if (bs.nchunks > 0) {
+                jit_launch(p.k_build, grid_for(p.k_build, bs.nchunks, p.staged), &F, sizeof F, rc.s);
+                launch_check(rc.s, "p.k_build (direct-mapped)");
+            }
+            rc.launches += 1;
+            if (spec) {
+                VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+                p.dmap_used = true;
+                join_keys = p.join_keys_seen;
+                break;
+            }
+            int herr = 0;
+            unsigned long long nk = 0, ntot = 0;
+            VQ_CUDA(cudaMemcpyAsync(&herr, B.error, 4, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&nk, B.jnkeys, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaMemcpyAsync(&ntot, B.jtotal, 8, cudaMemcpyDeviceToHost, rc.s));
+            VQ_CUDA(cudaEventRecord(p.ev[5], rc.s));
+            VQ_CUDA(cudaStreamSynchronize(rc.s));
+            rc.kernel_ms += elapsed(p.ev[4], p.ev[5]);
+            if (herr & 8) fail(VEXQ_ETIMEDOUT, "a staged tile copy did not complete within the kernel's wait limit");
+            if (!(herr & (16 | 32)) && nk == ntot) {
+                p.dmap_used = true;
+                join_keys = (long long)nk;
+                p.gid_groups = join_keys;
+                p.join_keys_seen = join_keys;
+                p.join_rows_seen = bs.rows;
+                break;
+            }
+            // a repeated key (or a key outside the column's recorded range):
+            // the hash table from here on
+            p.dmap_failed = true;
+            direct = false;
+            continue;
+        }
         long long nslots = jcap + 1;
         p.jt_keys.ensure(nslots * 8);
         p.jt_count.ensure(nslots * 4);
@@ -1803,6 +1984,7 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         }
         break;
         }
+        explain_tag(p, "build", direct ? "direct" : "hash");
         bytes += scanned_bytes(p, bt, bs.rows, true);
         rows_scanned += bs.rows;
         // ---- probe phase parameters ----
@@ -1814,6 +1996,11 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         P.jslot = p.jt_meta.as<ulonglong2>();
         P.jgid = p.jt_gid.as<int>();
         P.jmask = B.jmask;
+        P.dmap = direct ? p.jt_dmap.as<unsigned long long>() : nullptr;
+        P.dmin = dmin;
+        P.drange = drange;
+        P.berr = spec ? (const int*)(p.jt_scalar.as<char>() + 8) : nullptr;
+        P.bnk = spec ? p.jt_scalar.as<unsigned long long>() : nullptr;
         if (join_keys == 0) {  // empty build: the join emits nothing (parallel_join.go:790-795)
             Groups g;
             g.ival.assign(p.ni, {});
@@ -1892,7 +2079,17 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         r->launches = rc.launches;
     } else {
         long long est = estimate_groups(p, ss.rows, join_keys);
-        r = finish_groups(rc, P, ss.nchunks, est, ss.rows);
+        try {
+            r = finish_groups(rc, P, ss.nchunks, est, ss.rows);
+        } catch (const SpecRetry& e) {
+            // the build the probe did not wait for failed (a repeated key: the
+            // hash table from here on), was empty or numbered more keys: run
+            // again with the host reading the build's outcome first
+            if (e.bits & 64) p.dmap_failed = true;
+            p.dmap_used = false;
+            return run_plan(p, rg_start, rg_end);
+        }
+        if (spec) r->kernel_ms += elapsed(p.ev[4], p.ev[5]);
     }
     r->rows_scanned = rows_scanned;
     r->bytes_scanned = bytes;

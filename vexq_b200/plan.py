@@ -244,6 +244,7 @@ class JoinPlan:
                  aggs: Sequence[Agg], order_col: int = -1, descending: bool = False,
                  limit: int = -1, radix_bits: int = -1, having: Optional[E] = None, visible: int = -1):
         self.group_by, self.aggs = list(group_by), list(aggs)
+        self.order_col, self.descending, self.limit = order_col, descending, limit
         self.having = having_arrays(having, visible)
         a = _Arena()
         bp, pp, rp = a.add(build_predicate), a.add(probe_predicate), a.add(residual)
