@@ -304,7 +304,7 @@ struct Batch {
         int m = 0;
         for (int i : ck[1].items) {
             const Item& it = items[i];
-            if (!it.hash) m = std::max(m, dense_cache_groups(*it.p, cache_kb) * (8 + 8 * it.ni + 36 * it.nf));
+            if (!it.hash) m = std::max(m, dense_cache_groups(*it.p, cache_kb) * cache_group_bytes(*it.p));
         }
         return m;
     }

@@ -1524,16 +1524,20 @@ struct CacheLayout {
 };
 // The cached group count is the launch-time value P.cache_n (vq_C in the
 // generated code), so plans that differ only in domain share a kernel.
+// Limb form (cache_limbs): the fixed-point region holds, per float sum, sixteen
+// 32-bit limb counters a group (eight positive, eight negative; limb j of
+// every group contiguous) instead of four 64-bit digit counters.
 CacheLayout cache_layout(const Plan& p) {
     CacheLayout L;
     L.C = p.smem_groups;
     L.first = "((long long*)vq_smem)";
     L.ints = "(((long long*)vq_smem) + vq_C)";
     L.fx = "(((long long*)vq_smem) + (long long)vq_C * " + std::to_string(1 + p.ni) + ")";
-    L.sp = "((unsigned*)(((long long*)vq_smem) + (long long)vq_C * " + std::to_string(1 + p.ni + 4 * p.nf) + "))";
+    const int fx_longs = (p.cache_limbs ? 8 : 4) * p.nf;
+    L.sp = "((unsigned*)(((long long*)vq_smem) + (long long)vq_C * " + std::to_string(1 + p.ni + fx_longs) + "))";
     return L;
 }
-int cache_bytes(const Plan& p) { return p.smem_groups * (8 + 8 * p.ni + 36 * p.nf); }
+
 
 // Opens "if (slot < C) { shared-memory update } else {" — the caller emits the
 // global update and closes the brace.
@@ -1554,7 +1558,9 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
             case S_CNT:
             case S_NN:
                 // a block's count stays below 2^32: a 32-bit add on the counter's low word
-                if (p.cache_cnt32) os << in << "if (ag" << S << ") atomicAdd((unsigned*)(" << ai << "), (unsigned)ag" << S << ");\n";
+                if (p.cache_limbs && s == 0)  // the row count, read back: every 32,768 rows the group's limbs are normalised
+                    os << in << "const unsigned vq_c0 = atomicAdd((unsigned*)(" << ai << "), (unsigned)ag" << S << ");\n";
+                else if (p.cache_cnt32) os << in << "if (ag" << S << ") atomicAdd((unsigned*)(" << ai << "), (unsigned)ag" << S << ");\n";
                 else os << in << "if (ag" << S << ") atomicAdd(" << aiu << ", (unsigned long long)ag" << S << ");\n";
                 break;
             case S_ISUM:
@@ -1566,11 +1572,23 @@ void emit_cache_update(std::ostringstream& os, const Plan& p, const std::string&
             case S_FMIN: os << in << "if (ah" << S << " && ag" << S << " < *" << aiu << ") atomicMin(" << aiu << ", ag" << S << ");\n"; break;
             case S_FMAX: os << in << "if (ah" << S << " && ag" << S << " > *" << aiu << ") atomicMax(" << aiu << ", ag" << S << ");\n"; break;
             case S_FSUM:
+                if (p.cache_limbs) {
+                    os << in << "if (ah" << S << ") { vq_limbs_add((unsigned*)" << L.fx << " + (long long)" << pos << " * 16 * " << C
+                       << " + (long long)slot, " << C << ", fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
+                       << ") atomicOr(" << L.sp << " + " << pos << " * " << C << " + slot, fsp" << S << "); }\n";
+                    break;
+                }
                 os << in << "if (ah" << S << ") { " << (p.cache_fx32 ? "vq_fx_add_digits_s32(" : "vq_fx_add_digits_s(") << L.fx << " + (long long)" << pos << " * 4 * " << C
                    << " + (long long)slot, " << C << ", fd" << S << "_0, fd" << S << "_1, fd" << S << "_2, fd" << S << "_3); if (fsp" << S
                    << ") atomicOr(" << L.sp << " + " << pos << " * " << C << " + slot, fsp" << S << "); }\n";
                 break;
         }
+    }
+    if (p.cache_limbs && p.nf > 0) {
+        os << in << "if (((vq_c0 + (unsigned)ag0) >> 15) != (vq_c0 >> 15)) {\n";
+        for (int f = 0; f < p.nf; f++)
+            os << in << "    vq_limbs_norm((unsigned*)" << L.fx << " + (long long)" << f << " * 16 * " << C << " + (long long)slot, " << C << ");\n";
+        os << in << "}\n";
     }
     os << ind << "} else {\n";
 }
@@ -1586,7 +1604,10 @@ void emit_cache_init(std::ostringstream& os, const Plan& p, bool declare_smem = 
         const Slot& sl = p.slots[s];
         if (sl.kind == S_FSUM) {
             std::string pos = std::to_string(p.slot_pos[s]);
-            os << "        for (int d = 0; d < 4; d++) " << L.fx << "[(" << pos << " * 4 + d) * " << C << " + i] = 0;\n";
+            if (p.cache_limbs)
+                os << "        for (int d = 0; d < 16; d++) ((unsigned*)" << L.fx << ")[(" << pos << " * 16 + d) * " << C << " + i] = 0u;\n";
+            else
+                os << "        for (int d = 0; d < 4; d++) " << L.fx << "[(" << pos << " * 4 + d) * " << C << " + i] = 0;\n";
             os << "        " << L.sp << "[" << pos << " * " << C << " + i] = 0u;\n";
             continue;
         }
@@ -1622,8 +1643,13 @@ void emit_cache_flush(std::ostringstream& os, const Plan& p) {
             case S_FMIN: os << "        atomicMin((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
             case S_FMAX: os << "        atomicMax((unsigned long long*)&" << g << ", (unsigned long long)" << v << ");\n"; break;
             case S_FSUM:
-                os << "        for (int d = 0; d < 4; d++) { const long long x = " << L.fx << "[(" << P_ << " * 4 + d) * " << C
-                   << " + i]; if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_ << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
+                if (p.cache_limbs)
+                    os << "        for (int d = 0; d < 4; d++) { const long long x = vq_limbs_digit((const unsigned*)" << L.fx << " + (long long)" << P_
+                       << " * 16 * " << C << " + i, " << C << ", d); if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_
+                       << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
+                else
+                    os << "        for (int d = 0; d < 4; d++) { const long long x = " << L.fx << "[(" << P_ << " * 4 + d) * " << C
+                       << " + i]; if (x) atomicAdd((unsigned long long*)&P.acc_fx[(" << P_ << " * stride + i) * 4 + d], (unsigned long long)x); }\n";
                 os << "        if (" << L.sp << "[" << P_ << " * " << C << " + i]) atomicOr(&P.special[" << P_ << " * stride + i], "
                    << L.sp << "[" << P_ << " * " << C << " + i]);\n";
                 break;
@@ -1647,6 +1673,10 @@ bool hot_on(const Plan& p) { return p.hot_n > 0 && p.path == AggPath::Dense && !
 // cached, else the global table.
 void emit_lead_update(std::ostringstream& os, const Plan& p, const std::string& in3, bool cache) {
     if (cache) emit_cache_update(os, p, in3);
+    // unguarded (fire-and-forget) MIN/MAX and first-row atomics: a read of the
+    // current value to skip them measured slower on the global table (4M rows,
+    // 65,536 Zipf groups mostly uncached: 118.9 against 74.8 us; 200K hash
+    // keys: 201.6 against 197.7 us)
     os << in3 << "atomicMin(&P.first[slot], ag_first);\n";
     for (size_t s = 0; s < p.slots.size(); s++) {
         std::string S = std::to_string(s);
@@ -2165,6 +2195,9 @@ struct ScanLoop {
 
 }  // namespace
 
+int cache_group_bytes(const Plan& p) { return 8 + 8 * p.ni + (p.cache_limbs ? 68 : 36) * p.nf; }
+int cache_bytes(const Plan& p) { return p.smem_groups * cache_group_bytes(p); }
+
 static std::string gen_kind_tables(const Plan& p, const std::string& prefix = "P_");
 
 // The four rows a lane holds in the current chunk: filter, project, aggregate.
@@ -2323,7 +2356,7 @@ std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::ve
 
 int dense_cache_groups(const Plan& p, int cache_kb) {
     if (p.path != AggPath::Dense || p.is_join || cache_kb <= 0) return 0;
-    int per = 8 + 8 * p.ni + 36 * p.nf;
+    int per = cache_group_bytes(p);
     return (int)std::min<int64_t>(p.domain, (int64_t)cache_kb * 1024 / per);
 }
 
@@ -2349,6 +2382,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     // 16-byte slots; a lane's fresh slots wait in registers for their group
     // numbers, claimed once per warp and chunk
     os << "        long long vq_fs[4]; int vq_fr[4]; unsigned long long vq_fk[4]; int vq_nf = 0;\n";
+    // mode 3: the lane's four table words, CAS'd together after the filter
+    os << "        unsigned long long vq_d3[4] = {~0ull, ~0ull, ~0ull, ~0ull}, vq_k3[4];\n";
     os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
     os << "            const long long r = r0 + k;\n";
     os << "            if (r < s0 || r >= s1) continue;\n";
@@ -2366,11 +2401,8 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            if (P.mode == 3) {\n";
     os << "                const unsigned long long di = jk - (unsigned long long)P.dmin;\n";
     os << "                if (di >= P.drange) { atomicOr(P.error, 32); continue; }  // outside the range: the general build runs\n";
-    os << "                const unsigned long long old = atomicCAS(P.dmap + di, 0ull, (unsigned long long)(unsigned)r | 0xFFFFFFFF00000000ull);\n";
-    os << "                if (old != 0ull) { atomicOr(P.error, 16); continue; }  // a repeated key: the general build runs\n";
-    os << "                vq_nrows++;\n";
-    os << "                if (P.jgid) { vq_fs[vq_nf] = (long long)di; vq_fr[vq_nf] = (int)r; vq_fk[vq_nf] = jk; vq_nf++; }\n";
-    os << "                else vq_nk++;\n";
+    os << "                vq_d3[k] = di;\n";
+    os << "                vq_k3[k] = jk;\n";
     os << "            } else if (P.mode == 2) {\n";
     os << "                ulonglong2* sl = const_cast<ulonglong2*>(P.jslot);\n";
     os << "                long long at = -1;\n";
@@ -2407,6 +2439,19 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            } else {\n";
     os << "                const unsigned long long js = vq_find(P.jkeys, P.jmask, P.jmask + 1, jk);\n";
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
+    os << "            }\n";
+    os << "        }\n";
+    // mode 3: four CAS in flight a lane, then their outcomes
+    os << "        if (P.mode == 3) {\n";
+    os << "            unsigned long long vq_o3[4];\n";
+    os << "#pragma unroll\n            for (int k = 0; k < 4; k++)\n";
+    os << "                vq_o3[k] = vq_d3[k] != ~0ull ? atomicCAS(P.dmap + vq_d3[k], 0ull, (unsigned long long)(unsigned)(r0 + k) | 0xFFFFFFFF00000000ull) : 0ull;\n";
+    os << "#pragma unroll\n            for (int k = 0; k < 4; k++) {\n";
+    os << "                if (vq_d3[k] == ~0ull) continue;\n";
+    os << "                if (vq_o3[k] != 0ull) { atomicOr(P.error, 16); continue; }  // a repeated key: the general build runs\n";
+    os << "                vq_nrows++;\n";
+    os << "                if (P.jgid) { vq_fs[vq_nf] = (long long)vq_d3[k]; vq_fr[vq_nf] = (int)(r0 + k); vq_fk[vq_nf] = vq_k3[k]; vq_nf++; }\n";
+    os << "                else vq_nk++;\n";
     os << "            }\n";
     os << "        }\n";
     // modes 2 and 3 with group numbers (GROUP BY the join key): one claim per warp
@@ -2789,6 +2834,11 @@ static const int kBlock = 256;
 static void choose_tunables(Plan& p) {
     int64_t acc = p.path == AggPath::Regs ? p.domain * (int64_t)(p.slots.size() + 1) : 0;
     p.block = acc > 24 ? 128 : 256;
+    // dense group tables with the shared-memory cache: two 512-thread blocks
+    // an SM (32 warps) hide the shared-atomic latency better than 256-thread
+    // blocks at the same cache size (4M Zipf(1.1) rows: 46.1-48.2 / 69.6-76.8
+    // us against 54.3-56.3 / 74.8 us at 1,000 / 65,536 groups)
+    if (p.path == AggPath::Dense && !p.is_join) p.block = 512;
     // measured: software prefetch costs registers the register-accumulator path
     // needs (6M-row Q1: 74.9 µs without, 87.0 µs with); neutral for Q6
     // joins (measured, 6M-row probe): prefetch helps the register path and
@@ -2806,6 +2856,12 @@ static void choose_tunables(Plan& p) {
     // than they save (67 / 82 us with one)
     p.cache_cnt32 = p.cache_fx32 = true;
     p.hot_n = 0;
+    // float sums in the cache as 16-bit limbs with plain adds (no returned
+    // value, no carry) instead of 32-bit word pairs whose carry comes back
+    // from the returned old value: more atomics a row, measured slower (4M
+    // Zipf rows, 1,000 / 65,536 groups: 54.2 / 79.1 against 48.2 / 76.8 us),
+    // so a tunable (limbs=1)
+    p.cache_limbs = false;
     // register path with many accumulators: three 128-thread blocks an SM
     // (~148 registers a thread), too few loads in flight to fill HBM; a
     // two-chunk cp.async pipeline a warp keeps the next chunk's columns in
@@ -2840,6 +2896,8 @@ static void choose_tunables(Plan& p) {
         const int sp = get("spec=");
         if (sp >= 0) p.spec_on = sp != 0;
         if (gs >= 0) p.grid_per_sm = gs;
+        const int lb = get("limbs=");
+        if (lb >= 0) p.cache_limbs = lb != 0;
         if (c32 >= 0) p.cache_cnt32 = c32 != 0;
         if (f32 >= 0) p.cache_fx32 = f32 != 0;
         if (ho >= 0 && p.path == AggPath::Dense && !p.is_join) p.hot_n = std::min(ho, VQ_MAXHOT);
@@ -2854,9 +2912,12 @@ static void choose_tunables(Plan& p) {
         if (st >= 0) p.staged = st != 0;
         if (sb > 0) p.stage_budget = sb * 1024;
     }
+    // limbs take one row's canonical image at a time: not with warp folds or
+    // the register hot groups, which add sums of several rows
+    if (p.warp_agg || p.hot_n > 0) p.cache_limbs = false;
     p.smem_groups = 0;
     if (p.path == AggPath::Dense && !p.is_join && cache_kb > 0) {
-        int per = 8 + 8 * p.ni + 36 * p.nf;
+        int per = cache_group_bytes(p);
         p.smem_groups = (int)std::min<int64_t>(p.domain, (int64_t)cache_kb * 1024 / per);
         p.staged = false;  // the cache owns the dynamic shared memory
     }

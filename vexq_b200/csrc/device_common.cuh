@@ -193,6 +193,49 @@ __device__ __forceinline__ void vq_fx_add_digits_s32(vq_i64* c, long long stride
     vq_add64_as32(c + 3 * stride, d3);
 }
 
+// The shared-memory group cache in limb form: a float sum's 128-bit fixed-point
+// image as eight 16-bit limbs of its magnitude, each added with a plain 32-bit
+// atomic (no returned value, no carry) into its own counter, positive and
+// negative values in separate sets of eight (L[j * C], L[(8 + j) * C]). A
+// counter takes at most 0xFFFF a row, so 32,768 rows of a group between two
+// normalisations (vq_limbs_norm) keep every counter below 2^31. d0..d3 are
+// the canonical 32-bit words of the two's-complement image (d3 signed).
+__device__ __forceinline__ void vq_limbs_add(unsigned* L, long long C, long long d0, long long d1, long long d2, long long d3) {
+    unsigned m0 = (unsigned)d0, m1 = (unsigned)d1, m2 = (unsigned)d2, m3 = (unsigned)d3;
+    if (d3 < 0) {  // magnitude of a negative image: ~x + 1 over 128 bits
+        m0 = ~m0; m1 = ~m1; m2 = ~m2; m3 = ~m3;
+        m0 += 1u;
+        const unsigned c0 = m0 == 0u;
+        m1 += c0;
+        const unsigned c1 = c0 & (m1 == 0u);
+        m2 += c1;
+        m3 += c1 & (m2 == 0u);
+        L += 8 * C;
+    }
+    const unsigned m[4] = {m0, m1, m2, m3};
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const unsigned limb = (m[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
+        if (limb) atomicAdd(L + j * C, limb);
+    }
+}
+// Moves every counter's bits above 16 into the next limb up (both sets; the
+// top limb keeps its high bits): atomic, so adds landing meanwhile are kept.
+__device__ __forceinline__ void vq_limbs_norm(unsigned* L, long long C) {
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int j = 0; j < 7; j++) {
+            const unsigned old = atomicAnd(L + (8 * s + j) * C, 0xFFFFu);
+            if (old >> 16) atomicAdd(L + (8 * s + j + 1) * C, old >> 16);
+        }
+}
+// The block's limbs as the global table's carry-save digit d (weight 2^(32d)).
+__device__ __forceinline__ long long vq_limbs_digit(const unsigned* L, long long C, int d) {
+    return (long long)L[(2 * d) * C] + ((long long)L[(2 * d + 1) * C] << 16) - (long long)L[(8 + 2 * d) * C] -
+           ((long long)L[(8 + 2 * d + 1) * C] << 16);
+}
+
 // ---- warp reductions over a peer mask (redux.sync; every lane named in the
 // mask executes the same call with the same mask) ----
 __device__ __forceinline__ unsigned vq_redux_add(unsigned mask, unsigned v) {

@@ -208,6 +208,7 @@ struct Plan {
     // counter's low word; fixed-point digits as 32-bit atomics with the carry
     // (from the returned old value) added to the high word
     bool cache_cnt32 = false, cache_fx32 = false;
+    bool cache_limbs = false;      // cached float sums as 16-bit limbs (plain adds, normalised every 32,768 rows)
     std::vector<unsigned long long> hot_keys;
     mutable std::mutex hot_mu;
     long long hash_rows_seen = 0;          //   and the rows that run scanned
@@ -279,6 +280,8 @@ std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::ve
                              int& nbodies);
 // Groups a dense plan caches in shared memory within cache_kb KB (0: not dense).
 int dense_cache_groups(const Plan& p, int cache_kb);
+int cache_group_bytes(const Plan& p);  // shared-memory cache bytes a group
+int cache_bytes(const Plan& p);
 
 // ---- runtime pieces shared by the plain and batched paths (run.cu) ----
 // Host-side group rows collected from either path.

@@ -92,7 +92,7 @@ void apply(Plan& p, int choice) {
         return;
     }
     p.smem_groups = dense_cache_groups(p, choice);
-    const int smem = p.smem_groups * (8 + 8 * p.ni + 36 * p.nf);
+    const int smem = cache_bytes(p);
     p.smem = smem;
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, smem);
 }
