@@ -2441,21 +2441,40 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
-    // mode 3: four CAS in flight a lane, then their outcomes
+    // mode 3: four CAS in flight a lane, then their outcomes; with group
+    // numbers, one claim per warp and chunk (registers only: the lane's
+    // fresh rows are its four flags, in row order)
     os << "        if (P.mode == 3) {\n";
     os << "            unsigned long long vq_o3[4];\n";
     os << "#pragma unroll\n            for (int k = 0; k < 4; k++)\n";
     os << "                vq_o3[k] = vq_d3[k] != ~0ull ? atomicCAS(P.dmap + vq_d3[k], 0ull, (unsigned long long)(unsigned)(r0 + k) | 0xFFFFFFFF00000000ull) : 0ull;\n";
+    os << "            bool vq_ok3[4];\n";
+    os << "            int vq_n3 = 0;\n";
     os << "#pragma unroll\n            for (int k = 0; k < 4; k++) {\n";
-    os << "                if (vq_d3[k] == ~0ull) continue;\n";
-    os << "                if (vq_o3[k] != 0ull) { atomicOr(P.error, 16); continue; }  // a repeated key: the general build runs\n";
-    os << "                vq_nrows++;\n";
-    os << "                if (P.jgid) { vq_fs[vq_nf] = (long long)vq_d3[k]; vq_fr[vq_nf] = (int)(r0 + k); vq_fk[vq_nf] = vq_k3[k]; vq_nf++; }\n";
-    os << "                else vq_nk++;\n";
+    os << "                vq_ok3[k] = vq_d3[k] != ~0ull && vq_o3[k] == 0ull;\n";
+    os << "                if (vq_d3[k] != ~0ull && vq_o3[k] != 0ull) atomicOr(P.error, 16);  // a repeated key: the general build runs\n";
+    os << "                vq_n3 += vq_ok3[k] ? 1 : 0;\n";
+    os << "            }\n";
+    os << "            vq_nrows += (unsigned long long)vq_n3;\n";
+    os << "            if (P.jgid) {\n";
+    os << "                int inc = vq_n3;\n";
+    os << "                for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
+    os << "                const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
+    os << "                unsigned long long g = 0ull;\n";
+    os << "                if (lane == 31 && tot) g = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
+    os << "                g = __shfl_sync(0xffffffffu, g, 31) + (unsigned long long)(inc - vq_n3);\n";
+    os << "#pragma unroll\n                for (int k = 0; k < 4; k++) {\n";
+    os << "                    if (!vq_ok3[k]) continue;\n";
+    os << "                    P.dmap[vq_d3[k]] = (unsigned long long)(unsigned)(r0 + k) | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
+    os << "                    P.jgkey[g] = (unsigned long long)((long long)vq_k3[k] - P.jgoff);\n";
+    os << "                    g++;\n";
+    os << "                }\n";
+    os << "            } else {\n";
+    os << "                vq_nk += (unsigned)vq_n3;\n";
     os << "            }\n";
     os << "        }\n";
-    // modes 2 and 3 with group numbers (GROUP BY the join key): one claim per warp
-    os << "        if ((P.mode == 2 || P.mode == 3) && P.jgid) {\n";
+    // mode 2 with group numbers (GROUP BY the join key): one claim per warp
+    os << "        if (P.mode == 2 && P.jgid) {\n";
     os << "            int inc = vq_nf;\n";
     os << "            for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
     os << "            const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
@@ -2466,7 +2485,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "            for (int j = 0; j < vq_nf; j++) {\n";
     os << "                const unsigned long long g = base + (unsigned long long)j;\n";
     os << "                const unsigned long long w = (unsigned long long)(unsigned)vq_fr[j] | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
-    os << "                if (P.mode == 3) P.dmap[vq_fs[j]] = w; else sl[vq_fs[j]].y = w;\n";
+    os << "                sl[vq_fs[j]].y = w;\n";
     os << "                P.jgkey[g] = (unsigned long long)((long long)vq_fk[j] - P.jgoff);\n";
     os << "            }\n";
     os << "        }\n";
@@ -3107,6 +3126,7 @@ Plan::~Plan() {
         std::lock_guard<std::mutex> lk(g_zone_mu);
         g_zone_strings.erase(this);
     }
+    if (rg_exec) cudaGraphExecDestroy(rg_exec);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);

@@ -99,6 +99,19 @@ struct ScanMemo {
     int64_t bytes = 0;  // algorithmic bytes the scan of those segments reads
 };
 
+// What a captured register-path run depends on: the parameter block, the
+// scan kernel and its shape, the merge's outputs and the stream.
+struct RegsGraphKey {
+    VQParams P;
+    void* fn;
+    cudaStream_t s;
+    void* out_f;
+    void* out_i;
+    void* err_out;
+    const void* d_kinds;
+    int grid, block, smem, mode;
+};
+
 struct Plan {
     bool is_join = false;
     Table* t = nullptr;        // aggregate table or probe table
@@ -231,6 +244,11 @@ struct Plan {
     bool spec_on = true;                   // a repeated direct-mapped build goes without a host wait (VEXQ_TUNE spec=0: off)
     DevBuf jt_dmap;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [4], [5]: join build phase
+    // the register path's launches captured as a graph, replayed while
+    // rg_key matches (graph_off: capture was refused, direct launches)
+    cudaGraphExec_t rg_exec = nullptr;
+    RegsGraphKey rg_key{};
+    bool graph_off = false;
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
@@ -310,6 +328,7 @@ std::mutex& plan_mutex(Plan* p);
 // VEXQ_SYNC_CHECK=1: synchronise after every launch and name the kernel on
 // an error (diagnostics; off by default).
 void launch_check(cudaStream_t s, const char* what);
+bool launch_checks_on();  // VEXQ_SYNC_CHECK: a synchronize after every launch
 std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge);
 
 // Batched execution of many plans (batch.cu).

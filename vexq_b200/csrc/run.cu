@@ -741,27 +741,78 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         P.mdone = p.mdone.as<unsigned>();
     }
     bind_distinct(p, P, nchunks * 128, rc.s);
-    VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
-    jit_launch(K, grid, &P, sizeof P, rc.s);
-    launch_check(rc.s, "p.k_main");
-    // no event between the scan and its merge: an event record there stops the
-    // merge's launch from overlapping the scan's drain (measured 5-6 us a run)
-    if (!fused && !last) {
-        const int tot = G * nf + G * (ni + 1);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((tot + 7) / 8);
-        cfg.blockDim = dim3(256);
-        cfg.stream = rc.s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        VQ_CUDA(cudaLaunchKernelEx(&cfg, k_merge_regs_dep, (const double*)P.part_f, (const long long*)P.part_i, grid, G, nf,
-                                   ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
+    // the run's launches: start event, scan, merge, end event (events recorded
+    // as external nodes when captured, so a replayed graph still times them)
+    auto launch_all = [&](bool checks) {
+        VQ_CUDA(cudaEventRecordWithFlags(p.ev[0], rc.s, cudaEventRecordExternal));
+        jit_launch(K, grid, &P, sizeof P, rc.s);
+        if (checks) launch_check(rc.s, "p.k_main");
+        // no event between the scan and its merge: an event record there stops the
+        // merge's launch from overlapping the scan's drain (measured 5-6 us a run)
+        if (!fused && !last) {
+            const int tot = G * nf + G * (ni + 1);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((tot + 7) / 8);
+            cfg.blockDim = dim3(256);
+            cfg.stream = rc.s;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            VQ_CUDA(cudaLaunchKernelEx(&cfg, k_merge_regs_dep, (const double*)P.part_f, (const long long*)P.part_i, grid, G, nf,
+                                       ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
+            if (checks) launch_check(rc.s, "k_merge_regs_dep");
+        }
+        VQ_CUDA(cudaEventRecordWithFlags(p.ev[2], rc.s, cudaEventRecordExternal));
+    };
+    // replayed as one CUDA graph while the parameter block and launch shape
+    // are those it was captured with: one host call a run instead of four
+    RegsGraphKey key;
+    std::memset(&key, 0, sizeof key);
+    key.P = P;
+    key.fn = K.fn;
+    key.s = rc.s;
+    key.out_f = out_f;
+    key.out_i = out_i;
+    key.err_out = err_out;
+    key.d_kinds = d_kinds;
+    key.grid = grid;
+    key.block = K.block;
+    key.smem = K.smem;
+    key.mode = fused ? 1 : last ? 2 : 0;
+    if (p.graph_off || launch_checks_on()) {
+        launch_all(true);
+    } else if (p.rg_exec && std::memcmp(&key, &p.rg_key, sizeof key) == 0) {
+        VQ_CUDA(cudaGraphLaunch(p.rg_exec, rc.s));
+    } else {
+        if (p.rg_exec) {
+            cudaGraphExecDestroy(p.rg_exec);
+            p.rg_exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        bool ok = cudaStreamBeginCapture(rc.s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            try {
+                launch_all(false);
+            } catch (const Status&) {
+                ok = false;
+            }
+            const cudaError_t e = cudaStreamEndCapture(rc.s, &graph);
+            ok = ok && e == cudaSuccess && graph;
+        }
+        if (ok) ok = cudaGraphInstantiate(&p.rg_exec, graph, 0) == cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        if (ok) {
+            std::memcpy(&p.rg_key, &key, sizeof key);  // padding included: compared bytewise
+            VQ_CUDA(cudaGraphLaunch(p.rg_exec, rc.s));
+        } else {  // capture refused: direct launches from here on
+            (void)cudaGetLastError();
+            p.rg_exec = nullptr;
+            p.graph_off = true;
+            launch_all(true);
+        }
     }
-    if (!fused && !last) launch_check(rc.s, "k_merge_regs_dep");
-    VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
     if (!mapped) VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
     VQ_CUDA(cudaStreamSynchronize(rc.s));
     p.regs_err_clean = true;
@@ -1541,12 +1592,16 @@ std::mutex& plan_mutex(Plan* p) {
     return *u;
 }
 
-void launch_check(cudaStream_t s, const char* what) {
+bool launch_checks_on() {
     static const bool on = [] {
         const char* e = std::getenv("VEXQ_SYNC_CHECK");
         return e && *e && *e != '0';
     }();
-    if (!on) return;
+    return on;
+}
+
+void launch_check(cudaStream_t s, const char* what) {
+    if (!launch_checks_on()) return;
     cudaError_t e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) fail(VEXQ_EDEVICE, std::string("after ") + what + ": " + cudaGetErrorString(e));
