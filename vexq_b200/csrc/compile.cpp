@@ -2291,20 +2291,105 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
     return os.str();
 }
 
+static void emit_direct_build_tail(std::ostringstream& os);
+static void emit_probe_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool strided);
+
+// Batch body of a join's direct-mapped build over build chunks [cbeg, cend)
+// (P: the build side's parameter block, mode 3): the build kernel's rows and
+// tail, with the row and key counts added once per warp.
+static std::string gen_build_body(Plan& p, const std::string& name, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.bpred, cols);
+    collect_cols(p, p.bkey_node, cols);
+    os << "__device__ __noinline__ void " << name
+       << "(const VQParams& P, const long long cbeg, const long long cend, const long long pslot, unsigned char* vq_smem) {\n";
+    os << "    const int lane = threadIdx.x & 31;\n";
+    os << "    unsigned long long vq_nrows = 0ull;\n";
+    os << "    unsigned vq_nk = 0u;\n";
+    os << "    for (long long c = cbeg + (threadIdx.x >> 5); c < cend; c += " << block / 32 << ") {\n";
+    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    emit_loads(os, p, p.bt, cols, "cv", "cm", "r0", "        ", true);
+    os << "        unsigned long long vq_d3[4] = {~0ull, ~0ull, ~0ull, ~0ull}, vq_k3[4];\n";
+    os << "#pragma unroll\n        for (int k = 0; k < 4; k++) {\n";
+    os << "            const long long r = r0 + k;\n";
+    os << "            if (r < s0 || r >= s1) continue;\n";
+    Gen g(p, os);
+    if (p.bpred >= 0) {
+        g.emit(p.bpred);
+        os << "            if (!(x" << p.bpred << " && ok" << p.bpred << ")) continue;\n";
+    }
+    g.emit(p.bkey_node);
+    const std::string K = std::to_string(p.bkey_node);
+    os << "            if (!ok" << K << ") continue;  // NULL keys never join (exec/join.go:227-230)\n";
+    os << "            const unsigned long long jk = (unsigned long long)(long long)x" << K << ";\n";
+    os << "            const unsigned long long di = jk - (unsigned long long)P.dmin;\n";
+    os << "            if (di >= P.drange) { atomicOr(P.error, 32); continue; }\n";
+    os << "            vq_d3[k] = di;\n";
+    os << "            vq_k3[k] = jk;\n";
+    os << "        }\n";
+    emit_direct_build_tail(os);
+    os << "    }\n";
+    os << "    for (int o = 16; o > 0; o >>= 1) {\n";
+    os << "        vq_nrows += __shfl_xor_sync(0xffffffffu, vq_nrows, o);\n";
+    os << "        vq_nk += __shfl_xor_sync(0xffffffffu, vq_nk, o);\n";
+    os << "    }\n";
+    os << "    if (lane == 0 && vq_nrows) atomicAdd(P.jtotal, vq_nrows);\n";
+    os << "    if (lane == 0 && vq_nk) atomicAdd(P.jnkeys, (unsigned long long)vq_nk);\n";
+    os << "}\n";
+    return os.str();
+}
+
+// Batch body of a join's probe over probe chunks [cbeg, cend): the probe
+// kernel's rows (direct-mapped table), folding into the plan's group table
+// or, on the register path, into the unit's partial row at pslot.
+static std::string gen_probe_body(Plan& p, const std::string& name, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    collect_cols(p, p.probe_key, cols);
+    collect_cols(p, p.resid, cols);
+    for (int k : p.key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    if (p.path == AggPath::Regs) os << gen_kind_tables(p, name + "_");
+    os << "__device__ __noinline__ void " << name
+       << "(const VQParams& P, const long long cbeg, const long long cend, const long long pslot, unsigned char* vq_smem) {\n";
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    os << "    const int lane = threadIdx.x & 31;\n";
+    os << "    for (long long c = cbeg + (threadIdx.x >> 5); c < cend; c += " << block / 32 << ") {\n";
+    os << "        long long s0 = 0, s1 = 0, r0 = 0;\n        " << seg_lookup("c", "s0", "s1", "r0");
+    emit_loads(os, p, p.t, cols, "cv", "cm", "r0", "        ", true);
+    emit_probe_rows(os, p, p.key_nodes, false);
+    os << "    }\n";
+    if (p.path == AggPath::Regs) {
+        FlushCtx fc;
+        fc.part_index = "pslot";
+        fc.kinds = name + "_";
+        fc.dyn_smem = true;
+        emit_regs_flush(os, p, block, fc);
+    }
+    os << "}\n";
+    return os.str();
+}
+
 std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::vector<int>& body_of, int& smem,
-                             int& nbodies) {
+                             int& nbodies, bool build_role) {
     std::vector<std::string> bodies;
     std::map<std::string, int> index;
     body_of.clear();
     smem = 0;
     const std::string ph = "VQ_BODY_PLACEHOLDER";
     for (Plan* p : plans) {
-        if (p->is_join) fail(VEXQ_ENOTSUP, "batched launches take aggregate plans");
+        if (build_role && !p->is_join) fail(VEXQ_EINVAL, "a batched build body needs a join plan");
         std::string text;
         {
+            // bodies cached per block size and role (aggregate or probe; build)
             std::lock_guard<std::mutex> lk(p->body_mu);
-            auto it = p->batch_body.find(block);
-            if (it == p->batch_body.end()) it = p->batch_body.emplace(block, gen_agg_body(*p, ph, block)).first;
+            const int key = block + (build_role ? (1 << 20) : 0);
+            auto it = p->batch_body.find(key);
+            if (it == p->batch_body.end())
+                it = p->batch_body.emplace(key, build_role ? gen_build_body(*p, ph, block)
+                                                : p->is_join ? gen_probe_body(*p, ph, block) : gen_agg_body(*p, ph, block)).first;
             text = it->second;
         }
         auto it = index.find(text);
@@ -2358,6 +2443,43 @@ int dense_cache_groups(const Plan& p, int cache_kb) {
     if (p.path != AggPath::Dense || p.is_join || cache_kb <= 0) return 0;
     int per = cache_group_bytes(p);
     return (int)std::min<int64_t>(p.domain, (int64_t)cache_kb * 1024 / per);
+}
+
+// The direct-mapped build's chunk tail (vq_d3/vq_k3 hold the lane's four
+// keys' table words and keys, ~0 where a row does not insert): four CAS in
+// flight a lane, then their outcomes; with group numbers, one claim per warp
+// and chunk (registers only: the lane's fresh rows are its four flags, in
+// row order). Shared by the build kernel (mode 3) and the batched build body.
+static void emit_direct_build_tail(std::ostringstream& os) {
+    os << "        if (P.mode == 3) {\n";
+    os << "            unsigned long long vq_o3[4];\n";
+    os << "#pragma unroll\n            for (int k = 0; k < 4; k++)\n";
+    os << "                vq_o3[k] = vq_d3[k] != ~0ull ? atomicCAS(P.dmap + vq_d3[k], 0ull, (unsigned long long)(unsigned)(r0 + k) | 0xFFFFFFFF00000000ull) : 0ull;\n";
+    os << "            bool vq_ok3[4];\n";
+    os << "            int vq_n3 = 0;\n";
+    os << "#pragma unroll\n            for (int k = 0; k < 4; k++) {\n";
+    os << "                vq_ok3[k] = vq_d3[k] != ~0ull && vq_o3[k] == 0ull;\n";
+    os << "                if (vq_d3[k] != ~0ull && vq_o3[k] != 0ull) atomicOr(P.error, 16);  // a repeated key: the general build runs\n";
+    os << "                vq_n3 += vq_ok3[k] ? 1 : 0;\n";
+    os << "            }\n";
+    os << "            vq_nrows += (unsigned long long)vq_n3;\n";
+    os << "            if (P.jgid) {\n";
+    os << "                int inc = vq_n3;\n";
+    os << "                for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
+    os << "                const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
+    os << "                unsigned long long g = 0ull;\n";
+    os << "                if (lane == 31 && tot) g = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
+    os << "                g = __shfl_sync(0xffffffffu, g, 31) + (unsigned long long)(inc - vq_n3);\n";
+    os << "#pragma unroll\n                for (int k = 0; k < 4; k++) {\n";
+    os << "                    if (!vq_ok3[k]) continue;\n";
+    os << "                    P.dmap[vq_d3[k]] = (unsigned long long)(unsigned)(r0 + k) | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
+    os << "                    P.jgkey[g] = (unsigned long long)((long long)vq_k3[k] - P.jgoff);\n";
+    os << "                    g++;\n";
+    os << "                }\n";
+    os << "            } else {\n";
+    os << "                vq_nk += (unsigned)vq_n3;\n";
+    os << "            }\n";
+    os << "        }\n";
 }
 
 // Join build kernel: filtered build rows with non-NULL keys are inserted into
@@ -2441,38 +2563,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
-    // mode 3: four CAS in flight a lane, then their outcomes; with group
-    // numbers, one claim per warp and chunk (registers only: the lane's
-    // fresh rows are its four flags, in row order)
-    os << "        if (P.mode == 3) {\n";
-    os << "            unsigned long long vq_o3[4];\n";
-    os << "#pragma unroll\n            for (int k = 0; k < 4; k++)\n";
-    os << "                vq_o3[k] = vq_d3[k] != ~0ull ? atomicCAS(P.dmap + vq_d3[k], 0ull, (unsigned long long)(unsigned)(r0 + k) | 0xFFFFFFFF00000000ull) : 0ull;\n";
-    os << "            bool vq_ok3[4];\n";
-    os << "            int vq_n3 = 0;\n";
-    os << "#pragma unroll\n            for (int k = 0; k < 4; k++) {\n";
-    os << "                vq_ok3[k] = vq_d3[k] != ~0ull && vq_o3[k] == 0ull;\n";
-    os << "                if (vq_d3[k] != ~0ull && vq_o3[k] != 0ull) atomicOr(P.error, 16);  // a repeated key: the general build runs\n";
-    os << "                vq_n3 += vq_ok3[k] ? 1 : 0;\n";
-    os << "            }\n";
-    os << "            vq_nrows += (unsigned long long)vq_n3;\n";
-    os << "            if (P.jgid) {\n";
-    os << "                int inc = vq_n3;\n";
-    os << "                for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
-    os << "                const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
-    os << "                unsigned long long g = 0ull;\n";
-    os << "                if (lane == 31 && tot) g = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
-    os << "                g = __shfl_sync(0xffffffffu, g, 31) + (unsigned long long)(inc - vq_n3);\n";
-    os << "#pragma unroll\n                for (int k = 0; k < 4; k++) {\n";
-    os << "                    if (!vq_ok3[k]) continue;\n";
-    os << "                    P.dmap[vq_d3[k]] = (unsigned long long)(unsigned)(r0 + k) | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
-    os << "                    P.jgkey[g] = (unsigned long long)((long long)vq_k3[k] - P.jgoff);\n";
-    os << "                    g++;\n";
-    os << "                }\n";
-    os << "            } else {\n";
-    os << "                vq_nk += (unsigned)vq_n3;\n";
-    os << "            }\n";
-    os << "        }\n";
+    emit_direct_build_tail(os);
     // mode 2 with group numbers (GROUP BY the join key): one claim per warp
     os << "        if (P.mode == 2 && P.jgid) {\n";
     os << "            int inc = vq_nf;\n";
@@ -2501,34 +2592,13 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     return os.str();
 }
 
-// Join probe kernel: probe rows pass the probe filter, look their key up, and
-// every (build row, probe row) match runs the residual filter and is folded
-// into the aggregate, in (probe row, chain position) order keys.
-static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
-    std::ostringstream os;
-    std::set<int> cols;
-    collect_cols(p, p.pred, cols);
-    collect_cols(p, p.probe_key, cols);
-    collect_cols(p, p.resid, cols);
-    for (int k : key_nodes) collect_cols(p, k, cols);
-    for (auto& s : p.slots) collect_cols(p, s.input, cols);
-    // the cp.async ring (register path only, where registers limit occupancy)
-    ScanLoop loop(p, p.t, cols, block, "probe", p.path == AggPath::Regs);
-    p.tile = loop.tile_rows();
-    p.smem = loop.smem();
-    loop.prologue(os);
-    os << kernel_head("vq_agg", block);
-    // a build the host did not wait for: its failure or emptiness is raised
-    // in this kernel's error word, which comes back with the results
-    os << "    if (P.berr && blockIdx.x == 0 && threadIdx.x == 0) {\n";
-    os << "        const int be = *P.berr;\n";
-    os << "        if (be & 8) atomicOr(P.error, 8);\n";
-    os << "        if (be & ~8) atomicOr(P.error, 64);\n";
-    os << "        else if (*P.bnk == 0ull) atomicOr(P.error, 128);\n";
-    os << "    }\n";
-    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
-    loop.open(os);
-    const std::string rk = std::string("r0 + ") + (loop.strided() ? "(k << 5)" : "k");
+// One chunk of the join probe (a lane's four rows, loaded): a first pass runs
+// the filter and the key and issues the four table loads, a second resolves
+// them, runs the residual and folds every match into the aggregate in
+// (probe row, chain position) order keys. Shared by the probe kernel and the
+// batched probe body.
+static void emit_probe_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool strided) {
+    const std::string rk = std::string("r0 + ") + (strided ? "(k << 5)" : "k");
     std::string K = std::to_string(p.probe_key);
     // first pass over the lane's four rows: the filter, the key and the load
     // of the key's home slot, so four table loads are in flight at once
@@ -2539,7 +2609,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     os << "            if (r < s0 || r >= s1) continue;\n";
     {
         Gen g0(p, os);
-        if (loop.strided()) g0.kidx = "(k << 5)";
+        if (strided) g0.kidx = "(k << 5)";
         if (p.pred >= 0) {
             g0.emit(p.pred);
             os << "            if (!(x" << p.pred << " && ok" << p.pred << ")) continue;\n";
@@ -2562,7 +2632,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     os << "            const long long r = " << rk << ";\n";
     os << "            if (!vq_on[k]) continue;\n";
     Gen g(p, os);
-    if (loop.strided()) g.kidx = "(k << 5)";
+    if (strided) g.kidx = "(k << 5)";
     g.emit(p.probe_key);
     os << "            unsigned long long jc, jat = 0ull;\n";
     os << "            if (P.dmap) { jc = vq_s[k].y; if (jc == 0ull) continue; }\n";
@@ -2595,6 +2665,36 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     if (p.path == AggPath::Regs) emit_regs_update(os, p, "                ", order);
     else emit_atomic_update(os, p, "                ", order, p.join_gid);
     os << "            }\n        }\n";
+}
+
+// Join probe kernel: probe rows pass the probe filter, look their key up, and
+// every (build row, probe row) match runs the residual filter and is folded
+// into the aggregate, in (probe row, chain position) order keys.
+static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, int block) {
+    std::ostringstream os;
+    std::set<int> cols;
+    collect_cols(p, p.pred, cols);
+    collect_cols(p, p.probe_key, cols);
+    collect_cols(p, p.resid, cols);
+    for (int k : key_nodes) collect_cols(p, k, cols);
+    for (auto& s : p.slots) collect_cols(p, s.input, cols);
+    // the cp.async ring (register path only, where registers limit occupancy)
+    ScanLoop loop(p, p.t, cols, block, "probe", p.path == AggPath::Regs);
+    p.tile = loop.tile_rows();
+    p.smem = loop.smem();
+    loop.prologue(os);
+    os << kernel_head("vq_agg", block);
+    // a build the host did not wait for: its failure or emptiness is raised
+    // in this kernel's error word, which comes back with the results
+    os << "    if (P.berr && blockIdx.x == 0 && threadIdx.x == 0) {\n";
+    os << "        const int be = *P.berr;\n";
+    os << "        if (be & 8) atomicOr(P.error, 8);\n";
+    os << "        if (be & ~8) atomicOr(P.error, 64);\n";
+    os << "        else if (*P.bnk == 0ull) atomicOr(P.error, 128);\n";
+    os << "    }\n";
+    if (p.path == AggPath::Regs) emit_regs_decl(os, p);
+    loop.open(os);
+    emit_probe_rows(os, p, key_nodes, loop.strided());
     loop.close(os);
     if (p.path == AggPath::Regs) emit_regs_flush(os, p, block);
     os << "}\n";
@@ -2944,6 +3044,7 @@ static void choose_tunables(Plan& p) {
 
 static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join, int build_key_node) {
     p.key_nodes = key_nodes;
+    p.bkey_node = build_key_node;
     p.range_epoch = p.t ? p.t->range_epoch : 0;
     p.brange_epoch = p.bt ? p.bt->range_epoch : 0;
     analyze(p);

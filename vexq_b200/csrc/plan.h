@@ -121,6 +121,7 @@ struct Plan {
     int bpred = -1;            // join build predicate
     int resid = -1;            // join residual
     int build_key = -1, probe_key = -1;
+    int bkey_node = -1;        // join: the build key's IR node (scoped to the build table)
     // SQL-level predicate trees kept for zone maps
     std::vector<vexq_expr> zn_nodes;
     std::vector<int32_t> zn_children;
@@ -249,6 +250,7 @@ struct Plan {
     cudaGraphExec_t rg_exec = nullptr;
     RegsGraphKey rg_key{};
     bool graph_off = false;
+    long long topk_seen = 0;       // top-k candidates the last run gathered (sizes the next copy back)
     std::atomic<bool> cancel{false};
     cudaStream_t stream = nullptr;       // the plan's own stream (created lazily)
     cudaStream_t ext_stream = nullptr;   // caller-owned stream, when set
@@ -295,7 +297,7 @@ void check_ranges(const Plan& p);
 // distinct plan shape (body_of[i] for plans[i]) and the vq_batch dispatcher;
 // smem = dynamic shared memory the bodies need beyond the dense caches.
 std::string gen_batch_source(const std::vector<Plan*>& plans, int block, std::vector<int>& body_of, int& smem,
-                             int& nbodies);
+                             int& nbodies, bool build_role = false);
 // Groups a dense plan caches in shared memory within cache_kb KB (0: not dense).
 int dense_cache_groups(const Plan& p, int cache_kb);
 int cache_group_bytes(const Plan& p);  // shared-memory cache bytes a group

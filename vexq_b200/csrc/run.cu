@@ -403,7 +403,7 @@ __global__ void k_sample(const unsigned long long* rank, const unsigned long lon
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < S) out[j] = n > 0 ? rank[(long long)j * n / S] : 0ull;
 }
-// One block finds the q-th largest of the S samples (S <= 4096, q < S) by radix
+// One block finds the q-th largest of the S samples (S <= 16384, q < S) by radix
 // select, most significant byte first: each round counts, in shared memory,
 // the next byte of the samples that match the bytes chosen so far, and one
 // warp walks the 256 counts from the top to the byte holding the q-th largest.
@@ -418,14 +418,23 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
         return;
     }
     // expected (q+1)·n/S groups at or above the q-th largest sample: about
-    // 4·LIMIT + 64 (n above 4·LIMIT + 4096 keeps q below S)
-    const int q = (int)ceil((4.0 * limit + 64.0) * S / (double)n) - 1;
+    // 4·LIMIT + 64 (n above 4·LIMIT + 4096 keeps q below S), and q at least 7:
+    // the count above the q-th largest sample spreads like a Gamma(q+1)
+    // variable, so with q = 0 about one run in 20 kept fewer than LIMIT groups
+    // and fetched every group instead; from q = 7 that is below 1e-12
+    const int q = max((int)ceil((4.0 * limit + 64.0) * S / (double)n) - 1, min(7, S - 1));
     __shared__ unsigned hist[256];
     __shared__ unsigned long long prefix;
     __shared__ unsigned need;
-    unsigned long long v[4];
-    int nv = 0;
-    for (int i = threadIdx.x; i < S && nv < 4; i += blockDim.x) v[nv++] = samp[i];
+    // 16 samples a thread in registers (blockDim × 16 ≥ S), valid bits in a mask
+    unsigned long long v[16];
+    unsigned valid = 0u;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int i = (int)threadIdx.x + k * (int)blockDim.x;
+        v[k] = i < S ? samp[i] : 0ull;
+        if (i < S) valid |= 1u << k;
+    }
     if (threadIdx.x == 0) { prefix = 0ull; need = (unsigned)q; }
     for (int shift = 56; shift >= 0; shift -= 8) {
         for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0u;
@@ -433,8 +442,9 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
         const unsigned long long hi_mask = shift == 56 ? 0ull : (~0ull << (shift + 8));
         const unsigned long long pre = prefix;
         const unsigned nd = need;  // both rewritten only after the next barrier
-        for (int k = 0; k < nv; k++)
-            if ((v[k] & hi_mask) == pre) atomicAdd(&hist[(v[k] >> shift) & 255u], 1u);
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            if (((valid >> k) & 1u) && (v[k] & hi_mask) == pre) atomicAdd(&hist[(v[k] >> shift) & 255u], 1u);
         __syncthreads();
         if (threadIdx.x < 32) {
             const int lane = threadIdx.x;
@@ -1076,7 +1086,9 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
     int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
     if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
-    const int S = 4096;
+    // 16,384 samples: with q at least 7 about 8·n/S ≈ 350 candidates for
+    // Q3's ~700K groups (4,096 samples kept ~1,400, whose host sort cost more)
+    const int S = 16384;
     const long long w = 2 + p.ni + p.nf;
     const long long nmax = c.n >= 0 ? c.n : c.cap_out;
     // rank | samples | threshold, count | selected indices | gathered rows
@@ -1105,8 +1117,9 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
     VQ_CUDA(cudaGetLastError());
     rc.launches += 5;
     // one copy back: group count, error word, selected count, and the first
-    // R gathered rows (twice the expected candidates)
-    const long long R = std::min<long long>(kCap, 2 * (4LL * o.limit + 64));
+    // R gathered rows (twice the last run's candidates and 256 more, at least
+    // twice the expected 4·LIMIT + 64)
+    const long long R = std::min<long long>(kCap, std::max<long long>(2 * (4LL * o.limit + 64), p.topk_seen * 2 + 256));
     p.h_stage.ensure(32 + (size_t)R * w * 8);
     char* hs = (char*)p.h_stage.p;
     std::memset(hs, 0, 32);
@@ -1135,6 +1148,7 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
         }
     }
     const long long ns = (long long)*(const unsigned long long*)(hs + 16);
+    p.topk_seen = std::min(ns, kCap);
     // few groups: all of them were selected; otherwise an unlucky sample (fewer
     // than LIMIT selected) or too many ties at the threshold: the caller
     // fetches every group
