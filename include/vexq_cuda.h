@@ -401,7 +401,11 @@ int32_t vexq_project_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes,
  * ticket, largest first. Table init, both launches (on forked streams), the
  * partial merge and the table finalize are captured in a CUDA graph on the
  * first vexq_batch_exec and replayed by every later one, each followed by one
- * copy of all outputs to pinned host memory. Join plans are not batched; they run after the graph, one
+ * copy of all outputs to pinned host memory. A join whose build key column
+ * allows a direct-mapped table runs inside the batch: its build as units of a
+ * third persistent launch ahead of the other two, its probe as units of the
+ * register or group-table class; a join whose build turns out to repeat a key
+ * or be empty, and every other join, runs on its own after the graph, one
  * after another. Results match vexq_plan_run's: keys, counts, integer
  * aggregates and group-table float sums bit for bit; register-path float sums
  * may differ in the last bits (a different row partition), both within their

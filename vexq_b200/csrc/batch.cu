@@ -11,8 +11,13 @@
 // output back to pinned host memory. The autotuner picks the shared-memory group
 // cache size (the shared-versus-global table cutover), the unit size and the
 // block shape of each class by timing graph replays, and keeps its choice in a
-// JSON file keyed by the batch's shape. Join plans are not batched: they run
-// after the graph, one after another, as vexq_plan_run would run them.
+// JSON file keyed by the batch's shape. A join whose build key range allows a
+// direct-mapped table is batched too: its build runs as units of a third,
+// build-class persistent launch ahead of the other two, its probe as units of
+// the register or group-table class; the build's counts and error word come
+// back with the outputs, and a build that failed (a repeated key) or was empty
+// sends the join to a plain run. Other joins run after the graph, one after
+// another, as vexq_plan_run would run them.
 #include <unistd.h>
 
 #include <algorithm>
@@ -56,6 +61,17 @@ struct Item {
     size_t a_keys = 0, a_first = 0, a_acc_i = 0, a_acc_fx = 0, a_special = 0, a_init = 0, a_lsb = 0, a_ngroups = 0;
     size_t o_nout = 0, o_err = 0, o_key = 0, o_first = 0, o_i = 0, o_f = 0;
     size_t a_seg = 0;
+    // join (direct-mapped build): the build side's row ranges, its work units
+    // in the build class, its parameter block (bparams[bix]), the key table,
+    // the number → key array (GROUP BY the join key) and the build's counts
+    // and error word, copied back with the outputs
+    bool join = false, gid = false;
+    int bix = -1, bbody = -1;
+    std::vector<long long> bseg;
+    long long bnchunks = 0, brows = 0, bunits = 0;
+    long long dmin = 0;
+    unsigned long long drange = 0;
+    size_t a_bseg = 0, a_dmap = 0, a_jgkey = 0, o_jscal = 0;
 };
 
 struct ClassKernel {
@@ -72,11 +88,12 @@ struct ClassKernel {
 struct Batch {
     std::vector<vexq_plan_s*> handles;
     std::vector<Item> items;
-    ClassKernel ck[2];
+    ClassKernel ck[3];  // register path, group tables, join builds (run before both)
     int cache_kb = 96, unit_div = 4;
     DevBuf dev, out;
     PinnedBuf h_out;
-    size_t out_bytes = 0, a_params = 0, a_tdesc = 0, a_mdesc = 0, a_ticket = 0, o_aerr = 0;
+    size_t out_bytes = 0, a_params = 0, a_bparams = 0, a_tdesc = 0, a_mdesc = 0, a_ticket = 0, o_aerr = 0;
+    int njoins = 0;
     int n_tdesc = 0, n_mdesc = 0, merge_entries = 0;
     long long table_slots = 0;
     cudaStream_t s = nullptr, s2 = nullptr;
@@ -111,23 +128,25 @@ struct Batch {
         drop_graph();
         // units: about unit_div units per resident block of each class, at
         // least 16 chunks (2,048 rows) each
-        for (int c = 0; c < 2; c++) {
+        for (int c = 0; c < 3; c++) {
             long long chunks = 0;
-            for (int i : ck[c].items) chunks += items[i].nchunks;
+            for (int i : ck[c].items) chunks += c == 2 ? items[i].bnchunks : items[i].nchunks;
             long long target = std::max<long long>(1, (long long)ck[c].grid * unit_div);
             long long U = std::max<long long>(16, (chunks + target - 1) / target);
             ck[c].nunits = 0;
             for (int i : ck[c].items) {
                 Item& it = items[i];
-                it.units = (it.nchunks + U - 1) / U;
-                ck[c].nunits += it.units;
+                long long& u = c == 2 ? it.bunits : it.units;
+                u = ((c == 2 ? it.bnchunks : it.nchunks) + U - 1) / U;
+                ck[c].nunits += u;
             }
         }
         size_t off = 0, oo = 0;
         auto take = [&](size_t b) { size_t o = off; off += al(std::max<size_t>(b, 8)); return o; };
         auto otake = [&](size_t b) { size_t o = oo; oo += al(std::max<size_t>(b, 8)); return o; };
         a_params = take(items.size() * sizeof(VQParams));
-        for (int c = 0; c < 2; c++) ck[c].a_units = take((size_t)ck[c].nunits * sizeof(VQUnit));
+        a_bparams = take((size_t)std::max(njoins, 1) * sizeof(VQParams));
+        for (int c = 0; c < 3; c++) ck[c].a_units = take((size_t)ck[c].nunits * sizeof(VQUnit));
         n_tdesc = (int)ck[1].items.size();
         n_mdesc = (int)ck[0].items.size();
         a_tdesc = take(n_tdesc * sizeof(VQTableDesc));
@@ -140,6 +159,7 @@ struct Batch {
         for (Item& it : items) {
             if (it.cls == 2) continue;
             it.a_seg = take(it.seg.size() * 8);
+            if (it.join) it.a_bseg = take(it.bseg.size() * 8);
             if (it.cls == 0) {
                 it.a_kinds = take((size_t)(it.nfb + it.ni + 1) * 4);
             } else {
@@ -150,6 +170,11 @@ struct Batch {
         const size_t upload = off;
         for (Item& it : items) {
             if (it.cls == 2) continue;
+            if (it.join) {
+                it.a_dmap = take((size_t)it.drange * 8);
+                it.a_jgkey = take((size_t)std::max<long long>(it.brows, 1) * 8);
+                it.o_jscal = otake(32);
+            }
             if (it.cls == 0) {
                 it.a_part_f = take((size_t)it.units * it.G * it.nfb * 8);
                 it.a_part_i = take((size_t)it.units * it.G * (it.ni + 1) * 8);
@@ -158,7 +183,7 @@ struct Batch {
                 merge_entries += it.G * it.nf + it.G * (it.ni + 1);
             } else {
                 const long long ns = it.nslots;
-                it.cache_n = it.hash ? 0 : dense_cache_groups(*it.p, cache_kb);
+                it.cache_n = it.hash || it.join ? 0 : dense_cache_groups(*it.p, cache_kb);
                 it.a_keys = it.hash ? take(ns * 8) : 0;
                 it.a_first = take(ns * 8);
                 it.a_acc_i = take((size_t)it.ni * ns * 8);
@@ -181,8 +206,8 @@ struct Batch {
         char* D = (char*)dev.p;
         char* O = (char*)out.p;
         // host images of the uploaded part
-        std::vector<VQParams> params(items.size());
-        std::vector<VQUnit> units[2];
+        std::vector<VQParams> params(items.size()), bparams((size_t)std::max(njoins, 1));
+        std::vector<VQUnit> units[3];
         std::vector<VQTableDesc> td;
         std::vector<VQMergeDesc> md;
         std::vector<char> blob(upload, 0);
@@ -205,6 +230,37 @@ struct Batch {
             P.present = p.d_present.as<unsigned char>();
             for (size_t i = 0, o = 0; i < p.sets.size(); i++) { P.sets[i] = p.d_sets.as<unsigned>() + o; o += p.sets[i].size(); }
             put(it.a_seg, it.seg.data(), it.seg.size() * 8);
+            if (it.join) {
+                // probe: build-side columns read through build rows, the
+                // direct-mapped key table
+                set_columns(P, *p.bt, true);
+                P.dmap = (unsigned long long*)(D + it.a_dmap);
+                P.dmin = it.dmin;
+                P.drange = it.drange;
+                // build: its own parameter block over the build table (mode 3)
+                VQParams& B = bparams[it.bix];
+                std::memset(&B, 0, sizeof B);
+                set_plan_constants(p, B);
+                set_columns(B, *p.bt, false);
+                B.seg = (const long long*)(D + it.a_bseg);
+                B.nseg = (int)it.bseg.size() / 3;
+                B.nchunks = it.bnchunks;
+                B.rg_rows = p.bt->rg_rows;
+                B.n_rg = p.bt->n_rg;
+                B.present = p.d_bpresent.as<unsigned char>();
+                for (size_t i = 0, o = 0; i < p.sets.size(); i++) { B.sets[i] = p.d_sets.as<unsigned>() + o; o += p.sets[i].size(); }
+                B.mode = 3;
+                B.dmap = P.dmap;
+                B.dmin = it.dmin;
+                B.drange = it.drange;
+                B.jgkey = (unsigned long long*)(D + it.a_jgkey);
+                B.jgid = it.gid ? (int*)B.jgkey : nullptr;  // a non-null flag: group numbers are handed out
+                B.jgoff = p.gid_koff;
+                B.jnkeys = (unsigned long long*)(O + it.o_jscal);
+                B.error = (int*)(O + it.o_jscal + 8);
+                B.jtotal = (unsigned long long*)(O + it.o_jscal + 16);
+                put(it.a_bseg, it.bseg.data(), it.bseg.size() * 8);
+            }
             if (it.cls == 0) {
                 P.part_f = (double*)(D + it.a_part_f);
                 P.part_i = (long long*)(D + it.a_part_i);
@@ -246,6 +302,7 @@ struct Batch {
                 put(it.a_init, iv.data(), (size_t)it.ni * 8);
                 put(it.a_lsb, p.fx_lsb.data(), (size_t)it.nf * 4);
                 VQTableDesc t;
+                std::memset(&t, 0, sizeof t);
                 t.keys = P.keys;
                 t.first = P.first;
                 t.acc_i = P.acc_i;
@@ -257,6 +314,11 @@ struct Batch {
                 t.ni = it.ni;
                 t.nf = it.nf;
                 t.hash = it.hash ? 1 : 0;
+                if (it.gid) {  // keys come from the build's number → key array
+                    t.keys = (unsigned long long*)(D + it.a_jgkey);
+                    t.hash = 1;
+                    t.gid = 1;
+                }
                 t.n_out = (unsigned long long*)(O + it.o_nout);
                 t.ngroups = P.ngroups;
                 t.error = P.error;
@@ -270,17 +332,18 @@ struct Batch {
                 td.push_back(t);
             }
         }
-        for (int c = 0; c < 2; c++) {
+        for (int c = 0; c < 3; c++) {
             for (int i : ck[c].items) {
                 const Item& it = items[i];
-                if (!it.units) continue;
-                const long long u = (it.nchunks + it.units - 1) / it.units;
-                for (long long k = 0; k < it.units; k++) {
+                const long long nu = c == 2 ? it.bunits : it.units, nc = c == 2 ? it.bnchunks : it.nchunks;
+                if (!nu) continue;
+                const long long u = (nc + nu - 1) / nu;
+                for (long long k = 0; k < nu; k++) {
                     VQUnit w;
-                    w.plan = i;
-                    w.body = it.body;
+                    w.plan = c == 2 ? it.bix : i;  // build units index the build parameter blocks
+                    w.body = c == 2 ? it.bbody : it.body;
                     w.cbeg = k * u;
-                    w.cend = std::min(it.nchunks, (k + 1) * u);
+                    w.cend = std::min(nc, (k + 1) * u);
                     w.pslot = k;
                     units[c].push_back(w);
                 }
@@ -290,13 +353,15 @@ struct Batch {
             put(ck[c].a_units, units[c].data(), units[c].size() * sizeof(VQUnit));
         }
         put(a_params, params.data(), params.size() * sizeof(VQParams));
+        put(a_bparams, bparams.data(), (size_t)njoins * sizeof(VQParams));
         put(a_tdesc, td.data(), td.size() * sizeof(VQTableDesc));
         put(a_mdesc, md.data(), md.size() * sizeof(VQMergeDesc));
         h2d(dev.p, blob.data(), upload, s);
         std::ostringstream ex;
         ex << "batch plans=" << items.size() << " regs_plans=" << ck[0].items.size() << " regs_bodies=" << ck[0].nbodies
            << " regs_units=" << ck[0].nunits << " table_plans=" << ck[1].items.size() << " table_bodies=" << ck[1].nbodies
-           << " table_units=" << ck[1].nunits << " cache_kb=" << cache_kb << " unit_div=" << unit_div;
+           << " table_units=" << ck[1].nunits << " joins=" << njoins << " build_units=" << ck[2].nunits << " cache_kb=" << cache_kb
+           << " unit_div=" << unit_div;
         explain = ex.str();
     }
 
@@ -315,11 +380,24 @@ struct Batch {
         char* D = (char*)dev.p;
         VQ_CUDA(cudaMemsetAsync(D + a_ticket, 0, 16, s));
         VQ_CUDA(cudaMemsetAsync((char*)out.p + o_aerr, 0, 8, s));
+        for (const Item& it : items) {
+            if (!it.join || it.cls == 2) continue;
+            VQ_CUDA(cudaMemsetAsync(D + it.a_dmap, 0, (size_t)it.drange * 8, s));
+            VQ_CUDA(cudaMemsetAsync((char*)out.p + it.o_jscal, 0, 32, s));
+        }
         if (table_slots > 0) {
             int g = (int)std::min<long long>((table_slots + 255) / 256, (long long)sm_count() * 16);
             k_init_batch<<<g, 256, 0, s>>>((const VQTableDesc*)(D + a_tdesc), n_tdesc, table_slots);
             VQ_CUDA(cudaGetLastError());
             chk(s, "k_init_batch");
+        }
+        // the joins' builds: one persistent launch of build units, before
+        // every probe (both classes below wait for it)
+        if (ck[2].nunits > 0) {
+            VQBatchArgs A{(const VQParams*)(D + a_bparams), (const VQUnit*)(D + ck[2].a_units), (unsigned*)(D + a_ticket) + 2,
+                          (int)ck[2].nunits};
+            jit_launch(ck[2].k, ck[2].grid, &A, sizeof A, s);
+            chk(s, "vq_batch (join builds)");
         }
         VQ_CUDA(cudaEventRecord(ev[2], s));
         VQ_CUDA(cudaStreamWaitEvent(s2, ev[2], 0));
@@ -411,10 +489,10 @@ struct Batch {
         if (ps.empty()) return;
         std::vector<int> body_of;
         int smem = 0, nb = 0;
-        ck[c].k_src = gen_batch_source(ps, ck[c].block, body_of, smem, nb);
+        ck[c].k_src = gen_batch_source(ps, ck[c].block, body_of, smem, nb, c == 2);
         ck[c].smem_extra = smem;
         ck[c].nbodies = nb;
-        for (size_t j = 0; j < ps.size(); j++) items[ck[c].items[j]].body = body_of[j];
+        for (size_t j = 0; j < ps.size(); j++) (c == 2 ? items[ck[c].items[j]].bbody : items[ck[c].items[j]].body) = body_of[j];
     }
 
     // The batch's shape for the tuning cache: per class, the plans, distinct
@@ -435,9 +513,9 @@ struct Batch {
 
     // grid of each class at the current shared-memory size
     void size_grids() {
-        for (int c = 0; c < 2; c++) {
+        for (int c = 0; c < 3; c++) {
             if (ck[c].items.empty()) continue;
-            int smem = c == 0 ? ck[c].smem_extra : table_smem();
+            int smem = c == 1 ? table_smem() : ck[c].smem_extra;
             ck[c].k = jit_get(ck[c].k_src, "vq_batch", ck[c].block, smem);
             ck[c].grid = sm_count() * std::max(1, ck[c].k.max_blocks_per_sm);
         }
@@ -581,12 +659,38 @@ struct Batch {
 // (Re)builds a batch over a plan set: ranges, classes, generated source,
 // grids and layout. Device buffers only grow, so a reused batch allocates
 // nothing once it has seen its largest plan set.
+// A join joins the batch when its build can be direct-mapped (the build key
+// column's range at most a few times its rows, keys not seen repeating): its
+// build runs as units of the build class and its probe as units of the
+// register or group-table class. Other joins run on their own afterwards.
+static bool setup_join(Plan& p, Item& it) {
+    if (p.radix_bits > 0 || !p.dmap_on || p.dmap_failed || p.staged) return false;
+    Table& bt = *p.bt;
+    const Column& bkc = bt.cols[p.build_key];
+    if (!bkc.has_range || bkc.imax < bkc.imin) return false;
+    const __int128 r = (__int128)bkc.imax - (__int128)bkc.imin + 1;
+    if (r > ((__int128)1 << 31) || r > 4 * (__int128)std::max<int64_t>(bt.nrows, 1) + 65536) return false;
+    std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
+    ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, 128);
+    if (bs.nchunks == 0) return false;  // an empty build emits nothing: the plain run says so
+    it.join = true;
+    it.gid = p.join_gid;
+    it.dmin = bkc.imin;
+    it.drange = (unsigned long long)r;
+    it.bseg = bs.seg;
+    it.bnchunks = bs.nchunks;
+    it.brows = bs.rows;
+    it.bytes += scanned_bytes(p, bt, bs.rows, true);
+    return true;
+}
+
 void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
     b->drop_graph();
     b->handles.assign(handles, handles + n);
     b->items.clear();
     b->bytes = b->rows = 0;
-    for (int c = 0; c < 2; c++) {
+    b->njoins = 0;
+    for (int c = 0; c < 3; c++) {
         b->ck[c].items.clear();
         b->ck[c].k_src.clear();
         b->ck[c].nunits = 0;
@@ -597,17 +701,20 @@ void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
         Item it;
         Plan* p = handles[i]->p;
         it.p = p;
-        if (p->is_join || p->ndist > 0) {  // joins and COUNT(DISTINCT) run on their own after the graph
+        // COUNT(DISTINCT) and joins without a direct-mapped build run on their own after the graph
+        if (p->ndist > 0 || (p->is_join && !setup_join(*p, it))) {
+            it.join = false;
             b->items.push_back(std::move(it));
             continue;
         }
+        if (it.join) it.bix = b->njoins++;
         Table& t = *p->t;
         std::vector<uint8_t> m = prune_mask(*p, t, p->zn_pred, 0, t.n_rg);
         ScanSegs ss = make_segments(t, m, 0, t.n_rg, 128);
         it.seg = ss.seg;
         it.nchunks = ss.nchunks;
         it.rows = ss.rows;
-        it.bytes = scanned_bytes(*p, t, ss.rows, false);
+        it.bytes += scanned_bytes(*p, t, ss.rows, false);
         it.nf = p->nf;
         it.ni = p->ni;
         it.nfb = std::max(p->nf, 1);
@@ -616,9 +723,11 @@ void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
             it.G = (int)p->domain;
         } else {
             it.cls = 1;
-            it.hash = p->path == AggPath::Hash;
-            if (it.hash) {
-                long long est = estimate_groups(*p, ss.rows, 0), cap = 16;
+            it.hash = p->path == AggPath::Hash && !it.gid;
+            if (it.gid) {
+                it.cap = std::max<long long>(it.brows, 1);  // group numbers never exceed the build rows
+            } else if (it.hash) {
+                long long est = estimate_groups(*p, ss.rows, it.join ? it.brows : 0), cap = 16;
                 while (cap < 2 * std::max<long long>(est, 8)) cap <<= 1;
                 it.cap = cap;
             } else {
@@ -633,11 +742,13 @@ void build_batch(Batch* b, vexq_plan_s* const* handles, int n) {
     }
     b->ck[0].block = kBlockRegs;
     b->ck[1].block = kBlockTable;
-    for (int c = 0; c < 2; c++) {
+    b->ck[2].block = 256;
+    for (int c = 0; c < 2; c++)
         for (size_t i = 0; i < b->items.size(); i++)
             if (b->items[i].cls == c) b->ck[c].items.push_back((int)i);
-        b->gen_class(c);
-    }
+    for (size_t i = 0; i < b->items.size(); i++)
+        if (b->items[i].join && b->items[i].cls != 2) b->ck[2].items.push_back((int)i);
+    for (int c = 0; c < 3; c++) b->gen_class(c);
     b->size_grids();
     b->layout();
 }
@@ -667,10 +778,23 @@ static void collect(Batch& b, vexq_result_s** out) {
     std::vector<std::string> errs(n);
     std::vector<int32_t> codes(n, 0);
     std::atomic<size_t> next{0};
+    // the register class shares one error word: any flag sends its plans to plain runs
+    const int rerr = *(const int*)(H + b.o_aerr);
     auto work = [&]() {
         for (size_t i = next++; i < n; i = next++) {
             Item& it = b.items[i];
             if (it.cls == 2) { plain[i] = 1; continue; }
+            if (it.cls == 0 && rerr) { plain[i] = 1; continue; }
+            if (it.join) {
+                // the build's outcome: a repeated or out-of-range key (the hash
+                // build from then on), no key, or uneven counts: a plain run
+                const unsigned long long nk = *(const unsigned long long*)(H + it.o_jscal);
+                const int berr = *(const int*)(H + it.o_jscal + 8);
+                const unsigned long long ntot = *(const unsigned long long*)(H + it.o_jscal + 16);
+                if (berr & (16 | 32)) it.p->dmap_failed = true;
+                if (berr || nk == 0 || nk != ntot) { plain[i] = 1; continue; }
+                if (it.cls == 1 && (*(const int*)(H + it.o_err) & 256)) { plain[i] = 1; continue; }
+            }
             try {
                 Plan& p = *it.p;
                 Groups g;
@@ -707,7 +831,7 @@ static void collect(Batch& b, vexq_result_s** out) {
                 r->kernel_ms = b.kernel_ms;
                 r->scan_ms = b.kernel_ms;
                 r->launches = 0;
-                r->rows_scanned = it.rows;
+                r->rows_scanned = it.rows + it.brows;
                 r->bytes_scanned = it.bytes;
                 out[i] = r;
             } catch (const Status& e) {

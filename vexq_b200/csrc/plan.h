@@ -355,6 +355,7 @@ struct VQTableDesc {           // one group table
     const int* fx_lsb;
     long long nslots;
     int ni, nf, hash;
+    int gid;                   // a join's build-key-numbered table: keys[] is the number → key array, not initialised
     unsigned long long* n_out;
     unsigned long long* ngroups;
     int* error;

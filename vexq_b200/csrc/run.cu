@@ -173,7 +173,7 @@ __global__ void k_init_batch(const VQTableDesc* d, int n, long long total) {
     for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
         const VQTableDesc& t = d[table_of(d, n, g)];
         const long long i = g - t.slot0;
-        if (t.hash) t.keys[i] = (i == t.nslots - 1) ? 0ull : VQ_EMPTY_KEY;
+        if (t.hash && !t.gid) t.keys[i] = (i == t.nslots - 1) ? 0ull : VQ_EMPTY_KEY;
         t.first[i] = 0x7FFFFFFFFFFFFFFFLL;
         for (int s = 0; s < t.ni; s++) t.acc_i[(long long)s * t.nslots + i] = t.init_i[s];
         for (int f = 0; f < t.nf; f++) {
