@@ -75,9 +75,8 @@ def serve_workload(args):
     build.build()
     X.init(0)
     fact = args.fact_rows
-    li = X.GpuTable(D.lineitem(fact, seed=77, rg_rows=RG_ROWS))
-    o = X.GpuTable(D.orders(fact // 4, seed=78))
-    it = X.GpuTable(D.items(fact, fact // 4, seed=79))
+    h_li, h_o, h_it = D.lineitem(fact, seed=77, rg_rows=RG_ROWS), D.orders(fact // 4, seed=78), D.items(fact, fact // 4, seed=79)
+    li, o, it = X.GpuTable(h_li), X.GpuTable(h_o), X.GpuTable(h_it)
 
     def day(n):
         return (datetime.date(1970, 1, 1) + datetime.timedelta(days=int(n))).isoformat()
@@ -141,6 +140,28 @@ def serve_workload(args):
     arrivals = np.cumsum(rng.exponential(1.0 / qps, n))
     poisson_plain = arm(arrivals, 1, abi.SERVE_NO_BATCH)
     poisson_batched = arm(arrivals, 2, 0)
+    # host-CPU baseline: the C++ restatement of the reference's parallel path
+    # (all host threads) on one query of each kind from the same mix, the
+    # mix's queries/s from their times weighted 50/20/30
+    cpu = None
+    if not args.no_cpu:
+        from oracle import refcpu as R
+        workers = os.cpu_count() or 1
+        tli, to, tit = R.RefTable(h_li), R.RefTable(h_o), R.RefTable(h_it)
+        secs = {}
+        for k, mk in (("q1", lambda: W.q1_plan(day(8036 + 2000))), ("q6", lambda: W.q6_plan(day(9036), day(9401))),
+                      ("q3", lambda: W.q3_plan(0.45, 0.45))):
+            t0 = time.perf_counter()
+            if k == "q3":
+                R.join_raw(to, tit, mk(), workers=workers)
+            else:
+                R.agg_raw(tli, mk(), workers=workers)
+            secs[k] = time.perf_counter() - t0
+        per_query = 0.5 * secs["q1"] + 0.2 * secs["q6"] + 0.3 * secs["q3"]
+        cpu = {"value": round(1.0 / per_query, 3), "unit": "queries/s", "cores": workers, "cpu": cpu_model(), "kind": "port",
+               "sample": "one query of each kind on the same tables (C++ restatement of ParallelHashAggregate / "
+                         "ParallelHashJoinAggregate), queries/s of the 50/20/30 mix from their times",
+               "seconds": {k: round(v, 3) for k, v in secs.items()}}
     line = {"metric": "queries/s", "value": closed_batched["qps"], "unit": "queries/s", "n_gpus": 1,
             "steps": n, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded lineitem / orders / items generators)",
@@ -148,7 +169,8 @@ def serve_workload(args):
                                    "50% Q1 / 20% Q6 / 30% Q3 with randomised cutoffs"},
             "alone_ms_median": {k: round(float(statistics.median(v)), 3) for k, v in alone.items()},
             "closed_plain": closed_plain, "closed_batched": closed_batched,
-            "poisson_qps": round(qps, 2), "poisson_plain": poisson_plain, "poisson_batched": poisson_batched}
+            "poisson_qps": round(qps, 2), "poisson_plain": poisson_plain, "poisson_batched": poisson_batched,
+            "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
 
 
