@@ -665,6 +665,9 @@ struct Batch {
 // register or group-table class. Other joins run on their own afterwards.
 static bool setup_join(Plan& p, Item& it) {
     if (p.radix_bits > 0 || !p.dmap_on || p.dmap_failed || p.staged) return false;
+    // GROUP BY the join key with a LIMIT over more than 2^20 build rows: the
+    // plain run keeps its device top-k (a batch copies every group back)
+    if (p.join_gid && p.order.limit >= 0 && p.bt->nrows > (1 << 20)) return false;
     Table& bt = *p.bt;
     const Column& bkc = bt.cols[p.build_key];
     if (!bkc.has_range || bkc.imax < bkc.imin) return false;

@@ -11,6 +11,8 @@
 #include <unistd.h>
 
 #include <atomic>
+#include <map>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -149,9 +151,33 @@ std::string jit_cache_dir() {
 
 // Compiles (or fetches) the cubin for `source`; loading on the device
 // happens on first use in the calling thread's current device.
+// Finished kernels by (source hash, device, entry, block, dynamic shared
+// memory): a repeated request (a batch rebuilt for every served batch, a plan
+// recompiled) returns without copying the cubin or querying the driver.
+struct KernelKey {
+    uint64_t h;
+    int dev, block, smem;
+    std::string entry;
+    bool operator<(const KernelKey& o) const {
+        return std::tie(h, dev, block, smem, entry) < std::tie(o.h, o.dev, o.block, o.smem, o.entry);
+    }
+};
+static std::map<KernelKey, JitKernel> g_kernels;
+
 JitKernel jit_get(const std::string& source, const std::string& entry, int block, int smem) {
     uint64_t h = fnv1a(source) ^ (fnv1a(entry) * 31);
     for (const char* o : kOptions) h = h * 1099511628211ull ^ fnv1a(o);
+    int cur_dev = -1;
+    if (cudaGetDevice(&cur_dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cur_dev = -1;
+    }
+    const KernelKey kk{h, cur_dev, block, smem, entry};
+    if (cur_dev >= 0) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_kernels.find(kk);
+        if (it != g_kernels.end()) return it->second;
+    }
     // one compile and one module load per source: a thread that finds another
     // working on the same source waits for it
     std::shared_ptr<std::mutex> cm;
@@ -214,6 +240,10 @@ JitKernel jit_get(const std::string& source, const std::string& entry, int block
     if (d.occ(&nb, f, block, (size_t)smem) == CUDA_SUCCESS) k.max_blocks_per_sm = nb;
     int regs = 0;
     if (d.getattr(&regs, CU_FUNC_ATTRIBUTE_NUM_REGS, f) == CUDA_SUCCESS) k.regs = regs;
+    if (dev == cur_dev) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_kernels[kk] = k;
+    }
     return k;
 }
 
