@@ -214,6 +214,7 @@ struct Plan {
     void* h_stage_mapped_for = nullptr;    // the staging allocation that address belongs to
     bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
     ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
+    ScanMemo build_memo;                   // join build side's pruning (whole table), until its zone maps change
     long long hash_groups_seen = -1;       // hash path: groups the last run found (sizes the next table)
     // dense path: the kernel accumulates hot_n groups per thread in registers;
     // which groups is a launch value, the largest-count groups of the last run

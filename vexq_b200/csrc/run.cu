@@ -418,11 +418,12 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
         return;
     }
     // expected (q+1)·n/S groups at or above the q-th largest sample: about
-    // 4·LIMIT + 64 (n above 4·LIMIT + 4096 keeps q below S), and q at least 7:
+    // 4·LIMIT + 64 (n above 4·LIMIT + 4096 keeps q below S), and q at least 3:
     // the count above the q-th largest sample spreads like a Gamma(q+1)
     // variable, so with q = 0 about one run in 20 kept fewer than LIMIT groups
-    // and fetched every group instead; from q = 7 that is below 1e-12
-    const int q = max((int)ceil((4.0 * limit + 64.0) * S / (double)n) - 1, min(7, S - 1));
+    // and fetched every group instead; from q = 3 (about 4·n/S candidates)
+    // that is about one run in 10,000 at LIMIT 10
+    const int q = max((int)ceil((4.0 * limit + 64.0) * S / (double)n) - 1, min(3, S - 1));
     __shared__ unsigned hist[256];
     __shared__ unsigned long long prefix;
     __shared__ unsigned need;
@@ -1086,8 +1087,9 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
     int vbank = (p.slots[vslot].kind == S_FSUM) ? 1 : 0;
     int fmin_key = (p.slots[vslot].kind == S_FMIN || p.slots[vslot].kind == S_FMAX) ? 1 : 0;
     if (a.kind == VEXQ_AGG_COUNT) vbank = 0;
-    // 16,384 samples: with q at least 7 about 8·n/S ≈ 350 candidates for
-    // Q3's ~700K groups (4,096 samples kept ~1,400, whose host sort cost more)
+    // 16,384 samples: with q at least 3 about 4·n/S ≈ 175 candidates for
+    // Q3's ~700K groups (4,096 samples with q at least 7 kept ~1,400, whose
+    // host sort cost more)
     const int S = 16384;
     const long long w = 2 + p.ni + p.nf;
     const long long nmax = c.n >= 0 ? c.n : c.cap_out;
@@ -1118,8 +1120,12 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
     rc.launches += 5;
     // one copy back: group count, error word, selected count, and the first
     // R gathered rows (twice the last run's candidates and 256 more, at least
-    // twice the expected 4·LIMIT + 64)
-    const long long R = std::min<long long>(kCap, std::max<long long>(2 * (4LL * o.limit + 64), p.topk_seen * 2 + 256));
+    // twice the expected 4·LIMIT + 64), rounded up to a power of two so the
+    // pinned staging buffer grows only at doublings
+    const long long want = std::max<long long>(2 * (4LL * o.limit + 64), p.topk_seen * 2 + 256);
+    long long R = 1024;
+    while (R < want) R <<= 1;
+    R = std::min(R, kCap);
     p.h_stage.ensure(32 + (size_t)R * w * 8);
     char* hs = (char*)p.h_stage.p;
     std::memset(hs, 0, 32);
@@ -1785,8 +1791,15 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     }
     if (p.is_join && !use_radix) {
         Table& bt = *p.bt;
-        std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
-        ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
+        ScanMemo& bmemo = p.build_memo;  // the build side's pruning, kept until its zone maps change
+        if (bmemo.zone_version != bt.zone_version || bmemo.rgs != 0 || bmemo.rge != bt.n_rg) {
+            std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
+            bmemo.ss = make_segments(bt, bm, 0, bt.n_rg, p.btile);
+            bmemo.zone_version = bt.zone_version;
+            bmemo.rgs = 0;
+            bmemo.rge = bt.n_rg;
+        }
+        const ScanSegs& bs = bmemo.ss;
         // build table: twice the distinct keys the last build found (scaled by
         // the rows scanned), else twice the rows; a build that hits the probe
         // limit reruns at the row-bounded size (a table sized by rows leaves
