@@ -2683,7 +2683,7 @@ static std::string gen_probe_kernel(Plan& p, const std::vector<int>& key_nodes, 
     p.tile = loop.tile_rows();
     p.smem = loop.smem();
     loop.prologue(os);
-    os << kernel_head("vq_agg", block);
+    os << kernel_head("vq_agg", block, p.min_blocks);
     // a build the host did not wait for: its failure or emptiness is raised
     // in this kernel's error word, which comes back with the results
     os << "    if (P.berr && blockIdx.x == 0 && threadIdx.x == 0) {\n";

@@ -398,18 +398,13 @@ __device__ __forceinline__ unsigned long long vq_rank(long long bits, bool isnul
 }
 // The top-k kernels read the group count from the device (*np, written by
 // the finalize or HAVING compaction), so they follow it without a copy back.
-__global__ void k_sample(const unsigned long long* rank, const unsigned long long* np, long long nmax, int S, unsigned long long* out) {
-    const long long n = (long long)min(*np, (unsigned long long)nmax);
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < S) out[j] = n > 0 ? rank[(long long)j * n / S] : 0ull;
-}
-// One block finds the q-th largest of the S samples (S <= 16384, q < S) by radix
-// select, most significant byte first: each round counts, in shared memory,
+// One block samples S evenly spaced group ranks (S <= 16384) and finds the
+// q-th largest of them (q < S) by radix select, most significant byte first: each round counts, in shared memory,
 // the next byte of the samples that match the bytes chosen so far, and one
 // warp walks the 256 counts from the top to the byte holding the q-th largest.
 // The result is the selection threshold, so the host needs no copy of the
 // samples.
-__global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* samp, int S, const unsigned long long* np, long long nmax,
+__global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* rank, int S, const unsigned long long* np, long long nmax,
                                                     int limit, unsigned long long* thr) {
     const long long n = (long long)min(*np, (unsigned long long)nmax);
     // few groups (at most 4·LIMIT + 4096): every group is a candidate
@@ -433,7 +428,7 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         const int i = (int)threadIdx.x + k * (int)blockDim.x;
-        v[k] = i < S ? samp[i] : 0ull;
+        v[k] = i < S ? rank[(long long)i * n / S] : 0ull;  // the sample: S evenly spaced groups
         if (i < S) valid |= 1u << k;
     }
     if (threadIdx.x == 0) { prefix = 0ull; need = (unsigned)q; }
@@ -474,14 +469,24 @@ __global__ void __launch_bounds__(1024) k_threshold(const unsigned long long* sa
     }
     if (threadIdx.x == 0) *thr = q < S ? prefix : 0ull;
 }
+// The groups at or above the threshold, each gathered straight into its
+// claimed row of the staging block (key, first-row key, integer bank, float
+// bank as raw bits).
 __global__ void k_select(const unsigned long long* rank, const unsigned long long* np, long long nmax, const unsigned long long* thrp,
-                         unsigned long long* nsel, long long* sel, long long cap) {
+                         unsigned long long* nsel, long long cap, const unsigned long long* key, const long long* first,
+                         const long long* ival, const double* fval, long long cap_out, int ni, int nf, long long* out) {
     const long long n = (long long)min(*np, (unsigned long long)nmax);
     const unsigned long long thr = *thrp;
+    const long long w = 2 + ni + nf;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         if (rank[i] >= thr) {
-            unsigned long long p = atomicAdd(nsel, 1ull);
-            if ((long long)p < cap) sel[p] = i;
+            const unsigned long long p = atomicAdd(nsel, 1ull);
+            if ((long long)p >= cap) continue;
+            long long* o = out + (long long)p * w;
+            o[0] = (long long)key[i];
+            o[1] = first[i];
+            for (int s = 0; s < ni; s++) o[2 + s] = ival[(long long)s * cap_out + i];
+            for (int f = 0; f < nf; f++) o[2 + ni + f] = __double_as_longlong(fval[(long long)f * cap_out + i]);
         }
     }
 }
@@ -506,21 +511,6 @@ __global__ void k_sortrank(const long long* o_i, const double* o_f, long long ca
     }
 }
 
-// Gathers the selected compacted groups into a dense staging block.
-__global__ void k_gather(const long long* sel, const unsigned long long* nsel, long long cap, const unsigned long long* key,
-                         const long long* first, const long long* ival, const double* fval, long long cap_out, int ni, int nf,
-                         long long* out) {
-    long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long n = (long long)min(*nsel, (unsigned long long)cap);
-    if (j >= n) return;
-    long long i = sel[j];
-    long long w = 2 + ni + nf;
-    long long* o = out + j * w;
-    o[0] = (long long)key[i];
-    o[1] = first[i];
-    for (int s = 0; s < ni; s++) o[2 + s] = ival[(long long)s * cap_out + i];
-    for (int f = 0; f < nf; f++) o[2 + ni + f] = __double_as_longlong(fval[(long long)f * cap_out + i]);
-}
 
 }  // namespace vq
 
@@ -1093,31 +1083,25 @@ int topk_groups(RunCtx& rc, Compacted& c, Groups& g) {
     const int S = 16384;
     const long long w = 2 + p.ni + p.nf;
     const long long nmax = c.n >= 0 ? c.n : c.cap_out;
-    // rank | samples | threshold, count | selected indices | gathered rows
-    size_t need = (size_t)nmax * 8 + S * 8 + 16 + kCap * 8 + (size_t)kCap * w * 8 + 64;
+    // rank | threshold, count | gathered rows
+    size_t need = (size_t)nmax * 8 + 16 + (size_t)kCap * w * 8 + 64;
     p.scratch_d.ensure(need);
     unsigned long long* rank = p.scratch_d.as<unsigned long long>();
-    unsigned long long* samp = rank + nmax;
-    unsigned long long* thr = samp + S;
+    unsigned long long* thr = rank + nmax;
     unsigned long long* nsel = thr + 1;
-    long long* dsel = (long long*)(nsel + 1);
-    long long* dout = dsel + kCap;
+    long long* dout = (long long*)(nsel + 1);
     int gr = (int)std::min<long long>((nmax + 255) / 256, (long long)sm_count() * 8);
     k_sortrank<<<std::max(gr, 1), 256, 0, rc.s>>>(c.ival, c.fval, c.cap_out, c.n_dev, a.kind, vbank, p.slot_pos[vslot],
                                                   p.slot_pos[a.nn_slot], fmin_key, o.descending, rank);
     launch_check(rc.s, "k_sortrank");
-    k_sample<<<(S + 255) / 256, 256, 0, rc.s>>>(rank, c.n_dev, nmax, S, samp);
-    launch_check(rc.s, "k_sample");
-    k_threshold<<<1, 1024, 0, rc.s>>>(samp, S, c.n_dev, nmax, (int)o.limit, thr);
+    k_threshold<<<1, 1024, 0, rc.s>>>(rank, S, c.n_dev, nmax, (int)o.limit, thr);
     launch_check(rc.s, "k_threshold");
     VQ_CUDA(cudaMemsetAsync(nsel, 0, 8, rc.s));
-    k_select<<<std::max(gr, 1), 256, 0, rc.s>>>(rank, c.n_dev, nmax, thr, nsel, dsel, kCap);
+    k_select<<<std::max(gr, 1), 256, 0, rc.s>>>(rank, c.n_dev, nmax, thr, nsel, kCap, c.key, c.first, c.ival, c.fval, c.cap_out,
+                                                p.ni, p.nf, dout);
     launch_check(rc.s, "k_select");
-    k_gather<<<(int)((kCap + 127) / 128), 128, 0, rc.s>>>(dsel, nsel, kCap, c.key, c.first, c.ival, c.fval, c.cap_out, p.ni,
-                                                          p.nf, dout);
-    launch_check(rc.s, "k_gather");
     VQ_CUDA(cudaGetLastError());
-    rc.launches += 5;
+    rc.launches += 3;
     // one copy back: group count, error word, selected count, and the first
     // R gathered rows (twice the last run's candidates and 256 more, at least
     // twice the expected 4·LIMIT + 64), rounded up to a power of two so the
