@@ -512,6 +512,13 @@ int32_t vexq_debug_fail_alloc(int32_t after);
 /* Bytes of device memory the library holds right now (tables, plan buffers,
  * batch workspaces), all devices together: a leak check for the tests. */
 int32_t vexq_debug_live_device_bytes(int64_t* out);
+/* Makes the join plan's next run take the speculative direct-mapped build (the
+ * probe launched without the host reading the build's outcome) as if the last
+ * build had been direct-mapped over the same rows with `keys_seen` keys, so a
+ * test can reach the probe-raised retries on the host: a build that repeats a
+ * key, an empty build, or more keys than the group table sized from
+ * `keys_seen` holds. VEXQ_EINVAL for aggregate plans; no device fault is made. */
+int32_t vexq_debug_join_spec(vexq_plan_t p, int64_t keys_seen);
 
 /* ---- global aggregate without allocation --------------------------------
  * No counterpart in the reference: its operators work on the Go heap.

@@ -156,7 +156,7 @@ EXPORTS = [
     "vexq_batch_run",
     "vexq_server_start", "vexq_server_submit", "vexq_server_poll",
     "vexq_server_wait", "vexq_server_latency", "vexq_server_stop",
-    "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes", "vexq_plan_autotune",
+    "vexq_cancel", "vexq_debug_fail_alloc", "vexq_debug_live_device_bytes", "vexq_debug_join_spec", "vexq_plan_autotune",
     "vexq_plan_run_partial", "vexq_partial_info", "vexq_partial_serialize", "vexq_partial_deserialize",
     "vexq_partial_merge", "vexq_partial_free",
     "vexq_plan_run_global_noalloc",
@@ -244,6 +244,7 @@ def load() -> C.CDLL:
         "vexq_partial_merge": (i32, [vp, C.POINTER(vp), i32, C.POINTER(vp)]),
         "vexq_partial_free": (i32, [vp]),
         "vexq_debug_live_device_bytes": (i32, [C.POINTER(i64)]),
+        "vexq_debug_join_spec": (i32, [C.c_void_p, i64]),
         "vexq_plan_run_global_noalloc": (i32, [vp, i32, i32, vp, C.POINTER(i64), C.POINTER(C.c_uint8), i32]),
         "vexq_batch_create": (i32, [C.POINTER(vp), i32, C.c_uint32, C.POINTER(vp)]),
         "vexq_batch_exec": (i32, [vp, C.POINTER(vp)]),

@@ -354,4 +354,14 @@ int32_t vexq_debug_live_device_bytes(int64_t* out) {
     return VEXQ_OK;
 }
 
+int32_t vexq_debug_join_spec(vexq_plan_t p, int64_t keys_seen) {
+    return guard([&]() -> int32_t {
+        if (!p || !p->p->is_join || keys_seen < 1) fail(VEXQ_EINVAL, "a join plan and a positive key count");
+        vq::Plan& pl = *p->p;
+        std::lock_guard<std::mutex> lk(vq::plan_mutex(&pl));
+        vq::force_join_spec(pl, keys_seen);
+        return VEXQ_OK;
+    });
+}
+
 }  // extern "C"

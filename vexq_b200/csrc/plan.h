@@ -332,6 +332,7 @@ std::mutex& plan_mutex(Plan* p);
 // an error (diagnostics; off by default).
 void launch_check(cudaStream_t s, const char* what);
 bool launch_checks_on();  // VEXQ_SYNC_CHECK: a synchronize after every launch
+void force_join_spec(Plan& p, long long keys_seen);
 std::vector<uint8_t> prune_mask(const Plan& p, const Table& t, int root, int rgs, int rge);
 
 // Batched execution of many plans (batch.cu).

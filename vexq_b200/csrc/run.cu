@@ -1684,6 +1684,19 @@ static long long radix_pass(RunCtx& rc, const JitKernel& kp, VQParams Q, int pbi
     return total;
 }
 
+// The next run speculates (vexq_debug_join_spec): the state a direct-mapped
+// build over the current build rows with keys_seen keys would have left.
+void force_join_spec(Plan& p, long long keys_seen) {
+    Table& bt = *p.bt;
+    std::vector<uint8_t> bm = prune_mask(p, bt, p.zn_bpred, 0, bt.n_rg);
+    const ScanSegs bs = make_segments(bt, bm, 0, bt.n_rg, p.btile);
+    p.dmap_failed = false;
+    p.dmap_used = true;
+    p.join_rows_seen = bs.rows;
+    p.join_keys_seen = keys_seen;
+    p.gid_groups = keys_seen;
+}
+
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
     check_ranges(p);
