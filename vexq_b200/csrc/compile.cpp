@@ -2291,7 +2291,7 @@ static std::string gen_agg_body(Plan& p, const std::string& name, int block) {
     return os.str();
 }
 
-static void emit_direct_build_tail(std::ostringstream& os);
+static void emit_direct_build_tail(std::ostringstream& os, bool block_claim);
 static void emit_probe_rows(std::ostringstream& os, Plan& p, const std::vector<int>& key_nodes, bool strided);
 
 // Batch body of a join's direct-mapped build over build chunks [cbeg, cend)
@@ -2328,7 +2328,7 @@ static std::string gen_build_body(Plan& p, const std::string& name, int block) {
     os << "            vq_d3[k] = di;\n";
     os << "            vq_k3[k] = jk;\n";
     os << "        }\n";
-    emit_direct_build_tail(os);
+    emit_direct_build_tail(os, false);
     os << "    }\n";
     os << "    for (int o = 16; o > 0; o >>= 1) {\n";
     os << "        vq_nrows += __shfl_xor_sync(0xffffffffu, vq_nrows, o);\n";
@@ -2450,7 +2450,13 @@ int dense_cache_groups(const Plan& p, int cache_kb) {
 // flight a lane, then their outcomes; with group numbers, one claim per warp
 // and chunk (registers only: the lane's fresh rows are its four flags, in
 // row order). Shared by the build kernel (mode 3) and the batched build body.
-static void emit_direct_build_tail(std::ostringstream& os) {
+// block_claim (a chunk loop every warp of the block walks the same number of
+// times): the warps' counts are summed in shared memory and the block takes
+// its group numbers with one atomic per iteration instead of one per warp,
+// the single counter every build row's claim serialises on; two buffers by
+// iteration parity (vq_wsum, vq_gb, vq_par declared by the kernel) leave two
+// barriers an iteration.
+static void emit_direct_build_tail(std::ostringstream& os, bool block_claim) {
     os << "        if (P.mode == 3) {\n";
     os << "            unsigned long long vq_o3[4];\n";
     os << "#pragma unroll\n            for (int k = 0; k < 4; k++)\n";
@@ -2468,8 +2474,26 @@ static void emit_direct_build_tail(std::ostringstream& os) {
     os << "                for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += t; }\n";
     os << "                const int tot = __shfl_sync(0xffffffffu, inc, 31);\n";
     os << "                unsigned long long g = 0ull;\n";
-    os << "                if (lane == 31 && tot) g = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
-    os << "                g = __shfl_sync(0xffffffffu, g, 31) + (unsigned long long)(inc - vq_n3);\n";
+    if (block_claim) {
+        os << "                if (lane == 31) vq_wsum[vq_par][warp] = (unsigned)tot;\n";
+        os << "                __syncthreads();\n";
+        os << "                if (warp == 0) {\n";
+        os << "                    const unsigned t = lane < (int)(blockDim.x >> 5) ? vq_wsum[vq_par][lane] : 0u;\n";
+        os << "                    unsigned s = t;\n";
+        os << "                    for (int o = 1; o < 32; o <<= 1) { const unsigned u = __shfl_up_sync(0xffffffffu, s, o); if (lane >= o) s += u; }\n";
+        os << "                    unsigned long long b = 0ull;\n";
+        os << "                    if (lane == 31 && s) b = atomicAdd(P.jnkeys, (unsigned long long)s);\n";
+        os << "                    b = __shfl_sync(0xffffffffu, b, 31);\n";
+        os << "                    if (lane < (int)(blockDim.x >> 5)) vq_wsum[vq_par][lane] = s - t;\n";
+        os << "                    if (lane == 0) vq_gb[vq_par] = b;\n";
+        os << "                }\n";
+        os << "                __syncthreads();\n";
+        os << "                g = vq_gb[vq_par] + (unsigned long long)vq_wsum[vq_par][warp] + (unsigned long long)(inc - vq_n3);\n";
+        os << "                vq_par ^= 1;\n";
+    } else {
+        os << "                if (lane == 31 && tot) g = atomicAdd(P.jnkeys, (unsigned long long)tot);\n";
+        os << "                g = __shfl_sync(0xffffffffu, g, 31) + (unsigned long long)(inc - vq_n3);\n";
+    }
     os << "#pragma unroll\n                for (int k = 0; k < 4; k++) {\n";
     os << "                    if (!vq_ok3[k]) continue;\n";
     os << "                    P.dmap[vq_d3[k]] = (unsigned long long)(unsigned)(r0 + k) | ((unsigned long long)(unsigned)(~(int)g) << 32);\n";
@@ -2499,7 +2523,23 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "    unsigned long long vq_nrows = 0ull;\n";
     os << "    unsigned vq_nk = 0u;  // mode 2: fresh keys of this lane\n";
     os << "    if (threadIdx.x == 0) vq_nkeys = 0u;\n    __syncthreads();\n";
-    loop.open(os);
+    // every warp of a block walks the same number of chunks (the TMA-staged
+    // tile loop, or the plain chunk loop below with warps past the end idle),
+    // so the direct build's group numbers are claimed once per block
+    const bool block_claim = p.block_claim && (loop.staged || !p.pipeline);
+    if (block_claim) os << "    __shared__ unsigned vq_wsum[2][32];\n    __shared__ unsigned long long vq_gb[2];\n    int vq_par = 0;\n";
+    if (block_claim && !loop.staged) {
+        os << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+        os << "    for (long long vb = (long long)blockIdx.x * (blockDim.x >> 5); vb < P.nchunks; vb += (long long)gridDim.x * (blockDim.x >> 5)) {\n";
+        os << "        const long long c = vb + warp;\n";
+        os << "        long long s0 = 0, s1 = 0, r0 = 0;\n";
+        emit_declare_regs(os, p.bt, cols, "cv", "cm", "        ");
+        os << "        if (c < P.nchunks) {\n            " << seg_lookup("c", "s0", "s1", "r0");
+        emit_loads(os, p, p.bt, cols, "cv", "cm", "r0", "            ", false);
+        os << "        }\n";
+    } else {
+        loop.open(os);
+    }
     // mode 2 (keys unique in the last build): insert straight into the probe's
     // 16-byte slots; a lane's fresh slots wait in registers for their group
     // numbers, claimed once per warp and chunk
@@ -2563,7 +2603,7 @@ static std::string gen_build_kernel(Plan& p, int key_node, int block) {
     os << "                if (js != VQ_NOSLOT) P.jrows[P.jstart[js] + atomicAdd(P.jfill + js, 1)] = (int)r;\n";
     os << "            }\n";
     os << "        }\n";
-    emit_direct_build_tail(os);
+    emit_direct_build_tail(os, block_claim);
     // mode 2 with group numbers (GROUP BY the join key): one claim per warp
     os << "        if (P.mode == 2 && P.jgid) {\n";
     os << "            int inc = vq_nf;\n";
@@ -3014,6 +3054,8 @@ static void choose_tunables(Plan& p) {
         if (dm >= 0) p.dmap_on = dm != 0;
         const int sp = get("spec=");
         if (sp >= 0) p.spec_on = sp != 0;
+        const int bc = get("bclaim=");
+        if (bc >= 0) p.block_claim = bc != 0;
         if (gs >= 0) p.grid_per_sm = gs;
         const int lb = get("limbs=");
         if (lb >= 0) p.cache_limbs = lb != 0;

@@ -2,6 +2,8 @@
 // generated scan kernels.
 #pragma once
 
+#include <functional>
+
 #include "internal.h"
 
 namespace vq {
@@ -156,6 +158,7 @@ struct Plan {
     int radix_bits = 0;
     // tunables of the generated scan kernel (chosen at compile time)
     int block = 256;
+    bool block_claim = true;   // direct join build: group numbers claimed once per block and chunk step
     bool pipeline = true;
     bool staged = true;        // TMA bulk-copy staging of row tiles into shared memory
     bool regs_pred = true;     // register path: branch-free predicated updates
@@ -213,6 +216,11 @@ struct Plan {
     void* h_stage_mapped = nullptr;        // its device address (null: not addressable, copy back)
     void* h_stage_mapped_for = nullptr;    // the staging allocation that address belongs to
     bool regs_err_clean = false;           // register path: the error word is zero (the merge clears it)
+    // a submitted register-path run whose result has not been read: its
+    // output is in h_stage until the result settles (the next run of the
+    // plan, or its destruction, settles it first)
+    vexq_result_s* pending = nullptr;
+    bool submit_lazy = false;              // set for the duration of a vexq_plan_submit call
     ScanMemo scan_memo;                    // main-table pruning of the last run's row-group range
     ScanMemo build_memo;                   // join build side's pruning (whole table), until its zone maps change
     long long hash_groups_seen = -1;       // hash path: groups the last run found (sizes the next table)
@@ -326,6 +334,16 @@ int64_t scanned_bytes(const Plan& p, const Table& t, long long rows, bool build)
 long long estimate_groups(const Plan& p, long long rows, long long join_keys);
 void set_columns(VQParams& P, const Table& t, bool build_side);
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end);
+// The same run, returning as soon as its launches are queued when the plan
+// takes the register path (no join, no shard partial): the result settles
+// on its first read. Any other plan returns a finished result.
+vexq_result_s* run_plan_submit(Plan& p, int rg_start, int rg_end);
+// Waits for a submitted run and fills its result (nothing for a finished
+// one); throws the run's status, which the result keeps.
+void settle(vexq_result_s* r);
+// Settles the plan's pending result before its buffers are used again; a
+// failure stays with that result (its next read returns it).
+void settle_pending(Plan& p);
 // One plain run of a plan at a time: its group/join tables are per plan.
 std::mutex& plan_mutex(Plan* p);
 // VEXQ_SYNC_CHECK=1: synchronise after every launch and name the kernel on
@@ -418,6 +436,14 @@ void drop_host_mirror(const Table* t);
 }  // namespace vq
 
 struct vexq_result_s {
+    // a submitted run not yet waited for (vexq_plan_submit): the first read
+    // waits for its kernels and fills the fields below; owner is the plan
+    // whose staging buffer holds its output until then. A run that failed
+    // keeps its status, returned by every later read.
+    std::function<void(vexq_result_s*)> settle_fn;
+    vq::Plan* owner = nullptr;
+    int32_t settle_code = 0;
+    std::string settle_msg;
     std::vector<vq::OutColumn> cols;
     int64_t nrows = 0;
     int64_t pos = 0;
