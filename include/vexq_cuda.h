@@ -273,6 +273,20 @@ int32_t vexq_zone_prune(vexq_plan_t p, uint8_t* out_mask, int32_t n_rg);
  * returns the merged result on the host. Synchronous on the plan's stream. */
 int32_t vexq_plan_run(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_result_t* out);
 
+/* Submits the same run and returns once its launches are queued, when the
+ * plan takes the register path (no join); any other plan returns a finished
+ * result as vexq_plan_run does. The first read of the result
+ * (vexq_result_info, _num_rows, _num_cols, _next, _stats, _scan_ms) waits
+ * for the run and returns its status, as the reference's aggregate does its
+ * work and reports its error in the first Next
+ * (ParallelHashAggregate.Next, exec/parallel.go:109-120). The plan's next
+ * run, vexq_plan_set_having and vexq_plan_destroy settle a pending result
+ * first; freeing it unread drops it. Runs of different plans submitted on
+ * one stream execute back to back while the host reads the earlier ones.
+ * A table is refilled (vexq_plan_run_host) only while no run over it is
+ * pending on another stream. */
+int32_t vexq_plan_submit(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_result_t* out);
+
 /* Same as vexq_plan_run, but the plan's table columns are first re-filled
  * from the given HOST buffers (same layout as at upload) inside the call:
  * the end-to-end form used when the caller owns the data in host memory. */

@@ -148,7 +148,7 @@ EXPORTS = [
     "vexq_table_device_bytes", "vexq_table_zone_map", "vexq_table_dict_size",
     "vexq_table_dict_entry", "vexq_table_load_vxq", "vexq_vxq_verify",
     "vexq_agg_plan_create", "vexq_join_plan_create", "vexq_plan_destroy",
-    "vexq_plan_explain", "vexq_plan_set_having", "vexq_zone_prune", "vexq_plan_run", "vexq_plan_run_host",
+    "vexq_plan_explain", "vexq_plan_set_having", "vexq_zone_prune", "vexq_plan_run", "vexq_plan_submit", "vexq_plan_run_host",
     "vexq_result_num_rows", "vexq_result_num_cols", "vexq_result_next",
     "vexq_result_free", "vexq_result_stats", "vexq_result_scan_ms", "vexq_result_info", "vexq_plan_set_stream",
     "vexq_filter_run", "vexq_selvec_from_bits",
@@ -208,6 +208,7 @@ def load() -> C.CDLL:
         "vexq_plan_set_having": (i32, [vp, C.POINTER(Expr), i32, C.POINTER(i32), i32, i32, i32]),
         "vexq_zone_prune": (i32, [vp, C.POINTER(C.c_uint8), i32]),
         "vexq_plan_run": (i32, [vp, i32, i32, C.POINTER(vp)]),
+        "vexq_plan_submit": (i32, [vp, i32, i32, C.POINTER(vp)]),
         "vexq_plan_run_host": (i32, [vp, C.POINTER(ColumnDesc), i32, C.POINTER(vp)]),
         "vexq_result_num_rows": (i32, [vp, C.POINTER(i64)]),
         "vexq_result_num_cols": (i32, [vp, C.POINTER(i32)]),

@@ -156,6 +156,7 @@ int32_t vexq_join_plan_create(vexq_table_t build, vexq_table_t probe, const vexq
 int32_t vexq_plan_destroy(vexq_plan_t p) {
     return guard([&]() -> int32_t {
         if (!p) return VEXQ_OK;
+        settle_pending(*p->p);  // a submitted run's result stays readable without its plan
         delete p->p;
         delete p;
         return VEXQ_OK;
@@ -169,6 +170,7 @@ int32_t vexq_plan_set_having(vexq_plan_t p, const vexq_expr* nodes, int32_t nnod
     return guard([&]() -> int32_t {
         if (!p) fail(VEXQ_EINVAL, "null plan");
         std::lock_guard<std::mutex> lk(plan_mutex(p->p));
+        settle_pending(*p->p);  // a submitted run settles under the HAVING it ran with
         set_having(*p->p, nodes, nnodes, children, nchildren, predicate, visible);
         return VEXQ_OK;
     });
@@ -192,6 +194,14 @@ int32_t vexq_plan_run(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_resu
     });
 }
 
+int32_t vexq_plan_submit(vexq_plan_t p, int32_t rg_start, int32_t rg_end, vexq_result_t* out) {
+    return guard([&]() -> int32_t {
+        if (!p || !out) fail(VEXQ_EINVAL, "null argument");
+        *out = run_plan_submit(*p->p, rg_start, rg_end);
+        return VEXQ_OK;
+    });
+}
+
 int32_t vexq_plan_run_host(vexq_plan_t p, const vexq_column_desc* cols, int32_t ncols, vexq_result_t* out) {
     return guard([&]() -> int32_t {
         if (!p || !out || !cols) fail(VEXQ_EINVAL, "null argument");
@@ -200,56 +210,77 @@ int32_t vexq_plan_run_host(vexq_plan_t p, const vexq_column_desc* cols, int32_t 
     });
 }
 
+// Every read of a result settles a submitted run first (vq::settle): it waits
+// for the run's kernels and returns the run's status.
 int32_t vexq_result_num_rows(vexq_result_t r, int64_t* out) {
-    if (!r || !out) return VEXQ_EINVAL;
-    *out = r->nrows;
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!r || !out) return VEXQ_EINVAL;
+        settle(r);
+        *out = r->nrows;
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_result_num_cols(vexq_result_t r, int32_t* out) {
-    if (!r || !out) return VEXQ_EINVAL;
-    *out = (int32_t)r->cols.size();
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!r || !out) return VEXQ_EINVAL;
+        settle(r);
+        *out = (int32_t)r->cols.size();
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_result_next(vexq_result_t r, vexq_batch_view* out) {
     return guard([&]() -> int32_t {
         if (!r || !out) fail(VEXQ_EINVAL, "null argument");
+        settle(r);
         return result_next(r, out);
     });
 }
 
 int32_t vexq_result_free(vexq_result_t r) {
+    // a submitted run freed unread: its plan stops waiting for it (the kernels
+    // finish on the stream before the plan's next run reuses the buffers)
+    if (r && r->owner && r->owner->pending == r) r->owner->pending = nullptr;
     delete r;
     return VEXQ_OK;
 }
 
 int32_t vexq_result_stats(vexq_result_t r, double* kernel_ms, int32_t* launches, int64_t* rows_scanned,
                           int64_t* bytes_scanned) {
-    if (!r) return VEXQ_EINVAL;
-    if (kernel_ms) *kernel_ms = r->kernel_ms;
-    if (launches) *launches = r->launches;
-    if (rows_scanned) *rows_scanned = r->rows_scanned;
-    if (bytes_scanned) *bytes_scanned = r->bytes_scanned;
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!r) return VEXQ_EINVAL;
+        settle(r);
+        if (kernel_ms) *kernel_ms = r->kernel_ms;
+        if (launches) *launches = r->launches;
+        if (rows_scanned) *rows_scanned = r->rows_scanned;
+        if (bytes_scanned) *bytes_scanned = r->bytes_scanned;
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_result_scan_ms(vexq_result_t r, double* out) {
-    if (!r || !out) return VEXQ_EINVAL;
-    *out = r->scan_ms;
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!r || !out) return VEXQ_EINVAL;
+        settle(r);
+        *out = r->scan_ms;
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_result_info(vexq_result_t r, vexq_result_summary* out) {
-    if (!r || !out) return VEXQ_EINVAL;
-    out->nrows = r->nrows;
-    out->ncols = (int32_t)r->cols.size();
-    out->launches = r->launches;
-    out->kernel_ms = r->kernel_ms;
-    out->scan_ms = r->scan_ms;
-    out->rows_scanned = r->rows_scanned;
-    out->bytes_scanned = r->bytes_scanned;
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!r || !out) return VEXQ_EINVAL;
+        settle(r);
+        out->nrows = r->nrows;
+        out->ncols = (int32_t)r->cols.size();
+        out->launches = r->launches;
+        out->kernel_ms = r->kernel_ms;
+        out->scan_ms = r->scan_ms;
+        out->rows_scanned = r->rows_scanned;
+        out->bytes_scanned = r->bytes_scanned;
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_plan_set_stream(vexq_plan_t p, void* stream) {

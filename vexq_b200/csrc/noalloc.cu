@@ -79,6 +79,7 @@ void run_global_noalloc(Plan& p, int rg_start, int rg_end, cudaStream_t s, int64
         fail(VEXQ_EINVAL, "n_out is " + std::to_string(n_out) + " but the plan has " + std::to_string(p.outs.size()) +
                               " output columns");
     if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
+    settle_pending(p);  // a submitted run of this plan finishes reading its staging buffer first
     Table& t = *p.t;
     int dev = -1;
     VQ_CUDA(cudaGetDevice(&dev));

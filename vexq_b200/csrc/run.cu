@@ -640,10 +640,18 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-// Register path over prepared params: launch, merge, one copy back, one sync.
-Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
+// A register-path run whose launches are queued: what collecting it needs.
+struct RegsPending {
+    size_t nout_f = 0, nout_i = 0;
+    bool mapped = false;
+    int launches = 0;
+    bool lazy = false;  // an event after the copy back marks the run's end (other runs may follow on the stream)
+};
+
+// Register path over prepared params: launch, merge, one copy back; the sync
+// and the decode are regs_collect's.
+static RegsPending regs_launch(RunCtx& rc, VQParams& P, long long nchunks, bool lazy) {
     Plan& p = rc.p;
-    Groups g;
     int G = (int)p.domain, nf = p.nf, ni = p.ni;
     int nfb = std::max(nf, 1);
     const JitKernel& K = rc.k ? *rc.k : p.k_main;
@@ -815,13 +823,30 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         }
     }
     if (!mapped) VQ_CUDA(cudaMemcpyAsync(p.h_stage.p, p.scratch_c.p, nout_f + nout_i + 4, cudaMemcpyDeviceToHost, rc.s));
-    VQ_CUDA(cudaStreamSynchronize(rc.s));
+    if (lazy) VQ_CUDA(cudaEventRecord(p.ev[3], rc.s));
+    RegsPending q;
+    q.nout_f = nout_f;
+    q.nout_i = nout_i;
+    q.mapped = mapped != nullptr;
+    q.launches = fused || last ? 1 : 2;
+    q.lazy = lazy;
+    return q;
+}
+
+// Waits for a queued register-path run and decodes its merged row.
+static Groups regs_collect(RunCtx& rc, const RegsPending& q) {
+    Plan& p = rc.p;
+    Groups g;
+    const int G = (int)p.domain, nf = p.nf, ni = p.ni;
+    const size_t nout_f = q.nout_f, nout_i = q.nout_i;
+    if (q.lazy) VQ_CUDA(cudaEventSynchronize(p.ev[3]));
+    else VQ_CUDA(cudaStreamSynchronize(rc.s));
     p.regs_err_clean = true;
     check_regs_flags(*(const int*)((const char*)p.h_stage.p + nout_f + nout_i));
     const float span = elapsed(p.ev[0], p.ev[2]);  // the scan and the merge (overlapping its drain, or inside it)
     rc.scan_ms += span;
     rc.kernel_ms += span;
-    rc.launches += fused || last ? 1 : 2;
+    rc.launches += q.launches;
     const double* hf = (const double*)p.h_stage.p;
     const long long* hi = (const long long*)((const char*)p.h_stage.p + nout_f);
     g.ival.assign(ni, {});
@@ -835,6 +860,11 @@ Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
         for (int s = 0; s < nf; s++) g.fval[s].push_back(hf[(size_t)gi * nf + s]);
     }
     return g;
+}
+
+Groups run_regs(RunCtx& rc, VQParams& P, long long nchunks) {
+    const RegsPending q = regs_launch(rc, P, nchunks, false);
+    return regs_collect(rc, q);
 }
 
 // Atomic path: group table, main kernel (retried with a larger table when a
@@ -1542,6 +1572,64 @@ static vexq_result_s* finish_groups(RunCtx& rc, VQParams& P, long long nchunks, 
     return r;
 }
 
+cudaStream_t plan_stream(Plan& p);
+
+// A submitted register-path run: the launches are queued and the result
+// settles on its first read (the sync, the merged row's decode and the
+// result columns), so the host prepares the next run while this one runs.
+static vexq_result_s* submit_regs(RunCtx& rc, VQParams& P, long long nchunks) {
+    Plan& p = rc.p;
+    const RegsPending q = regs_launch(rc, P, nchunks, true);
+    auto* r = new vexq_result_s;
+    Plan* pp = &p;
+    const float k0 = rc.kernel_ms, s0 = rc.scan_ms;
+    const int l0 = rc.launches;
+    r->settle_fn = [pp, q, k0, s0, l0](vexq_result_s* res) {
+        RunCtx rc2{*pp, plan_stream(*pp)};
+        rc2.kernel_ms = k0;
+        rc2.scan_ms = s0;
+        rc2.launches = l0;
+        Groups g = regs_collect(rc2, q);
+        std::unique_ptr<vexq_result_s> full(build_result(*pp, g));
+        const int64_t rows = res->rows_scanned, bytes = res->bytes_scanned;
+        *res = std::move(*full);
+        res->rows_scanned = rows;
+        res->bytes_scanned = bytes;
+        res->kernel_ms = rc2.kernel_ms;
+        res->scan_ms = rc2.scan_ms;
+        res->launches = rc2.launches;
+    };
+    r->owner = pp;
+    p.pending = r;
+    return r;
+}
+
+void settle(vexq_result_s* r) {
+    if (!r) return;
+    if (r->settle_code) fail(r->settle_code, r->settle_msg);
+    if (!r->settle_fn) return;
+    std::function<void(vexq_result_s*)> f = std::move(r->settle_fn);
+    r->settle_fn = nullptr;
+    if (r->owner && r->owner->pending == r) r->owner->pending = nullptr;
+    r->owner = nullptr;
+    try {
+        f(r);
+    } catch (const Status& e) {
+        r->settle_code = e.code;
+        r->settle_msg = e.what();
+        throw;
+    }
+}
+
+void settle_pending(Plan& p) {
+    if (!p.pending) return;
+    try {
+        settle(p.pending);
+    } catch (const Status&) {
+        // kept in the pending result: its next read returns the status
+    }
+}
+
 void note_hot_groups(Plan& p, const Groups& g) {
     if (p.hot_n <= 0 || p.path != AggPath::Dense || p.is_join || g.key.empty()) return;
     int cs = -1;
@@ -1698,6 +1786,7 @@ void force_join_spec(Plan& p, long long keys_seen) {
 }
 
 vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
+    settle_pending(p);  // the last submitted run's output is still in the staging buffer
     if (p.cancel.load()) { p.cancel = false; fail(VEXQ_ECANCELED, "plan cancelled"); }
     check_ranges(p);
     RunCtx rc{p, plan_stream(p)};
@@ -2158,6 +2247,12 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
         r->launches = rc.launches;
     } else {
         long long est = estimate_groups(p, ss.rows, join_keys);
+        if (p.submit_lazy && p.path == AggPath::Regs && !p.is_join && !p.partial_out && !rc.k) {
+            r = submit_regs(rc, P, ss.nchunks);
+            r->rows_scanned = rows_scanned;
+            r->bytes_scanned = bytes;
+            return r;
+        }
         try {
             r = finish_groups(rc, P, ss.nchunks, est, ss.rows);
         } catch (const SpecRetry& e) {
@@ -2173,6 +2268,15 @@ vexq_result_s* run_plan(Plan& p, int rg_start, int rg_end) {
     r->rows_scanned = rows_scanned;
     r->bytes_scanned = bytes;
     return r;
+}
+
+vexq_result_s* run_plan_submit(Plan& p, int rg_start, int rg_end) {
+    struct Lazy {
+        Plan& p;
+        explicit Lazy(Plan& q) : p(q) { p.submit_lazy = true; }
+        ~Lazy() { p.submit_lazy = false; }
+    } lazy(p);
+    return run_plan(p, rg_start, rg_end);
 }
 
 vexq_result_s* run_plan_host(Plan& p, const vexq_column_desc* cols, int32_t ncols) {

@@ -130,15 +130,30 @@ def _decode(t: int, raw: bytes, n: int):
 
 
 class Result:
-    """A finished run: Next()-style batches plus device timing."""
+    """A run's result: Next()-style batches plus device timing. A submitted
+    run (lazy) waits for its kernels at its first read, which raises the
+    run's error if it failed."""
 
-    def __init__(self, h: C.c_void_p):
+    def __init__(self, h: C.c_void_p, lazy: bool = False):
         self.h = h
-        s = abi.ResultSummary()
-        abi.check(abi.load().vexq_result_info(h, C.byref(s)))
-        self.nrows, self.ncols = s.nrows, s.ncols
-        self.kernel_ms, self.launches, self.rows_scanned, self.bytes_scanned = s.kernel_ms, s.launches, s.rows_scanned, s.bytes_scanned
-        self.scan_ms = s.scan_ms
+        self._info = None
+        if not lazy:
+            self.wait()
+
+    def wait(self) -> "Result":
+        if self._info is None:
+            s = abi.ResultSummary()
+            abi.check(abi.load().vexq_result_info(self.h, C.byref(s)))
+            self._info = s
+        return self
+
+    nrows = property(lambda self: self.wait()._info.nrows)
+    ncols = property(lambda self: self.wait()._info.ncols)
+    kernel_ms = property(lambda self: self.wait()._info.kernel_ms)
+    scan_ms = property(lambda self: self.wait()._info.scan_ms)
+    launches = property(lambda self: self.wait()._info.launches)
+    rows_scanned = property(lambda self: self.wait()._info.rows_scanned)
+    bytes_scanned = property(lambda self: self.wait()._info.bytes_scanned)
 
     def next(self) -> Optional[Batch]:
         """Operator.Next: ≤1024 rows, None at EOF."""
@@ -201,6 +216,13 @@ class _PlanOp:
         h = C.c_void_p()
         abi.check(abi.load().vexq_plan_run(self.h, rg_start, rg_end, C.byref(h)))
         return Result(h)
+
+    def submit(self, rg_start: int = 0, rg_end: int = -1) -> Result:
+        """vexq_plan_submit: returns once the run's launches are queued; the
+        result waits for them at its first read."""
+        h = C.c_void_p()
+        abi.check(abi.load().vexq_plan_submit(self.h, rg_start, rg_end, C.byref(h)))
+        return Result(h, lazy=True)
 
     def run_host(self, table: HostTable) -> Result:
         """End-to-end form: refills the columns from host buffers, then runs."""
