@@ -720,8 +720,9 @@ def main():
     tr = profile_traffic().get("q1_scan_dram_bytes_per_launch")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": tr, "peak_source": f"{src} hbm_gbs",
-            "kernel": ("vq_agg (Q1 scan-filter-project-aggregate) and the partial merge launched as its programmatic "
-                       "dependent, which writes the merged row into pinned host memory (one event span)"),
+            "kernel": ("vq_agg (Q1 scan-filter-project-aggregate, one launch: every block adds its partials as exact "
+                       "fixed-point atomics into one of 8 accumulator copies and the last block to finish writes the "
+                       "merged row into pinned host memory; one event span)"),
             "q6_kernel_gbs": round(stats[0][1] / (q6_scan / 1e3) / 1e9, 1)}
     if rank == 0:
         line = {

@@ -198,9 +198,9 @@ def fused_aggs():
 
 def test_merge_inside_the_scan_resets_between_runs(gpu_lib, monkeypatch):
     """Sums of finite bounded floats, integer sums, integer MIN/MAX and counts:
-    the scan merges its own block partials (global accumulators, the last
-    block writes the row and restores the identities; forced here for six
-    groups, which by default keep the merge kernel). Repeated runs, runs over
+    the scan merges its own block partials (global accumulators in 8 copies,
+    block b adding into copy b % 8; the last block folds the copies, writes
+    the row and restores the identities). Repeated runs, runs over
     sub-ranges of row groups and a run that prunes every row group each match
     the oracle, so nothing of one run leaks into the next."""
     X = gpu_lib
@@ -262,8 +262,10 @@ def test_float_min_max_keep_the_merge_kernel(gpu_lib):
 
 
 def test_merge_placement_by_accumulator_count(gpu_lib, monkeypatch):
-    """Default placement: a one-group sum and count merges inside the scan;
-    six groups of eight accumulators keep the merge kernel."""
+    """Default placement: a one-group sum and count merges inside the scan
+    into one set of accumulators; six groups of eight (84 atomics a block)
+    merge inside the scan into 8 copies; a bank of more than 128 atomics a
+    block keeps the merge kernel."""
     X = gpu_lib
     monkeypatch.delenv("VEXQ_TUNE", raising=False)
     host = key_table(200_000, 12)
@@ -273,5 +275,17 @@ def test_merge_placement_by_accumulator_count(gpu_lib, monkeypatch):
     r = R.agg(R.RefTable(host), small, workers=0)
     assert_rows_match(g.rows(), r.rows(), ordered=True)
     assert_float_vs_exact(g.rows(), r)
-    g, ex = run(X, host, P.AggPlan(None, [0, 1], fused_aggs()))
-    assert "merge=kernel" in ex, ex
+    assert "rcopies" not in ex, ex
+    six = P.AggPlan(None, [0, 1], fused_aggs())
+    g, ex = run(X, host, six)
+    assert "merge=in_scan" in ex and "rcopies=8" in ex, ex
+    r = R.agg(R.RefTable(host), six, workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_float_vs_exact(g.rows(), r)
+    wide = P.AggPlan(None, [0, 1], fused_aggs() + [P.sum_(P.col(2) * 2.0, "s2"), P.sum_(P.col(2) * 3.0, "s3"),
+                                                  P.sum_(P.col(2) * 4.0, "s4")])
+    g, ex = run(X, host, wide)
+    assert "merge=kernel" in ex, ex  # 6 groups x (6 float sums x 3 digits + 5 integers) = 138 atomics a block
+    r = R.agg(R.RefTable(host), wide, workers=0)
+    assert_rows_match(g.rows(), r.rows(), ordered=True)
+    assert_float_vs_exact(g.rows(), r)

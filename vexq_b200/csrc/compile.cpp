@@ -1165,9 +1165,10 @@ static void choose_regs_forms(Plan& p) {
 // depend on the order in which blocks finish, and integer sums, MIN, MAX and
 // first-row keys are order-free as atomics. Float MIN/MAX keep the merge
 // kernel, whose fold in block order keeps the first of two equal extremes
-// (+0 against -0), and so do plans with many accumulators, where the merge
-// kernel measured faster. VEXQ_TUNE "rfuse=0" keeps the merge kernel for
-// measurement, "rfuse=2" folds any eligible plan into the scan.
+// (+0 against -0), and so do plans whose blocks would add more than 128
+// atomics. VEXQ_TUNE "rfuse=0" keeps the merge kernel for measurement,
+// "rfuse=2" folds any eligible plan into the scan, "rcopies=K" sets the
+// accumulator copies.
 static void choose_regs_fused(Plan& p) {
     p.rfused = false;
     if (p.path != AggPath::Regs || p.is_join || !p.t || p.nf > 16) return;
@@ -1180,11 +1181,15 @@ static void choose_regs_fused(Plan& p) {
     if (force == 0) return;
     // atomics a block adds: up to three fixed-point digits a float sum, one
     // a counter. 6M-row scans: one group of 2 entries (5 atomics) 37.4 us in
-    // the scan against 39.5 us with the merge kernel; six groups of 8 (108)
-    // 66.5 us against 60.3 us (every block arrives at once, so the atomics
-    // on the same few L2 lines serialise)
+    // the scan against 39.5 us with the merge kernel. Six groups of 8 (108,
+    // the Q1 shape): every block arrives at once and the atomics on the same
+    // few L2 lines serialise, so the blocks add into 8 copies of the
+    // accumulators (block b into copy b % 8): 59.2 us against 63.2 us with
+    // the merge kernel and 63.6 us with one copy (4, 16 copies: 59.8, 59.6;
+    // the 5-atomic Q6 shape is fastest with one copy, 34.8 against 35.0 with
+    // 8). Larger banks keep the merge kernel (unmeasured).
     const int64_t atomics = p.domain * (3 * (int64_t)p.nf + p.ni + 1);
-    if (atomics > 16 && force != 2) return;
+    if (atomics > 128 && force != 2) return;
     std::vector<int> lsb(std::max(p.nf, 1), 0);
     for (size_t s = 0; s < p.slots.size(); s++) {
         const Slot& sl = p.slots[s];
@@ -1200,6 +1205,7 @@ static void choose_regs_fused(Plan& p) {
     }
     p.fx_lsb = lsb;
     p.rfused = true;
+    if (p.rcopies == 0) p.rcopies = atomics > 16 ? 8 : 1;
 }
 
 // The predicated update of an aggregate scan writes first-row keys only on a
@@ -1402,19 +1408,24 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
     // with an exchange that also restores its identity for the next run
     const bool fused = p.rfused && !fc.dyn_smem;
     if (fused) {
-        const int NF = std::max(nf, 1), NI1 = ni + 1;
+        // K copies of the accumulators, block b adding into copy b % K, so
+        // the blocks that finish together spread their atomics over K times
+        // the L2 lines; the last block folds the copies (exact integer adds,
+        // or min / max)
+        const int NF = std::max(nf, 1), NI1 = ni + 1, K = std::max(1, p.rcopies);
         os << "    if (P.racc_i) {\n";
+        os << "        const int vq_cp = (int)(blockIdx.x % " << K << "u);\n";
         os << "        for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
         os << "            const int s = t % " << NF << ";\n";
         os << "            double v = sh_f[0][t];\n";
         os << "            for (int w = 1; w < " << warps << "; w++) v = vq_fcomb(" << fc.kinds << "fkind(s), v, sh_f[w][t]);\n";
-        os << "            vq_fx_add<true>(P.racc_fx + (long long)t * 4, v, P.fx_lsb[s], P.racc_sp + t, P.error);\n";
+        os << "            vq_fx_add<true>(P.racc_fx + ((long long)vq_cp * " << G * nf << " + t) * 4, v, P.fx_lsb[s], P.racc_sp + t, P.error);\n";
         os << "        }\n";
         os << "        for (int t = threadIdx.x; t < " << G * NI1 << "; t += blockDim.x) {\n";
         os << "            const int s = t % " << NI1 << ";\n";
         os << "            long long v = sh_i[0][t];\n";
         os << "            for (int w = 1; w < " << warps << "; w++) v = vq_icomb(" << fc.kinds << "ikind(s), v, sh_i[w][t]);\n";
-        os << "            vq_racc_add(P.racc_i + t, " << fc.kinds << "ikind(s), v);\n";
+        os << "            vq_racc_add(P.racc_i + (long long)vq_cp * " << G * NI1 << " + t, " << fc.kinds << "ikind(s), v);\n";
         os << "        }\n";
         os << "        __threadfence();\n";
         os << "        __syncthreads();\n";
@@ -1424,14 +1435,22 @@ void emit_regs_flush(std::ostringstream& os, const Plan& p, int block, const Flu
         os << "        if (vq_rlast) {\n";
         os << "            __threadfence();\n";
         os << "            for (int t = threadIdx.x; t < " << G * nf << "; t += blockDim.x) {\n";
-        os << "                vq_i64 c[4];\n";
+        os << "                vq_i64 c[4] = {0, 0, 0, 0};\n";
+        os << "                for (int k = 0; k < " << K << "; k++)\n";
         os << "#pragma unroll\n";
-        os << "                for (int d = 0; d < 4; d++) c[d] = (vq_i64)atomicExch((unsigned long long*)(P.racc_fx + (long long)t * 4 + d), 0ull);\n";
+        os << "                    for (int d = 0; d < 4; d++)\n";
+        os << "                        c[d] = (vq_i64)((vq_u64)c[d] + atomicExch((unsigned long long*)(P.racc_fx + ((long long)k * " << G * nf
+           << " + t) * 4 + d), 0ull));\n";
         os << "                P.rout_f[t] = vq_fx_result(c, P.fx_lsb[t % " << NF << "], atomicExch(P.racc_sp + t, 0u));\n";
         os << "            }\n";
-        os << "            for (int t = threadIdx.x; t < " << G * NI1 << "; t += blockDim.x)\n";
-        os << "                P.rout_i[t] = (long long)atomicExch((unsigned long long*)(P.racc_i + t), (unsigned long long)vq_racc_identity("
-           << fc.kinds << "ikind(t % " << NI1 << ")));\n";
+        os << "            for (int t = threadIdx.x; t < " << G * NI1 << "; t += blockDim.x) {\n";
+        os << "                const int kd = " << fc.kinds << "ikind(t % " << NI1 << ");\n";
+        os << "                vq_i64 v = vq_racc_identity(kd);\n";
+        os << "                for (int k = 0; k < " << K << "; k++)\n";
+        os << "                    v = vq_icomb(kd, v, (vq_i64)atomicExch((unsigned long long*)(P.racc_i + (long long)k * " << G * NI1
+           << " + t), (unsigned long long)vq_racc_identity(kd)));\n";
+        os << "                P.rout_i[t] = (long long)v;\n";
+        os << "            }\n";
         os << "            if (threadIdx.x == 0) {\n";
         os << "                *P.rerr_out = atomicExch(P.error, 0);\n";
         os << "                atomicExch(P.racc_done, 0u);\n";
@@ -3056,6 +3075,10 @@ static void choose_tunables(Plan& p) {
         if (sp >= 0) p.spec_on = sp != 0;
         const int bc = get("bclaim=");
         if (bc >= 0) p.block_claim = bc != 0;
+        const int rc = get("rcopies=");
+        if (rc >= 1 && rc <= 64) p.rcopies = rc;
+        const int gr = get("graph=");
+        if (gr == 0) p.graph_off = true;  // register-path runs as direct launches, not a replayed graph
         if (gs >= 0) p.grid_per_sm = gs;
         const int lb = get("limbs=");
         if (lb >= 0) p.cache_limbs = lb != 0;
@@ -3199,6 +3222,7 @@ static void finish_compile(Plan& p, const std::vector<int>& key_nodes, bool join
         }
         ex << " exact_int_sums=" << nx << " fma_sums=" << nm << " shared_sums=" << na;
         ex << " merge=" << (p.rfused ? "in_scan" : "kernel");
+        if (p.rfused && p.rcopies > 1) ex << " rcopies=" << p.rcopies;
     }
     p.k_main = jit_get(p.src_main, "vq_agg", p.block, p.smem);
     ex << " regs=" << p.k_main.regs << " blocks_per_sm=" << p.k_main.max_blocks_per_sm;

@@ -189,6 +189,7 @@ struct Plan {
     // the last block writes the merged row; racc holds those accumulators
     // (kept at their identities between runs) and the arrival counter
     bool rfused = false;
+    int rcopies = 0;  // copies of those accumulators (block b adds into copy b % rcopies); 0: chosen with the fold
     DevBuf racc;
     // HAVING over the merged output (exec.Filter above the aggregate,
     // planner/build.go:59-75): predicate IR over the output columns (group-by

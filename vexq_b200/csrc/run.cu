@@ -711,7 +711,8 @@ static RegsPending regs_launch(RunCtx& rc, VQParams& P, long long nchunks, bool 
         // accumulators at their identities: fixed-point digits and flags 0,
         // integer entries by combiner kind, arrival count 0; the last block
         // of every run restores this state
-        const size_t b_fx = (size_t)G * nf * 32, b_i = (size_t)G * (ni + 1) * 8, b_sp = (size_t)G * nf * 4;
+        const size_t K = (size_t)std::max(1, p.rcopies);  // accumulator copies (block b adds into copy b % K)
+        const size_t b_fx = K * G * nf * 32, b_i = K * G * (ni + 1) * 8, b_sp = (size_t)G * nf * 4;
         if (!p.racc.p) {
             std::vector<unsigned char> img(b_fx + b_i + b_sp + 16, 0);
             std::vector<long long> ident(ni + 1, 0);
@@ -722,8 +723,9 @@ static RegsPending regs_launch(RunCtx& rc, VQParams& P, long long nchunks, bool 
                 ident[p.slot_pos[s]] = kd == S_IMIN ? LLONG_MAX : kd == S_IMAX ? LLONG_MIN : 0;
             }
             long long* ii = (long long*)(img.data() + b_fx);
-            for (int gi = 0; gi < G; gi++)
-                for (int u = 0; u <= ni; u++) ii[(size_t)gi * (ni + 1) + u] = ident[u];
+            for (size_t k = 0; k < K; k++)
+                for (int gi = 0; gi < G; gi++)
+                    for (int u = 0; u <= ni; u++) ii[(k * G + gi) * (ni + 1) + u] = ident[u];
             p.racc.alloc(img.size());
             h2d(p.racc.p, img.data(), img.size(), rc.s);
         }
