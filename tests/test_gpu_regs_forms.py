@@ -282,10 +282,12 @@ def test_merge_placement_by_accumulator_count(gpu_lib, monkeypatch):
     r = R.agg(R.RefTable(host), six, workers=0)
     assert_rows_match(g.rows(), r.rows(), ordered=True)
     assert_float_vs_exact(g.rows(), r)
-    wide = P.AggPlan(None, [0, 1], fused_aggs() + [P.sum_(P.col(2) * 2.0, "s2"), P.sum_(P.col(2) * 3.0, "s3"),
-                                                  P.sum_(P.col(2) * 4.0, "s4")])
+    # eight float sums over six groups (plus the row count the plan keeps):
+    # 6 x 10 accumulators fit the register path, and a block would add
+    # 6 x (8 x 3 digits + the count + the first-row key) = 156 atomics
+    wide = P.AggPlan(None, [0, 1], [P.sum_(P.col(2) * float(c), f"s{c}") for c in range(2, 10)])
     g, ex = run(X, host, wide)
-    assert "merge=kernel" in ex, ex  # 6 groups x (6 float sums x 3 digits + 5 integers) = 138 atomics a block
+    assert "path=regs" in ex and "merge=kernel" in ex, ex
     r = R.agg(R.RefTable(host), wide, workers=0)
     assert_rows_match(g.rows(), r.rows(), ordered=True)
     assert_float_vs_exact(g.rows(), r)

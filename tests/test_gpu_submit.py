@@ -123,3 +123,28 @@ def test_join_submit_returns_finished_result(gpu_lib):
         op.close()
         go.close()
         gi.close()
+
+
+def test_direct_launches_match_the_graph(lineitem, monkeypatch):
+    """VEXQ_TUNE graph=0: the register path's launches go out directly (the
+    path a refused capture falls back to) with the same rows, through run and
+    submit, as the replayed graph."""
+    X, _, gt = lineitem
+    ref = []
+    for pl in (W.q1_plan(), W.q6_plan()):
+        op = X.GpuHashAggregate(gt, pl)
+        try:
+            ref.append(op.run().rows())
+        finally:
+            op.close()
+    monkeypatch.setenv("VEXQ_TUNE", "graph=0")
+    for k, pl in enumerate((W.q1_plan(), W.q6_plan())):
+        op = X.GpuHashAggregate(gt, pl)
+        try:
+            for _ in range(2):
+                assert bits_equal(op.run().rows(), ref[k])
+                r = op.submit()
+                assert bits_equal(r.rows(), ref[k]) and r.kernel_ms > 0
+                r.close()
+        finally:
+            op.close()

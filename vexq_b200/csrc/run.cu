@@ -753,9 +753,11 @@ static RegsPending regs_launch(RunCtx& rc, VQParams& P, long long nchunks, bool 
     }
     bind_distinct(p, P, nchunks * 128, rc.s);
     // the run's launches: start event, scan, merge, end event (events recorded
-    // as external nodes when captured, so a replayed graph still times them)
+    // as external nodes when captured, so a replayed graph still times them;
+    // plain records when launched directly, where the external flag is refused)
     auto launch_all = [&](bool checks) {
-        VQ_CUDA(cudaEventRecordWithFlags(p.ev[0], rc.s, cudaEventRecordExternal));
+        if (checks) VQ_CUDA(cudaEventRecord(p.ev[0], rc.s));
+        else VQ_CUDA(cudaEventRecordWithFlags(p.ev[0], rc.s, cudaEventRecordExternal));
         jit_launch(K, grid, &P, sizeof P, rc.s);
         if (checks) launch_check(rc.s, "p.k_main");
         // no event between the scan and its merge: an event record there stops the
@@ -775,7 +777,8 @@ static RegsPending regs_launch(RunCtx& rc, VQParams& P, long long nchunks, bool 
                                        ni, d_kinds, d_kinds + nfb, out_f, out_i, P.error, err_out));
             if (checks) launch_check(rc.s, "k_merge_regs_dep");
         }
-        VQ_CUDA(cudaEventRecordWithFlags(p.ev[2], rc.s, cudaEventRecordExternal));
+        if (checks) VQ_CUDA(cudaEventRecord(p.ev[2], rc.s));
+        else VQ_CUDA(cudaEventRecordWithFlags(p.ev[2], rc.s, cudaEventRecordExternal));
     };
     // replayed as one CUDA graph while the parameter block and launch shape
     // are those it was captured with: one host call a run instead of four
