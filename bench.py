@@ -518,6 +518,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_config(world, step_bytes):
+    """The `config` object of both arms' line (the same workload, keys and values)."""
+    return {"workload": WORKLOAD, "rows_per_gpu": NROWS, "rg_rows": RG_ROWS,
+            "bytes_per_step_per_gpu": step_bytes, "parallelism": f"replicas{world}",
+            "l2": "inputs (264 MB / 168 MB per query) exceed the 126 MB L2; no flush"}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -543,7 +550,7 @@ def run_reference(args, world, rank):
     q1, q6 = W.q1_plan(), W.q6_plan()
     workers = os.cpu_count() or 1
     step_bytes = 44 * NROWS + 28 * NROWS
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 3)):
         cpu_reference_step(tbl, [q1, q6], workers)
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -555,7 +562,7 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded lineitem-shaped generator)",
-        "config": {"workload": WORKLOAD, "rows": NROWS, "rg_rows": RG_ROWS},
+        "config": workload_config(world, step_bytes),
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": workers, "kind": "port",
                          "sample": f"full workload per step ({NROWS} rows, Q1+Q6), {args.steps} steps"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -730,9 +737,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded lineitem-shaped generator, no TPC-H rows)",
-            "config": {"workload": WORKLOAD, "rows_per_gpu": NROWS, "rg_rows": RG_ROWS,
-                       "bytes_per_step_per_gpu": step_bytes, "parallelism": f"replicas{world}",
-                       "l2": "inputs (264 MB / 168 MB per query) exceed the 126 MB L2; no flush"},
+            "config": workload_config(world, step_bytes),
             "rows_per_s": round(2 * NROWS * world / (ms_step / 1e3), 1),
             "kernel_only_gbs": round(step_bytes / ((q1_scan + q6_scan) / 1e3) / 1e9, 1),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
