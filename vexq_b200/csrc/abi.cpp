@@ -157,6 +157,9 @@ int32_t vexq_plan_destroy(vexq_plan_t p) {
     return guard([&]() -> int32_t {
         if (!p) return VEXQ_OK;
         settle_pending(*p->p);  // a submitted run's result stays readable without its plan
+        // a submitted run freed unread may still be writing the plan's pinned
+        // staging buffer: its end event is waited for before the buffer goes
+        if (p->p->ev[3]) (void)cudaEventSynchronize(p->p->ev[3]);
         delete p->p;
         delete p;
         return VEXQ_OK;
