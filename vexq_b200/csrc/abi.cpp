@@ -287,9 +287,15 @@ int32_t vexq_result_info(vexq_result_t r, vexq_result_summary* out) {
 }
 
 int32_t vexq_plan_set_stream(vexq_plan_t p, void* stream) {
-    if (!p) return VEXQ_EINVAL;
-    p->p->ext_stream = (cudaStream_t)stream;
-    return VEXQ_OK;
+    return guard([&]() -> int32_t {
+        if (!p) return VEXQ_EINVAL;
+        // runs on the old stream finish first: a later run on the new stream
+        // reuses the plan's buffers
+        settle_pending(*p->p);
+        if (p->p->ev[3]) (void)cudaEventSynchronize(p->p->ev[3]);
+        p->p->ext_stream = (cudaStream_t)stream;
+        return VEXQ_OK;
+    });
 }
 
 int32_t vexq_filter_run(vexq_table_t t, const vexq_expr* nodes, int32_t nnodes, const int32_t* children, int32_t nchildren,
