@@ -342,8 +342,9 @@ typedef struct {
 int32_t vexq_result_info(vexq_result_t r, vexq_result_summary* out);
 
 /* Runs a plan on a caller-owned CUDA stream (a cudaStream_t, e.g. the stream
- * the caller times with events); NULL restores the plan's own stream.
- * No reference counterpart: the Go engine has no streams. */
+ * the caller times with events); NULL restores the plan's own stream. A
+ * submitted run still pending settles first, and one freed unread is waited
+ * for. No reference counterpart: the Go engine has no streams. */
 int32_t vexq_plan_set_stream(vexq_plan_t p, void* stream);
 
 /* ---- standalone filter: Filter.Next + BoolToSelVecInto ----------------- */
