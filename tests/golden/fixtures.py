@@ -57,6 +57,8 @@ def expr(e):
         return P.or_(*[expr(x) for x in e[1:]])
     if k == "not":
         return P.not_(expr(e[1]))
+    if k == "neg":
+        return P.neg(expr(e[1]))
     if k == "between":
         return P.between(expr(e[1]), expr(e[2]), expr(e[3]))
     if k == "in":

@@ -18,9 +18,11 @@ NULL = None
 CASES = []
 
 
-def case(name, ref, tables, plan, rows, ordered=False, kind="agg"):
+def case(name, ref, tables, plan, rows, ordered=False, kind="agg", device=True):
+    """device: the case is also part of the GPU known-answer test (False:
+    checked on the oracle only, until the device run of it is recorded)."""
     CASES.append({"name": name, "ref": ref, "kind": kind, "tables": tables, "plan": plan,
-                  "expect": {"ordered": ordered, "rows": rows}})
+                  "expect": {"ordered": ordered, "rows": rows}, "device": device})
 
 
 def strcol(name, rg_dicts, codes, valid=None):
@@ -187,6 +189,58 @@ case("string_min_max_with_count_distinct", "exec/agg_string_fallback_test.go:252
       "aggs": [["MIN", ["col", 1], "lo"], ["MAX", ["col", 1], "hi"], ["COUNT_DISTINCT", ["col", 1], "ndistinct"],
                ["COUNT", ["col", 1], "n"]]},
      [["east", "AIR", "MAIL", 2, 3], ["west", "SHIP", "SHIP", 1, 1]])
+
+
+# exec/expr_eval_test.go:15-57 writeExprTestFile: one row group of n rows,
+# id = i, amount = i * 2.5, status cycling alpha/beta/gamma, order_date =
+# 17000 + i (days). The tests count the rows a WHERE keeps or read projected
+# values; here the counts are COUNT(*) and the projected values SUM(expr)
+# grouped by id (one row a group, so the sum is the row's value).
+def expr_table(n):
+    return {"rg_rows": 65536, "nrows": n, "columns": [
+        col("id", "INT64", list(range(n))),
+        col("amount", "FLOAT64", [i * 2.5 for i in range(n)]),
+        strcol("status", [["alpha", "beta", "gamma"]], [i % 3 for i in range(n)]),
+        col("order_date", "DATE", [17000 + i for i in range(n)])]}
+
+
+COUNT_ONLY = [["COUNT", None, "n"]]
+case("expr_not_string_eq", "exec/expr_eval_test.go:130-148", {"t": expr_table(30)},
+     {"predicate": ["not", ["bin", "EQ", ["col", 2], ["lit", "alpha"]]], "group_by": [], "aggs": COUNT_ONLY},
+     [[20]], device=False)
+case("expr_not_int_gt", "exec/expr_eval_test.go:150-167", {"t": expr_table(30)},
+     {"predicate": ["not", ["bin", "GT", ["col", 0], ["lit", 10]]], "group_by": [], "aggs": COUNT_ONLY},
+     [[11]], device=False)
+case("expr_date_gt_int_literal", "exec/expr_eval_test.go:187-204", {"t": expr_table(30)},
+     {"predicate": ["bin", "GT", ["col", 3], ["lit", 17010]], "group_by": [], "aggs": COUNT_ONLY},
+     [[19]], device=False)
+case("expr_date_between_int_literals", "exec/expr_eval_test.go:206-223", {"t": expr_table(30)},
+     {"predicate": ["between", ["col", 3], ["lit", 17005], ["lit", 17015]], "group_by": [], "aggs": COUNT_ONLY},
+     [[11]], device=False)
+case("expr_unary_minus", "exec/expr_eval_test.go:249-304", {"t": expr_table(10)},
+     {"predicate": None, "group_by": [0],
+      "aggs": [["SUM", ["neg", ["col", 1]], "neg_amount"], ["SUM", ["neg", ["col", 0]], "neg_id"]]},
+     [[i, -(i * 2.5), -i] for i in range(10)], device=False)
+A, I = ["col", 1], ["col", 0]
+case("expr_mixed_type_arith", "exec/expr_eval_test.go:389-473", {"t": expr_table(5)},
+     {"predicate": None, "group_by": [0],
+      "aggs": [["SUM", ["bin", "ADD", A, I], "a_plus_i"], ["SUM", ["bin", "ADD", I, A], "i_plus_a"],
+               ["SUM", ["bin", "SUB", A, I], "a_minus_i"], ["SUM", ["bin", "SUB", I, A], "i_minus_a"],
+               ["SUM", ["bin", "MUL", A, I], "a_times_i"], ["SUM", ["bin", "MUL", I, A], "i_times_a"]]},
+     [[0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0], [1, 3.5, 3.5, 1.5, -1.5, 2.5, 2.5], [2, 7.0, 7.0, 3.0, -3.0, 10.0, 10.0],
+      [3, 10.5, 10.5, 4.5, -4.5, 22.5, 22.5], [4, 14.0, 14.0, 6.0, -6.0, 40.0, 40.0]], device=False)
+case("expr_mixed_type_div", "exec/expr_eval_test.go:441-456", {"t": expr_table(5)},
+     {"predicate": ["bin", "GT", I, ["lit", 0]], "group_by": [0],
+      "aggs": [["SUM", ["bin", "DIV", A, I], "a_div_i"], ["SUM", ["bin", "DIV", I, A], "i_div_a"]]},
+     [[i, 2.5, 0.4] for i in range(1, 5)], device=False)
+case("expr_mixed_type_under_selection", "exec/expr_eval_test.go:475-506", {"t": expr_table(20)},
+     {"predicate": ["bin", "GT", I, ["lit", 15]], "group_by": [0], "aggs": [["SUM", ["bin", "MUL", A, I], "v"]]},
+     [[16, 640.0], [17, 722.5], [18, 810.0], [19, 902.5]], device=False)
+case("expr_same_type_arith", "exec/expr_eval_test.go:593-650", {"t": expr_table(5)},
+     {"predicate": ["bin", "GT", I, ["lit", 0]], "group_by": [0],
+      "aggs": [["SUM", ["bin", "MUL", I, I], "i_sq"], ["SUM", ["bin", "MUL", A, A], "a_sq"],
+               ["SUM", ["bin", "DIV", I, I], "i_div_i"]]},
+     [[i, i * i, (i * 2.5) ** 2, 1] for i in range(1, 5)], device=False)
 
 
 if __name__ == "__main__":

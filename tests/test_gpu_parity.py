@@ -16,7 +16,7 @@ from vexq_b200.table import HostTable, date_column, float_column, int_column, st
 
 pytestmark = pytest.mark.gpu
 
-CASES = load_cases()
+CASES = [c for c in load_cases() if c.get("device", True)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
