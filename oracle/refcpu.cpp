@@ -2091,6 +2091,12 @@ extern "C" {
 
 const char* ref_last_error(void) { return g_err.c_str(); }
 
+// The radix-partition choice and partition index of the partitioned join
+// (RadixBitsFor and radixPart, parallel_join.go:72-109), for the tests that
+// pin them on the reference's own cases.
+int32_t ref_radix_bits_for(int64_t est_rows) { return radixBitsFor(est_rows); }
+int32_t ref_radix_part(int64_t key, uint64_t mask) { return mask == 0 ? 0 : (int32_t)(radixHash(key) & mask); }
+
 int32_t ref_table_new(const vexq_column_desc* cols, int32_t ncols, int64_t nrows, int32_t rg_rows, ref_table_t* out) {
     return guarded([&]() -> int32_t {
         auto* h = new ref_table_s;

@@ -30,6 +30,9 @@ typedef struct ref_result_s* ref_result_t;
 int32_t ref_table_new(const vexq_column_desc* cols, int32_t ncols, int64_t nrows,
                       int32_t rg_rows, ref_table_t* out);
 void    ref_table_free(ref_table_t t);
+/* RadixBitsFor / radixPart (exec/parallel_join.go:72-109). */
+int32_t ref_radix_bits_for(int64_t est_rows);
+int32_t ref_radix_part(int64_t key, uint64_t mask);
 int32_t ref_table_zone_map(ref_table_t t, int32_t col, int32_t rg, vexq_zone_map* out);
 
 /* workers = 0: serial planner.Physical path (strict row-order fold, the

@@ -63,6 +63,10 @@ def lib() -> C.CDLL:
                                         C.POINTER(abi.OrderDesc)]
         L.ref_result_having.restype = i32
         L.ref_last_error.restype = C.c_char_p
+        L.ref_radix_bits_for.argtypes = [i64]
+        L.ref_radix_bits_for.restype = i32
+        L.ref_radix_part.argtypes = [i64, C.c_uint64]
+        L.ref_radix_part.restype = i32
         _lib = L
     return _lib
 
@@ -240,3 +244,13 @@ def ref_filter_lib():
             f.restype = C.c_size_t
         _ref_filter = L
     return _ref_filter
+
+
+def radix_bits_for(est_rows: int) -> int:
+    """RadixBitsFor (exec/parallel_join.go:72-81) as the oracle restates it."""
+    return int(lib().ref_radix_bits_for(int(est_rows)))
+
+
+def radix_part(key: int, mask: int) -> int:
+    """radixPart (exec/parallel_join.go:91-109): fmix64 of the key, masked."""
+    return int(lib().ref_radix_part(int(key), int(mask)))
