@@ -3,7 +3,9 @@ own tests assert: stacked filters with literal operands and BETWEEN
 (exec/stacked_filter_test.go:76-176: a stacked filter is the AND of the two
 predicates over the rows the first kept), unary minus and mixed-type
 arithmetic with NULL propagation in projections (exec/expr_eval_test.go:249-
-573)."""
+573), and the scan operators of exec/exec_test.go:125-302 and 762-853
+(Filter, Project, Filter → Project, zone-map pruning by row group, CASE with
+string results with and without ELSE)."""
 from __future__ import annotations
 
 import numpy as np
@@ -61,3 +63,39 @@ def test_mixed_type_arithmetic_null_propagation():
 def test_mixed_type_arithmetic_under_selection():
     rows = R.project(expr_table(20), [P.col(1) * P.col(0)], P.col(0) > 15).rows()
     assert rows == [(640.0,), (722.5,), (810.0,), (902.5,)]
+
+
+def scan_table(n, rg=65536):
+    # exec/exec_test.go:20-54 writeTestFile: id = i, val = i * 2.5, 65,536-row row groups
+    return R.RefTable(HostTable([int_column("id", np.arange(n, dtype=np.int64)),
+                                 float_column("val", np.arange(n) * 2.5)], n, rg))
+
+
+def test_filter_project_operators():
+    # exec/exec_test.go:125-265: Filter id >= 1024 over 2,048 rows; Project id * 2
+    # over 512 rows; Filter id < 100 then Project id over two row groups
+    bits, n = R.filter_bits(scan_table(2048), P.col(0) >= 1024)
+    assert n == 1024
+    assert R.project(scan_table(512), [P.col(0) * 2]).rows() == [(2 * i,) for i in range(512)]
+    rows = R.project(scan_table(2 * 65536), [P.col(0)], P.col(0) < 100).rows()
+    assert len(rows) == 100 and max(r[0] for r in rows) == 99
+
+
+def test_zone_map_pruning():
+    # exec/exec_test.go:267-302: four row groups, only those whose max(id) >=
+    # 131,072 are read (row groups 2 and 3, 2 x 65,536 rows)
+    t = scan_table(4 * 65536)
+    plan = P.AggPlan(P.col(0) >= 131072, [], [P.count_star("n")])
+    assert R.zone_prune(t, plan) == [0, 0, 1, 1]
+    assert R.agg(t, plan, workers=0).rows() == [(2 * 65536,)]
+
+
+def test_case_when_string_branches():
+    # exec/exec_test.go:762-853: CASE over val with string results, with and without ELSE
+    def vals(v):
+        return R.RefTable(HostTable([float_column("val", np.asarray(v, dtype=np.float64))], len(v), 65536))
+    x = P.col(0)
+    three = P.case([(x > 500.0, P.lit("high")), (x > 200.0, P.lit("medium"))], P.lit("low"))
+    assert R.project(vals([100, 300, 600, 50]), [three]).rows() == [("low",), ("medium",), ("high",), ("low",)]
+    no_else = P.case([(x > 500.0, P.lit("high"))], None)
+    assert R.project(vals([100, 300, 600, 800]), [no_else]).rows() == [(None,), (None,), ("high",), ("high",)]
