@@ -99,3 +99,14 @@ def test_case_when_string_branches():
     assert R.project(vals([100, 300, 600, 50]), [three]).rows() == [("low",), ("medium",), ("high",), ("low",)]
     no_else = P.case([(x > 500.0, P.lit("high"))], None)
     assert R.project(vals([100, 300, 600, 800]), [no_else]).rows() == [(None,), (None,), ("high",), ("high",)]
+
+
+def test_limit_after_filter():
+    # exec/exec_test.go:353-415: LIMIT 2 over the rows id >= 5 keeps ids 5 and 6
+    # (the first rows the filter passes, not the first physical rows); restated
+    # as the first two groups, in first-occurrence order, of a GROUP BY id
+    plan = P.AggPlan(P.col(0) >= 5, [0], [P.count_star("n")], limit=2)
+    assert R.agg(scan_table(10), plan, workers=0).rows() == [(5, 1), (6, 1)]
+    # exec/exec_test.go:417-450: LIMIT 3 with no filter keeps the first three
+    assert R.agg(scan_table(100), P.AggPlan(None, [0], [P.count_star("n")], limit=3), workers=0).rows() == \
+        [(0, 1), (1, 1), (2, 1)]
