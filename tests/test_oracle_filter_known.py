@@ -3,9 +3,9 @@ own tests assert: stacked filters with literal operands and BETWEEN
 (exec/stacked_filter_test.go:76-176: a stacked filter is the AND of the two
 predicates over the rows the first kept), unary minus and mixed-type
 arithmetic with NULL propagation in projections (exec/expr_eval_test.go:249-
-573), and the scan operators of exec/exec_test.go:125-302 and 762-853
-(Filter, Project, Filter → Project, zone-map pruning by row group, CASE with
-string results with and without ELSE)."""
+573), and the scan operators of exec/exec_test.go:125-450 and 762-853
+(Filter, Project, Filter → Project, zone-map pruning by row group, LIMIT
+after a filter, CASE with string results with and without ELSE)."""
 from __future__ import annotations
 
 import numpy as np
