@@ -243,6 +243,40 @@ case("expr_same_type_arith", "exec/expr_eval_test.go:593-650", {"t": expr_table(
      [[i, i * i, (i * 2.5) ** 2, 1] for i in range(1, 5)], device=False)
 
 
+# exec/agg_string_minmax_test.go:51-100 strAggBatch: grp and mode are
+# dictionary-coded strings (mode's dictionary in the order the test gives,
+# which differs from the lexicographic one); ungrouped MIN/MAX/COUNT over mode.
+def str_agg_table(modes, mode_dict):
+    n = len(modes)
+    return {"rg_rows": 65536, "nrows": n, "columns": [
+        strcol("grp", [[""]], [0] * n),
+        strcol("mode", [mode_dict], [mode_dict.index(m) if m is not None else 0 for m in modes],
+               [m is not None for m in modes])]}
+
+
+MINMAX_COUNT = [["MIN", ["col", 1], "min_mode"], ["MAX", ["col", 1], "max_mode"], ["COUNT", ["col", 1], "cnt"]]
+case("string_minmax_ungrouped", "exec/agg_string_minmax_test.go:242-274",
+     {"t": str_agg_table(["MAIL", "TRUCK", "AIR", "SHIP"], ["TRUCK", "SHIP", "MAIL", "AIR"])},
+     {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT}, [["AIR", "TRUCK", 4]], device=False)
+case("string_minmax_ungrouped_with_nulls", "exec/agg_string_minmax_test.go:276-301",
+     {"t": str_agg_table([None, "MAIL", None, "AIR", None], ["MAIL", "AIR"])},
+     {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT}, [["AIR", "MAIL", 2]], device=False)
+case("string_minmax_all_null_ungrouped", "exec/agg_string_minmax_test.go:303-326",
+     {"t": str_agg_table([None, None], ["AIR"])},
+     {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT}, [[NULL, NULL, 0]], device=False)
+case("string_minmax_empty_input", "exec/agg_string_minmax_test.go:328-348",
+     {"t": str_agg_table([], ["AIR"])},
+     {"predicate": None, "group_by": [],
+      "aggs": [["MIN", ["col", 1], "min_mode"], ["MAX", ["col", 1], "max_mode"], ["COUNT", None, "cnt_star"]]},
+     [[NULL, NULL, 0]], device=False)
+case("string_minmax_empty_string_is_data", "exec/agg_string_minmax_test.go:350-376",
+     {"t": str_agg_table(["MAIL", "", "AIR"], ["MAIL", "", "AIR"])},
+     {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT[:2]}, [["", "MAIL"]], device=False)
+case("string_minmax_only_empty_string", "exec/agg_string_minmax_test.go:378-399",
+     {"t": str_agg_table(["", None], [""])},
+     {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT[:2]}, [["", ""]], device=False)
+
+
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(out, "w") as f:
