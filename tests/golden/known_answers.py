@@ -276,6 +276,43 @@ case("string_minmax_only_empty_string", "exec/agg_string_minmax_test.go:378-399"
      {"t": str_agg_table(["", None], [""])},
      {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT[:2]}, [["", ""]], device=False)
 
+# grouped forms (:401-528): by the grp string, by an int64 region, with the
+# mode dictionary differing between row groups, and under a selection (the
+# selected rows restated as a predicate on an added 0/1 column)
+GRP_ROWS = [("east", "MAIL"), ("west", "TRUCK"), ("east", "AIR"), ("west", "SHIP"), ("east", None), ("solo", "RAIL")]
+MODE_DICT = ["TRUCK", "SHIP", "RAIL", "MAIL", "AIR"]
+case("string_minmax_grouped_by_string", "exec/agg_string_minmax_test.go:401-427",
+     {"t": {"rg_rows": 65536, "nrows": 6, "columns": [
+         strcol("grp", [["east", "west", "solo"]], [["east", "west", "solo"].index(g) for g, _ in GRP_ROWS]),
+         strcol("mode", [MODE_DICT], [MODE_DICT.index(m) if m else 0 for _, m in GRP_ROWS],
+                [m is not None for _, m in GRP_ROWS])]}},
+     {"predicate": None, "group_by": [0], "aggs": MINMAX_COUNT},
+     [["east", "AIR", "MAIL", 2], ["west", "SHIP", "TRUCK", 2], ["solo", "RAIL", "RAIL", 1]], device=False)
+REGION_MODES = ["MAIL", "TRUCK", "AIR", "SHIP", None]
+case("string_minmax_grouped_by_int", "exec/agg_string_minmax_test.go:429-462",
+     {"t": {"rg_rows": 65536, "nrows": 5, "columns": [
+         strcol("grp", [[""]], [0] * 5),
+         strcol("mode", [["TRUCK", "SHIP", "MAIL", "AIR"]],
+                [["TRUCK", "SHIP", "MAIL", "AIR"].index(m) if m else 0 for m in REGION_MODES],
+                [m is not None for m in REGION_MODES]),
+         col("region", "INT64", [1, 2, 1, 2, 3])]}},
+     {"predicate": None, "group_by": [2], "aggs": MINMAX_COUNT[:2]},
+     [[1, "AIR", "MAIL"], [2, "SHIP", "TRUCK"], [3, NULL, NULL]], device=False)
+case("string_minmax_cross_row_group_dicts", "exec/agg_string_minmax_test.go:464-488",
+     {"t": {"rg_rows": 2, "nrows": 4, "columns": [
+         strcol("grp", [["east"], ["east"]], [0, 0, 0, 0]),
+         strcol("mode", [["MAIL", "SHIP"], ["TRUCK", "AIR"]], [0, 1, 0, 1])]}},
+     {"predicate": None, "group_by": [0], "aggs": MINMAX_COUNT[:2]}, [["east", "AIR", "TRUCK"]], device=False)
+SEL_T = {"rg_rows": 65536, "nrows": 4, "columns": [
+    strcol("grp", [["east"]], [0, 0, 0, 0]),
+    strcol("mode", [["ZZZZZ", "SHIP", "MAIL", "AAAAA"]], [2, 3, 1, 0]),
+    col("region", "INT64", [1, 1, 1, 1]),
+    col("selected", "INT64", [1, 0, 1, 0])]}
+for key, name in ((0, "string_key"), (2, "int_key")):
+    case(f"string_minmax_under_selection_{name}", "exec/agg_string_minmax_test.go:490-528", {"t": SEL_T},
+         {"predicate": ["bin", "EQ", ["col", 3], ["lit", 1]], "group_by": [key], "aggs": MINMAX_COUNT},
+         [["east" if key == 0 else 1, "MAIL", "SHIP", 2]], device=False)
+
 
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
