@@ -313,6 +313,21 @@ for key, name in ((0, "string_key"), (2, "int_key")):
          {"predicate": ["bin", "EQ", ["col", 3], ["lit", 1]], "group_by": [key], "aggs": MINMAX_COUNT},
          [["east" if key == 0 else 1, "MAIL", "SHIP", 2]], device=False)
 
+case("string_minmax_with_numeric_aggregates", "exec/agg_string_minmax_test.go:530-588",
+     {"t": {"rg_rows": 65536, "nrows": 3, "columns": [
+         strcol("grp", [["east"]], [0, 0, 0]),
+         strcol("mode", [["MAIL", "AIR", "SHIP"]], [0, 1, 2]),
+         col("region", "INT64", [0, 0, 0]),
+         col("price", "FLOAT64", [10.0, 30.0, 20.0]),
+         col("day", "DATE", [100, 300, 200]),
+         col("flagb", "BOOL", [False, True, True])]}},
+     {"predicate": None, "group_by": [0],
+      "aggs": [["MIN", ["col", 1], "min_mode"], ["MAX", ["col", 1], "max_mode"], ["MIN", ["col", 3], "min_price"],
+               ["MAX", ["col", 3], "max_price"], ["SUM", ["col", 3], "sum_price"], ["AVG", ["col", 3], "avg_price"],
+               ["MIN", ["col", 4], "min_day"], ["MAX", ["col", 4], "max_day"], ["MIN", ["col", 5], "min_flag"],
+               ["MAX", ["col", 5], "max_flag"], ["COUNT", None, "cnt_star"]]},
+     [["east", "AIR", "SHIP", 10.0, 30.0, 60.0, 20.0, 100, 300, 0, 1, 3]], device=False)
+
 
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
