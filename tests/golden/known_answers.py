@@ -329,6 +329,36 @@ case("string_minmax_with_numeric_aggregates", "exec/agg_string_minmax_test.go:53
      [["east", "AIR", "SHIP", 10.0, 30.0, 60.0, 20.0, 100, 300, 0, 1, 3]], device=False)
 
 
+# exec/agg_string_merge_test.go:63-165 mergePartialAgg over string MIN/MAX
+# partials: each partial is one row group here (the oracle's parallel runs
+# merge one partial a row group; the serial run folds the same rows), with
+# its own dictionary.
+def rg_modes(groups):
+    """groups: the mode values of each row group (None = NULL), equal sizes."""
+    rows = [m for g in groups for m in g]
+    dicts = [sorted({m for m in g if m is not None}, key=g.index) or ["MAIL"] for g in groups]
+    codes = [d.index(m) if m is not None else 0 for g, d in zip(groups, dicts) for m in g]
+    return {"rg_rows": len(groups[0]), "nrows": len(rows), "columns": [
+        strcol("grp", [[""] for _ in groups], [0] * len(rows)),
+        strcol("mode", dicts, codes, [m is not None for m in rows])]}
+
+
+UNGROUPED = {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT}
+case("string_merge_min_max", "exec/agg_string_merge_test.go:63-81",
+     {"t": rg_modes([["MAIL", "SHIP"], ["TRUCK", "AIR"]])}, UNGROUPED, [["AIR", "TRUCK", 4]], device=False)
+case("string_merge_all_null_partial_last", "exec/agg_string_merge_test.go:83-115",
+     {"t": rg_modes([["MAIL", "SHIP"], [None, None]])}, UNGROUPED, [["MAIL", "SHIP", 2]], device=False)
+case("string_merge_all_null_partial_first", "exec/agg_string_merge_test.go:83-115",
+     {"t": rg_modes([[None, None], ["MAIL", "SHIP"]])}, UNGROUPED, [["MAIL", "SHIP", 2]], device=False)
+case("string_merge_empty_string_partial", "exec/agg_string_merge_test.go:117-135",
+     {"t": rg_modes([["MAIL"], [""]])}, {"predicate": None, "group_by": [], "aggs": MINMAX_COUNT[:2]},
+     [["", "MAIL"]], device=False)
+for order, vals in (("forward", ["MAIL", "RAIL", "TRUCK", "AIR", "FOB", "SHIP"]),
+                    ("reversed", ["SHIP", "FOB", "AIR", "TRUCK", "RAIL", "MAIL"])):
+    case(f"string_merge_order_invariant_{order}", "exec/agg_string_merge_test.go:137-165",
+         {"t": rg_modes([[v] for v in vals])}, UNGROUPED, [["AIR", "TRUCK", 6]], device=False)
+
+
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(out, "w") as f:
