@@ -359,6 +359,20 @@ for order, vals in (("forward", ["MAIL", "RAIL", "TRUCK", "AIR", "FOB", "SHIP"])
          {"t": rg_modes([[v] for v in vals])}, UNGROUPED, [["AIR", "TRUCK", 6]], device=False)
 
 
+# exec/agg_string_fallback_test.go:28-123 TestStringMinMaxIntKeyNullGroupByRow:
+# a nullable string GROUP BY key (rows 2 and 5 NULL form the NULL group), mode
+# dictionary in reverse lexicographic order
+FB_MODES = ["MAIL", "TRUCK", "ZULU", "AIR", "SHIP", "ALPHA"]
+FB_DICT = ["ZULU", "TRUCK", "SHIP", "MAIL", "ALPHA", "AIR"]
+case("string_minmax_null_group_key", "exec/agg_string_fallback_test.go:28-123",
+     {"t": {"rg_rows": 65536, "nrows": 6, "columns": [
+         strcol("grp", [["east", "west"]], [0, 1, 0, 0, 1, 0], [True, True, False, True, True, False]),
+         strcol("mode", [FB_DICT], [FB_DICT.index(m) for m in FB_MODES])]}},
+     {"predicate": None, "group_by": [0],
+      "aggs": [["MIN", ["col", 1], "lo"], ["MAX", ["col", 1], "hi"], ["COUNT", None, "cnt"]]},
+     [["east", "AIR", "MAIL", 2], ["west", "SHIP", "TRUCK", 2], [NULL, "ALPHA", "ZULU", 2]], device=False)
+
+
 if __name__ == "__main__":
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(out, "w") as f:
